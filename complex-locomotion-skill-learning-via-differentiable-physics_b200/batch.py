@@ -1,0 +1,247 @@
+"""Host front-end of the batched mass-spring simulator (``cls_*`` C ABI).
+
+A ``MassSpringBatch`` holds any number of environments of one or more robot
+types on one GPU.  Each robot type has its own geometry and its own controller
+weights; environments of the same type share the weights, as the reference's
+batch shares one ``Model`` (multitask/diffphy_trainer.py:178-185).
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import ctypes
+import numpy as np
+
+from . import _capi
+from ._capi import check, ptr
+
+
+@dataclass
+class Robot:
+    """One robot type: the reference builder's ``objects`` / ``springs`` rows
+    ``[a, b, rest_length, stiffness, actuation]`` (robot_design.py:344-349) and
+    the controller shape."""
+    objects: np.ndarray
+    springs: np.ndarray
+    robot_id: int = -1
+    hidden: Sequence[int] = (64,)
+    n_outputs: int = 0                       # 0: one output per spring (reference)
+    spring_output: Optional[np.ndarray] = None
+
+    def __post_init__(self):
+        self.objects = np.ascontiguousarray(np.asarray(self.objects, np.float64).reshape(-1, 3))
+        self.springs = np.ascontiguousarray(np.asarray(self.springs, np.float64).reshape(-1, 5))
+        if self.spring_output is not None:
+            self.spring_output = np.ascontiguousarray(self.spring_output, dtype=np.int32)
+
+    @property
+    def n_vertices(self):
+        return self.objects.shape[0]
+
+    @property
+    def n_springs(self):
+        return self.springs.shape[0]
+
+    @classmethod
+    def actuated_outputs(cls, objects, springs, **kw):
+        """Controller outputs only for actuated springs (actuation coef > 0)."""
+        springs = np.asarray(springs, np.float64).reshape(-1, 5)
+        act = springs[:, 4] > 0
+        so = np.full(springs.shape[0], -1, dtype=np.int32)
+        so[act] = np.arange(int(act.sum()), dtype=np.int32)
+        return cls(objects, springs, n_outputs=int(act.sum()), spring_output=so, **kw)
+
+
+def default_params(**over):
+    """Reference defaults (cfg3d/sim_quad.json after ConfigSim) with overrides."""
+    p = _capi.SimParams()
+    _capi.load().cls_default_params(ctypes.byref(p))
+    for k, v in over.items():
+        if k in ("activation_hidden", "activation_output") and isinstance(v, str):
+            v = _capi.ACT[v]
+        if k == "loss" and not isinstance(v, int):
+            k, v = "loss_mask", sum(_capi.LOSS_BITS[n] for n in v)
+        if k == "precision" and isinstance(v, str):
+            v = {"fp32": 32, "fp64": 64, "float32": 32, "float64": 64}[v]
+        setattr(p, k, v)
+    return p
+
+
+class MassSpringBatch:
+    """A batch of environments advanced by the fused sm_100a segment kernels."""
+
+    def __init__(self, robots: List[Robot], env_robot: Sequence[int], params=None, **over):
+        self.lib = _capi.load()
+        self.robots = list(robots)
+        self.env_robot = np.ascontiguousarray(env_robot, dtype=np.int32)
+        self.params = params if params is not None else default_params(**over)
+        descs = (_capi.RobotDesc * len(self.robots))()
+        self._keep = []
+        for d, r in zip(descs, self.robots):
+            d.n_vertices = r.n_vertices
+            d.n_springs = r.n_springs
+            d.objects = ptr(r.objects)
+            d.springs = ptr(r.springs)
+            d.robot_id = r.robot_id
+            d.n_outputs = r.n_outputs
+            d.spring_output = ptr(r.spring_output, _capi.P_I)
+            d.n_hidden_layers = len(r.hidden)
+            for i, h in enumerate(r.hidden):
+                d.hidden[i] = h
+            self._keep.append(r)
+        h = ctypes.c_void_p()
+        rc = self.lib.cls_create(descs, len(self.robots), ptr(self.env_robot, _capi.P_I),
+                                 len(self.env_robot), ctypes.byref(self.params), ctypes.byref(h))
+        check(rc, None)
+        self.h = h
+        ne, nv, T = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(self.lib.cls_get_sizes(self.h, ctypes.byref(ne), ctypes.byref(nv), ctypes.byref(T)), self.h)
+        self.n_envs, self.n_vertices_total, self.T = ne.value, nv.value, T.value
+        self.env_vertex_offset = np.concatenate(
+            [[0], np.cumsum([self.robots[r].n_vertices for r in self.env_robot])]).astype(np.int64)
+        self._stream = None
+
+    # -------------------------------------------------------------- lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cls_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        check(rc, self.h)
+
+    def set_stream(self, stream_handle):
+        """Bind to a cudaStream_t (int handle, e.g. torch.cuda.Stream().cuda_stream)."""
+        self._stream = stream_handle
+        self._c(self.lib.cls_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def layer_shape(self, robot, layer):
+        r, c = ctypes.c_int32(), ctypes.c_int32()
+        self._c(self.lib.cls_get_layer_shape(self.h, robot, layer, ctypes.byref(r), ctypes.byref(c)))
+        return r.value, c.value
+
+    def n_layers(self, robot=0):
+        return len(self.robots[robot].hidden) + 1
+
+    # ------------------------------------------------------------------ inputs
+    @staticmethod
+    def _f64(a, shape=None):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        if shape is not None:
+            a = a.reshape(shape)
+        return a
+
+    def set_state(self, x0, v0=None):
+        x0 = self._f64(x0, (self.n_vertices_total, 3))
+        v0 = None if v0 is None else self._f64(v0, (self.n_vertices_total, 3))
+        self._c(self.lib.cls_set_state(self.h, ptr(x0), ptr(v0)))
+
+    def set_targets(self, target_v, target_h, target_c=None):
+        tv = self._f64(target_v, (self.T, self.n_envs, 3))
+        th = self._f64(target_h, (self.T, self.n_envs))
+        tc = None if target_c is None else self._f64(target_c, (self.T, self.n_envs))
+        self._c(self.lib.cls_set_targets(self.h, ptr(tv), ptr(th), ptr(tc)))
+
+    def set_weights(self, robot, layer, W, b):
+        rows, cols = self.layer_shape(robot, layer)
+        W = None if W is None else self._f64(W, (rows, cols))
+        b = None if b is None else self._f64(b, (rows,))
+        self._c(self.lib.cls_set_weights(self.h, robot, layer, ptr(W), ptr(b)))
+
+    def get_weights(self, robot, layer):
+        rows, cols = self.layer_shape(robot, layer)
+        W, b = np.zeros((rows, cols)), np.zeros(rows)
+        self._c(self.lib.cls_get_weights(self.h, robot, layer, ptr(W), ptr(b)))
+        return W, b
+
+    def get_grads(self, robot, layer):
+        rows, cols = self.layer_shape(robot, layer)
+        W, b = np.zeros((rows, cols)), np.zeros(rows)
+        self._c(self.lib.cls_get_grads(self.h, robot, layer, ptr(W), ptr(b)))
+        return W, b
+
+    # ------------------------------------------------------------------ passes
+    def forward(self, steps):
+        self._c(self.lib.cls_forward(self.h, steps))
+
+    def forward_eval(self, steps):
+        self._c(self.lib.cls_forward_eval(self.h, steps))
+
+    def loss(self):
+        terms = np.zeros(8)
+        env = np.zeros((8, self.n_envs))
+        self._c(self.lib.cls_loss(self.h, ptr(terms), ptr(env)))
+        return dict(zip(_capi.LOSS_SLOTS, terms.tolist())), env
+
+    def backward(self):
+        self._c(self.lib.cls_backward(self.h))
+
+    def simulate(self, steps, per_env=False):
+        out = ctypes.c_double()
+        fn = self.lib.cls_simulate_per_env if per_env else self.lib.cls_simulate
+        self._c(fn(self.h, steps, ctypes.byref(out)))
+        return out.value
+
+    def adam_step(self, it):
+        tns = ctypes.c_double()
+        self._c(self.lib.cls_adam_step(self.h, it, ctypes.byref(tns)))
+        return tns.value
+
+    def clear_adam(self):
+        self._c(self.lib.cls_clear_adam(self.h))
+
+    def weights_init(self, seed):
+        self._c(self.lib.cls_weights_init(self.h, seed))
+
+    def initialize_train(self, it, steps, seed, max_speed):
+        self._c(self.lib.cls_initialize_train(self.h, it, steps, seed, max_speed))
+
+    def profile(self, on=True):
+        self._c(self.lib.cls_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self, reset=False):
+        ms = np.zeros(len(_capi.PROFILE_KINDS))
+        n = np.zeros(len(_capi.PROFILE_KINDS), dtype=np.int64)
+        self._c(self.lib.cls_profile_read(self.h, ptr(ms), n.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                          1 if reset else 0))
+        return dict(zip(_capi.PROFILE_KINDS, ms.tolist())), dict(zip(_capi.PROFILE_KINDS, n.tolist()))
+
+    def synchronize(self):
+        self._c(self.lib.cls_synchronize(self.h))
+
+    def graph_capture(self, steps, with_adam=False):
+        self._c(self.lib.cls_graph_capture(self.h, steps, 1 if with_adam else 0))
+
+    def graph_launch(self, it=0):
+        self._c(self.lib.cls_graph_launch(self.h, it))
+
+    # ----------------------------------------------------------------- outputs
+    def observables(self):
+        T, E = self.T, self.n_envs
+        c, h, u, r = np.zeros((T, E, 3)), np.zeros((T, E)), np.zeros((T, E)), np.zeros((T, E))
+        self._c(self.lib.cls_get_observables(self.h, ptr(c), ptr(h), ptr(u), ptr(r)))
+        return dict(center=c, height=h, upper_height=u, rotation=r)
+
+    def trajectory(self):
+        x = np.zeros((self.T, self.n_vertices_total, 3))
+        self._c(self.lib.cls_get_trajectory(self.h, ptr(x)))
+        return x
+
+    def final_state(self):
+        x, v = np.zeros((self.n_vertices_total, 3)), np.zeros((self.n_vertices_total, 3))
+        self._c(self.lib.cls_get_final_state(self.h, ptr(x), ptr(v)))
+        return x, v
+
+    def state_grads(self):
+        gx, gv = np.zeros((self.n_vertices_total, 3)), np.zeros((self.n_vertices_total, 3))
+        self._c(self.lib.cls_get_state_grads(self.h, ptr(gx), ptr(gv)))
+        return gx, gv
+
+    def env_slice(self, e):
+        """Rows of the packed [n_vertices_total] arrays that belong to env e."""
+        return slice(int(self.env_vertex_offset[e]), int(self.env_vertex_offset[e + 1]))

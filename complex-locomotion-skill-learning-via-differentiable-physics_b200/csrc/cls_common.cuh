@@ -1,0 +1,122 @@
+// cls_common.cuh -- shared device types and helpers for the sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cls {
+
+constexpr int kMaxLayers = 5;   // weight layers (hidden layers + output)
+
+enum Act : int { ACT_SIN = 0, ACT_TANH = 1 };
+enum LossBit : int {
+  LOSS_VELOCITY = 1, LOSS_HEIGHT = 2, LOSS_POSE = 4,
+  LOSS_ACTUATION = 8, LOSS_ROTATION = 16, LOSS_CRAWL = 32
+};
+// slots of the per-env loss record, in the reference's loss_dict order
+// (multitask/taichi_env.py:82-88), total excluded
+enum LossSlot : int { LS_VEL = 0, LS_HEIGHT = 1, LS_POSE = 2, LS_ROT = 3, LS_WEIGHT = 4,
+                      LS_ACT = 5, LS_CRAWL = 6, LS_COUNT = 7 };
+
+// error bits written to the device status word
+enum ErrBit : int { ERR_NONFINITE = 1, ERR_SMEM = 2, ERR_CONFIG = 4 };
+
+// 4-wide vector, 16 B (float) / 32 B (double) aligned, for vectorised state I/O
+template <typename R>
+struct alignas(4 * sizeof(R)) V4 {
+  R x, y, z, w;
+};
+
+// read-only (non-coherent) vector load
+template <typename R> __device__ __forceinline__ V4<R> ldg4(const V4<R>* p);
+template <> __device__ __forceinline__ V4<float> ldg4<float>(const V4<float>* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  V4<float> r; r.x = v.x; r.y = v.y; r.z = v.z; r.w = v.w;
+  return r;
+}
+template <> __device__ __forceinline__ V4<double> ldg4<double>(const V4<double>* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  V4<double> r; r.x = a.x; r.y = a.y; r.z = b.x; r.w = b.y;
+  return r;
+}
+
+template <typename R>
+__device__ __forceinline__ R comp(const V4<R>& v, int d) {
+  return d == 0 ? v.x : (d == 1 ? v.y : v.z);
+}
+
+template <typename R> __device__ __forceinline__ R dsqrt(R x);
+template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
+template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+
+template <typename R> __device__ __forceinline__ R dsin(R x);
+template <> __device__ __forceinline__ float dsin<float>(float x) { return sinf(x); }
+template <> __device__ __forceinline__ double dsin<double>(double x) { return sin(x); }
+template <typename R> __device__ __forceinline__ R dcos(R x);
+template <> __device__ __forceinline__ float dcos<float>(float x) { return cosf(x); }
+template <> __device__ __forceinline__ double dcos<double>(double x) { return cos(x); }
+template <typename R> __device__ __forceinline__ R dtanh(R x);
+template <> __device__ __forceinline__ float dtanh<float>(float x) { return tanhf(x); }
+template <> __device__ __forceinline__ double dtanh<double>(double x) { return tanh(x); }
+template <typename R> __device__ __forceinline__ R datan2(R y, R x);
+template <> __device__ __forceinline__ float datan2<float>(float y, float x) { return atan2f(y, x); }
+template <> __device__ __forceinline__ double datan2<double>(double y, double x) { return atan2(y, x); }
+template <typename R> __device__ __forceinline__ R dabs(R x);
+template <> __device__ __forceinline__ float dabs<float>(float x) { return fabsf(x); }
+template <> __device__ __forceinline__ double dabs<double>(double x) { return fabs(x); }
+template <typename R> __device__ __forceinline__ R dpow_half(R x);
+template <> __device__ __forceinline__ float dpow_half<float>(float x) { return sqrtf(x); }
+template <> __device__ __forceinline__ double dpow_half<double>(double x) { return sqrt(x); }
+
+// activation and its derivative, evaluated at the pre-activation u = z + b
+template <typename R>
+__device__ __forceinline__ R act_f(int kind, R u) {
+  return kind == ACT_TANH ? dtanh<R>(u) : dsin<R>(u);
+}
+template <typename R>
+__device__ __forceinline__ R act_d(int kind, R u) {
+  if (kind == ACT_TANH) {
+    R y = dtanh<R>(u);
+    return R(1) - y * y;
+  }
+  return dcos<R>(u);
+}
+
+template <typename R>
+__device__ __forceinline__ bool finite(R x) {
+  return isfinite(x);
+}
+
+// deterministic block reduction (fixed tree for a fixed blockDim); `red` must
+// hold >= 32 elements; every thread receives the result
+template <typename T, typename Op>
+__device__ __forceinline__ T block_reduce(T v, T* red, Op op) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    T w = (lane < nw) ? red[lane] : red[0];
+    // lanes >= nw hold a duplicate of red[0]; the tree below only combines
+    // lanes < nw because the identity is applied through a mask
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      T other = __shfl_down_sync(0xffffffffu, w, o);
+      if (lane + o < nw) w = op(w, other);
+    }
+    if (lane == 0) red[0] = w;
+  }
+  __syncthreads();
+  T r = red[0];
+  __syncthreads();
+  return r;
+}
+
+struct OpSum {
+  template <typename T> __device__ __forceinline__ T operator()(T a, T b) const { return a + b; }
+};
+
+}  // namespace cls

@@ -1,0 +1,333 @@
+// ms_kernels.cuh -- fused mass-spring + MLP-controller segment kernels.
+//
+// One CTA owns one environment (a robot instance) at a time and advances it
+// through a whole segment of substeps with the state resident in shared memory,
+// so a substep costs no kernel launch and no global round trip of the state.
+// Environments are independent in the forward pass (the reference couples them
+// only through the shared weights, which are read-only here), so CTAs never
+// synchronise with one another.  Per substep, for the env it owns, a CTA runs
+// the reference's chain
+//   compute_center / compute_height / compute_rotation
+//     (multitask/solver_mass_spring.py:150-192)
+//   nn_input (multitask/taichi_env.py:149-183)
+//   Model.nn1 / nn2 (multitask/nn.py:130-146), generalised to L layers
+//   apply_spring_force (multitask/solver_mass_spring.py:86-105)
+//   advance_toi (multitask/solver_mass_spring.py:117-148)
+// and the reverse kernel replays the hand-written adjoint of that chain in
+// reverse order (what ti.ad.Tape does for multitask/diffphy_trainer.py:246-256).
+//
+// Spring forces are gathered per vertex from a CSR incidence list (springs
+// sorted by endpoint) instead of scattered with atomics: every vertex sums its
+// own incident impulses in a fixed order, so v_inc needs no atomics and the
+// checkpoint recompute reproduces the first pass bit for bit.
+#pragma once
+#include "cls_common.cuh"
+
+namespace cls {
+
+struct RobotDesc {
+  int n_v, n_s, n_out, n_c;          // vertices, springs, MLP outputs, compact inputs
+  int ptr_off;                       // CSR row pointers start (n_v + 1 entries)
+  int inc_off;                       // incidence entries start (2 n_s entries)
+  int spr_off;                       // per-spring arrays start (n_s entries)
+  int robot_id;                      // 100 selects the hard-coded heading vertices
+  int pos_pad;                       // first compact column after the position block
+  int n_layers;
+  int width[kMaxLayers + 1];         // width[0] = n_c ... width[n_layers] = n_out
+  int pitch[kMaxLayers];             // row pitch (elements, multiple of 4) of layer l
+  long long w_off[kMaxLayers];       // compact weight offsets (elements)
+  int b_off[kMaxLayers];             // bias offsets
+  int n_env;                         // envs of this type: B in the loss normalisation
+  int env_first;                     // envs are sorted by type
+  int rot_idx[4];                    // heading vertices for robot 100
+};
+
+struct EnvDesc {
+  int robot;
+  int v_off;                         // vertex offset in packed state arrays
+  int in_off;                        // offset in the compact-input record slab
+  int z_off[kMaxLayers];             // offset in each layer's record slab
+};
+
+template <typename R>
+struct MsArgs {
+  // sizes and constants
+  int n_envs, T, steps, K;           // trajectory length, episode steps, checkpoint interval
+  int n_items;                       // work items (entries of `order`) in this launch
+  int n_sin, dup_v, dup_h, dup_c;
+  int act_hidden, act_out;
+  int run_period, turn_period, jump_period;
+  int loss_mask;
+  int v_total, in_total;
+  int z_total[kMaxLayers];
+  long long z_base[kMaxLayers];      // layer offsets inside rec_z / rec_dz (per-step slab * K)
+  // shared-memory capacities (elements): vertices, compact input (pitch 0),
+  // layer outputs (max of hidden widths and n_out, padded to 4), reverse
+  // buffer A (max of outputs and the position block), MLP outputs alone
+  int smem_nmax, smem_p0max, smem_dmax, smem_amax, smem_omax;
+  R dt, gravity, ground, drag_s, dashpot, friction, max_speed;
+  // tables
+  const RobotDesc* robots;
+  const EnvDesc* envs;
+  const int* order;                  // env processing order (largest first)
+  int* queue;                        // work-queue counter, zeroed before each launch
+  const int* inc_ptr;                // CSR row pointers (relative to inc_off)
+  const int4* inc_i;                 // {other vertex, side (0: a, 1: b), spring, out index}
+  const V4<R>* inc_f;                // {rest length, stiffness, actuation coef, 0}
+  const int* spring_out;             // per spring: MLP output index or -1
+  const R* w;                        // compact weights
+  const R* bias;
+  const R* sin_table;                // [T + 1][n_sin], sin(omega (t) dt + 2 pi j / n_sin)
+  // state
+  V4<R>* ckpt_x; V4<R>* ckpt_v;      // [n_ckpt][v_total]
+  V4<R>* fin_x; V4<R>* fin_v;        // [v_total] state after the last processed step
+  V4<R>* rec_x; V4<R>* rec_v;        // [K][v_total]
+  R* rec_in;                         // [K][in_total]
+  R* rec_z;                          // per layer z_base[l] + [K][z_total[l]]
+  R* rec_dz;                         // same layout as rec_z
+  unsigned char* head;               // [v_total] head/tail split at t = 0
+  // observables, [T][n_envs] (zero where the reference never writes them)
+  V4<R>* obs_center; R* obs_height; R* obs_upper; R* obs_rot;
+  V4<R>* x_full;                     // [T][v_total] or null
+  R* act_full;                       // [T][z_total[L-1]] or null
+  // targets [T][n_envs]
+  const V4<R>* tv; const R* th; const R* tc;
+  const V4<R>* init_obj;             // [v_total] initial_objects per env (pose loss)
+  // adjoint carries between segments
+  V4<R>* adj_x; V4<R>* adj_v; R* adj_h;
+  // status
+  int* status;
+};
+
+// ------------------------------------------------------------ shared memory
+// reduction scratch: 8 values x 32 warps, then 32 ints for arg-reductions
+constexpr int kRed = 320;
+constexpr int kRedInt = 256;
+template <typename R>
+struct FwdSmem {
+  V4<R>* xs; V4<R>* vs; V4<R>* vinc;
+  R* ain;          // compact input, padded
+  R* buf0; R* buf1;
+  R* red;          // kRed entries
+};
+
+template <typename R>
+__device__ __forceinline__ FwdSmem<R> carve_fwd(char* base, const MsArgs<R>& a) {
+  FwdSmem<R> s;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base + off; off += (bytes + 255) & ~size_t(255); return p; };
+  s.xs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.vs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.vinc = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.ain = (R*)take(sizeof(R) * a.smem_p0max);
+  s.buf0 = (R*)take(sizeof(R) * a.smem_dmax);
+  s.buf1 = (R*)take(sizeof(R) * a.smem_dmax);
+  s.red = (R*)take(sizeof(R) * kRed);
+  return s;
+}
+
+template <typename R>
+__host__ __device__ inline size_t fwd_smem_bytes(int nmax, int dmax, int p0max) {
+  auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return 3 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * p0max) + 2 * rb(sizeof(R) * dmax) +
+         rb(sizeof(R) * kRed);
+}
+
+// Reverse-pass shared memory.  gvinc (v_inc, then its adjoint) is live only
+// from the v_inc recompute to the end of the spring adjoint; dz and part are
+// live only in the MLP adjoint that follows, so they share one region.
+template <typename R>
+struct RevSmem {
+  V4<R>* xs; V4<R>* vs; V4<R>* gx; V4<R>* gv;
+  R* bufA;         // controller outputs, then the transposed products
+  R* bufB;         // d loss / d output
+  V4<R>* gvinc;    // union region, vertex phase
+  R* dz;           // union region, MLP phase
+  V4<R>* part;     // union region, MLP phase: blockDim partials
+  R* red;
+};
+
+template <typename R>
+__host__ __device__ inline size_t rev_union_bytes(int nmax, int dmax, int threads) {
+  auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t vert = rb(sizeof(V4<R>) * nmax);
+  const size_t mlp = rb(sizeof(R) * dmax) + rb(sizeof(V4<R>) * threads);
+  return vert > mlp ? vert : mlp;
+}
+
+template <typename R>
+__device__ __forceinline__ RevSmem<R> carve_rev(char* base, const MsArgs<R>& a) {
+  RevSmem<R> s;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base + off; off += (bytes + 255) & ~size_t(255); return p; };
+  s.xs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.vs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.gx = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.gv = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.bufA = (R*)take(sizeof(R) * a.smem_amax);
+  s.bufB = (R*)take(sizeof(R) * a.smem_omax);
+  s.red = (R*)take(sizeof(R) * kRed);
+  char* u = take(rev_union_bytes<R>(a.smem_nmax, a.smem_dmax, blockDim.x));
+  s.gvinc = (V4<R>*)u;
+  s.dz = (R*)u;
+  s.part = (V4<R>*)(u + ((sizeof(R) * a.smem_dmax + 255) & ~size_t(255)));
+  return s;
+}
+
+template <typename R>
+__host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, int dmax, int threads) {
+  auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return 4 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * amax) + rb(sizeof(R) * omax) +
+         rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads);
+}
+
+// ------------------------------------------------------------- primitives
+
+// Hooke + dashpot impulse of one spring seen from one of its endpoints
+// (solver_mass_spring.py:89-103).  xa/xb/va/vb are the spring's a/b endpoints.
+template <typename R>
+__device__ __forceinline__ void spring_impulse(const V4<R>& xa, const V4<R>& xb, const V4<R>& va,
+                                               const V4<R>& vb, R l0, R k, R coef, R act, R dt,
+                                               R dashpot, R imp[3]) {
+  R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
+  R n2 = d0 * d0 + d1 * d1 + d2 * d2;
+  R length = dsqrt<R>(n2 + R(1e-8)) + R(1e-4);
+  R target = l0 * (R(1) + coef * act);
+  R sc = dt * (length - target) * k / length;
+  R invlen = R(1) / dsqrt<R>(n2);
+  R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
+  R vrel = (va.x - vb.x) * n0 + (va.y - vb.y) * n1 + (va.z - vb.z) * nz;
+  R c = dashpot * vrel;
+  imp[0] = sc * d0 + c * n0;
+  imp[1] = sc * d1 + c * n1;
+  imp[2] = sc * d2 + c * nz;
+}
+
+// v_inc of vertex i: sum over incident springs, a-side gets -impulse, b-side +impulse
+template <typename R>
+__device__ __forceinline__ V4<R> gather_vinc(const MsArgs<R>& a, const RobotDesc& rb, int i,
+                                             const V4<R>* xs, const V4<R>* vs, const R* out) {
+  const int beg = a.inc_ptr[rb.ptr_off + i], end = a.inc_ptr[rb.ptr_off + i + 1];
+  R s0 = 0, s1 = 0, s2 = 0;
+  const V4<R> xi = xs[i], vi = vs[i];
+  for (int q = beg; q < end; ++q) {
+    const int4 ii = a.inc_i[rb.inc_off + q];
+    const V4<R> ff = a.inc_f[rb.inc_off + q];
+    const int o = ii.x;
+    const R act = ii.w >= 0 ? out[ii.w] : R(0);
+    R imp[3];
+    if (ii.y == 0) {  // this vertex is endpoint a
+      spring_impulse<R>(xi, xs[o], vi, vs[o], ff.x, ff.y, ff.z, act, a.dt, a.dashpot, imp);
+      s0 -= imp[0]; s1 -= imp[1]; s2 -= imp[2];
+    } else {          // endpoint b
+      spring_impulse<R>(xs[o], xi, vs[o], vi, ff.x, ff.y, ff.z, act, a.dt, a.dashpot, imp);
+      s0 += imp[0]; s1 += imp[1]; s2 += imp[2];
+    }
+  }
+  V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = 0;
+  return r;
+}
+
+// advance_toi for one vertex (solver_mass_spring.py:119-148); in place
+template <typename R>
+__device__ __forceinline__ void advance_vertex(const MsArgs<R>& a, V4<R>& x, V4<R>& v, const V4<R>& vi) {
+  R ov0 = a.drag_s * v.x + vi.x;
+  R ov1 = a.drag_s * v.y + a.dt * a.gravity + vi.y;
+  R ov2 = a.drag_s * v.z + vi.z;
+  R nv0 = ov0, nv1 = ov1, nv2 = ov2, toi = 0;
+  R nx1 = x.y + a.dt * ov1;
+  if (nx1 < a.ground && ov1 < R(-1e-4)) {
+    toi = -(x.y - a.ground) / ov1;
+    R f = a.friction * (-ov1);
+    nv1 = 0;
+    nv0 = (ov0 < 0) ? fmin(R(0), ov0 + f) : fmax(R(0), ov0 - f);
+    nv2 = (ov2 < 0) ? fmin(R(0), ov2 + f) : fmax(R(0), ov2 - f);
+  }
+  R dtt = a.dt - toi;
+  x.x = x.x + toi * ov0 + dtt * nv0;
+  x.y = x.y + toi * ov1 + dtt * nv1;
+  x.z = x.z + toi * ov2 + dtt * nv2;
+  v.x = nv0; v.y = nv1; v.z = nv2;
+}
+
+// y = act(W x + b) for one layer, one warp per output row, float4 loads.
+// Records z (pre-bias sums) when zrec != null.
+template <typename R>
+__device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch, int nout,
+                                              const R* __restrict__ bias, const R* xin, R* y,
+                                              R* zrec, int act) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int n4 = pitch >> 2;
+  const V4<R>* x4 = reinterpret_cast<const V4<R>*>(xin);
+  for (int i = wid; i < nout; i += nw) {
+    const V4<R>* w4 = reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch);
+    R s = 0;
+#pragma unroll 4
+    for (int j = lane; j < n4; j += 32) {
+      const V4<R> wv = ldg4<R>(w4 + j);
+      const V4<R> xv = x4[j];
+      s += wv.x * xv.x + wv.y * xv.y + wv.z * xv.z + wv.w * xv.w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      if (zrec) zrec[i] = s;
+      y[i] = act_f<R>(act, s + bias[i]);
+    }
+  }
+}
+
+// g_in[j] = sum_i W[i, j] dz[i] for j in [0, ncols) (ncols multiple of 4 or
+// padded), deterministic: fixed row slices, fixed reduction order.
+// Result written to out4[j/4] (V4 groups).  Uses s.part as scratch.
+template <typename R>
+__device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pitch, int nrows,
+                                                 int ncols, const R* dz, V4<R>* part, V4<R>* out4) {
+  const int c4 = (ncols + 3) >> 2;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (c4 >= nt || nrows == 1) {
+    for (int g = tid; g < c4; g += nt) {
+      R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll 4
+      for (int i = 0; i < nrows; ++i) {
+        const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g);
+        const R d = dz[i];
+        s0 += wv.x * d; s1 += wv.y * d; s2 += wv.z * d; s3 += wv.w * d;
+      }
+      V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = s3;
+      out4[g] = r;
+    }
+    __syncthreads();
+    return;
+  }
+  int slices = nt / c4;
+  if (slices > nrows) slices = nrows;
+  const int used = slices * c4;
+  if (tid < used) {
+    const int g = tid % c4, r0 = tid / c4;
+    R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll 4
+    for (int i = r0; i < nrows; i += slices) {
+      const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g);
+      const R d = dz[i];
+      s0 += wv.x * d; s1 += wv.y * d; s2 += wv.z * d; s3 += wv.w * d;
+    }
+    V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = s3;
+    part[tid] = r;
+  }
+  __syncthreads();
+  for (int g = tid; g < c4; g += nt) {
+    V4<R> acc = part[g];
+    for (int r = 1; r < slices; ++r) {
+      const V4<R> p = part[r * c4 + g];
+      acc.x += p.x; acc.y += p.y; acc.z += p.z; acc.w += p.w;
+    }
+    out4[g] = acc;
+  }
+  __syncthreads();
+}
+
+template <typename R>
+struct MinIdx { R v; int i; };
+
+}  // namespace cls

@@ -1,0 +1,1330 @@
+// ms_runtime.cu -- the cls_* C ABI: batch packing, device buffers, the
+// checkpointed forward / reverse schedule and CUDA-graph capture.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/cls_b200.h"
+#include "ms_segment.cuh"
+
+namespace cls {
+
+static thread_local std::string g_create_error;
+
+struct Fail {
+  int code;
+  std::string msg;
+};
+
+#define CLS_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      throw Fail{e_ == cudaErrorMemoryAllocation ? CLS_ERR_OOM : CLS_ERR_CUDA,          \
+                 std::string(#call) + ": " + cudaGetErrorString(e_)};                   \
+  } while (0)
+
+#define CLS_REQUIRE(cond, msg)                                                          \
+  do {                                                                                  \
+    if (!(cond)) throw Fail{CLS_ERR_INVALID, (msg)};                                    \
+  } while (0)
+
+static inline int round4(int x) { return (x + 3) & ~3; }
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    n = count;
+    if (count) CLS_CUDA(cudaMalloc(&p, sizeof(T) * count));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { free(); }
+};
+
+// ------------------------------------------------------------ host-side pack
+struct HostRobot {
+  int n_v = 0, n_s = 0, n_out = 0, n_c = 0, pos_pad = 0, robot_id = -1, n_layers = 0;
+  int width[kMaxLayers + 1] = {0};
+  int full_cols[kMaxLayers] = {0};
+  std::vector<double> objects;           // [n_v][3]
+  std::vector<int> sa, sb, out;          // per spring
+  std::vector<double> len, stiff, coef;  // per spring (stiffness scaled)
+};
+
+// launch categories for the per-kernel CUDA-event profile
+enum ProfKind : int { PK_FWD = 0, PK_RECOMP, PK_REV, PK_WGRAD, PK_LOSS, PK_ADAM, PK_OTHER, PK_COUNT };
+
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;    // pairs (start, stop)
+  std::vector<int> kind;
+  size_t used = 0;
+  double ms[PK_COUNT] = {0};
+  long long launches[PK_COUNT] = {0};
+  ~Profiler() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+
+class SimBase {
+ public:
+  virtual ~SimBase() = default;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  virtual void set_state(const double* x0, const double* v0) = 0;
+  virtual void set_targets(const double* tv, const double* th, const double* tc) = 0;
+  virtual void set_weights(int r, int l, const double* W, const double* b) = 0;
+  virtual void get_weights(int r, int l, double* W, double* b) = 0;
+  virtual void get_grads(int r, int l, double* gW, double* gb) = 0;
+  virtual void forward(int steps, bool eval, bool per_env) = 0;
+  virtual void loss(double* terms, double* env) = 0;
+  virtual void backward(bool per_env) = 0;
+  virtual void adam(int iter, double* tns) = 0;
+  virtual void clear_adam() = 0;
+  virtual void observables(double* c, double* h, double* u, double* rot) = 0;
+  virtual void trajectory(double* x) = 0;
+  virtual void final_state(double* x, double* v) = 0;
+  virtual void state_grads(double* gx, double* gv) = 0;
+  virtual int synchronize() = 0;
+  virtual void graph_capture(int steps, bool with_adam) = 0;
+  virtual void graph_launch(int iter) = 0;
+  virtual void weights_init(unsigned long long seed) = 0;
+  virtual void initialize_train(int iter, int steps, unsigned long long seed, double max_speed) = 0;
+  virtual void profile_enable(bool on) = 0;
+  virtual void profile_read(double* ms, long long* launches, bool reset) = 0;
+  virtual void sizes(int* ne, int* nv, int* T) const = 0;
+  virtual void layer_shape(int r, int l, int* rows, int* cols) const = 0;
+};
+
+template <typename R>
+class SimImpl final : public SimBase {
+ public:
+  SimImpl(const std::vector<HostRobot>& robots, const std::vector<int>& env_robot,
+          const cls_sim_params& p)
+      : hr_(robots), p_(p) {
+    build(env_robot);
+  }
+  ~SimImpl() override {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+  }
+
+  // ---------------------------------------------------------------- build
+  void build(const std::vector<int>& env_robot) {
+    const int E = (int)env_robot.size();
+    const int nr = (int)hr_.size();
+    E_ = E;
+    T_ = p_.max_steps;
+    K_ = std::max(1, p_.checkpoint_every);
+    L_ = hr_[0].n_layers;
+    // internal order: envs grouped by robot type (stable)
+    perm_.resize(E);  // internal -> user
+    std::iota(perm_.begin(), perm_.end(), 0);
+    std::stable_sort(perm_.begin(), perm_.end(),
+                     [&](int a, int b) { return env_robot[a] < env_robot[b]; });
+    identity_perm_ = true;
+    for (int i = 0; i < E; ++i) identity_perm_ &= (perm_[i] == i);
+    // robot descriptors
+    std::vector<RobotDesc> rd(nr);
+    std::vector<int> inc_ptr;
+    std::vector<int4> inc_i;
+    std::vector<V4<R>> inc_f;
+    std::vector<int> spring_out;
+    long long woff = 0, moff = 0;
+    int boff = 0;
+    nmax_ = 0;
+    int p0max = 4, dmax = 4, amax = 4, omax = 4;
+    m_off_.assign(nr, std::vector<long long>(L_));
+    for (int r = 0; r < nr; ++r) {
+      const HostRobot& h = hr_[r];
+      RobotDesc& d = rd[r];
+      std::memset(&d, 0, sizeof(d));
+      d.n_v = h.n_v;
+      d.n_s = h.n_s;
+      d.n_out = h.n_out;
+      d.n_c = h.n_c;
+      d.pos_pad = h.pos_pad;
+      d.robot_id = h.robot_id;
+      d.n_layers = h.n_layers;
+      for (int l = 0; l <= L_; ++l) d.width[l] = h.width[l];
+      for (int l = 0; l < L_; ++l) {
+        d.pitch[l] = round4(h.width[l]);
+        d.w_off[l] = woff;
+        woff += (long long)d.pitch[l] * h.width[l + 1];
+        woff = (woff + 7) & ~7LL;  // keep every row block 32-byte aligned
+        d.b_off[l] = boff;
+        boff += h.width[l + 1];
+        m_off_[r][l] = moff;
+        moff += (long long)h.width[l + 1] * h.full_cols[l];
+      }
+      int rid[4] = {45, 46, 34, 36};
+      for (int q = 0; q < 4; ++q) d.rot_idx[q] = rid[q];
+      if (h.robot_id == 100) CLS_REQUIRE(h.n_v > 46, "robot_id 100 needs >= 47 vertices");
+      // CSR incidence, springs sorted by endpoint then by spring index
+      d.ptr_off = (int)inc_ptr.size();
+      d.inc_off = (int)inc_i.size();
+      d.spr_off = (int)spring_out.size();
+      std::vector<std::vector<int>> per(h.n_v);
+      for (int s = 0; s < h.n_s; ++s) {
+        per[h.sa[s]].push_back(2 * s);
+        per[h.sb[s]].push_back(2 * s + 1);
+      }
+      int run = 0;
+      for (int i = 0; i < h.n_v; ++i) {
+        inc_ptr.push_back(run);
+        for (int code : per[i]) {
+          const int s = code >> 1, side = code & 1;
+          int4 ii;
+          ii.x = side ? h.sa[s] : h.sb[s];
+          ii.y = side;
+          ii.z = s;
+          ii.w = h.out[s];
+          inc_i.push_back(ii);
+          V4<R> f;
+          f.x = (R)h.len[s];
+          f.y = (R)h.stiff[s];
+          f.z = (R)h.coef[s];
+          f.w = 0;
+          inc_f.push_back(f);
+          ++run;
+        }
+      }
+      inc_ptr.push_back(run);
+      for (int s = 0; s < h.n_s; ++s) spring_out.push_back(h.out[s]);
+      nmax_ = std::max(nmax_, h.n_v);
+      p0max = std::max(p0max, round4(h.width[0]));
+      omax = std::max(omax, round4(h.n_out));
+      dmax = std::max(dmax, round4(h.n_out));
+      for (int l = 1; l < L_; ++l) dmax = std::max(dmax, round4(h.width[l]));
+      amax = std::max(amax, std::max(round4(h.n_out), h.pos_pad));
+      for (int l = 1; l < L_; ++l) amax = std::max(amax, round4(h.width[l]));
+    }
+    // env descriptors (internal order)
+    std::vector<EnvDesc> ed(E);
+    int voff = 0, inoff = 0;
+    int zoff[kMaxLayers] = {0};
+    std::vector<int> count(nr, 0), first(nr, -1);
+    for (int ie = 0; ie < E; ++ie) {
+      const int r = env_robot[perm_[ie]];
+      EnvDesc& d = ed[ie];
+      std::memset(&d, 0, sizeof(d));
+      d.robot = r;
+      d.v_off = voff;
+      voff += hr_[r].n_v;
+      d.in_off = inoff;
+      inoff += hr_[r].n_c;
+      for (int l = 0; l < L_; ++l) {
+        d.z_off[l] = zoff[l];
+        zoff[l] += hr_[r].width[l + 1];
+      }
+      if (first[r] < 0) first[r] = ie;
+      count[r]++;
+    }
+    for (int r = 0; r < nr; ++r) {
+      rd[r].n_env = count[r];
+      rd[r].env_first = first[r] < 0 ? 0 : first[r];
+    }
+    user_voff_.assign(E, 0);
+    {
+      std::vector<int> nv_user(E);
+      for (int ue = 0; ue < E; ++ue) nv_user[ue] = hr_[env_robot[ue]].n_v;
+      int run = 0;
+      for (int ue = 0; ue < E; ++ue) { user_voff_[ue] = run; run += nv_user[ue]; }
+    }
+    env_robot_ = env_robot;
+    ed_host_ = ed;
+    rd_host_ = rd;
+    V_ = voff;
+    in_total_ = inoff;
+    for (int l = 0; l < L_; ++l) z_total_[l] = zoff[l];
+    long long zb = 0;
+    for (int l = 0; l < L_; ++l) {
+      z_base_[l] = zb;
+      zb += (long long)K_ * z_total_[l];
+    }
+    rec_z_total_ = zb;
+    // processing order: heaviest envs first (longest-processing-time first)
+    order_host_.resize(E);
+    std::iota(order_host_.begin(), order_host_.end(), 0);
+    auto cost = [&](int ie) {
+      const HostRobot& h = hr_[ed[ie].robot];
+      double c = 0;
+      for (int l = 0; l < L_; ++l) c += (double)h.width[l + 1] * round4(h.width[l]);
+      return c + 40.0 * h.n_s + 20.0 * h.n_v;
+    };
+    std::stable_sort(order_host_.begin(), order_host_.end(),
+                     [&](int a, int b) { return cost(a) > cost(b); });
+    // launch shape
+    threads_ = p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads();
+    CLS_REQUIRE(threads_ % 32 == 0 && threads_ >= 64 && threads_ <= 1024,
+                "threads_per_block must be a multiple of 32 in [64, 1024]");
+    smem_p0max_ = p0max;
+    smem_dmax_ = dmax;
+    smem_amax_ = amax;
+    smem_omax_ = omax;
+    fwd_smem_ = fwd_smem_bytes<R>(nmax_, dmax, p0max);
+    rev_smem_ = rev_smem_bytes<R>(nmax_, amax, omax, dmax, threads_);
+    int dev = 0, optin = 0;
+    CLS_CUDA(cudaGetDevice(&dev));
+    CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CLS_CUDA(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, dev));
+    const size_t static_smem = sizeof(RobotDesc) + sizeof(EnvDesc) + 64;
+    CLS_REQUIRE(fwd_smem_ + static_smem <= (size_t)optin && rev_smem_ + static_smem <= (size_t)optin,
+                "robot too large for one CTA's shared memory (" + std::to_string(rev_smem_) +
+                    " bytes needed)");
+    CLS_CUDA(cudaFuncSetAttribute(ms_forward_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fwd_smem_));
+    CLS_CUDA(cudaFuncSetAttribute(ms_reverse_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)rev_smem_));
+    // GEMM tiles (per robot, per layer)
+    for (int r = 0; r < nr; ++r) {
+      if (count[r] == 0) continue;
+      for (int l = 0; l < L_; ++l)
+        for (int i0 = 0; i0 < hr_[r].width[l + 1]; i0 += 64)
+          for (int j0 = 0; j0 < hr_[r].width[l]; j0 += 64) tiles_host_.push_back({r, l, i0, j0});
+    }
+    // device allocations
+    const int n_seg_max = (T_ - 1 + K_ - 1) / K_ + 1;
+    n_ckpt_ = n_seg_max + 1;
+    d_robots_.alloc(nr);
+    d_envs_.alloc(E);
+    d_order_.alloc(E);
+    d_inc_ptr_.alloc(inc_ptr.size());
+    d_inc_i_.alloc(std::max<size_t>(1, inc_i.size()));
+    d_inc_f_.alloc(std::max<size_t>(1, inc_f.size()));
+    d_spring_out_.alloc(std::max<size_t>(1, spring_out.size()));
+    d_w_.alloc(woff);
+    d_gw_.alloc(woff);
+    d_bias_.alloc(boff);
+    d_gb_.alloc(boff);
+    d_bm_.alloc(boff);
+    d_bv_.alloc(boff);
+    d_wm_.alloc(moff);
+    d_wmm_.alloc(moff);
+    d_wmv_.alloc(moff);
+    d_sin_.alloc((size_t)(T_ + 2) * std::max(1, p_.n_sin_waves));
+    d_ckx_.alloc((size_t)n_ckpt_ * V_);
+    d_ckv_.alloc((size_t)n_ckpt_ * V_);
+    d_finx_.alloc(V_);
+    d_finv_.alloc(V_);
+    d_recx_.alloc((size_t)K_ * V_);
+    d_recv_.alloc((size_t)K_ * V_);
+    d_recin_.alloc((size_t)K_ * in_total_);
+    d_recz_.alloc(rec_z_total_);
+    d_recdz_.alloc(rec_z_total_);
+    d_head_.alloc(V_);
+    d_obsc_.alloc((size_t)T_ * E);
+    d_obsh_.alloc((size_t)T_ * E);
+    d_obsu_.alloc((size_t)T_ * E);
+    d_obsr_.alloc((size_t)T_ * E);
+    keep_x_ = (p_.loss_mask & (LOSS_ROTATION | LOSS_POSE)) != 0;
+    if (keep_x_) d_xfull_.alloc((size_t)T_ * V_);
+    if (p_.loss_mask & LOSS_ACTUATION) d_actfull_.alloc((size_t)T_ * z_total_[L_ - 1]);
+    d_tv_.alloc((size_t)T_ * E);
+    d_th_.alloc((size_t)T_ * E);
+    d_tc_.alloc((size_t)T_ * E);
+    d_init_.alloc(V_);
+    d_adjx_.alloc(V_);
+    d_adjv_.alloc(V_);
+    d_adjh_.alloc(E);
+    d_status_.alloc(1);
+    d_iter_.alloc(1);
+    d_lossenv_.alloc((size_t)E * 8);
+    d_tiles_.alloc(std::max<size_t>(1, tiles_host_.size()));
+    n_queue_ = (size_t)(1 + 2 * n_seg_max) * E;
+    d_queue_.alloc(n_queue_);
+    size_t stage = std::max<size_t>((size_t)T_ * E * 3, (size_t)V_ * 3);
+    stage = std::max<size_t>(stage, (size_t)moff);
+    stage = std::max<size_t>(stage, (size_t)boff);
+    d_stage_.alloc(stage);
+    d_tns_.alloc(kAdamBlocks);
+    // uploads
+    CLS_CUDA(cudaMemcpy(d_robots_.p, rd.data(), sizeof(RobotDesc) * nr, cudaMemcpyHostToDevice));
+    CLS_CUDA(cudaMemcpy(d_envs_.p, ed.data(), sizeof(EnvDesc) * E, cudaMemcpyHostToDevice));
+    CLS_CUDA(cudaMemcpy(d_order_.p, order_host_.data(), sizeof(int) * E, cudaMemcpyHostToDevice));
+    CLS_CUDA(cudaMemcpy(d_inc_ptr_.p, inc_ptr.data(), sizeof(int) * inc_ptr.size(), cudaMemcpyHostToDevice));
+    if (!inc_i.empty()) {
+      CLS_CUDA(cudaMemcpy(d_inc_i_.p, inc_i.data(), sizeof(int4) * inc_i.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_inc_f_.p, inc_f.data(), sizeof(V4<R>) * inc_f.size(), cudaMemcpyHostToDevice));
+    }
+    if (!spring_out.empty())
+      CLS_CUDA(cudaMemcpy(d_spring_out_.p, spring_out.data(), sizeof(int) * spring_out.size(),
+                          cudaMemcpyHostToDevice));
+    if (!tiles_host_.empty())
+      CLS_CUDA(cudaMemcpy(d_tiles_.p, tiles_host_.data(), sizeof(GemmTile) * tiles_host_.size(),
+                          cudaMemcpyHostToDevice));
+    {
+      const int ns = std::max(1, p_.n_sin_waves);
+      std::vector<R> st((size_t)(T_ + 2) * ns, R(0));
+      for (int t = 0; t < T_ + 2; ++t)
+        for (int j = 0; j < p_.n_sin_waves; ++j)
+          st[(size_t)t * ns + j] =
+              (R)std::sin(p_.spring_omega * (double)t * p_.dt + 2 * M_PI / p_.n_sin_waves * (double)j);
+      CLS_CUDA(cudaMemcpy(d_sin_.p, st.data(), sizeof(R) * st.size(), cudaMemcpyHostToDevice));
+    }
+    CLS_CUDA(cudaMemset(d_w_.p, 0, sizeof(R) * d_w_.n));
+    CLS_CUDA(cudaMemset(d_wm_.p, 0, sizeof(R) * d_wm_.n));
+    CLS_CUDA(cudaMemset(d_bias_.p, 0, sizeof(R) * d_bias_.n));
+    CLS_CUDA(cudaMemset(d_ckx_.p, 0, sizeof(V4<R>) * d_ckx_.n));
+    CLS_CUDA(cudaMemset(d_ckv_.p, 0, sizeof(V4<R>) * d_ckv_.n));
+    CLS_CUDA(cudaMemset(d_tv_.p, 0, sizeof(V4<R>) * d_tv_.n));
+    CLS_CUDA(cudaMemset(d_th_.p, 0, sizeof(R) * d_th_.n));
+    CLS_CUDA(cudaMemset(d_tc_.p, 0, sizeof(R) * d_tc_.n));
+    CLS_CUDA(cudaMemset(d_status_.p, 0, sizeof(int)));
+    CLS_CUDA(cudaMemset(d_init_.p, 0, sizeof(V4<R>) * d_init_.n));
+    clear_adam();
+    // initial state: the robots' own objects
+    std::vector<double> x0((size_t)V_ * 3, 0.0);
+    for (int ue = 0; ue < E; ++ue) {
+      const HostRobot& h = hr_[env_robot[ue]];
+      std::memcpy(&x0[(size_t)user_voff_[ue] * 3], h.objects.data(), sizeof(double) * 3 * h.n_v);
+    }
+    std::vector<double> v0((size_t)V_ * 3, 0.0);
+    set_state(x0.data(), v0.data());
+    CLS_CUDA(cudaDeviceSynchronize());
+  }
+
+  int auto_threads() const {
+    // enough warps for the per-row MLP products and the vertex loops; more
+    // threads than that only adds barrier cost
+    int work = 0;
+    for (const HostRobot& h : hr_) {
+      work = std::max(work, h.n_v);
+      for (int l = 1; l <= L_; ++l) work = std::max(work, h.width[l] * 4);
+    }
+    int t = 128;
+    while (t < 1024 && t < work) t *= 2;
+    return t;
+  }
+
+  MsArgs<R> args(int steps) const {
+    MsArgs<R> a;
+    std::memset(&a, 0, sizeof(a));
+    a.n_envs = E_;
+    a.n_items = E_;
+    a.T = T_;
+    a.steps = steps;
+    a.K = K_;
+    a.n_sin = p_.n_sin_waves;
+    a.dup_v = p_.duplicate_v;
+    a.dup_h = p_.duplicate_h;
+    a.dup_c = p_.duplicate_c;
+    a.act_hidden = p_.activation_hidden;
+    a.act_out = p_.activation_output;
+    a.run_period = p_.run_period;
+    a.turn_period = p_.turn_period;
+    a.jump_period = p_.jump_period;
+    a.loss_mask = p_.loss_mask;
+    a.v_total = V_;
+    a.in_total = in_total_;
+    for (int l = 0; l < L_; ++l) {
+      a.z_total[l] = z_total_[l];
+      a.z_base[l] = z_base_[l];
+    }
+    a.smem_nmax = nmax_;
+    a.smem_p0max = smem_p0max_;
+    a.smem_dmax = smem_dmax_;
+    a.smem_amax = smem_amax_;
+    a.smem_omax = smem_omax_;
+    a.dt = (R)p_.dt;
+    a.gravity = (R)p_.gravity;
+    a.ground = (R)p_.ground_height;
+    a.drag_s = (R)std::exp(-p_.dt * p_.drag_damping);
+    a.dashpot = (R)p_.dashpot_damping;
+    a.friction = (R)p_.friction;
+    a.max_speed = (R)p_.max_speed;
+    a.robots = d_robots_.p;
+    a.envs = d_envs_.p;
+    a.order = d_order_.p;
+    a.queue = d_queue_.p;
+    a.inc_ptr = d_inc_ptr_.p;
+    a.inc_i = d_inc_i_.p;
+    a.inc_f = d_inc_f_.p;
+    a.spring_out = d_spring_out_.p;
+    a.w = d_w_.p;
+    a.bias = d_bias_.p;
+    a.sin_table = d_sin_.p;
+    a.ckpt_x = d_ckx_.p;
+    a.ckpt_v = d_ckv_.p;
+    a.fin_x = d_finx_.p;
+    a.fin_v = d_finv_.p;
+    a.rec_x = d_recx_.p;
+    a.rec_v = d_recv_.p;
+    a.rec_in = d_recin_.p;
+    a.rec_z = d_recz_.p;
+    a.rec_dz = d_recdz_.p;
+    a.head = d_head_.p;
+    a.obs_center = d_obsc_.p;
+    a.obs_height = d_obsh_.p;
+    a.obs_upper = d_obsu_.p;
+    a.obs_rot = d_obsr_.p;
+    a.x_full = d_xfull_.p;
+    a.act_full = d_actfull_.p;
+    a.tv = d_tv_.p;
+    a.th = d_th_.p;
+    a.tc = d_tc_.p;
+    a.init_obj = d_init_.p;
+    a.adj_x = d_adjx_.p;
+    a.adj_v = d_adjv_.p;
+    a.adj_h = d_adjh_.p;
+    a.status = d_status_.p;
+    return a;
+  }
+
+  int grid_for(int items) const { return std::max(1, std::min(items, n_sm_ * 2)); }
+
+  // one batched launch (all envs) or one launch per env
+  template <typename F>
+  void each_launch(bool per_env, MsArgs<R> a, int& qslot, F&& launch) {
+    if (!per_env) {
+      a.queue = d_queue_.p + (size_t)qslot * 1;
+      qslot += 1;
+      launch(a, grid_for(E_));
+      return;
+    }
+    for (int k = 0; k < E_; ++k) {
+      MsArgs<R> b = a;
+      b.order = d_order_.p + k;
+      b.n_items = 1;
+      b.queue = d_queue_.p + (size_t)qslot;
+      qslot += 1;
+      launch(b, 1);
+    }
+  }
+
+  // run one kernel launch, counted and (when profiling) bracketed by events
+  template <typename F>
+  void timed(int kind, F&& f) {
+    prof_.launches[kind] += 1;
+    if (!prof_.on) {
+      f();
+      return;
+    }
+    if (prof_.used + 2 > prof_.ev.size()) {
+      for (int q = 0; q < 64; ++q) {
+        cudaEvent_t e;
+        CLS_CUDA(cudaEventCreate(&e));
+        prof_.ev.push_back(e);
+      }
+    }
+    cudaEvent_t a = prof_.ev[prof_.used], b = prof_.ev[prof_.used + 1];
+    prof_.used += 2;
+    prof_.kind.push_back(kind);
+    CLS_CUDA(cudaEventRecord(a, stream));
+    f();
+    CLS_CUDA(cudaEventRecord(b, stream));
+  }
+
+  void profile_collect() {
+    if (prof_.used == 0) return;
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    for (size_t q = 0; q < prof_.kind.size(); ++q) {
+      float t = 0;
+      CLS_CUDA(cudaEventElapsedTime(&t, prof_.ev[2 * q], prof_.ev[2 * q + 1]));
+      prof_.ms[prof_.kind[q]] += t;
+    }
+    prof_.kind.clear();
+    prof_.used = 0;
+  }
+
+  void profile_enable(bool on) override {
+    CLS_REQUIRE(!capturing_, "profiling cannot be switched during graph capture");
+    profile_collect();
+    prof_.on = on;
+  }
+
+  void profile_read(double* ms, long long* launches, bool reset) override {
+    profile_collect();
+    for (int k = 0; k < PK_COUNT; ++k) {
+      if (ms) ms[k] = prof_.ms[k];
+      if (launches) launches[k] = prof_.launches[k];
+    }
+    if (reset) {
+      for (int k = 0; k < PK_COUNT; ++k) { prof_.ms[k] = 0; prof_.launches[k] = 0; }
+    }
+  }
+
+  void weights_init(unsigned long long seed) override {
+    for (size_t r = 0; r < hr_.size(); ++r) {
+      const HostRobot& h = hr_[r];
+      for (int l = 0; l < L_; ++l) {
+        const long long n = (long long)h.width[l + 1] * h.full_cols[l];
+        timed(PK_OTHER, [&] {
+          ms_weights_init_kernel<R><<<blocks_for(n), 256, 0, stream>>>(
+              d_wm_.p, m_off_[r][l], n, h.full_cols[l], seed, (unsigned long long)(r * 16 + l));
+        });
+        pack_layer((int)r, l);
+      }
+    }
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void initialize_train(int iter, int steps, unsigned long long seed, double max_speed) override {
+    CLS_REQUIRE(steps >= 1 && steps <= T_, "steps out of range");
+    const long long n = (long long)T_ * E_;
+    // the sampled tasks are defined per internal env; targets of envs are
+    // independent draws, so the env numbering only relabels the draws
+    timed(PK_OTHER, [&] {
+      ms_initialize_train_kernel<R><<<blocks_for(n), 256, 0, stream>>>(
+          d_tv_.p, d_th_.p, T_, steps, E_, p_.turn_period, seed, iter, max_speed);
+    });
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  // --------------------------------------------------------------- passes
+  void forward(int steps, bool eval, bool per_env) override {
+    if (eval) {
+      CLS_REQUIRE(steps >= 0 && steps + 1 < T_, "evaluation rollout needs steps + 1 < max_steps");
+    } else {
+      CLS_REQUIRE(steps >= 2 && steps <= T_, "training rollout needs 2 <= steps <= max_steps");
+    }
+    steps_ = steps;
+    eval_ = eval;
+    per_env_ = per_env;
+    CLS_CUDA(cudaMemsetAsync(d_queue_.p, 0, sizeof(int) * d_queue_.n, stream));
+    CLS_CUDA(cudaMemsetAsync(d_obsc_.p, 0, sizeof(V4<R>) * d_obsc_.n, stream));
+    CLS_CUDA(cudaMemsetAsync(d_obsh_.p, 0, sizeof(R) * d_obsh_.n, stream));
+    CLS_CUDA(cudaMemsetAsync(d_obsu_.p, 0, sizeof(R) * d_obsu_.n, stream));
+    CLS_CUDA(cudaMemsetAsync(d_obsr_.p, 0, sizeof(R) * d_obsr_.n, stream));
+    if (d_xfull_.p) CLS_CUDA(cudaMemsetAsync(d_xfull_.p, 0, sizeof(V4<R>) * d_xfull_.n, stream));
+    if (d_actfull_.p) CLS_CUDA(cudaMemsetAsync(d_actfull_.p, 0, sizeof(R) * d_actfull_.n, stream));
+    const int t_end = eval ? steps + 1 : steps - 1;
+    MsArgs<R> a = args(steps);
+    qslot_ = 0;
+    each_launch(per_env, a, qslot_, [&](const MsArgs<R>& b, int grid) {
+      timed(PK_FWD, [&] {
+        ms_forward_kernel<R><<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
+      });
+    });
+    CLS_CUDA(cudaGetLastError());
+    fwd_done_ = true;
+  }
+
+  void loss_device() {
+    MsArgs<R> a = args(steps_);
+    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p); });
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void loss(double* terms, double* env) override {
+    CLS_REQUIRE(fwd_done_, "cls_loss called before a forward rollout");
+    loss_device();
+    std::vector<double> raw((size_t)E_ * 8);
+    CLS_CUDA(cudaMemcpyAsync(raw.data(), d_lossenv_.p, sizeof(double) * raw.size(),
+                             cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    loss_from_raw(raw, terms, env);
+  }
+
+  void loss_from_raw(const std::vector<double>& raw, double* terms, double* env) {
+    double t8[8] = {0};
+    for (int ie = 0; ie < E_; ++ie)
+      for (int l = 0; l < LS_COUNT; ++l) t8[1 + l] += raw[(size_t)ie * 8 + l];
+    for (int l = 1; l < 8; ++l) t8[0] += t8[l];
+    if (terms) std::memcpy(terms, t8, sizeof(t8));
+    if (env) {
+      for (int ie = 0; ie < E_; ++ie) {
+        const int ue = perm_[ie];
+        const double B = rd_host_[ed_host_[ie].robot].n_env;
+        double tot = 0;
+        for (int l = 0; l < LS_COUNT; ++l) {
+          const double v = raw[(size_t)ie * 8 + l] * B;
+          env[(size_t)(1 + l) * E_ + ue] = v;
+          tot += v;
+        }
+        env[ue] = tot;
+      }
+    }
+    max_height_ = 0;
+    for (int ie = 0; ie < E_; ++ie) max_height_ = std::max(max_height_, raw[(size_t)ie * 8 + 7]);
+  }
+
+  void backward(bool per_env) override {
+    CLS_REQUIRE(fwd_done_ && !eval_, "cls_backward needs a training rollout first");
+    const int steps = steps_;
+    const int t_last = steps - 1;  // x[steps-1] is the last state
+    const int n_seg = (t_last + K_ - 1) / K_;
+    CLS_CUDA(cudaMemsetAsync(d_gw_.p, 0, sizeof(R) * d_gw_.n, stream));
+    CLS_CUDA(cudaMemsetAsync(d_gb_.p, 0, sizeof(R) * d_gb_.n, stream));
+    MsArgs<R> a = args(steps);
+    int qslot = qslot_;
+    for (int s = n_seg - 1; s >= 0; --s) {
+      const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
+      each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
+        timed(PK_RECOMP, [&] {
+          ms_forward_kernel<R><<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+        });
+      });
+      each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
+        timed(PK_REV, [&] {
+          ms_reverse_kernel<R><<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
+        });
+      });
+      if (!tiles_host_.empty())
+        timed(PK_WGRAD, [&] {
+          ms_wgrad_kernel<R><<<(int)tiles_host_.size(), 256, 0, stream>>>(a, d_tiles_.p, t1 - t0,
+                                                                           d_gw_.p, d_gb_.p);
+        });
+    }
+    CLS_CUDA(cudaGetLastError());
+    bwd_done_ = true;
+  }
+
+  void adam_device(int iter_or_neg, bool apply) {
+    // iteration taken from d_iter_ when iter_or_neg < 0 (graph replays)
+    for (size_t r = 0; r < hr_.size(); ++r) {
+      const HostRobot& h = hr_[r];
+      const RobotDesc& d = rd_host_[r];
+      for (int l = 0; l < L_; ++l) {
+        timed(PK_ADAM, [&] {
+          ms_adam_kernel<R><<<kAdamBlocks - 1, 256, 0, stream>>>(
+              d_wm_.p, d_wmm_.p, d_wmv_.p, d_gw_.p, m_off_[r][l], d.w_off[l], h.width[l + 1],
+              h.full_cols[l], d.pitch[l], l, h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v,
+              p_.duplicate_h, p_.duplicate_c, p_.learning_rate, p_.adam_b1, p_.adam_b2,
+              iter_or_neg, d_iter_.p, apply ? 1 : 0, d_tns_.p);
+        });
+        timed(PK_ADAM, [&] {
+          ms_adam_bias_kernel<R><<<1, 256, 0, stream>>>(
+              d_bias_.p + d.b_off[l], d_bm_.p + d.b_off[l], d_bv_.p + d.b_off[l], d_gb_.p + d.b_off[l],
+              h.width[l + 1], p_.learning_rate, p_.adam_b1, p_.adam_b2, iter_or_neg, d_iter_.p,
+              apply ? 1 : 0, d_tns_.p + kAdamBlocks - 1);
+        });
+        pack_layer((int)r, l);
+      }
+    }
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void adam(int iter, double* tns) override {
+    CLS_REQUIRE(bwd_done_, "cls_adam_step needs gradients (cls_backward) first");
+    if (tns) *tns = tns_sum();
+    adam_device(iter, true);
+  }
+
+  double tns_sum() {
+    // squared norm of the full-layout gradient (Model.get_TNS)
+    double s = 0;
+    std::vector<double> part(kAdamBlocks);
+    for (size_t r = 0; r < hr_.size(); ++r) {
+      const HostRobot& h = hr_[r];
+      const RobotDesc& d = rd_host_[r];
+      for (int l = 0; l < L_; ++l) {
+        ms_adam_kernel<R><<<kAdamBlocks - 1, 256, 0, stream>>>(
+            d_wm_.p, d_wmm_.p, d_wmv_.p, d_gw_.p, m_off_[r][l], d.w_off[l], h.width[l + 1],
+            h.full_cols[l], d.pitch[l], l, h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v,
+            p_.duplicate_h, p_.duplicate_c, p_.learning_rate, p_.adam_b1, p_.adam_b2, 0, d_iter_.p,
+            0, d_tns_.p);
+        ms_adam_bias_kernel<R><<<1, 256, 0, stream>>>(
+            d_bias_.p + d.b_off[l], d_bm_.p + d.b_off[l], d_bv_.p + d.b_off[l], d_gb_.p + d.b_off[l],
+            h.width[l + 1], p_.learning_rate, p_.adam_b1, p_.adam_b2, 0, d_iter_.p, 0,
+            d_tns_.p + kAdamBlocks - 1);
+        CLS_CUDA(cudaMemcpyAsync(part.data(), d_tns_.p, sizeof(double) * kAdamBlocks,
+                                 cudaMemcpyDeviceToHost, stream));
+        CLS_CUDA(cudaStreamSynchronize(stream));
+        for (double q : part) s += q;
+      }
+    }
+    return s;
+  }
+
+  void clear_adam() override {
+    CLS_CUDA(cudaMemset(d_wmm_.p, 0, sizeof(R) * d_wmm_.n));
+    CLS_CUDA(cudaMemset(d_wmv_.p, 0, sizeof(R) * d_wmv_.n));
+    CLS_CUDA(cudaMemset(d_bm_.p, 0, sizeof(R) * d_bm_.n));
+    CLS_CUDA(cudaMemset(d_bv_.p, 0, sizeof(R) * d_bv_.n));
+  }
+
+  void pack_layer(int r, int l) {
+    const HostRobot& h = hr_[r];
+    const RobotDesc& d = rd_host_[r];
+    const long long total = (long long)h.width[l + 1] * d.pitch[l];
+    const int blocks = (int)std::min<long long>(1024, (total + 255) / 256);
+    timed(PK_ADAM, [&] {
+      ms_pack_weights_kernel<R><<<std::max(1, blocks), 256, 0, stream>>>(
+          d_wm_.p, m_off_[r][l], h.width[l + 1], h.full_cols[l], d_w_.p, d.w_off[l], d.pitch[l], l,
+          h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v, p_.duplicate_h, p_.duplicate_c);
+    });
+  }
+
+  // ---------------------------------------------------------------- I/O
+  void upload_doubles(const double* host, size_t n) {
+    CLS_REQUIRE(n <= d_stage_.n, "staging buffer too small");
+    CLS_CUDA(cudaMemcpyAsync(d_stage_.p, host, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+  }
+
+  template <typename T>
+  static int blocks_for(T n) { return (int)std::max<long long>(1, std::min<long long>(4096, ((long long)n + 255) / 256)); }
+
+  // user-order [V][3] <-> internal-order [V][3]
+  void to_internal(const double* in, std::vector<double>& out) const {
+    out.resize((size_t)V_ * 3);
+    for (int ie = 0; ie < E_; ++ie) {
+      const int ue = perm_[ie];
+      std::memcpy(&out[(size_t)ed_host_[ie].v_off * 3], in + (size_t)user_voff_[ue] * 3,
+                  sizeof(double) * 3 * rd_host_[ed_host_[ie].robot].n_v);
+    }
+  }
+  void to_user(const std::vector<double>& in, double* out) const {
+    for (int ie = 0; ie < E_; ++ie) {
+      const int ue = perm_[ie];
+      std::memcpy(out + (size_t)user_voff_[ue] * 3, &in[(size_t)ed_host_[ie].v_off * 3],
+                  sizeof(double) * 3 * rd_host_[ed_host_[ie].robot].n_v);
+    }
+  }
+
+  void set_vstate(const double* host, V4<R>* dst) {
+    const double* src = host;
+    std::vector<double> tmp;
+    if (!identity_perm_) { to_internal(host, tmp); src = tmp.data(); }
+    upload_doubles(src, (size_t)V_ * 3);
+    ms_xyz_to_v4_kernel<R><<<blocks_for(V_), 256, 0, stream>>>(d_stage_.p, dst, V_);
+    CLS_CUDA(cudaGetLastError());
+    if (!identity_perm_) CLS_CUDA(cudaStreamSynchronize(stream));  // tmp lifetime
+  }
+
+  void get_vstate(const V4<R>* srcd, double* host) {
+    ms_v4_to_xyz_kernel<R><<<blocks_for(V_), 256, 0, stream>>>(srcd, d_stage_.p, V_);
+    CLS_CUDA(cudaGetLastError());
+    if (identity_perm_) {
+      CLS_CUDA(cudaMemcpyAsync(host, d_stage_.p, sizeof(double) * V_ * 3, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    } else {
+      std::vector<double> tmp((size_t)V_ * 3);
+      CLS_CUDA(cudaMemcpyAsync(tmp.data(), d_stage_.p, sizeof(double) * V_ * 3, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      to_user(tmp, host);
+    }
+  }
+
+  void set_state(const double* x0, const double* v0) override {
+    CLS_REQUIRE(x0 != nullptr, "x0 is required");
+    set_vstate(x0, d_ckx_.p);
+    CLS_CUDA(cudaMemcpyAsync(d_init_.p, d_ckx_.p, sizeof(V4<R>) * V_, cudaMemcpyDeviceToDevice, stream));
+    if (v0) set_vstate(v0, d_ckv_.p);
+    else CLS_CUDA(cudaMemsetAsync(d_ckv_.p, 0, sizeof(V4<R>) * V_, stream));
+    fwd_done_ = bwd_done_ = false;
+  }
+
+  // [T][user env] -> [T][internal env]
+  void permute_te(const double* in, int width, std::vector<double>& out) const {
+    out.resize((size_t)T_ * E_ * width);
+    for (int t = 0; t < T_; ++t)
+      for (int ie = 0; ie < E_; ++ie)
+        std::memcpy(&out[((size_t)t * E_ + ie) * width], in + ((size_t)t * E_ + perm_[ie]) * width,
+                    sizeof(double) * width);
+  }
+
+  void set_targets(const double* tv, const double* th, const double* tc) override {
+    std::vector<double> tmp;
+    if (tv) {
+      const double* src = tv;
+      if (!identity_perm_) { permute_te(tv, 3, tmp); src = tmp.data(); }
+      upload_doubles(src, (size_t)T_ * E_ * 3);
+      ms_xyz_to_v4_kernel<R><<<blocks_for(T_ * E_), 256, 0, stream>>>(d_stage_.p, d_tv_.p, (long long)T_ * E_);
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    const double* arrs[2] = {th, tc};
+    R* dsts[2] = {d_th_.p, d_tc_.p};
+    for (int q = 0; q < 2; ++q) {
+      if (!arrs[q]) {
+        CLS_CUDA(cudaMemsetAsync(dsts[q], 0, sizeof(R) * (size_t)T_ * E_, stream));
+        continue;
+      }
+      const double* src = arrs[q];
+      if (!identity_perm_) { permute_te(arrs[q], 1, tmp); src = tmp.data(); }
+      upload_doubles(src, (size_t)T_ * E_);
+      ms_convert_kernel<R><<<blocks_for(T_ * E_), 256, 0, stream>>>(d_stage_.p, dsts[q], (long long)T_ * E_);
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void check_layer(int r, int l) const {
+    CLS_REQUIRE(r >= 0 && r < (int)hr_.size(), "robot index out of range");
+    CLS_REQUIRE(l >= 0 && l < L_, "layer index out of range");
+  }
+
+  void set_weights(int r, int l, const double* W, const double* b) override {
+    check_layer(r, l);
+    const HostRobot& h = hr_[r];
+    const long long n = (long long)h.width[l + 1] * h.full_cols[l];
+    if (W) {
+      upload_doubles(W, n);
+      ms_convert_kernel<R><<<blocks_for(n), 256, 0, stream>>>(d_stage_.p, d_wm_.p + m_off_[r][l], n);
+      pack_layer(r, l);
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    if (b) {
+      upload_doubles(b, h.width[l + 1]);
+      ms_convert_kernel<R><<<1, 256, 0, stream>>>(d_stage_.p, d_bias_.p + rd_host_[r].b_off[l], h.width[l + 1]);
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void get_weights(int r, int l, double* W, double* b) override {
+    check_layer(r, l);
+    const HostRobot& h = hr_[r];
+    const long long n = (long long)h.width[l + 1] * h.full_cols[l];
+    if (W) {
+      ms_to_double_kernel<R><<<blocks_for(n), 256, 0, stream>>>(d_wm_.p + m_off_[r][l], d_stage_.p, n);
+      CLS_CUDA(cudaMemcpyAsync(W, d_stage_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    if (b) {
+      ms_to_double_kernel<R><<<1, 256, 0, stream>>>(d_bias_.p + rd_host_[r].b_off[l], d_stage_.p, h.width[l + 1]);
+      CLS_CUDA(cudaMemcpyAsync(b, d_stage_.p, sizeof(double) * h.width[l + 1], cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+  }
+
+  void get_grads(int r, int l, double* gW, double* gb) override {
+    check_layer(r, l);
+    CLS_REQUIRE(bwd_done_, "gradients requested before cls_backward");
+    const HostRobot& h = hr_[r];
+    const RobotDesc& d = rd_host_[r];
+    const long long n = (long long)h.width[l + 1] * h.full_cols[l];
+    if (gW) {
+      ms_unpack_grad_kernel<R><<<blocks_for(n), 256, 0, stream>>>(
+          d_gw_.p, d.w_off[l], d.pitch[l], h.width[l + 1], h.full_cols[l], l, h.n_v, h.pos_pad,
+          p_.n_sin_waves, p_.duplicate_v, p_.duplicate_h, p_.duplicate_c, d_stage_.p);
+      CLS_CUDA(cudaMemcpyAsync(gW, d_stage_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    if (gb) {
+      ms_to_double_kernel<R><<<1, 256, 0, stream>>>(d_gb_.p + d.b_off[l], d_stage_.p, h.width[l + 1]);
+      CLS_CUDA(cudaMemcpyAsync(gb, d_stage_.p, sizeof(double) * h.width[l + 1], cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+  }
+
+  void observables(double* c, double* h, double* u, double* rot) override {
+    const long long n = (long long)T_ * E_;
+    auto fetch_scalar = [&](const R* src, double* dst) {
+      if (!dst) return;
+      ms_to_double_kernel<R><<<blocks_for(n), 256, 0, stream>>>(src, d_stage_.p, n);
+      std::vector<double> tmp(n);
+      CLS_CUDA(cudaMemcpyAsync(tmp.data(), d_stage_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      for (int t = 0; t < T_; ++t)
+        for (int ie = 0; ie < E_; ++ie) dst[(size_t)t * E_ + perm_[ie]] = tmp[(size_t)t * E_ + ie];
+    };
+    if (c) {
+      ms_v4_to_xyz_kernel<R><<<blocks_for(n), 256, 0, stream>>>(d_obsc_.p, d_stage_.p, n);
+      std::vector<double> tmp(n * 3);
+      CLS_CUDA(cudaMemcpyAsync(tmp.data(), d_stage_.p, sizeof(double) * n * 3, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      for (int t = 0; t < T_; ++t)
+        for (int ie = 0; ie < E_; ++ie)
+          std::memcpy(c + ((size_t)t * E_ + perm_[ie]) * 3, &tmp[((size_t)t * E_ + ie) * 3], sizeof(double) * 3);
+    }
+    fetch_scalar(d_obsh_.p, h);
+    fetch_scalar(d_obsu_.p, u);
+    fetch_scalar(d_obsr_.p, rot);
+  }
+
+  void trajectory(double* x) override {
+    CLS_REQUIRE(d_xfull_.p != nullptr, "trajectory is only kept with a rotation or pose loss");
+    for (int t = 0; t < T_; ++t) get_vstate(d_xfull_.p + (size_t)t * V_, x + (size_t)t * V_ * 3);
+  }
+
+  void final_state(double* x, double* v) override {
+    if (x) get_vstate(d_finx_.p, x);
+    if (v) get_vstate(d_finv_.p, v);
+  }
+
+  void state_grads(double* gx, double* gv) override {
+    CLS_REQUIRE(bwd_done_, "state gradients requested before cls_backward");
+    if (gx) get_vstate(d_adjx_.p, gx);
+    if (gv) get_vstate(d_adjv_.p, gv);
+  }
+
+  int synchronize() override {
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    int st = 0;
+    CLS_CUDA(cudaMemcpy(&st, d_status_.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+      CLS_CUDA(cudaMemset(d_status_.p, 0, sizeof(int)));
+      if (st & ERR_NONFINITE) {
+        err = "non-finite state detected";
+        return CLS_ERR_NONFINITE;
+      }
+    }
+    return CLS_OK;
+  }
+
+  void graph_capture(int steps, bool with_adam) override {
+    CLS_REQUIRE(stream != nullptr, "graph capture needs a non-default stream (cls_set_stream)");
+    if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    CLS_REQUIRE(!prof_.on, "disable profiling before graph capture");
+    CLS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing_ = true;
+    try {
+      forward(steps, false, false);
+      loss_device();
+      backward(false);
+      if (with_adam) adam_device(-1, true);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      capturing_ = false;
+      throw;
+    }
+    capturing_ = false;
+    CLS_CUDA(cudaStreamEndCapture(stream, &graph_));
+    CLS_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+    graph_adam_ = with_adam;
+  }
+
+  void graph_launch(int iter) override {
+    CLS_REQUIRE(graph_exec_ != nullptr, "no captured graph (cls_graph_capture)");
+    if (graph_adam_) {
+      iter_host_ = iter;
+      CLS_CUDA(cudaMemcpyAsync(d_iter_.p, &iter_host_, sizeof(int), cudaMemcpyHostToDevice, stream));
+    }
+    CLS_CUDA(cudaGraphLaunch(graph_exec_, stream));
+  }
+
+  void sizes(int* ne, int* nv, int* T) const override {
+    if (ne) *ne = E_;
+    if (nv) *nv = V_;
+    if (T) *T = T_;
+  }
+  void layer_shape(int r, int l, int* rows, int* cols) const override {
+    check_layer(r, l);
+    if (rows) *rows = hr_[r].width[l + 1];
+    if (cols) *cols = hr_[r].full_cols[l];
+  }
+
+  static constexpr int kAdamBlocks = 129;
+
+ private:
+  std::vector<HostRobot> hr_;
+  cls_sim_params p_;
+  int E_ = 0, T_ = 0, K_ = 1, L_ = 1, V_ = 0, in_total_ = 0, nmax_ = 0;
+  int z_total_[kMaxLayers] = {0};
+  long long z_base_[kMaxLayers] = {0};
+  long long rec_z_total_ = 0;
+  int smem_p0max_ = 0, smem_dmax_ = 0, smem_amax_ = 0, smem_omax_ = 0, threads_ = 256, n_sm_ = 148, n_ckpt_ = 0;
+  size_t fwd_smem_ = 0, rev_smem_ = 0, n_queue_ = 0;
+  std::vector<int> perm_, user_voff_, env_robot_, order_host_;
+  bool identity_perm_ = true;
+  std::vector<EnvDesc> ed_host_;
+  std::vector<RobotDesc> rd_host_;
+  std::vector<GemmTile> tiles_host_;
+  std::vector<std::vector<long long>> m_off_;
+  bool keep_x_ = false, fwd_done_ = false, bwd_done_ = false, eval_ = false, per_env_ = false;
+  bool graph_adam_ = false, capturing_ = false;
+  Profiler prof_;
+  int steps_ = 0, qslot_ = 0, iter_host_ = 0;
+  double max_height_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  DevBuf<RobotDesc> d_robots_;
+  DevBuf<EnvDesc> d_envs_;
+  DevBuf<int> d_order_, d_queue_, d_inc_ptr_, d_spring_out_, d_status_, d_iter_;
+  DevBuf<int4> d_inc_i_;
+  DevBuf<V4<R>> d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_obsc_, d_xfull_,
+      d_tv_, d_init_, d_adjx_, d_adjv_;
+  DevBuf<R> d_w_, d_gw_, d_bias_, d_gb_, d_bm_, d_bv_, d_wm_, d_wmm_, d_wmv_, d_sin_, d_recin_,
+      d_recz_, d_recdz_, d_obsh_, d_obsu_, d_obsr_, d_actfull_, d_th_, d_tc_, d_adjh_;
+  DevBuf<unsigned char> d_head_;
+  DevBuf<double> d_lossenv_, d_stage_, d_tns_;
+  DevBuf<GemmTile> d_tiles_;
+};
+
+}  // namespace cls
+
+// ===================================================================== C ABI
+struct cls_sim {
+  std::unique_ptr<cls::SimBase> impl;
+};
+
+using cls::Fail;
+
+template <typename F>
+static int guarded(cls_sim* s, F&& f) {
+  if (!s || !s->impl) return CLS_ERR_INVALID;
+  try {
+    f(*s->impl);
+    return CLS_OK;
+  } catch (const Fail& e) {
+    s->impl->err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    s->impl->err = e.what();
+    return CLS_ERR_INVALID;
+  }
+}
+
+extern "C" {
+
+void cls_default_params(cls_sim_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->max_steps = 1000;
+  p->dt = 0.004;
+  p->gravity = -1.8;
+  p->ground_height = 0.1;
+  p->drag_damping = 0.0;
+  p->dashpot_damping = 0.1;
+  p->friction = 0.4;
+  p->stiffness_scale = 0.1;
+  p->run_period = 100;
+  p->turn_period = 500;
+  p->jump_period = 500;
+  p->spring_omega = 2 * M_PI / 0.004 / 100;
+  p->n_sin_waves = 100;
+  p->duplicate_v = 150;
+  p->duplicate_h = 150;
+  p->duplicate_c = 0;
+  p->activation_hidden = CLS_ACT_SIN;
+  p->activation_output = CLS_ACT_SIN;
+  p->loss_mask = CLS_LOSS_VELOCITY | CLS_LOSS_ROTATION;
+  p->precision = 32;
+  p->checkpoint_every = 50;
+  p->max_speed = 0.1;
+  p->max_height = 0.1;
+  p->adam_b1 = 0.9;
+  p->adam_b2 = 0.9;
+  p->learning_rate = 3e-4;
+  p->threads_per_block = 0;
+}
+
+int cls_create(const cls_robot_desc* robots, int32_t n_robots, const int32_t* env_robot,
+               int32_t n_envs, const cls_sim_params* params, cls_sim** out) {
+  using namespace cls;
+  if (!out) return CLS_ERR_INVALID;
+  *out = nullptr;
+  try {
+    CLS_REQUIRE(robots && n_robots > 0 && env_robot && n_envs > 0 && params, "null or empty argument");
+    const cls_sim_params& p = *params;
+    CLS_REQUIRE(p.precision == 32 || p.precision == 64, "precision must be 32 or 64");
+    CLS_REQUIRE(p.max_steps >= 2, "max_steps must be >= 2");
+    CLS_REQUIRE(p.run_period > 0 && p.turn_period > 0 && p.jump_period > 0, "periods must be > 0");
+    CLS_REQUIRE(p.n_sin_waves >= 0 && p.duplicate_v >= 0 && p.duplicate_h >= 0 && p.duplicate_c >= 0,
+                "negative input sizes");
+    CLS_REQUIRE(p.activation_hidden == 0 || p.activation_hidden == 1, "bad hidden activation");
+    CLS_REQUIRE(p.activation_output == 0 || p.activation_output == 1, "bad output activation");
+    std::vector<HostRobot> hr(n_robots);
+    int nl = -1;
+    for (int r = 0; r < n_robots; ++r) {
+      const cls_robot_desc& d = robots[r];
+      HostRobot& h = hr[r];
+      CLS_REQUIRE(d.n_vertices > 0 && d.objects && (d.n_springs == 0 || d.springs), "robot geometry missing");
+      CLS_REQUIRE(d.n_hidden_layers >= 1 && d.n_hidden_layers <= CLS_MAX_HIDDEN, "1..4 hidden layers");
+      if (nl < 0) nl = d.n_hidden_layers;
+      CLS_REQUIRE(nl == d.n_hidden_layers, "all robots of a batch need the same MLP depth");
+      h.n_v = d.n_vertices;
+      h.n_s = d.n_springs;
+      h.robot_id = d.robot_id;
+      h.objects.assign(d.objects, d.objects + 3 * (size_t)d.n_vertices);
+      h.n_out = d.n_outputs > 0 ? d.n_outputs : d.n_springs;
+      CLS_REQUIRE(h.n_out > 0, "robot has no MLP outputs");
+      for (int s = 0; s < d.n_springs; ++s) {
+        const double* row = d.springs + 5 * (size_t)s;
+        const int a = (int)row[0], b = (int)row[1];
+        CLS_REQUIRE(a >= 0 && a < d.n_vertices && b >= 0 && b < d.n_vertices && a != b,
+                    "spring endpoint out of range");
+        h.sa.push_back(a);
+        h.sb.push_back(b);
+        h.len.push_back(row[2]);
+        h.stiff.push_back(row[3] * p.stiffness_scale);
+        h.coef.push_back(row[4]);
+        int o = d.spring_output ? d.spring_output[s] : s;
+        CLS_REQUIRE(o >= -1 && o < h.n_out, "spring_output index out of range");
+        h.out.push_back(o);
+      }
+      h.n_layers = d.n_hidden_layers + 1;
+      const int n_goal = (p.duplicate_v > 0 ? 2 : 0) + (p.duplicate_h > 0 ? 1 : 0) + (p.duplicate_c > 0 ? 1 : 0);
+      h.pos_pad = round4(3 * h.n_v);
+      h.n_c = h.pos_pad + p.n_sin_waves + n_goal;
+      h.width[0] = h.n_c;
+      h.full_cols[0] = p.n_sin_waves + 6 * h.n_v + 2 * p.duplicate_v + p.duplicate_h + p.duplicate_c;
+      for (int l = 1; l < h.n_layers; ++l) {
+        CLS_REQUIRE(d.hidden[l - 1] > 0, "hidden width must be > 0");
+        h.width[l] = d.hidden[l - 1];
+        h.full_cols[l] = d.hidden[l - 1];
+      }
+      h.width[h.n_layers] = h.n_out;
+    }
+    std::vector<int> er(env_robot, env_robot + n_envs);
+    for (int e : er) CLS_REQUIRE(e >= 0 && e < n_robots, "env_robot index out of range");
+    auto* s = new cls_sim;
+    try {
+      if (p.precision == 32) s->impl.reset(new SimImpl<float>(hr, er, p));
+      else s->impl.reset(new SimImpl<double>(hr, er, p));
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+    return CLS_OK;
+  } catch (const Fail& e) {
+    g_create_error = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return CLS_ERR_INVALID;
+  }
+}
+
+int cls_destroy(cls_sim* sim) {
+  if (!sim) return CLS_ERR_INVALID;
+  delete sim;
+  return CLS_OK;
+}
+
+const char* cls_last_error(const cls_sim* sim) {
+  if (!sim || !sim->impl) return cls::g_create_error.c_str();
+  return sim->impl->err.c_str();
+}
+
+int cls_set_stream(cls_sim* sim, void* stream) {
+  return guarded(sim, [&](cls::SimBase& b) { b.stream = (cudaStream_t)stream; });
+}
+
+int cls_get_sizes(const cls_sim* sim, int32_t* n_envs, int32_t* n_vertices_total, int32_t* max_steps) {
+  if (!sim || !sim->impl) return CLS_ERR_INVALID;
+  sim->impl->sizes(n_envs, n_vertices_total, max_steps);
+  return CLS_OK;
+}
+
+int cls_get_layer_shape(const cls_sim* sim, int32_t robot, int32_t layer, int32_t* rows, int32_t* cols) {
+  return guarded(const_cast<cls_sim*>(sim),
+                 [&](cls::SimBase& b) { b.layer_shape(robot, layer, rows, cols); });
+}
+
+int cls_set_state(cls_sim* sim, const double* x0, const double* v0) {
+  return guarded(sim, [&](cls::SimBase& b) { b.set_state(x0, v0); });
+}
+
+int cls_set_targets(cls_sim* sim, const double* tv, const double* th, const double* tc) {
+  return guarded(sim, [&](cls::SimBase& b) { b.set_targets(tv, th, tc); });
+}
+
+int cls_set_weights(cls_sim* sim, int32_t robot, int32_t layer, const double* W, const double* b) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_weights(robot, layer, W, b); });
+}
+
+int cls_get_weights(cls_sim* sim, int32_t robot, int32_t layer, double* W, double* b) {
+  return guarded(sim, [&](cls::SimBase& s) { s.get_weights(robot, layer, W, b); });
+}
+
+int cls_get_grads(cls_sim* sim, int32_t robot, int32_t layer, double* gW, double* gb) {
+  return guarded(sim, [&](cls::SimBase& s) { s.get_grads(robot, layer, gW, gb); });
+}
+
+int cls_forward(cls_sim* sim, int32_t steps) {
+  return guarded(sim, [&](cls::SimBase& s) { s.forward(steps, false, false); });
+}
+
+int cls_forward_eval(cls_sim* sim, int32_t steps) {
+  return guarded(sim, [&](cls::SimBase& s) { s.forward(steps, true, false); });
+}
+
+int cls_loss(cls_sim* sim, double* terms, double* env) {
+  return guarded(sim, [&](cls::SimBase& s) { s.loss(terms, env); });
+}
+
+int cls_backward(cls_sim* sim) {
+  return guarded(sim, [&](cls::SimBase& s) { s.backward(false); });
+}
+
+int cls_simulate(cls_sim* sim, int32_t steps, double* loss) {
+  return guarded(sim, [&](cls::SimBase& s) {
+    s.forward(steps, false, false);
+    double t8[8];
+    s.loss(t8, nullptr);
+    s.backward(false);
+    if (loss) *loss = t8[0];
+  });
+}
+
+int cls_simulate_per_env(cls_sim* sim, int32_t steps, double* loss) {
+  return guarded(sim, [&](cls::SimBase& s) {
+    s.forward(steps, false, true);
+    double t8[8];
+    s.loss(t8, nullptr);
+    s.backward(true);
+    if (loss) *loss = t8[0];
+  });
+}
+
+int cls_adam_step(cls_sim* sim, int32_t iter, double* tns) {
+  return guarded(sim, [&](cls::SimBase& s) { s.adam(iter, tns); });
+}
+
+int cls_clear_adam(cls_sim* sim) {
+  return guarded(sim, [&](cls::SimBase& s) { s.clear_adam(); });
+}
+
+int cls_get_observables(cls_sim* sim, double* center, double* height, double* upper, double* rot) {
+  return guarded(sim, [&](cls::SimBase& s) { s.observables(center, height, upper, rot); });
+}
+
+int cls_get_trajectory(cls_sim* sim, double* x) {
+  return guarded(sim, [&](cls::SimBase& s) { s.trajectory(x); });
+}
+
+int cls_get_final_state(cls_sim* sim, double* x, double* v) {
+  return guarded(sim, [&](cls::SimBase& s) { s.final_state(x, v); });
+}
+
+int cls_get_state_grads(cls_sim* sim, double* gx0, double* gv0) {
+  return guarded(sim, [&](cls::SimBase& s) { s.state_grads(gx0, gv0); });
+}
+
+int cls_synchronize(cls_sim* sim) {
+  if (!sim || !sim->impl) return CLS_ERR_INVALID;
+  int rc = CLS_OK;
+  int g = guarded(sim, [&](cls::SimBase& s) { rc = s.synchronize(); });
+  return g != CLS_OK ? g : rc;
+}
+
+int cls_weights_init(cls_sim* sim, uint64_t seed) {
+  return guarded(sim, [&](cls::SimBase& s) { s.weights_init(seed); });
+}
+
+int cls_initialize_train(cls_sim* sim, int32_t iter, int32_t steps, uint64_t seed, double max_speed) {
+  return guarded(sim, [&](cls::SimBase& s) { s.initialize_train(iter, steps, seed, max_speed); });
+}
+
+int cls_profile_enable(cls_sim* sim, int32_t on) {
+  return guarded(sim, [&](cls::SimBase& s) { s.profile_enable(on != 0); });
+}
+
+int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset) {
+  return guarded(sim, [&](cls::SimBase& s) {
+    long long l[cls::PK_COUNT];
+    s.profile_read(ms, l, reset != 0);
+    if (launches)
+      for (int k = 0; k < cls::PK_COUNT; ++k) launches[k] = l[k];
+  });
+}
+
+int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam) {
+  return guarded(sim, [&](cls::SimBase& s) { s.graph_capture(steps, with_adam != 0); });
+}
+
+int cls_graph_launch(cls_sim* sim, int32_t iter) {
+  return guarded(sim, [&](cls::SimBase& s) { s.graph_launch(iter); });
+}
+
+}  // extern "C"

@@ -1,0 +1,1031 @@
+// ms_segment.cuh -- segment kernels: forward (first pass / recompute), reverse,
+// losses, weight-gradient products, Adam and weight packing.
+#pragma once
+#include "ms_kernels.cuh"
+
+namespace cls {
+
+enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4 };
+
+// sum of M values over the block, deterministic; red must hold 32*M entries
+template <typename R, int M>
+__device__ __forceinline__ void block_sum(R (&v)[M], R* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[m] += __shfl_xor_sync(0xffffffffu, v[m], o);
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) red[m * 32 + wid] = v[m];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    R s = 0;
+    for (int w = 0; w < nw; ++w) s += red[m * 32 + w];
+    v[m] = s;
+  }
+  __syncthreads();
+}
+
+// min (or max) of y with the LAST index attaining it, over the block
+template <typename R>
+__device__ __forceinline__ void block_argext(R& val, int& idx, bool is_min, R* red, int* redi) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  auto better = [&](R v1, int i1, R v2, int i2) {  // is (v2,i2) preferred over (v1,i1)?
+    if (is_min) return (v2 < v1) || (v2 == v1 && i2 > i1);
+    return (v2 > v1) || (v2 == v1 && i2 > i1);
+  };
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    R v2 = __shfl_xor_sync(0xffffffffu, val, o);
+    int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (better(val, idx, v2, i2)) { val = v2; idx = i2; }
+  }
+  __syncthreads();
+  if (lane == 0) { red[wid] = val; redi[wid] = idx; }
+  __syncthreads();
+  R bv = red[0];
+  int bi = redi[0];
+  for (int w = 1; w < nw; ++w)
+    if (better(bv, bi, red[w], redi[w])) { bv = red[w]; bi = redi[w]; }
+  val = bv;
+  idx = bi;
+  __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ void load_descs(const MsArgs<R>& a, int e, RobotDesc& rb, EnvDesc& ed) {
+  // cooperative word copy of the two small descriptors into shared memory
+  const int* se = reinterpret_cast<const int*>(a.envs + e);
+  int* de = reinterpret_cast<int*>(&ed);
+  for (int q = threadIdx.x; q < (int)(sizeof(EnvDesc) / 4); q += blockDim.x) de[q] = se[q];
+  __syncthreads();
+  const int* sr = reinterpret_cast<const int*>(a.robots + ed.robot);
+  int* dr = reinterpret_cast<int*>(&rb);
+  for (int q = threadIdx.x; q < (int)(sizeof(RobotDesc) / 4); q += blockDim.x) dr[q] = sr[q];
+  __syncthreads();
+}
+
+// goal columns of the compact input: (vx, vz) / max_speed if duplicate_v > 0,
+// target height if duplicate_h > 0, crawl target if duplicate_c > 0
+template <typename R>
+__device__ __forceinline__ R goal_value(const MsArgs<R>& a, int g, size_t o) {
+  if (a.dup_v > 0) {
+    if (g == 0) return a.tv[o].x / a.max_speed;
+    if (g == 1) return a.tv[o].z / a.max_speed;
+    g -= 2;
+  }
+  if (a.dup_h > 0) {
+    if (g == 0) return a.th[o];
+    g -= 1;
+  }
+  if (a.dup_c > 0 && g == 0) return a.tc[o];
+  return R(0);
+}
+
+template <typename R>
+__device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
+  if (threadIdx.x == 0) *s_item = atomicAdd(a.queue, 1);
+  __syncthreads();
+  int it = *s_item;
+  __syncthreads();
+  return it;
+}
+
+// ---------------------------------------------------------------- forward
+// Advances every env from t_begin (state in checkpoint slot src_slot) through
+// t_end (exclusive), i.e. runs pre_advance/nn_input/forward/advance for each t.
+template <typename R>
+__global__ void __launch_bounds__(1024, 1)
+ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
+  extern __shared__ __align__(256) char smem_raw[];
+  __shared__ RobotDesc rb;
+  __shared__ EnvDesc ed;
+  __shared__ int s_item;
+  FwdSmem<R> s = carve_fwd<R>(smem_raw, a);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (;;) {
+    const int item = next_item(a, &s_item);
+    if (item >= a.n_items) break;
+    const int e = a.order[item];
+    load_descs(a, e, rb, ed);
+    const int N = rb.n_v, L = rb.n_layers;
+    const R invN = R(1) / R(N);
+    {
+      const V4<R>* cx = a.ckpt_x + (size_t)src_slot * a.v_total + ed.v_off;
+      const V4<R>* cv = a.ckpt_v + (size_t)src_slot * a.v_total + ed.v_off;
+      for (int i = tid; i < N; i += nt) { s.xs[i] = cx[i]; s.vs[i] = cv[i]; }
+    }
+    R hprev = 0;
+    if ((mode & FWD_OBS) && t_begin > 0) hprev = a.obs_height[(size_t)(t_begin - 1) * a.n_envs + e];
+    __syncthreads();
+    for (int t = t_begin; t < t_end; ++t) {
+      // -- checkpoints, records, trajectory
+      if ((mode & FWD_CKPT) && t > t_begin && (t % a.K) == 0) {
+        V4<R>* cx = a.ckpt_x + (size_t)(t / a.K) * a.v_total + ed.v_off;
+        V4<R>* cv = a.ckpt_v + (size_t)(t / a.K) * a.v_total + ed.v_off;
+        bool bad = false;
+        for (int i = tid; i < N; i += nt) {
+          cx[i] = s.xs[i]; cv[i] = s.vs[i];
+          bad |= !(finite(s.xs[i].x) && finite(s.xs[i].y) && finite(s.xs[i].z));
+        }
+        if (bad) atomicOr(a.status, ERR_NONFINITE);
+      }
+      if (mode & FWD_RECORD) {
+        V4<R>* rx = a.rec_x + (size_t)(t - t_begin) * a.v_total + ed.v_off;
+        V4<R>* rv = a.rec_v + (size_t)(t - t_begin) * a.v_total + ed.v_off;
+        for (int i = tid; i < N; i += nt) { rx[i] = s.xs[i]; rv[i] = s.vs[i]; }
+      }
+      if ((mode & FWD_OBS) && a.x_full) {
+        V4<R>* xf = a.x_full + (size_t)t * a.v_total + ed.v_off;
+        for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
+      }
+      // -- compute_center (solver_mass_spring.py:150-156): sum of x / n
+      R c[3] = {0, 0, 0};
+      for (int i = tid; i < N; i += nt) {
+        c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
+      }
+      block_sum<R, 3>(c, s.red);
+      if (mode & FWD_OBS) {
+        // compute_height / upper height (solver_mass_spring.py:158-173)
+        R lo = R(10), hi = R(-10);
+        for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
+        int li = 0, hiidx = 0;
+        block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+        block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+        // compute_rotation (solver_mass_spring.py:175-192)
+        R rot;
+        if (rb.robot_id == 100) {
+          R d0 = 0, d2 = 0;
+          if (tid == 0) {
+            const V4<R> p = s.xs[rb.rot_idx[0]], q = s.xs[rb.rot_idx[1]];
+            const V4<R> u = s.xs[rb.rot_idx[2]], w = s.xs[rb.rot_idx[3]];
+            d0 = p.x + q.x - u.x - w.x;
+            d2 = p.z + q.z - u.z - w.z;
+          }
+          rot = datan2<R>(d2, d0);
+        } else {
+          unsigned char* hd = a.head + ed.v_off;
+          if (t == 0) {
+            for (int i = tid; i < N; i += nt) hd[i] = (s.xs[i].x < c[0]) ? 1 : 0;
+            __syncthreads();
+          }
+          R hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          for (int i = tid; i < N; i += nt) {
+            const V4<R> p = s.xs[i];
+            if (hd[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
+            else { hs[4] += p.x; hs[5] += p.y; hs[6] += p.z; hs[7] += R(1); }
+          }
+          block_sum<R, 8>(hs, s.red);
+          const R d0 = -hs[0] * hs[7] + hs[4] * hs[3];
+          const R d2 = -hs[2] * hs[7] + hs[6] * hs[3];
+          rot = datan2<R>(d2, d0);
+        }
+        if (tid == 0) {
+          const size_t o = (size_t)t * a.n_envs + e;
+          V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
+          a.obs_center[o] = cc;
+          const R h = (t % a.jump_period == 0) ? lo : fmax(hprev, lo);
+          a.obs_height[o] = h;
+          a.obs_upper[o] = hi;
+          a.obs_rot[o] = rot;
+          s.red[0] = h;
+        }
+        __syncthreads();
+        hprev = s.red[0];
+        __syncthreads();
+      }
+      // -- nn_input (taichi_env.py:149-183) in the compact column order
+      {
+        const int p0 = rb.pos_pad, nc = rb.n_c, pitch0 = rb.pitch[0];
+        for (int q = tid; q < pitch0; q += nt) {
+          R val = 0;
+          if (q < 3 * N) {
+            const int i = q / 3, d = q - 3 * (q / 3);
+            val = (comp(s.xs[i], d) - c[d]) / R(0.2);
+          } else if (q >= p0 && q < p0 + a.n_sin) {
+            val = a.sin_table[(size_t)t * a.n_sin + (q - p0)];
+          } else if (q >= p0 + a.n_sin && q < nc) {
+            val = goal_value<R>(a, q - p0 - a.n_sin, (size_t)t * a.n_envs + e);
+          }
+          s.ain[q] = val;
+          if ((mode & FWD_RECORD) && q < nc)
+            a.rec_in[(size_t)(t - t_begin) * a.in_total + ed.in_off + q] = val;
+        }
+      }
+      __syncthreads();
+      // -- MLP (nn.py:130-146): z = W a, a' = act(z + b)
+      R* out = nullptr;
+      for (int l = 0; l < L; ++l) {
+        const R* in = (l == 0) ? s.ain : ((l & 1) ? s.buf0 : s.buf1);
+        R* y = (l & 1) ? s.buf1 : s.buf0;
+        const int nout = rb.width[l + 1];
+        R* zrec = (mode & FWD_RECORD)
+                      ? a.rec_z + a.z_base[l] + (size_t)(t - t_begin) * a.z_total[l] + ed.z_off[l]
+                      : nullptr;
+        dense_forward<R>(a.w + rb.w_off[l], rb.pitch[l], nout, a.bias + rb.b_off[l], in, y, zrec,
+                         l == L - 1 ? a.act_out : a.act_hidden);
+        // zero the padding up to the next layer's pitch
+        const int padto = (l + 1 < L) ? rb.pitch[l + 1] : ((nout + 3) & ~3);
+        for (int q = nout + tid; q < padto; q += nt) y[q] = 0;
+        __syncthreads();
+        out = y;
+      }
+      if ((mode & FWD_OBS) && a.act_full) {
+        R* af = a.act_full + (size_t)t * a.z_total[L - 1] + ed.z_off[L - 1];
+        for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
+      }
+      // -- apply_spring_force (gather form) then advance_toi
+      for (int i = tid; i < N; i += nt) s.vinc[i] = gather_vinc<R>(a, rb, i, s.xs, s.vs, out);
+      __syncthreads();
+      for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
+      __syncthreads();
+    }
+    // state after the last processed step
+    if (mode & FWD_OBS) {
+      for (int i = tid; i < N; i += nt) {
+        a.fin_x[ed.v_off + i] = s.xs[i];
+        a.fin_v[ed.v_off + i] = s.vs[i];
+      }
+      if (a.x_full && t_end < a.T) {
+        V4<R>* xf = a.x_full + (size_t)t_end * a.v_total + ed.v_off;
+        for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------------- loss seeds
+template <typename R>
+__device__ __forceinline__ V4<R> obs_c(const MsArgs<R>& a, int t, int e) {
+  return a.obs_center[(size_t)t * a.n_envs + e];
+}
+
+// d loss / d center[t] from the velocity loss (taichi_env.py:185-211)
+template <typename R>
+__device__ __forceinline__ void seed_center_velocity(const MsArgs<R>& a, int t, int e, R Br, R g[3]) {
+  const int rp = a.run_period, tp = a.turn_period, st = a.steps;
+  const R sc = R(2) * R(100) / R(st) / Br;
+  if (t >= rp && t % tp > rp && t <= st && t < a.T) {
+    const V4<R> c1 = obs_c(a, t, e), c0 = obs_c(a, t - rp, e);
+    const V4<R> tv = a.tv[(size_t)(t - rp) * a.n_envs + e];
+    g[0] += (c1.x - c0.x - tv.x) * sc;
+    g[2] += (c1.z - c0.z - tv.z) * sc;
+  }
+  const int u = t + rp;
+  if (u <= st && u < a.T && u % tp > rp) {
+    const V4<R> c1 = obs_c(a, u, e), c0 = obs_c(a, t, e);
+    const V4<R> tv = a.tv[(size_t)t * a.n_envs + e];
+    g[0] -= (c1.x - c0.x - tv.x) * sc;
+    g[2] -= (c1.z - c0.z - tv.z) * sc;
+  }
+}
+
+// d loss / d x[t, i] and d loss / d center[t] from the rotation loss
+// (taichi_env.py:235-252) and pose loss (:224-233).  Adds to gxi and gc.
+template <typename R>
+__device__ __forceinline__ void seed_x_rotation_pose(const MsArgs<R>& a, const RobotDesc& rb,
+                                                     const EnvDesc& ed, int t, int e, int i,
+                                                     const V4<R>& xi, R Br, R gxi[3], R gc[3]) {
+  const int rp = a.run_period, tp = a.turn_period, st = a.steps;
+  if (a.loss_mask & LOSS_ROTATION) {
+    const R k = R(2) / R(40) / R(st);
+    if (t >= 1 && t % tp > rp && t <= st && t < a.T) {
+      const V4<R> c1 = obs_c(a, t, e), c0 = obs_c(a, t - rp, e);
+      const V4<R> x0 = a.x_full[(size_t)(t - rp) * a.v_total + ed.v_off + i];
+      const R ang = a.th[(size_t)(t - rp) * a.n_envs + e] * R(72.) / R(180.) * R(3.1415926535);
+      const R ca = dcos<R>(ang), sn = dsin<R>(ang);
+      const R t0x = xi.x - c1.x, t0y = xi.y - c1.y, t0z = xi.z - c1.z;
+      const R t1x = x0.x - c0.x, t1y = x0.y - c0.y, t1z = x0.z - c0.z;
+      const R gx = (t0x - (ca * t1x - sn * t1z)) * k;
+      const R gy = (t0y - t1y) * k;
+      const R gz = (t0z - (sn * t1x + ca * t1z)) * k;
+      gxi[0] += gx; gxi[1] += gy; gxi[2] += gz;
+      gc[0] -= gx; gc[1] -= gy; gc[2] -= gz;
+    }
+    const int u = t + rp;
+    if (u <= st && u < a.T && u % tp > rp) {
+      const V4<R> c1 = obs_c(a, u, e), c0 = obs_c(a, t, e);
+      const V4<R> x1 = a.x_full[(size_t)u * a.v_total + ed.v_off + i];
+      const R ang = a.th[(size_t)t * a.n_envs + e] * R(72.) / R(180.) * R(3.1415926535);
+      const R ca = dcos<R>(ang), sn = dsin<R>(ang);
+      const R t0x = x1.x - c1.x, t0y = x1.y - c1.y, t0z = x1.z - c1.z;
+      const R t1x = xi.x - c0.x, t1y = xi.y - c0.y, t1z = xi.z - c0.z;
+      const R g2x = -(t0x - (ca * t1x - sn * t1z)) * k;
+      const R g2y = -(t0y - t1y) * k;
+      const R g2z = -(t0z - (sn * t1x + ca * t1z)) * k;
+      const R g1x = ca * g2x + sn * g2z, g1y = g2y, g1z = -sn * g2x + ca * g2z;
+      gxi[0] += g1x; gxi[1] += g1y; gxi[2] += g1z;
+      gc[0] -= g1x; gc[1] -= g1y; gc[2] -= g1z;
+    }
+  }
+  if (a.loss_mask & LOSS_POSE) {
+    const int jp = a.jump_period;
+    if (t >= 1 && t % jp == 0 && t <= st && t < a.T) {
+      const V4<R> p = a.init_obj[ed.v_off + i];
+      const R k = R(2) / R(st / jp) / Br;
+      gxi[0] += (xi.x - p.x) * k; gxi[1] += (xi.y - p.y) * k; gxi[2] += (xi.z - p.z) * k;
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ R seed_height(const MsArgs<R>& a, int t, int e, R Br) {
+  if (!(a.loss_mask & LOSS_HEIGHT)) return 0;
+  const int jp = a.jump_period, st = a.steps;
+  const size_t o = (size_t)t * a.n_envs + e;
+  if (t >= 1 && t <= st && t < a.T && t % jp == jp - 1 && a.th[o] > R(0.1 + 1e-6))
+    return R(2) * (a.obs_height[o] - a.th[o]) * R(100) / R(st / jp) / Br;
+  return 0;
+}
+
+template <typename R>
+__device__ __forceinline__ R seed_upper(const MsArgs<R>& a, int t, int e, R Br) {
+  if (!(a.loss_mask & LOSS_CRAWL)) return 0;
+  const int st = a.steps;
+  const size_t o = (size_t)t * a.n_envs + e;
+  if (t >= 1 && t <= st && t < a.T && a.tc[o] > R(1 - 1e-4)) {
+    const R d = a.obs_upper[o] - R(0.1);
+    if (R(0) < d) return R(2) * d * R(5) / R(st) / Br;
+  }
+  return 0;
+}
+
+// -------------------------------------------------------------- spring adjoint
+// Accumulates, for vertex i, the adjoint of every incident spring's impulse:
+// d x_i, d v_i; for a-side entries also d actuation (-> gout).
+template <typename R>
+__device__ __forceinline__ void spring_adjoint_vertex(const MsArgs<R>& a, const RobotDesc& rb, int i,
+                                                      const V4<R>* xs, const V4<R>* vs,
+                                                      const V4<R>* gvinc, const R* outv, R* gout,
+                                                      R act_seed_scale, R act_lim, bool act_seed,
+                                                      R gxi[3], R gvi[3]) {
+  const int beg = a.inc_ptr[rb.ptr_off + i], end = a.inc_ptr[rb.ptr_off + i + 1];
+  for (int q = beg; q < end; ++q) {
+    const int4 ii = a.inc_i[rb.inc_off + q];
+    const V4<R> ff = a.inc_f[rb.inc_off + q];
+    const int o = ii.x;
+    const bool side_a = (ii.y == 0);
+    const V4<R> xa = side_a ? xs[i] : xs[o], xb = side_a ? xs[o] : xs[i];
+    const V4<R> va = side_a ? vs[i] : vs[o], vb = side_a ? vs[o] : vs[i];
+    const V4<R> ga = side_a ? gvinc[i] : gvinc[o], gb = side_a ? gvinc[o] : gvinc[i];
+    const R act = ii.w >= 0 ? outv[ii.w] : R(0);
+    // forward recompute
+    const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
+    const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
+    const R r8 = dsqrt<R>(n2 + R(1e-8));
+    const R length = r8 + R(1e-4);
+    const R target = ff.x * (R(1) + ff.z * act);
+    const R sc = a.dt * (length - target) * ff.y / length;
+    const R r = dsqrt<R>(n2), invlen = R(1) / r;
+    const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
+    const R dv0 = va.x - vb.x, dv1 = va.y - vb.y, dv2 = va.z - vb.z;
+    const R vrel = dv0 * n0 + dv1 * n1 + dv2 * nz;
+    // g_imp = g v_inc[b] - g v_inc[a]
+    const R gi0 = gb.x - ga.x, gi1 = gb.y - ga.y, gi2 = gb.z - ga.z;
+    const R gsc = gi0 * d0 + gi1 * d1 + gi2 * d2;
+    const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
+    const R cdv = a.dashpot * vrel;
+    R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
+    R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
+    const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
+    const R gr = -ginv / (r * r);
+    gd0 += gr * d0 / r; gd1 += gr * d1 / r; gd2 += gr * d2 / r;
+    const R glen = gsc * a.dt * ff.y * target / (length * length);
+    gd0 += glen * d0 / r8; gd1 += glen * d1 / r8; gd2 += glen * d2 / r8;
+    const R sgn = side_a ? R(1) : R(-1);
+    gxi[0] += sgn * gd0; gxi[1] += sgn * gd1; gxi[2] += sgn * gd2;
+    gvi[0] += sgn * gvrel * n0; gvi[1] += sgn * gvrel * n1; gvi[2] += sgn * gvrel * nz;
+    if (side_a && ii.w >= 0) {
+      const R gtarget = -gsc * a.dt * ff.y / length;
+      R gact = gtarget * ff.x * ff.z;
+      if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
+        if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
+      }
+      atomicAdd(gout + ii.w, gact);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- reverse
+template <typename R>
+__global__ void __launch_bounds__(1024, 1)
+ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
+  extern __shared__ __align__(256) char smem_raw[];
+  __shared__ RobotDesc rb;
+  __shared__ EnvDesc ed;
+  __shared__ int s_item;
+  RevSmem<R> s = carve_rev<R>(smem_raw, a);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int* redi = reinterpret_cast<int*>(s.red + kRedInt);
+  for (;;) {
+    const int item = next_item(a, &s_item);
+    if (item >= a.n_items) break;
+    const int e = a.order[item];
+    load_descs(a, e, rb, ed);
+    const int N = rb.n_v, L = rb.n_layers;
+    const R Br = R(rb.n_env);
+    const R invN = R(1) / R(N);
+    R hcarry = 0;
+    if (last_seg) {
+      // x[steps-1] is written by the last advance but never passed through
+      // pre_advance, so only the direct loss terms at t = steps-1 reach it
+      const int tl = t_end;
+      for (int i = tid; i < N; i += nt) {
+        R gxi[3] = {0, 0, 0}, gcd[3] = {0, 0, 0};
+        if (a.x_full) {
+          const V4<R> xi = a.x_full[(size_t)tl * a.v_total + ed.v_off + i];
+          seed_x_rotation_pose<R>(a, rb, ed, tl, e, i, xi, Br, gxi, gcd);
+        }
+        V4<R> g; g.x = gxi[0]; g.y = gxi[1]; g.z = gxi[2]; g.w = 0;
+        V4<R> z; z.x = z.y = z.z = z.w = 0;
+        s.gx[i] = g;
+        s.gv[i] = z;
+      }
+    } else {
+      for (int i = tid; i < N; i += nt) { s.gx[i] = a.adj_x[ed.v_off + i]; s.gv[i] = a.adj_v[ed.v_off + i]; }
+      hcarry = a.adj_h[e];
+    }
+    __syncthreads();
+    const R* wout = a.w + rb.w_off[L - 1];
+    const R* bout = a.bias + rb.b_off[L - 1];
+    const int nout = rb.n_out;
+    for (int t = t_end - 1; t >= t_begin; --t) {
+      const int kk = t - t_begin;
+      {
+        const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
+        const V4<R>* rv = a.rec_v + (size_t)kk * a.v_total + ed.v_off;
+        for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; }
+        const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
+        for (int o = tid; o < nout; o += nt) {
+          s.bufA[o] = act_f<R>(a.act_out, zl[o] + bout[o]);
+          s.bufB[o] = 0;
+        }
+      }
+      __syncthreads();
+      // v_inc[t] recompute (into gvinc as scratch)
+      for (int i = tid; i < N; i += nt) s.gvinc[i] = gather_vinc<R>(a, rb, i, s.xs, s.vs, s.bufA);
+      __syncthreads();
+      // adjoint of advance_toi(t + 1)
+      for (int i = tid; i < N; i += nt) {
+        const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
+        const V4<R> gx1 = s.gx[i], gv1 = s.gv[i];
+        R ov0 = a.drag_s * v.x + vi.x;
+        R ov1 = a.drag_s * v.y + a.dt * a.gravity + vi.y;
+        R ov2 = a.drag_s * v.z + vi.z;
+        R nv0 = ov0, nv1 = ov1, nv2 = ov2, toi = 0, f = 0;
+        const R nx1 = x.y + a.dt * ov1;
+        const bool hit = (nx1 < a.ground && ov1 < R(-1e-4));
+        if (hit) {
+          toi = -(x.y - a.ground) / ov1;
+          f = a.friction * (-ov1);
+          nv1 = 0;
+          nv0 = (ov0 < 0) ? fmin(R(0), ov0 + f) : fmax(R(0), ov0 - f);
+          nv2 = (ov2 < 0) ? fmin(R(0), ov2 + f) : fmax(R(0), ov2 - f);
+        }
+        R gox0 = gx1.x, gox1 = gx1.y, gox2 = gx1.z;
+        R gov0 = toi * gx1.x, gov1 = toi * gx1.y, gov2 = toi * gx1.z;
+        const R dtt = a.dt - toi;
+        const R gnv0 = dtt * gx1.x + gv1.x, gnv1 = dtt * gx1.y + gv1.y, gnv2 = dtt * gx1.z + gv1.z;
+        const R gtoi = gx1.x * ov0 - gx1.x * nv0 + gx1.y * ov1 - gx1.y * nv1 + gx1.z * ov2 - gx1.z * nv2;
+        if (hit) {
+          R gf = 0;
+          if (ov0 < 0) { if (!(R(0) < ov0 + f)) { gov0 += gnv0; gf += gnv0; } }
+          else { if (!(ov0 - f < R(0))) { gov0 += gnv0; gf -= gnv0; } }
+          if (ov2 < 0) { if (!(R(0) < ov2 + f)) { gov2 += gnv2; gf += gnv2; } }
+          else { if (!(ov2 - f < R(0))) { gov2 += gnv2; gf -= gnv2; } }
+          gov1 += -a.friction * gf;
+          gox1 += -gtoi / ov1;
+          gov1 += gtoi * (x.y - a.ground) / (ov1 * ov1);
+        } else {
+          gov0 += gnv0; gov1 += gnv1; gov2 += gnv2;
+        }
+        V4<R> gx0; gx0.x = gox0; gx0.y = gox1; gx0.z = gox2; gx0.w = 0;
+        V4<R> gv0; gv0.x = a.drag_s * gov0; gv0.y = a.drag_s * gov1; gv0.z = a.drag_s * gov2; gv0.w = 0;
+        V4<R> gvi; gvi.x = gov0; gvi.y = gov1; gvi.z = gov2; gvi.w = 0;
+        s.gx[i] = gx0;
+        s.gv[i] = gv0;
+        s.gvinc[i] = gvi;
+      }
+      __syncthreads();
+      // adjoint of apply_spring_force(t)
+      {
+        const size_t o = (size_t)t * a.n_envs + e;
+        const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < a.steps && a.th[o] < R(0.1 + 1e-4);
+        const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
+        const R act_scale = R(10) / R(a.steps) / Br / R(rb.n_s);
+        for (int i = tid; i < N; i += nt) {
+          R gxi[3] = {0, 0, 0}, gvi[3] = {0, 0, 0};
+          spring_adjoint_vertex<R>(a, rb, i, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, act_scale, lim,
+                                   act_seed, gxi, gvi);
+          V4<R> g = s.gx[i];
+          g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
+          s.gx[i] = g;
+          V4<R> h = s.gv[i];
+          h.x += gvi[0]; h.y += gvi[1]; h.z += gvi[2];
+          s.gv[i] = h;
+        }
+      }
+      __syncthreads();
+      // adjoint of the MLP: output layer first
+      {
+        const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
+        R* dzr = a.rec_dz + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
+        for (int q = tid; q < nout; q += nt) {
+          const R dz = s.bufB[q] * act_d<R>(a.act_out, zl[q] + bout[q]);
+          s.dz[q] = dz;
+          dzr[q] = dz;
+        }
+      }
+      __syncthreads();
+      for (int l = L - 1; l >= 1; --l) {
+        const int nin = rb.width[l];
+        dense_transposed<R>(a.w + rb.w_off[l], rb.pitch[l], rb.width[l + 1], nin, s.dz, s.part,
+                            reinterpret_cast<V4<R>*>(s.bufA));
+        const R* zp = a.rec_z + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + ed.z_off[l - 1];
+        R* dzr = a.rec_dz + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + ed.z_off[l - 1];
+        const R* bp = a.bias + rb.b_off[l - 1];
+        for (int q = tid; q < nin; q += nt) {
+          const R dz = s.bufA[q] * act_d<R>(a.act_hidden, zp[q] + bp[q]);
+          s.dz[q] = dz;
+          dzr[q] = dz;
+        }
+        __syncthreads();
+      }
+      // first layer: only the position columns carry state dependence
+      dense_transposed<R>(a.w + rb.w_off[0], rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
+                          reinterpret_cast<V4<R>*>(s.bufA));
+      // adjoint of nn_input + compute_center + loss seeds at t
+      {
+        R gc[3] = {0, 0, 0};
+        for (int i = tid; i < N; i += nt) {
+          const R g0 = s.bufA[3 * i] / R(0.2), g1 = s.bufA[3 * i + 1] / R(0.2), g2 = s.bufA[3 * i + 2] / R(0.2);
+          R gxi[3] = {g0, g1, g2};
+          gc[0] -= g0; gc[1] -= g1; gc[2] -= g2;
+          if (a.x_full) seed_x_rotation_pose<R>(a, rb, ed, t, e, i, s.xs[i], Br, gxi, gc);
+          V4<R> g = s.gx[i];
+          g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
+          s.gx[i] = g;
+        }
+        block_sum<R, 3>(gc, s.red);
+        if (a.loss_mask & LOSS_VELOCITY) seed_center_velocity<R>(a, t, e, Br, gc);
+        for (int i = tid; i < N; i += nt) {
+          V4<R> g = s.gx[i];
+          g.x += gc[0] * invN; g.y += gc[1] * invN; g.z += gc[2] * invN;
+          s.gx[i] = g;
+        }
+      }
+      // adjoint of compute_height (running max of the lowest point) and upper height
+      if (a.loss_mask & (LOSS_HEIGHT | LOSS_CRAWL)) {
+        const R gh = seed_height<R>(a, t, e, Br) + hcarry;
+        const R gu = seed_upper<R>(a, t, e, Br);
+        hcarry = 0;
+        if (gh != R(0)) {
+          R lo = R(10); int li = -1;
+          for (int i = tid; i < N; i += nt) {
+            const R y = s.xs[i].y;
+            if (!(lo < y)) { lo = y; li = i; }
+          }
+          block_argext<R>(lo, li, true, s.red, redi);
+          R gmin = gh;
+          if (t % a.jump_period != 0) {
+            const R prev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
+            if (lo < prev) { hcarry = gh; gmin = 0; }
+          }
+          if (tid == 0 && li >= 0 && gmin != R(0)) s.gx[li].y += gmin;
+        }
+        if (gu != R(0)) {
+          R hi = R(-10); int hix = -1;
+          for (int i = tid; i < N; i += nt) {
+            const R y = s.xs[i].y;
+            if (!(y < hi)) { hi = y; hix = i; }
+          }
+          block_argext<R>(hi, hix, false, s.red, redi);
+          if (tid == 0 && hix >= 0) s.gx[hix].y += gu;
+        }
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < N; i += nt) {
+      a.adj_x[ed.v_off + i] = s.gx[i];
+      a.adj_v[ed.v_off + i] = s.gv[i];
+    }
+    if (tid == 0) a.adj_h[e] = hcarry;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ losses
+// Per-env loss terms (taichi_env.py:185-293) from the stored observables.
+// out[e * 8 + slot]: raw sums (reference's loss_x, not multiplied by B);
+// slot 7 holds the env's max height seen by the height loss.
+template <typename R>
+__global__ void ms_loss_kernel(MsArgs<R> a, double* out) {
+  const int e = blockIdx.x;
+  if (e >= a.n_envs) return;
+  __shared__ double red[32 * 8];
+  const EnvDesc ed = a.envs[e];
+  const RobotDesc& rb = a.robots[ed.robot];
+  const int N = rb.n_v, st = a.steps, rp = a.run_period, tp = a.turn_period, jp = a.jump_period;
+  const double Br = rb.n_env;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  acc[7] = 0.0;
+  const int tmax = (st < a.T - 1) ? st : a.T - 1;
+  for (int t = threadIdx.x; t <= tmax; t += blockDim.x) {
+    const size_t o = (size_t)t * a.n_envs + e;
+    if ((a.loss_mask & LOSS_VELOCITY) && t >= rp && t % tp > rp) {
+      const V4<R> c1 = a.obs_center[o], c0 = a.obs_center[o - (size_t)rp * a.n_envs];
+      const V4<R> tv = a.tv[o - (size_t)rp * a.n_envs];
+      const double ex = (double)c1.x - (double)c0.x - (double)tv.x;
+      const double ez = (double)c1.z - (double)c0.z - (double)tv.z;
+      acc[LS_VEL] += ex * ex / Br / st * 100 + ez * ez / Br / st * 100;
+    }
+    if ((a.loss_mask & LOSS_HEIGHT) && t >= 1 && t % jp == jp - 1 && (double)a.th[o] > 0.1 + 1e-6) {
+      const double d = (double)a.obs_height[o] - (double)a.th[o];
+      acc[LS_HEIGHT] += d * d / Br / (st / jp) * 100;
+      acc[7] = fmax(acc[7], (double)a.obs_height[o]);
+    }
+    if ((a.loss_mask & LOSS_CRAWL) && t >= 1 && (double)a.tc[o] > 1 - 1e-4) {
+      const double d = fmax((double)a.obs_upper[o] - 0.1, 0.0);
+      acc[LS_CRAWL] += d * d / Br / st * 5.;
+    }
+    if ((a.loss_mask & LOSS_ACTUATION) && t < st && a.act_full && (double)a.th[o] < 0.1 + 1e-4) {
+      const double lim = sqrt(fabs((double)a.tv[o].x) / 0.08);
+      const R* af = a.act_full + (size_t)t * a.z_total[rb.n_layers - 1] + ed.z_off[rb.n_layers - 1];
+      for (int s2 = 0; s2 < rb.n_s; ++s2) {
+        const int q = a.spring_out[rb.spr_off + s2];
+        const double act = q >= 0 ? (double)af[q] : 0.0;
+        acc[LS_ACT] += fmax(fabs(act) - lim, 0.0) / rb.n_s / Br / st * 10;
+      }
+    }
+    if ((a.loss_mask & LOSS_ROTATION) && a.x_full && t >= 1 && t % tp > rp) {
+      const V4<R> c1 = a.obs_center[o], c0 = a.obs_center[o - (size_t)rp * a.n_envs];
+      const double ang = (double)a.th[o - (size_t)rp * a.n_envs] * 72. / 180. * 3.1415926535;
+      const double ca = cos(ang), sn = sin(ang);
+      for (int i = 0; i < N; ++i) {
+        const V4<R> x1 = a.x_full[(size_t)t * a.v_total + ed.v_off + i];
+        const V4<R> x0 = a.x_full[(size_t)(t - rp) * a.v_total + ed.v_off + i];
+        const double t0x = (double)x1.x - c1.x, t0y = (double)x1.y - c1.y, t0z = (double)x1.z - c1.z;
+        const double t1x = (double)x0.x - c0.x, t1y = (double)x0.y - c0.y, t1z = (double)x0.z - c0.z;
+        const double ex = t0x - (ca * t1x - sn * t1z), ey = t0y - t1y, ez = t0z - (sn * t1x + ca * t1z);
+        acc[LS_ROT] += (ex * ex + ey * ey + ez * ez) / st / 40;
+      }
+    }
+    if ((a.loss_mask & LOSS_POSE) && a.x_full && t >= 1 && t % jp == 0) {
+      for (int i = 0; i < N; ++i) {
+        const V4<R> x1 = a.x_full[(size_t)t * a.v_total + ed.v_off + i];
+        const V4<R> p = a.init_obj[ed.v_off + i];
+        const double dx = (double)x1.x - p.x, dy = (double)x1.y - p.y, dz = (double)x1.z - p.z;
+        acc[LS_POSE] += (dx * dx + dy * dy + dz * dz) / Br / (st / jp);
+      }
+    }
+  }
+  // deterministic block reduction (max for slot 7)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int m = 0; m < 8; ++m) {
+    double v = acc[m];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double w = __shfl_xor_sync(0xffffffffu, v, off);
+      v = (m == 7) ? fmax(v, w) : v + w;
+    }
+    if (lane == 0) red[m * 32 + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int m = threadIdx.x;
+    double v = red[m * 32];
+    for (int w = 1; w < nw; ++w) v = (m == 7) ? fmax(v, red[m * 32 + w]) : v + red[m * 32 + w];
+    out[(size_t)e * 8 + m] = v;
+  }
+}
+
+// --------------------------------------------------- weight-gradient products
+// dW_l[i, j] += sum over rows rho = (substep k of the segment, env of the type)
+//   dz_l[rho, i] * a_l[rho, j]
+// with a_0 the compact input record and a_l = act(z_{l-1} + b_{l-1}).  One CTA
+// computes a 64 x 64 tile; 256 threads, 4 x 4 outputs each.
+struct GemmTile {
+  int robot, layer, i0, j0;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
+  constexpr int TM = 64, TN = 64, TK = 16;
+  __shared__ R sA[TK][TM];
+  __shared__ R sB[TK][TN];
+  const GemmTile tl = tiles[blockIdx.x];
+  const RobotDesc& rb = a.robots[tl.robot];
+  const int l = tl.layer;
+  const int M = rb.width[l + 1], Ncol = rb.width[l], pitch = rb.pitch[l];
+  const int nb = rb.n_env;
+  const EnvDesc& e0 = a.envs[rb.env_first];
+  const int rows = kseg * nb;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  R acc[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = 0;
+  R bacc[4] = {0, 0, 0, 0};
+  const R* biasp = (l > 0) ? a.bias + rb.b_off[l - 1] : nullptr;
+  for (int r0 = 0; r0 < rows; r0 += TK) {
+    for (int q = threadIdx.x; q < TK * TM; q += 256) {
+      const int rr = q / TM, ii = q % TM;
+      const int rho = r0 + rr, i = tl.i0 + ii;
+      R va = 0, vb = 0;
+      if (rho < rows) {
+        const int k = rho / nb, b = rho - k * nb;
+        if (i < M)
+          va = a.rec_dz[a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * M + i];
+        const int j = tl.j0 + ii;
+        if (j < Ncol) {
+          if (l == 0) {
+            vb = a.rec_in[(size_t)k * a.in_total + e0.in_off + (size_t)b * rb.n_c + j];
+          } else {
+            const R z = a.rec_z[a.z_base[l - 1] + (size_t)k * a.z_total[l - 1] + e0.z_off[l - 1] +
+                                (size_t)b * Ncol + j];
+            vb = act_f<R>(a.act_hidden, z + biasp[j]);
+          }
+        }
+      }
+      sA[rr][ii] = va;
+      sB[rr][ii] = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      R av[4], bv[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) av[p] = sA[kk][ty * 4 + p];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bv[q] = sB[kk][tx * 4 + q];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] += av[p] * bv[q];
+        if (tl.j0 == 0 && tx == 0) bacc[p] += av[p];
+      }
+    }
+    __syncthreads();
+  }
+  R* W = gw + rb.w_off[l];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int i = tl.i0 + ty * 4 + p;
+    if (i >= M) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = tl.j0 + tx * 4 + q;
+      if (j < Ncol) W[(size_t)i * pitch + j] += acc[p][q];
+    }
+    if (tl.j0 == 0 && tx == 0) gb[rb.b_off[l] + i] += bacc[p];
+  }
+}
+
+// ------------------------------------------------- full <-> compact weights
+// Column map of the first layer: the reference input
+//   [n_sin sinusoids | per vertex (pos xyz, vel xyz = 0) | dup_v x (vx, vz) | dup_h x h | dup_c x c]
+// (taichi_env.py:149-183) is stored compactly as
+//   [pos (3N) | pad to 4 | n_sin sinusoids | vx, vz | h | c]
+// velocity slots are always zero and duplicated goal columns always see equal
+// inputs, so W_c[:, col] = sum of the reference columns that map to col.
+__device__ __forceinline__ int full_to_compact(int j, int N, int pos_pad, int n_sin, int dup_v,
+                                               int dup_h, int dup_c) {
+  if (j < n_sin) return pos_pad + j;
+  int q = j - n_sin;
+  if (q < 6 * N) {
+    const int v = q / 6, r = q - 6 * v;
+    return r < 3 ? 3 * v + r : -1;
+  }
+  q -= 6 * N;
+  int g = pos_pad + n_sin;
+  if (q < 2 * dup_v) return g + (q & 1);
+  q -= 2 * dup_v;
+  if (dup_v > 0) g += 2;
+  if (q < dup_h) return g;
+  q -= dup_h;
+  if (dup_h > 0) g += 1;
+  if (q < dup_c) return g;
+  return -1;
+}
+
+// Pack reference-layout master weights (float64 or R) into the compact layout.
+template <typename R>
+__global__ void ms_pack_weights_kernel(const R* __restrict__ master, long long m_off, int rows,
+                                       int n_in_full, R* __restrict__ wc, long long c_off, int pitch,
+                                       int layer, int N, int pos_pad, int n_sin, int dup_v, int dup_h,
+                                       int dup_c) {
+  const long long total = (long long)rows * pitch;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / pitch), c = (int)(q % pitch);
+    const R* row = master + m_off + (long long)i * n_in_full;
+    R s = 0;
+    if (layer > 0) {
+      s = c < n_in_full ? row[c] : R(0);
+    } else if (c < 3 * N) {
+      const int v = c / 3, d = c - 3 * v;
+      s = row[n_sin + 6 * v + d];
+    } else if (c >= pos_pad && c < pos_pad + n_sin) {
+      s = row[c - pos_pad];
+    } else if (c >= pos_pad + n_sin) {
+      const int g = c - pos_pad - n_sin;
+      const int base = n_sin + 6 * N;
+      int gi = 0;
+      if (dup_v > 0) {
+        if (g < 2)
+          for (int m = 0; m < dup_v; ++m) s += row[base + 2 * m + g];
+        gi = 2;
+      }
+      if (dup_h > 0) {
+        if (g == gi)
+          for (int m = 0; m < dup_h; ++m) s += row[base + 2 * dup_v + m];
+        gi += 1;
+      }
+      if (dup_c > 0 && g == gi)
+        for (int m = 0; m < dup_c; ++m) s += row[base + 2 * dup_v + dup_h + m];
+    }
+    wc[c_off + q] = s;
+  }
+}
+
+// Adam on the reference-layout master weights (nn.py:184-191) with the
+// gradient read from the compact layout; also the per-block partial sums of
+// grad^2 over the full layout (Model.get_TNS, nn.py:173-182).
+template <typename R>
+__global__ void ms_adam_kernel(R* __restrict__ master, R* __restrict__ m, R* __restrict__ v,
+                               const R* __restrict__ gc, long long m_off, long long c_off, int rows,
+                               int n_in_full, int pitch, int layer, int N, int pos_pad, int n_sin,
+                               int dup_v, int dup_h, int dup_c, double lr, double b1, double b2,
+                               int iter, const int* iter_dev, int apply, double* tns_part) {
+  __shared__ double red[32];
+  if (iter < 0) iter = *iter_dev;
+  const double bc1 = 1.0 - pow(b1, (double)(iter + 1)), bc2 = 1.0 - pow(b2, (double)(iter + 1));
+  const long long total = (long long)rows * n_in_full;
+  double tns = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / n_in_full), j = (int)(q % n_in_full);
+    int c = j;
+    if (layer == 0) c = full_to_compact(j, N, pos_pad, n_sin, dup_v, dup_h, dup_c);
+    const R g = c >= 0 ? gc[c_off + (long long)i * pitch + c] : R(0);
+    tns += (double)g * (double)g;
+    if (apply) {
+      const long long w = m_off + q;
+      const R mm = R(b1) * m[w] + R(1 - b1) * g;
+      const R vv = R(b2) * v[w] + R(1 - b2) * g * g;
+      m[w] = mm;
+      v[w] = vv;
+      const R mc = mm / R(bc1), vc = vv / R(bc2);
+      master[w] -= (R(lr) * mc) / (sqrt(vc) + R(1e-8));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) tns += __shfl_xor_sync(0xffffffffu, tns, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tns;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    tns_part[blockIdx.x] = s;
+  }
+}
+
+// bias Adam (no column map)
+template <typename R>
+__global__ void ms_adam_bias_kernel(R* __restrict__ b, R* __restrict__ m, R* __restrict__ v,
+                                    const R* __restrict__ g, int n, double lr, double b1, double b2,
+                                    int iter, const int* iter_dev, int apply, double* tns_part) {
+  __shared__ double red[32];
+  if (iter < 0) iter = *iter_dev;
+  const double bc1 = 1.0 - pow(b1, (double)(iter + 1)), bc2 = 1.0 - pow(b2, (double)(iter + 1));
+  double tns = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const R gg = g[q];
+    tns += (double)gg * (double)gg;
+    if (apply) {
+      const R mm = R(b1) * m[q] + R(1 - b1) * gg;
+      const R vv = R(b2) * v[q] + R(1 - b2) * gg * gg;
+      m[q] = mm;
+      v[q] = vv;
+      b[q] -= (R(lr) * (mm / R(bc1))) / (sqrt(vv / R(bc2)) + R(1e-8));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) tns += __shfl_xor_sync(0xffffffffu, tns, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tns;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    tns_part[blockIdx.x] = s;
+  }
+}
+
+// grads of the reference layout from the compact layout (for export)
+template <typename R>
+__global__ void ms_unpack_grad_kernel(const R* __restrict__ gc, long long c_off, int pitch, int rows,
+                                      int n_in_full, int layer, int N, int pos_pad, int n_sin,
+                                      int dup_v, int dup_h, int dup_c, double* __restrict__ out) {
+  const long long total = (long long)rows * n_in_full;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / n_in_full), j = (int)(q % n_in_full);
+    int c = j;
+    if (layer == 0) c = full_to_compact(j, N, pos_pad, n_sin, dup_v, dup_h, dup_c);
+    out[q] = c >= 0 ? (double)gc[c_off + (long long)i * pitch + c] : 0.0;
+  }
+}
+
+template <typename R>
+__global__ void ms_convert_kernel(const double* __restrict__ in, R* __restrict__ out, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = (R)in[q];
+}
+
+template <typename R>
+__global__ void ms_to_double_kernel(const R* __restrict__ in, double* __restrict__ out, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = (double)in[q];
+}
+
+// xyz triples (double) <-> V4 state
+template <typename R>
+__global__ void ms_xyz_to_v4_kernel(const double* __restrict__ in, V4<R>* __restrict__ out, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    V4<R> r;
+    r.x = (R)in[3 * q]; r.y = (R)in[3 * q + 1]; r.z = (R)in[3 * q + 2]; r.w = 0;
+    out[q] = r;
+  }
+}
+
+template <typename R>
+__global__ void ms_v4_to_xyz_kernel(const V4<R>* __restrict__ in, double* __restrict__ out, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const V4<R> r = in[q];
+    out[3 * q] = r.x; out[3 * q + 1] = r.y; out[3 * q + 2] = r.z;
+  }
+}
+
+// ------------------------------------------------- initialisation kernels
+// counter-based uniform in [0, 1): splitmix64 of (seed, stream, index)
+__device__ __forceinline__ double u01(unsigned long long seed, unsigned long long stream,
+                                      unsigned long long idx) {
+  unsigned long long z = seed * 0x9E3779B97F4A7C15ULL + stream * 0xD1B54A32D192ED03ULL + idx;
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Model.weights_init (nn.py:59-67): W = (u * 2 - 1) * sqrt(6 / fan_in)
+template <typename R>
+__global__ void ms_weights_init_kernel(R* __restrict__ master, long long off, long long n, int fan_in,
+                                       unsigned long long seed, unsigned long long stream) {
+  const double q = sqrt(6.0 / fan_in);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    master[off + i] = (R)((u01(seed, stream, (unsigned long long)i) * 2 - 1) * q);
+}
+
+// TaichiEnv.initialize_train, 3D branch (taichi_env.py:385-447): one pool of
+// three uniforms per (turn period, env); 25 % turn -1, 25 % turn +1, 25 %
+// forward/backward along z, 25 % along x.  target_c is left unchanged.
+template <typename R>
+__global__ void ms_initialize_train_kernel(V4<R>* __restrict__ tv, R* __restrict__ th, int T,
+                                           int steps, int n_envs, int turn_period,
+                                           unsigned long long seed, int iter, double max_velocity) {
+  const long long total = (long long)T * n_envs;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(q / n_envs), k = (int)(q % n_envs);
+    if (t >= steps) continue;
+    const unsigned long long base = ((unsigned long long)(t / turn_period) * n_envs + k) * 3;
+    const double p0 = u01(seed, 0x7000000ULL + (unsigned long long)iter, base);
+    const double p1 = u01(seed, 0x7000000ULL + (unsigned long long)iter, base + 1);
+    V4<R> v; v.x = 0; v.y = 0; v.z = 0; v.w = 0;
+    R h = 0;
+    if (p0 < 0.25) {
+      h = R(-1);
+    } else if (p0 < 0.5) {
+      h = R(1);
+    } else if (p0 < 0.75) {
+      v.z = (R)((p1 * 2. - 1.) * max_velocity);
+    } else {
+      v.x = (R)((p1 * 2. - 1.) * max_velocity);
+    }
+    tv[q] = v;
+    th[q] = h;
+  }
+}
+
+}  // namespace cls

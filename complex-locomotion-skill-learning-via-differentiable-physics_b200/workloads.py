@@ -1,0 +1,127 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+All inputs are generated from a seed (no dataset is involved):
+
+* ``quadruped_batch``   -- one quadruped lattice (torso 4x2x1 cubes on four
+  1x1x2 legs), 32 envs, 1000 substeps, 1 hidden layer of 64 tanh;
+* ``uneven_batch``      -- 512 random lattices of 50-2000 vertices (log-uniform),
+  30 % of springs actuated, 2000 substeps, checkpoint every 50, MLP 2x128 tanh;
+* ``spider_batch``      -- 4096 envs of a spider-like lattice (3x3x1 torso, eight
+  1x1x3 legs, 96 actuators), 1000 substeps, MLP 2x256 tanh.
+
+Physics of these synthetic configurations: stiffness 3e4 (the reference's
+/10 scaling applies), dt 2e-3, gravity -9.8, ground at y = 0 with friction 0.5,
+velocity damping 0.99 per substep (drag = -ln(0.99) / dt).  The controller
+input is the reference's layout with 8 sinusoids and one copy of each goal
+value.
+"""
+import math
+
+import numpy as np
+
+from . import robot_design
+from .batch import MassSpringBatch, Robot, default_params
+
+PHYSICS = dict(dt=2e-3, gravity=-9.8, ground_height=0.0, friction=0.5,
+               drag_damping=-math.log(0.99) / 2e-3, dashpot_damping=0.1, stiffness_scale=0.1)
+
+
+def _params(steps, K, hidden_act="tanh", precision=32, loss=("velocity", "rotation"), **over):
+    p = dict(PHYSICS)
+    p.update(max_steps=steps, checkpoint_every=K, run_period=100, turn_period=500,
+             jump_period=500, spring_omega=2 * math.pi / p["dt"] / 100, n_sin_waves=8,
+             duplicate_v=1, duplicate_h=1, duplicate_c=0, activation_hidden=hidden_act,
+             activation_output=hidden_act, loss=list(loss), precision=precision,
+             max_speed=0.1, max_height=0.1)
+    p.update(over)
+    return p
+
+
+def targets(rng, T, n_envs, turn_period=500, lo=-0.1, hi=0.1):
+    """Goal values (target vx, vz, height) ~ U(lo, hi), one draw per env per
+    turn period, held for the period."""
+    n_blocks = T // turn_period + 1
+    draws = rng.uniform(lo, hi, size=(n_blocks, n_envs, 3))
+    idx = np.arange(T) // turn_period
+    tv = np.zeros((T, n_envs, 3))
+    tv[:, :, 0] = draws[idx, :, 0]
+    tv[:, :, 2] = draws[idx, :, 1]
+    th = draws[idx, :, 2]
+    return tv, th
+
+
+def uneven_robots(n_robots=512, seed=0, vmin=50, vmax=2000, hidden=(128, 128)):
+    rng = np.random.default_rng(seed)
+    robots = []
+    for _ in range(n_robots):
+        n = int(round(math.exp(rng.uniform(math.log(vmin), math.log(vmax)))))
+        obj, spr = robot_design.random_lattice(rng, n)
+        robots.append(Robot.actuated_outputs(obj, spr, hidden=list(hidden)))
+    return robots
+
+
+def uneven_batch(n_robots=512, steps=2000, K=50, seed=0, precision=32, hidden=(128, 128),
+                 vmin=50, vmax=2000, robots=None, **over):
+    """Batched uneven mass-spring: every robot its own type and controller."""
+    robots = robots if robots is not None else uneven_robots(n_robots, seed, vmin, vmax, hidden)
+    p = default_params(**_params(steps, K, precision=precision, **over))
+    b = MassSpringBatch(robots, list(range(len(robots))), p)
+    rng = np.random.default_rng(seed + 1)
+    tv, th = targets(rng, steps, len(robots))
+    b.set_targets(tv, th)
+    b.weights_init(seed + 2)
+    return b, robots, (tv, th)
+
+
+def quadruped_batch(n_envs=32, steps=1000, K=50, seed=0, precision=32, **over):
+    obj, spr = robot_design.quadruped_lattice()
+    robot = Robot.actuated_outputs(obj, spr, hidden=[64])
+    p = default_params(**_params(steps, K, precision=precision, **over))
+    b = MassSpringBatch([robot], [0] * n_envs, p)
+    rng = np.random.default_rng(seed + 1)
+    tv, th = targets(rng, steps, n_envs)
+    b.set_targets(tv, th)
+    b.weights_init(seed + 2)
+    return b, [robot], (tv, th)
+
+
+def spider_batch(n_envs=4096, steps=1000, K=50, seed=0, precision=32, **over):
+    obj, spr = robot_design.spider_lattice()
+    robot = Robot.actuated_outputs(obj, spr, hidden=[256, 256])
+    p = default_params(**_params(steps, K, precision=precision, **over))
+    b = MassSpringBatch([robot], [0] * n_envs, p)
+    rng = np.random.default_rng(seed + 1)
+    tv, th = targets(rng, steps, n_envs)
+    b.set_targets(tv, th)
+    b.weights_init(seed + 2)
+    return b, [robot], (tv, th)
+
+
+def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4):
+    """Compulsory DRAM bytes per substep of the whole batch, per kernel.
+
+    Per env-substep of robot r (N vertices, S springs, MLP rows x pitch):
+      weights:   sum_l rows_l * pitch_l * 4   (read once per pass; the batch's
+                 weights exceed L2, so every pass streams them)
+      forward:   weights + trajectory write 16 N (x[t], when kept)
+      recompute: weights + record writes 32 N (x, v) + 4 n_c (input) + 4 sum rows
+      reverse:   weights + record reads 32 N + 4 sum rows (z) + writes 4 sum rows
+                 (dz) + trajectory reads 32 N (rotation loss at t - rp, t + rp)
+    The spring table (32 B per incidence, 2 S per robot) is read from L2 each
+    substep and counted once per pass.
+    """
+    out = dict(forward=0.0, recompute=0.0, reverse=0.0)
+    for r in env_robot:
+        rb = robots[r]
+        N, S = rb.n_vertices, rb.n_springs
+        widths = [(-(-3 * N // 4) * 4) + 8 + 2 + 1] + list(rb.hidden) + [
+            rb.n_outputs if rb.n_outputs > 0 else S]
+        pitch = [-(-w // 4) * 4 for w in widths]
+        wbytes = sum(widths[l + 1] * pitch[l] for l in range(len(widths) - 1)) * dtype_bytes
+        rows = sum(widths[1:]) * dtype_bytes
+        springs = 2 * S * 32
+        traj = 16 * N if keep_trajectory else 0
+        out["forward"] += wbytes + springs + traj
+        out["recompute"] += wbytes + springs + 32 * N + widths[0] * dtype_bytes + rows
+        out["reverse"] += wbytes + springs + 32 * N + 2 * rows + 2 * traj
+    return out

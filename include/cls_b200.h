@@ -1,0 +1,204 @@
+/*
+ * cls_b200.h -- C ABI of the B200 differentiable soft-robot simulation step.
+ *
+ * The reference (erizmr/Complex-locomotion-skill-learning-via-differentiable-
+ * physics) has no foreign-function boundary: its trainer drives Taichi kernels
+ * through duck-typed Python objects.  Each entry point below replaces one
+ * step of that protocol; the reference interface it stands in for is cited
+ * beside it (paths relative to the reference root).
+ *
+ * Conventions
+ *   - every function returns CLS_OK (0) or a negative CLS_ERR_* code; the
+ *     message of the last failure is available from cls_last_error();
+ *   - host arrays are float64 and row-major, in the reference's field layouts
+ *     ([t][env][i] for trajectory fields, [env][vertex][3] for states);
+ *   - environments are numbered in the order given to cls_create; internally
+ *     they are grouped by robot, which callers never see;
+ *   - a handle is bound to one CUDA stream (cls_set_stream) and is not
+ *     thread-safe; distinct handles may be used concurrently;
+ *   - all work is asynchronous on the handle's stream except functions that
+ *     return host data, which synchronise that stream.
+ */
+#ifndef CLS_B200_H_
+#define CLS_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLS_OK 0
+#define CLS_ERR_INVALID (-1)   /* bad argument or configuration */
+#define CLS_ERR_CUDA (-2)      /* CUDA runtime error */
+#define CLS_ERR_OOM (-3)       /* device allocation failed */
+#define CLS_ERR_NONFINITE (-4) /* NaN/Inf detected in the simulated state */
+#define CLS_ERR_STATE (-5)     /* call out of order (e.g. backward before forward) */
+
+#define CLS_ACT_SIN 0
+#define CLS_ACT_TANH 1
+
+#define CLS_LOSS_VELOCITY 1
+#define CLS_LOSS_HEIGHT 2
+#define CLS_LOSS_POSE 4
+#define CLS_LOSS_ACTUATION 8
+#define CLS_LOSS_ROTATION 16
+#define CLS_LOSS_CRAWL 32
+
+#define CLS_MAX_HIDDEN 4
+
+typedef struct cls_sim cls_sim;
+
+/* One robot type: geometry plus its controller shape.
+ * Replaces config["robot"]{objects, springs} produced by
+ * RobotDesignMassSpring3D.build (multitask/robot_design.py:572-591, rows of
+ * add_spring :344-349) and the Model shape (multitask/nn.py:79-109). */
+typedef struct {
+  int32_t n_vertices;
+  int32_t n_springs;
+  const double* objects;        /* [n_vertices][3] initial positions */
+  const double* springs;        /* [n_springs][5]: a, b, rest length, stiffness, actuation */
+  int32_t robot_id;             /* 100: heading from vertices 45, 46, 34, 36 */
+  int32_t n_outputs;            /* MLP outputs; 0 = one per spring (reference) */
+  const int32_t* spring_output; /* [n_springs] output feeding each spring or -1; NULL = identity */
+  int32_t n_hidden_layers;      /* 1..CLS_MAX_HIDDEN (reference: 1) */
+  int32_t hidden[CLS_MAX_HIDDEN];
+} cls_robot_desc;
+
+/* Simulation / controller / optimiser constants: the cfg3d JSON schema after
+ * ConfigSim._add_adaptive_configs (multitask/config_sim.py:103-147). */
+typedef struct {
+  int32_t max_steps;            /* process.max_steps: trajectory length T */
+  double dt;                    /* process.dt */
+  double gravity;               /* simulator.gravity */
+  double ground_height;         /* simulator.ground_height */
+  double drag_damping;          /* simulator.drag_damping */
+  double dashpot_damping;       /* simulator.dashpot_damping */
+  double friction;              /* 0.4 in the reference (solver_mass_spring.py:136) */
+  double stiffness_scale;       /* 0.1 in the reference (solver_mass_spring.py:64) */
+  int32_t run_period, turn_period, jump_period;
+  double spring_omega;          /* process.spring_omega */
+  int32_t n_sin_waves, duplicate_v, duplicate_h, duplicate_c;
+  int32_t activation_hidden;    /* CLS_ACT_SIN (reference) or CLS_ACT_TANH */
+  int32_t activation_output;
+  int32_t loss_mask;            /* CLS_LOSS_* bits (reference 3D: velocity | rotation) */
+  int32_t precision;            /* 32 or 64 */
+  int32_t checkpoint_every;     /* substeps per checkpoint segment (K) */
+  double max_speed, max_height; /* process.max_speed / max_height */
+  double adam_b1, adam_b2, learning_rate;
+  int32_t threads_per_block;    /* 0: choose automatically */
+} cls_sim_params;
+
+/* Fills *p with the reference's defaults for cfg3d/sim_quad.json. */
+void cls_default_params(cls_sim_params* p);
+
+/* Allocates a batch of n_envs environments; env_robot[e] selects the robot type
+ * of env e.  Replaces TaichiEnv.__init__ + SolverMassSpring.__init__ +
+ * Model.__init__ (multitask/taichi_env.py:22-147, solver_mass_spring.py:8-56,
+ * nn.py:79-109) and SolverMassSpring.initialize_robot (:58-67). */
+int cls_create(const cls_robot_desc* robots, int32_t n_robots, const int32_t* env_robot,
+               int32_t n_envs, const cls_sim_params* params, cls_sim** out);
+int cls_destroy(cls_sim* sim);
+
+/* Message of the last failure on this handle (NULL handle: last cls_create
+ * failure of the calling thread). */
+const char* cls_last_error(const cls_sim* sim);
+
+/* Binds the handle to a cudaStream_t (NULL: legacy default stream). */
+int cls_set_stream(cls_sim* sim, void* stream);
+
+/* Sizes of the packed layouts. */
+int cls_get_sizes(const cls_sim* sim, int32_t* n_envs, int32_t* n_vertices_total,
+                  int32_t* max_steps);
+/* Width of weight layer `layer` of `robot` in the reference layout
+ * (rows = outputs, cols = inputs; layer 0 cols = n_input_states). */
+int cls_get_layer_shape(const cls_sim* sim, int32_t robot, int32_t layer, int32_t* rows,
+                        int32_t* cols);
+
+/* x[0], v[0] of every env ([n_vertices_total][3], envs in creation order).
+ * Replaces TaichiEnv.setup_robot / reset_robot / copy_robot
+ * (multitask/taichi_env.py:487-510). */
+int cls_set_state(cls_sim* sim, const double* x0, const double* v0);
+
+/* target_v [T][n_envs][3], target_h [T][n_envs], target_c [T][n_envs].
+ * Replaces initialize_train / initialize_validate / initialize_script
+ * (multitask/taichi_env.py:333-469) when targets come from the caller. */
+int cls_set_targets(cls_sim* sim, const double* target_v, const double* target_h,
+                    const double* target_c);
+
+/* Reference-layout weights W [rows][cols], b [rows] of one layer; layer 0 is
+ * weights1/bias1 (multitask/nn.py:31-43).  Replaces Model.load_weights. */
+int cls_set_weights(cls_sim* sim, int32_t robot, int32_t layer, const double* W, const double* b);
+int cls_get_weights(cls_sim* sim, int32_t robot, int32_t layer, double* W, double* b);
+/* Gradient of the loss w.r.t. the same (after cls_backward). */
+int cls_get_grads(cls_sim* sim, int32_t robot, int32_t layer, double* gW, double* gb);
+
+/* Training rollout of `steps` substeps (t in [0, steps-2], the loop of
+ * DiffPhyTrainer.simulate, multitask/diffphy_trainer.py:231-255), saving a
+ * checkpoint every K substeps and the per-step observables. */
+int cls_forward(cls_sim* sim, int32_t steps);
+/* Forward-only evaluation rollout (t in [0, steps], diffphy_trainer.py:257-268). */
+int cls_forward_eval(cls_sim* sim, int32_t steps);
+/* Loss of the last rollout (TaichiEnv.get_loss, multitask/taichi_env.py:304-331).
+ * loss_terms[8] = total, velocity, height, pose, rotation, weight, actuation,
+ * crawl; loss_env [8][n_envs] the per-env losses (loss_batch fields, scaled by
+ * B as the reference does); either may be NULL. */
+int cls_loss(cls_sim* sim, double* loss_terms, double* loss_env);
+/* Reverse pass (ti.ad.Tape exit, diffphy_trainer.py:246): recompute each
+ * segment from its checkpoint and run the hand-written adjoints. */
+int cls_backward(cls_sim* sim);
+/* forward + loss + backward in one call; returns the total loss. */
+int cls_simulate(cls_sim* sim, int32_t steps, double* loss);
+/* Same rollout, but every env runs in its own launch (one robot per launch). */
+int cls_simulate_per_env(cls_sim* sim, int32_t steps, double* loss);
+/* Adam step on all weights (Model.gradient_update, multitask/nn.py:163-171,
+ * 184-191) with bias correction for iteration `iter`; *tns receives the
+ * squared gradient norm (Model.get_TNS, :173-182) if non-NULL. */
+int cls_adam_step(cls_sim* sim, int32_t iter, double* tns);
+/* zero the Adam moments (Model.clear_adam, multitask/nn.py:111-114) */
+int cls_clear_adam(cls_sim* sim);
+
+/* Observables of the last rollout: center [T][n_envs][3], height, upper
+ * height, rotation [T][n_envs] (solver fields of the same names). */
+int cls_get_observables(cls_sim* sim, double* center, double* height, double* upper_height,
+                        double* rotation);
+/* Positions x[t] for all t ([T][n_vertices_total][3]); only available when a
+ * rotation or pose loss is enabled (the trajectory is then kept). */
+int cls_get_trajectory(cls_sim* sim, double* x);
+/* State after the last processed substep ([n_vertices_total][3]). */
+int cls_get_final_state(cls_sim* sim, double* x, double* v);
+/* d loss / d x[0], d v[0] after cls_backward ([n_vertices_total][3]). */
+int cls_get_state_grads(cls_sim* sim, double* gx0, double* gv0);
+
+/* Waits for the handle's stream; returns CLS_ERR_NONFINITE if a kernel saw
+ * NaN/Inf state since the last check. */
+int cls_synchronize(cls_sim* sim);
+
+/* Model.weights_init (multitask/nn.py:59-67) on the device:
+ * W = (u * 2 - 1) * sqrt(6 / fan_in) with u from a counter-based generator
+ * seeded by `seed` (the reference draws from ti.random); biases unchanged. */
+int cls_weights_init(cls_sim* sim, uint64_t seed);
+/* TaichiEnv.initialize_train (multitask/taichi_env.py:385-447, 3D branch) on
+ * the device for t < steps, drawing the task pool from (seed, iter). */
+int cls_initialize_train(cls_sim* sim, int32_t iter, int32_t steps, uint64_t seed,
+                         double max_speed);
+
+/* Per-kernel profile: when enabled, every launch is bracketed by CUDA events
+ * on the handle's stream.  cls_profile_read returns, per launch category
+ * (0 first-pass forward, 1 segment recompute, 2 reverse, 3 weight-gradient
+ * products, 4 loss, 5 optimiser/packing, 6 other), the summed device time in
+ * ms and the number of launches; launches are counted even when disabled. */
+#define CLS_PROFILE_KINDS 7
+int cls_profile_enable(cls_sim* sim, int32_t on);
+int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset);
+
+/* Captures one training iteration (forward + loss + backward, optionally the
+ * Adam step) into a CUDA graph and replays it; cls_graph_launch replays. */
+int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam);
+int cls_graph_launch(cls_sim* sim, int32_t iter);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLS_B200_H_ */
