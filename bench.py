@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: automatic)")
     return ap.parse_args()
 
 
@@ -167,7 +168,7 @@ class ClockSampler:
         smax = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
         loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -184,7 +185,8 @@ def run_ours(a):
     import cls_b200
     from cls_b200 import workloads
     b, robots, (tv, th) = workloads.uneven_batch(n_robots=a.robots, steps=a.substeps,
-                                                K=a.checkpoint, seed=1000 * rank)
+                                                K=a.checkpoint, seed=1000 * rank,
+                                                threads_per_block=a.threads)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     env_substeps = b.n_envs * (a.substeps - 1)
@@ -219,6 +221,8 @@ def run_ours(a):
         ms = float(t.item())
     ms_per_step = ms / a.steps
     value = world * env_substeps / (ms_per_step / 1e3)
+    print("timed: %.1f ms/step, %.3e %s, kernels %s" % (ms_per_step, value, UNIT, prof_ms),
+          file=sys.stderr)
 
     # roofline of the dominant kernel (CUDA events around each launch above)
     alg = workloads.algorithmic_bytes(robots, list(range(len(robots))))

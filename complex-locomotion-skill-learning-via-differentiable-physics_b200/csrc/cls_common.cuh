@@ -40,6 +40,47 @@ template <> __device__ __forceinline__ V4<double> ldg4<double>(const V4<double>*
   return r;
 }
 
+// L2 eviction-priority policies (PTX createpolicy).  Controller weights are
+// streamed once per substep and pass -- far more bytes than L2 holds -- so they
+// are loaded evict_first; the spring incidence tables are re-read every
+// substep and are loaded evict_last so the weight stream does not evict them.
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long policy_evict_last() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+template <typename R> __device__ __forceinline__ V4<R> ldg4_hint(const V4<R>* p, unsigned long long pol);
+template <> __device__ __forceinline__ V4<float> ldg4_hint<float>(const V4<float>* p, unsigned long long pol) {
+  V4<float> r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+template <> __device__ __forceinline__ V4<double> ldg4_hint<double>(const V4<double>* p, unsigned long long pol) {
+  V4<double> r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(r.x), "=d"(r.y)
+               : "l"(p), "l"(pol));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(r.z), "=d"(r.w)
+               : "l"(reinterpret_cast<const double*>(p) + 2), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ int4 ldg_i4_hint(const int4* p, unsigned long long pol) {
+  int4 r;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+
 template <typename R>
 __device__ __forceinline__ R comp(const V4<R>& v, int d) {
   return d == 0 ? v.x : (d == 1 ? v.y : v.z);
@@ -48,6 +89,20 @@ __device__ __forceinline__ R comp(const V4<R>& v, int d) {
 template <typename R> __device__ __forceinline__ R dsqrt(R x);
 template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
 template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+
+// Spring-geometry helpers.  FP32 uses the hardware reciprocal square root
+// (rsqrtf, <= 2 ulp) and the correctly rounded reciprocal (__frcp_rn) instead
+// of IEEE sqrt / division sequences; FP64 -- the precision-check build -- keeps
+// exact sqrt and division.
+template <typename R> __device__ __forceinline__ R rsqrt_s(R x);
+template <> __device__ __forceinline__ float rsqrt_s<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double rsqrt_s<double>(double x) { return 1.0 / sqrt(x); }
+template <typename R> __device__ __forceinline__ R rcp_s(R x);
+template <> __device__ __forceinline__ float rcp_s<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ double rcp_s<double>(double x) { return 1.0 / x; }
+template <typename R> __device__ __forceinline__ R sqrt_s(R x);
+template <> __device__ __forceinline__ float sqrt_s<float>(float x) { return x * rsqrtf(x); }
+template <> __device__ __forceinline__ double sqrt_s<double>(double x) { return sqrt(x); }
 
 template <typename R> __device__ __forceinline__ R dsin(R x);
 template <> __device__ __forceinline__ float dsin<float>(float x) { return sinf(x); }

@@ -74,7 +74,10 @@ struct MsArgs {
   const int* inc_ptr;                // CSR row pointers (relative to inc_off)
   const int4* inc_i;                 // {other vertex, side (0: a, 1: b), spring, out index}
   const V4<R>* inc_f;                // {rest length, stiffness, actuation coef, 0}
+  const int4* inc_p;                 // FP32 only: packed 16-byte incidence records
   const int* spring_out;             // per spring: MLP output index or -1
+  const int4* spr_i;                 // per spring {a, b, out index, 0}
+  const V4<R>* spr_f;                // per spring {rest length, stiffness, actuation coef, 0}
   const R* w;                        // compact weights
   const R* bias;
   const R* sin_table;                // [T + 1][n_sin], sin(omega (t) dt + 2 pi j / n_sin)
@@ -82,6 +85,7 @@ struct MsArgs {
   V4<R>* ckpt_x; V4<R>* ckpt_v;      // [n_ckpt][v_total]
   V4<R>* fin_x; V4<R>* fin_v;        // [v_total] state after the last processed step
   V4<R>* rec_x; V4<R>* rec_v;        // [K][v_total]
+  V4<R>* rec_vinc;                   // [K][v_total] v_inc[t] of the recompute
   R* rec_in;                         // [K][in_total]
   R* rec_z;                          // per layer z_base[l] + [K][z_total[l]]
   R* rec_dz;                         // same layout as rec_z
@@ -97,7 +101,30 @@ struct MsArgs {
   V4<R>* adj_x; V4<R>* adj_v; R* adj_h;
   // status
   int* status;
+  // per-phase clock totals, only written by builds with CLS_PHASE_TIMERS
+  unsigned long long* phase;
 };
+
+// Optional phase timers (profiling builds only, -DCLS_PHASE_TIMERS): thread 0
+// of every CTA adds the clock64 time since the previous mark to phase[k].
+#ifdef CLS_PHASE_TIMERS
+#define CLS_PHASE_START() long long cls_pt_ = clock64()
+#define CLS_PHASE(a, k)                                                        \
+  do {                                                                         \
+    if (threadIdx.x == 0 && (a).phase) {                                       \
+      const long long n_ = clock64();                                          \
+      atomicAdd((a).phase + (k), (unsigned long long)(n_ - cls_pt_));          \
+      cls_pt_ = n_;                                                            \
+    }                                                                          \
+  } while (0)
+#else
+#define CLS_PHASE_START() \
+  do {                    \
+  } while (0)
+#define CLS_PHASE(a, k) \
+  do {                  \
+  } while (0)
+#endif
 
 // ------------------------------------------------------------ shared memory
 // reduction scratch: 8 values x 32 warps, then 32 ints for arg-reductions
@@ -191,10 +218,10 @@ __device__ __forceinline__ void spring_impulse(const V4<R>& xa, const V4<R>& xb,
                                                R dashpot, R imp[3]) {
   R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
   R n2 = d0 * d0 + d1 * d1 + d2 * d2;
-  R length = dsqrt<R>(n2 + R(1e-8)) + R(1e-4);
+  R length = sqrt_s<R>(n2 + R(1e-8)) + R(1e-4);        // norm(1e-8) + 1e-4
   R target = l0 * (R(1) + coef * act);
-  R sc = dt * (length - target) * k / length;
-  R invlen = R(1) / dsqrt<R>(n2);
+  R sc = dt * (length - target) * k * rcp_s<R>(length);
+  R invlen = rsqrt_s<R>(n2);                           // normalized(): 1 / norm()
   R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
   R vrel = (va.x - vb.x) * n0 + (va.y - vb.y) * n1 + (va.z - vb.z) * nz;
   R c = dashpot * vrel;
@@ -203,29 +230,114 @@ __device__ __forceinline__ void spring_impulse(const V4<R>& xa, const V4<R>& xb,
   imp[2] = sc * d2 + c * nz;
 }
 
-// v_inc of vertex i: sum over incident springs, a-side gets -impulse, b-side +impulse
+// One spring incidence: the other endpoint, which side this vertex is on, the
+// controller output driving the spring, and the spring constants.
 template <typename R>
-__device__ __forceinline__ V4<R> gather_vinc(const MsArgs<R>& a, const RobotDesc& rb, int i,
-                                             const V4<R>* xs, const V4<R>* vs, const R* out) {
-  const int beg = a.inc_ptr[rb.ptr_off + i], end = a.inc_ptr[rb.ptr_off + i + 1];
-  R s0 = 0, s1 = 0, s2 = 0;
-  const V4<R> xi = xs[i], vi = vs[i];
-  for (int q = beg; q < end; ++q) {
-    const int4 ii = a.inc_i[rb.inc_off + q];
-    const V4<R> ff = a.inc_f[rb.inc_off + q];
-    const int o = ii.x;
-    const R act = ii.w >= 0 ? out[ii.w] : R(0);
-    R imp[3];
-    if (ii.y == 0) {  // this vertex is endpoint a
-      spring_impulse<R>(xi, xs[o], vi, vs[o], ff.x, ff.y, ff.z, act, a.dt, a.dashpot, imp);
-      s0 -= imp[0]; s1 -= imp[1]; s2 -= imp[2];
-    } else {          // endpoint b
-      spring_impulse<R>(xs[o], xi, vs[o], vi, ff.x, ff.y, ff.z, act, a.dt, a.dashpot, imp);
-      s0 += imp[0]; s1 += imp[1]; s2 += imp[2];
+struct Inc {
+  int other, side, out;
+  R l0, k, coef;
+};
+
+// FP32 records are packed in 16 bytes: {other | side << 15 | (out + 1) << 16,
+// l0, k, coef}; FP64 records use the two-array form (int4 + V4<double>).
+template <typename R>
+__device__ __forceinline__ Inc<R> load_inc(const MsArgs<R>& a, const RobotDesc& rb, int q,
+                                           unsigned long long pol);
+template <>
+__device__ __forceinline__ Inc<float> load_inc<float>(const MsArgs<float>& a, const RobotDesc& rb,
+                                                      int q, unsigned long long pol) {
+  const int4 p = ldg_i4_hint(a.inc_p + rb.inc_off + q, pol);
+  Inc<float> r;
+  r.other = p.x & 0x7fff;
+  r.side = (p.x >> 15) & 1;
+  r.out = (int)(((unsigned)p.x) >> 16) - 1;
+  r.l0 = __int_as_float(p.y);
+  r.k = __int_as_float(p.z);
+  r.coef = __int_as_float(p.w);
+  return r;
+}
+template <>
+__device__ __forceinline__ Inc<double> load_inc<double>(const MsArgs<double>& a, const RobotDesc& rb,
+                                                        int q, unsigned long long pol) {
+  const int4 ii = ldg_i4_hint(a.inc_i + rb.inc_off + q, pol);
+  const V4<double> ff = ldg4_hint<double>(a.inc_f + rb.inc_off + q, pol);
+  Inc<double> r;
+  r.other = ii.x; r.side = ii.y; r.out = ii.w;
+  r.l0 = ff.x; r.k = ff.y; r.coef = ff.z;
+  return r;
+}
+
+template <typename R>
+__device__ __forceinline__ void accumulate_incidence(const MsArgs<R>& a, const Inc<R>& in, const V4<R>& xi,
+                                                     const V4<R>& vi, const V4<R>* xs, const V4<R>* vs,
+                                                     const R* out, R& s0, R& s1, R& s2) {
+  const int o = in.other;
+  const R act = in.out >= 0 ? out[in.out] : R(0);
+  R imp[3];
+  if (in.side == 0) {  // this vertex is endpoint a: -impulse
+    spring_impulse<R>(xi, xs[o], vi, vs[o], in.l0, in.k, in.coef, act, a.dt, a.dashpot, imp);
+    s0 -= imp[0]; s1 -= imp[1]; s2 -= imp[2];
+  } else {             // endpoint b: +impulse
+    spring_impulse<R>(xs[o], xi, vs[o], vi, in.l0, in.k, in.coef, act, a.dt, a.dashpot, imp);
+    s0 += imp[0]; s1 += imp[1]; s2 += imp[2];
+  }
+}
+
+// v_inc of all vertices, half-warp per vertex: the 16 lanes of a half-warp
+// take the vertex's incidences in parallel (lane l: entries beg + l, beg + l +
+// 16, ...) and combine them with a fixed xor-shuffle tree, so the result does
+// not depend on scheduling (the recompute pass reproduces the first pass bit
+// for bit).  Each half-warp prefetches the first incidence of U vertices
+// before computing, so U records per lane are in flight.
+template <typename R>
+__device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotDesc& rb, int N,
+                                                const V4<R>* xs, const V4<R>* vs, const R* out,
+                                                V4<R>* vinc, V4<R>* rec) {
+  constexpr int U = 4;
+  const unsigned long long pol = policy_evict_last();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int l16 = lane & 15, half = lane >> 4;
+  const int* ptr = a.inc_ptr + rb.ptr_off;
+  const int stride = nw * 2;
+  // the loop bound is warp-uniform (vb0), so both half-warps run the same
+  // iterations and every full-mask shuffle below has all 32 lanes
+  for (int vb0 = wid * 2; vb0 < N; vb0 += stride * U) {
+    const int vb = vb0 + half;
+    int beg[U], end[U];
+    Inc<R> first[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int v = vb + k * stride;
+      beg[k] = 0;
+      end[k] = 0;
+      if (v < N) { beg[k] = ptr[v]; end[k] = ptr[v + 1]; }
+      const int q = beg[k] + l16;
+      if (q < end[k]) first[k] = load_inc<R>(a, rb, q, pol);
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int v = vb + k * stride;
+      R s0 = 0, s1 = 0, s2 = 0;
+      if (v < N) {
+        const V4<R> xi = xs[v], vi = vs[v];
+        int q = beg[k] + l16;
+        if (q < end[k]) accumulate_incidence<R>(a, first[k], xi, vi, xs, vs, out, s0, s1, s2);
+        for (q += 16; q < end[k]; q += 16)
+          accumulate_incidence<R>(a, load_inc<R>(a, rb, q, pol), xi, vi, xs, vs, out, s0, s1, s2);
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+      if (l16 == 0 && v < N) {
+        V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = 0;
+        vinc[v] = r;
+        if (rec) rec[v] = r;
+      }
     }
   }
-  V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = 0;
-  return r;
 }
 
 // advance_toi for one vertex (solver_mass_spring.py:119-148); in place
@@ -250,56 +362,133 @@ __device__ __forceinline__ void advance_vertex(const MsArgs<R>& a, V4<R>& x, V4<
   v.x = nv0; v.y = nv1; v.z = nv2;
 }
 
-// y = act(W x + b) for one layer, one warp per output row, float4 loads.
+// y = act(W x + b) for one layer.  Each warp owns RB consecutive rows at a
+// time and streams them together (RB independent float4 loads per lane per
+// column step), so short rows -- the 128-wide output layer of a robot with
+// thousands of actuators -- still keep enough loads in flight.
 // Records z (pre-bias sums) when zrec != null.
-template <typename R>
-__device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch, int nout,
-                                              const R* __restrict__ bias, const R* xin, R* y,
-                                              R* zrec, int act) {
+template <typename R, int RB>
+__device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pitch, int nout,
+                                                 const R* __restrict__ bias, const R* xin, R* y,
+                                                 R* zrec, int act) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int n4 = pitch >> 2;
   const V4<R>* x4 = reinterpret_cast<const V4<R>*>(xin);
-  for (int i = wid; i < nout; i += nw) {
-    const V4<R>* w4 = reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch);
-    R s = 0;
-#pragma unroll 4
+  const unsigned long long pol = policy_evict_first();
+  for (int i0 = wid * RB; i0 < nout; i0 += nw * RB) {
+    const V4<R>* w4[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int row = (i0 + r < nout) ? i0 + r : i0;
+      w4[r] = reinterpret_cast<const V4<R>*>(W + (size_t)row * pitch);
+    }
+    R s[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) s[r] = 0;
+#pragma unroll 2
     for (int j = lane; j < n4; j += 32) {
-      const V4<R> wv = ldg4<R>(w4 + j);
       const V4<R> xv = x4[j];
-      s += wv.x * xv.x + wv.y * xv.y + wv.z * xv.z + wv.w * xv.w;
+      V4<R> wv[RB];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) wv[r] = ldg4_hint<R>(w4[r] + j, pol);
+#pragma unroll
+      for (int r = 0; r < RB; ++r)
+        s[r] += wv[r].x * xv.x + wv[r].y * xv.y + wv[r].z * xv.z + wv[r].w * xv.w;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      if (zrec) zrec[i] = s;
-      y[i] = act_f<R>(act, s + bias[i]);
+    for (int r = 0; r < RB; ++r) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
+    }
+    if (lane < RB && i0 + lane < nout) {
+      R v = s[0];
+#pragma unroll
+      for (int r = 1; r < RB; ++r)
+        if (lane == r) v = s[r];
+      const int i = i0 + lane;
+      if (zrec) zrec[i] = v;
+      y[i] = act_f<R>(act, v + bias[i]);
     }
   }
 }
 
+template <typename R>
+__device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch, int nout,
+                                              const R* __restrict__ bias, const R* xin, R* y,
+                                              R* zrec, int act) {
+  if (pitch <= 256) dense_forward_rb<R, 8>(W, pitch, nout, bias, xin, y, zrec, act);
+  else dense_forward_rb<R, 4>(W, pitch, nout, bias, xin, y, zrec, act);
+}
+
 // g_in[j] = sum_i W[i, j] dz[i] for j in [0, ncols) (ncols multiple of 4 or
-// padded), deterministic: fixed row slices, fixed reduction order.
-// Result written to out4[j/4] (V4 groups).  Uses s.part as scratch.
+// padded), deterministic: fixed row splits, fixed reduction order.
+// Result written to out4[j/4] (V4 groups).  Uses `part` (blockDim entries) as
+// scratch in the narrow-row case.
 template <typename R>
 __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pitch, int nrows,
                                                  int ncols, const R* dz, V4<R>* part, V4<R>* out4) {
   const int c4 = (ncols + 3) >> 2;
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (c4 >= nt || nrows == 1) {
+  const unsigned long long pol = policy_evict_first();
+  if (nrows == 1) {
     for (int g = tid; g < c4; g += nt) {
-      R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-#pragma unroll 4
-      for (int i = 0; i < nrows; ++i) {
-        const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g);
-        const R d = dz[i];
-        s0 += wv.x * d; s1 += wv.y * d; s2 += wv.z * d; s3 += wv.w * d;
-      }
-      V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = s3;
+      const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W) + g);
+      const R d = dz[0];
+      V4<R> r; r.x = wv.x * d; r.y = wv.y * d; r.z = wv.z * d; r.w = wv.w * d;
       out4[g] = r;
     }
     __syncthreads();
     return;
   }
+  if (2 * c4 > nt) {
+    // Wide rows (the first layer of a large robot): two half-blocks split the
+    // rows; each thread keeps up to KMAX column-group partials in registers,
+    // the first half stores, the second half adds (fixed order).
+    constexpr int KMAX = 4;
+    const int H = nt >> 1, h = tid >= H ? 1 : 0, lt = tid - h * H;
+    const int rmid = nrows >> 1, r0 = h ? rmid : 0, r1 = h ? nrows : rmid;
+    for (int base = 0; base < c4; base += H * KMAX) {
+      R acc[KMAX][4];
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0;
+#pragma unroll 2
+      for (int i = r0; i < r1; ++i) {
+        const R d = dz[i];
+        const V4<R>* row = reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch);
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+          const int g = base + lt + k * H;
+          if (g < c4) {
+            const V4<R> wv = ldg4_hint<R>(row + g, pol);
+            acc[k][0] += wv.x * d; acc[k][1] += wv.y * d; acc[k][2] += wv.z * d; acc[k][3] += wv.w * d;
+          }
+        }
+      }
+      if (!h) {
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+          const int g = base + lt + k * H;
+          if (g < c4) { V4<R> r; r.x = acc[k][0]; r.y = acc[k][1]; r.z = acc[k][2]; r.w = acc[k][3]; out4[g] = r; }
+        }
+      }
+      __syncthreads();
+      if (h) {
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+          const int g = base + lt + k * H;
+          if (g < c4) {
+            V4<R> r = out4[g];
+            r.x += acc[k][0]; r.y += acc[k][1]; r.z += acc[k][2]; r.w += acc[k][3];
+            out4[g] = r;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  // Narrow rows (hidden / output layers): split the rows into `slices`
+  // interleaved sets, one partial per thread, then a fixed-order reduction.
   int slices = nt / c4;
   if (slices > nrows) slices = nrows;
   const int used = slices * c4;
@@ -308,7 +497,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
     R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll 4
     for (int i = r0; i < nrows; i += slices) {
-      const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g);
+      const V4<R> wv = ldg4_hint<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g, pol);
       const R d = dz[i];
       s0 += wv.x * d; s1 += wv.y * d; s2 += wv.z * d; s3 += wv.w * d;
     }

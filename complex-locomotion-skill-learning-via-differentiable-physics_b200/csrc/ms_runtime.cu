@@ -107,6 +107,7 @@ class SimBase {
   virtual void profile_enable(bool on) = 0;
   virtual void profile_read(double* ms, long long* launches, bool reset) = 0;
   virtual void sizes(int* ne, int* nv, int* T) const = 0;
+  virtual void phase_read(unsigned long long* out) = 0;
   virtual void layer_shape(int r, int l, int* rows, int* cols) const = 0;
 };
 
@@ -141,9 +142,11 @@ class SimImpl final : public SimBase {
     // robot descriptors
     std::vector<RobotDesc> rd(nr);
     std::vector<int> inc_ptr;
-    std::vector<int4> inc_i;
+    std::vector<int4> inc_i, inc_p;
     std::vector<V4<R>> inc_f;
     std::vector<int> spring_out;
+    std::vector<int4> spr_i;
+    std::vector<V4<R>> spr_f;
     long long woff = 0, moff = 0;
     int boff = 0;
     nmax_ = 0;
@@ -174,6 +177,7 @@ class SimImpl final : public SimBase {
       int rid[4] = {45, 46, 34, 36};
       for (int q = 0; q < 4; ++q) d.rot_idx[q] = rid[q];
       if (h.robot_id == 100) CLS_REQUIRE(h.n_v > 46, "robot_id 100 needs >= 47 vertices");
+      CLS_REQUIRE(h.n_v <= 32767 && h.n_out <= 65534, "robot exceeds the packed incidence limits");
       // CSR incidence, springs sorted by endpoint then by spring index
       d.ptr_off = (int)inc_ptr.size();
       d.inc_off = (int)inc_i.size();
@@ -200,11 +204,26 @@ class SimImpl final : public SimBase {
           f.z = (R)h.coef[s];
           f.w = 0;
           inc_f.push_back(f);
+          int4 pk;
+          pk.x = (int)((unsigned)ii.x | ((unsigned)side << 15) | ((unsigned)(ii.w + 1) << 16));
+          float fl = (float)h.len[s], fk = (float)h.stiff[s], fc = (float)h.coef[s];
+          std::memcpy(&pk.y, &fl, 4);
+          std::memcpy(&pk.z, &fk, 4);
+          std::memcpy(&pk.w, &fc, 4);
+          inc_p.push_back(pk);
           ++run;
         }
       }
       inc_ptr.push_back(run);
-      for (int s = 0; s < h.n_s; ++s) spring_out.push_back(h.out[s]);
+      for (int s = 0; s < h.n_s; ++s) {
+        spring_out.push_back(h.out[s]);
+        int4 si;
+        si.x = h.sa[s]; si.y = h.sb[s]; si.z = h.out[s]; si.w = 0;
+        spr_i.push_back(si);
+        V4<R> sf;
+        sf.x = (R)h.len[s]; sf.y = (R)h.stiff[s]; sf.z = (R)h.coef[s]; sf.w = 0;
+        spr_f.push_back(sf);
+      }
       nmax_ = std::max(nmax_, h.n_v);
       p0max = std::max(p0max, round4(h.width[0]));
       omax = std::max(omax, round4(h.n_out));
@@ -212,6 +231,36 @@ class SimImpl final : public SimBase {
       for (int l = 1; l < L_; ++l) dmax = std::max(dmax, round4(h.width[l]));
       amax = std::max(amax, std::max(round4(h.n_out), h.pos_pad));
       for (int l = 1; l < L_; ++l) amax = std::max(amax, round4(h.width[l]));
+    }
+    // optimiser / packing segment tables (all robots, all layers)
+    {
+      long long q = 0, qp = 0;
+      for (int r = 0; r < nr; ++r) {
+        const HostRobot& h = hr_[r];
+        for (int l = 0; l < L_; ++l) {
+          OptSeg o{};
+          o.start = q; o.m_off = m_off_[r][l]; o.c_off = rd[r].w_off[l];
+          o.rows = h.width[l + 1]; o.cols = h.full_cols[l]; o.pitch = rd[r].pitch[l];
+          o.layer = l; o.n_v = h.n_v; o.pos_pad = h.pos_pad;
+          opt_segs_.push_back(o);
+          q += (long long)o.rows * o.cols;
+          OptSeg pk = o;
+          pk.start = qp;
+          pack_segs_.push_back(pk);
+          qp += (long long)o.rows * o.pitch;
+        }
+      }
+      for (int r = 0; r < nr; ++r) {
+        for (int l = 0; l < L_; ++l) {
+          OptSeg o{};
+          o.start = q; o.m_off = rd[r].b_off[l]; o.c_off = rd[r].b_off[l];
+          o.rows = hr_[r].width[l + 1]; o.cols = 1; o.pitch = 1; o.layer = -1;
+          opt_segs_.push_back(o);
+          q += o.rows;
+        }
+      }
+      opt_total_ = q;
+      pack_total_ = qp;
     }
     // env descriptors (internal order)
     std::vector<EnvDesc> ed(E);
@@ -282,14 +331,20 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     CLS_CUDA(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, dev));
-    const size_t static_smem = sizeof(RobotDesc) + sizeof(EnvDesc) + 64;
-    CLS_REQUIRE(fwd_smem_ + static_smem <= (size_t)optin && rev_smem_ + static_smem <= (size_t)optin,
+    // The dynamic shared-memory limit is a per-kernel, process-wide attribute:
+    // raise it once to the device maximum (minus the kernel's static shared
+    // memory) so that handles with different robot sizes never lower it for
+    // one another.
+    cudaFuncAttributes fa{}, ra{};
+    CLS_CUDA(cudaFuncGetAttributes(&fa, fwd_fn()));
+    CLS_CUDA(cudaFuncGetAttributes(&ra, rev_fn()));
+    const size_t fwd_cap = (size_t)optin - fa.sharedSizeBytes;
+    const size_t rev_cap = (size_t)optin - ra.sharedSizeBytes;
+    CLS_REQUIRE(fwd_smem_ <= fwd_cap && rev_smem_ <= rev_cap,
                 "robot too large for one CTA's shared memory (" + std::to_string(rev_smem_) +
-                    " bytes needed)");
-    CLS_CUDA(cudaFuncSetAttribute(ms_forward_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)fwd_smem_));
-    CLS_CUDA(cudaFuncSetAttribute(ms_reverse_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)rev_smem_));
+                    " bytes needed, " + std::to_string(rev_cap) + " available)");
+    CLS_CUDA(cudaFuncSetAttribute(fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_cap));
+    CLS_CUDA(cudaFuncSetAttribute(rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_cap));
     // GEMM tiles (per robot, per layer)
     for (int r = 0; r < nr; ++r) {
       if (count[r] == 0) continue;
@@ -306,7 +361,10 @@ class SimImpl final : public SimBase {
     d_inc_ptr_.alloc(inc_ptr.size());
     d_inc_i_.alloc(std::max<size_t>(1, inc_i.size()));
     d_inc_f_.alloc(std::max<size_t>(1, inc_f.size()));
+    d_inc_p_.alloc(std::max<size_t>(1, inc_p.size()));
     d_spring_out_.alloc(std::max<size_t>(1, spring_out.size()));
+    d_spr_i_.alloc(std::max<size_t>(1, spr_i.size()));
+    d_spr_f_.alloc(std::max<size_t>(1, spr_f.size()));
     d_w_.alloc(woff);
     d_gw_.alloc(woff);
     d_bias_.alloc(boff);
@@ -323,6 +381,7 @@ class SimImpl final : public SimBase {
     d_finv_.alloc(V_);
     d_recx_.alloc((size_t)K_ * V_);
     d_recv_.alloc((size_t)K_ * V_);
+    d_recvinc_.alloc((size_t)K_ * V_);
     d_recin_.alloc((size_t)K_ * in_total_);
     d_recz_.alloc(rec_z_total_);
     d_recdz_.alloc(rec_z_total_);
@@ -342,16 +401,26 @@ class SimImpl final : public SimBase {
     d_adjv_.alloc(V_);
     d_adjh_.alloc(E);
     d_status_.alloc(1);
+#ifdef CLS_PHASE_TIMERS
+    d_phase_.alloc(32);
+    CLS_CUDA(cudaMemset(d_phase_.p, 0, sizeof(unsigned long long) * 32));
+#endif
     d_iter_.alloc(1);
     d_lossenv_.alloc((size_t)E * 8);
     d_tiles_.alloc(std::max<size_t>(1, tiles_host_.size()));
+    d_opt_segs_.alloc(opt_segs_.size());
+    d_pack_segs_.alloc(pack_segs_.size());
+    CLS_CUDA(cudaMemcpy(d_opt_segs_.p, opt_segs_.data(), sizeof(OptSeg) * opt_segs_.size(),
+                        cudaMemcpyHostToDevice));
+    CLS_CUDA(cudaMemcpy(d_pack_segs_.p, pack_segs_.data(), sizeof(OptSeg) * pack_segs_.size(),
+                        cudaMemcpyHostToDevice));
     n_queue_ = (size_t)(1 + 2 * n_seg_max) * E;
     d_queue_.alloc(n_queue_);
     size_t stage = std::max<size_t>((size_t)T_ * E * 3, (size_t)V_ * 3);
     stage = std::max<size_t>(stage, (size_t)moff);
     stage = std::max<size_t>(stage, (size_t)boff);
     d_stage_.alloc(stage);
-    d_tns_.alloc(kAdamBlocks);
+    d_tns_.alloc(1);
     // uploads
     CLS_CUDA(cudaMemcpy(d_robots_.p, rd.data(), sizeof(RobotDesc) * nr, cudaMemcpyHostToDevice));
     CLS_CUDA(cudaMemcpy(d_envs_.p, ed.data(), sizeof(EnvDesc) * E, cudaMemcpyHostToDevice));
@@ -360,10 +429,14 @@ class SimImpl final : public SimBase {
     if (!inc_i.empty()) {
       CLS_CUDA(cudaMemcpy(d_inc_i_.p, inc_i.data(), sizeof(int4) * inc_i.size(), cudaMemcpyHostToDevice));
       CLS_CUDA(cudaMemcpy(d_inc_f_.p, inc_f.data(), sizeof(V4<R>) * inc_f.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_inc_p_.p, inc_p.data(), sizeof(int4) * inc_p.size(), cudaMemcpyHostToDevice));
     }
-    if (!spring_out.empty())
+    if (!spring_out.empty()) {
       CLS_CUDA(cudaMemcpy(d_spring_out_.p, spring_out.data(), sizeof(int) * spring_out.size(),
                           cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_spr_i_.p, spr_i.data(), sizeof(int4) * spr_i.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_spr_f_.p, spr_f.data(), sizeof(V4<R>) * spr_f.size(), cudaMemcpyHostToDevice));
+    }
     if (!tiles_host_.empty())
       CLS_CUDA(cudaMemcpy(d_tiles_.p, tiles_host_.data(), sizeof(GemmTile) * tiles_host_.size(),
                           cudaMemcpyHostToDevice));
@@ -398,6 +471,18 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaDeviceSynchronize());
   }
 
+  // kernel instances by block size (the register budget follows MAXT)
+  using FwdFn = void (*)(MsArgs<R>, int, int, int, int);
+  using RevFn = void (*)(MsArgs<R>, int, int, int);
+  FwdFn fwd_fn() const {
+    return threads_ <= 256 ? ms_forward_kernel<R, 256>
+                           : (threads_ <= 512 ? ms_forward_kernel<R, 512> : ms_forward_kernel<R, 1024>);
+  }
+  RevFn rev_fn() const {
+    return threads_ <= 256 ? ms_reverse_kernel<R, 256>
+                           : (threads_ <= 512 ? ms_reverse_kernel<R, 512> : ms_reverse_kernel<R, 1024>);
+  }
+
   int auto_threads() const {
     // enough warps for the per-row MLP products and the vertex loops; more
     // threads than that only adds barrier cost
@@ -407,7 +492,7 @@ class SimImpl final : public SimBase {
       for (int l = 1; l <= L_; ++l) work = std::max(work, h.width[l] * 4);
     }
     int t = 128;
-    while (t < 1024 && t < work) t *= 2;
+    while (t < 512 && t < work) t *= 2;
     return t;
   }
 
@@ -454,7 +539,10 @@ class SimImpl final : public SimBase {
     a.inc_ptr = d_inc_ptr_.p;
     a.inc_i = d_inc_i_.p;
     a.inc_f = d_inc_f_.p;
+    a.inc_p = d_inc_p_.p;
     a.spring_out = d_spring_out_.p;
+    a.spr_i = d_spr_i_.p;
+    a.spr_f = d_spr_f_.p;
     a.w = d_w_.p;
     a.bias = d_bias_.p;
     a.sin_table = d_sin_.p;
@@ -464,6 +552,7 @@ class SimImpl final : public SimBase {
     a.fin_v = d_finv_.p;
     a.rec_x = d_recx_.p;
     a.rec_v = d_recv_.p;
+    a.rec_vinc = d_recvinc_.p;
     a.rec_in = d_recin_.p;
     a.rec_z = d_recz_.p;
     a.rec_dz = d_recdz_.p;
@@ -482,6 +571,7 @@ class SimImpl final : public SimBase {
     a.adj_v = d_adjv_.p;
     a.adj_h = d_adjh_.p;
     a.status = d_status_.p;
+    a.phase = d_phase_.p;
     return a;
   }
 
@@ -607,7 +697,7 @@ class SimImpl final : public SimBase {
     qslot_ = 0;
     each_launch(per_env, a, qslot_, [&](const MsArgs<R>& b, int grid) {
       timed(PK_FWD, [&] {
-        ms_forward_kernel<R><<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
+        fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
       });
     });
     CLS_CUDA(cudaGetLastError());
@@ -666,12 +756,12 @@ class SimImpl final : public SimBase {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
       each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
         timed(PK_RECOMP, [&] {
-          ms_forward_kernel<R><<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+          fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
         });
       });
       each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
         timed(PK_REV, [&] {
-          ms_reverse_kernel<R><<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
+          rev_fn()<<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
         });
       });
       if (!tiles_host_.empty())
@@ -684,61 +774,40 @@ class SimImpl final : public SimBase {
     bwd_done_ = true;
   }
 
-  void adam_device(int iter_or_neg, bool apply) {
+  void adam_device(int iter_or_neg, bool apply, double* tns_dev) {
     // iteration taken from d_iter_ when iter_or_neg < 0 (graph replays)
-    for (size_t r = 0; r < hr_.size(); ++r) {
-      const HostRobot& h = hr_[r];
-      const RobotDesc& d = rd_host_[r];
-      for (int l = 0; l < L_; ++l) {
-        timed(PK_ADAM, [&] {
-          ms_adam_kernel<R><<<kAdamBlocks - 1, 256, 0, stream>>>(
-              d_wm_.p, d_wmm_.p, d_wmv_.p, d_gw_.p, m_off_[r][l], d.w_off[l], h.width[l + 1],
-              h.full_cols[l], d.pitch[l], l, h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v,
-              p_.duplicate_h, p_.duplicate_c, p_.learning_rate, p_.adam_b1, p_.adam_b2,
-              iter_or_neg, d_iter_.p, apply ? 1 : 0, d_tns_.p);
-        });
-        timed(PK_ADAM, [&] {
-          ms_adam_bias_kernel<R><<<1, 256, 0, stream>>>(
-              d_bias_.p + d.b_off[l], d_bm_.p + d.b_off[l], d_bv_.p + d.b_off[l], d_gb_.p + d.b_off[l],
-              h.width[l + 1], p_.learning_rate, p_.adam_b1, p_.adam_b2, iter_or_neg, d_iter_.p,
-              apply ? 1 : 0, d_tns_.p + kAdamBlocks - 1);
-        });
-        pack_layer((int)r, l);
-      }
-    }
+    const int chunk = 256 * 16;
+    const int blocks = (int)((opt_total_ + chunk - 1) / chunk);
+    if (tns_dev) CLS_CUDA(cudaMemsetAsync(tns_dev, 0, sizeof(double), stream));
+    timed(PK_ADAM, [&] {
+      ms_adam_all_kernel<R><<<std::max(1, blocks), 256, 0, stream>>>(
+          d_opt_segs_.p, (int)opt_segs_.size(), opt_total_, chunk, d_wm_.p, d_wmm_.p, d_wmv_.p,
+          d_gw_.p, d_bias_.p, d_bm_.p, d_bv_.p, d_gb_.p, p_.n_sin_waves, p_.duplicate_v,
+          p_.duplicate_h, p_.duplicate_c, p_.learning_rate, p_.adam_b1, p_.adam_b2, iter_or_neg,
+          d_iter_.p, apply ? 1 : 0, tns_dev);
+    });
+    if (apply) pack_all();
     CLS_CUDA(cudaGetLastError());
+  }
+
+  void pack_all() {
+    const int chunk = 256 * 16;
+    const int blocks = (int)((pack_total_ + chunk - 1) / chunk);
+    timed(PK_ADAM, [&] {
+      ms_pack_all_kernel<R><<<std::max(1, blocks), 256, 0, stream>>>(
+          d_pack_segs_.p, (int)pack_segs_.size(), pack_total_, chunk, d_wm_.p, d_w_.p,
+          p_.n_sin_waves, p_.duplicate_v, p_.duplicate_h, p_.duplicate_c);
+    });
   }
 
   void adam(int iter, double* tns) override {
     CLS_REQUIRE(bwd_done_, "cls_adam_step needs gradients (cls_backward) first");
-    if (tns) *tns = tns_sum();
-    adam_device(iter, true);
-  }
-
-  double tns_sum() {
-    // squared norm of the full-layout gradient (Model.get_TNS)
-    double s = 0;
-    std::vector<double> part(kAdamBlocks);
-    for (size_t r = 0; r < hr_.size(); ++r) {
-      const HostRobot& h = hr_[r];
-      const RobotDesc& d = rd_host_[r];
-      for (int l = 0; l < L_; ++l) {
-        ms_adam_kernel<R><<<kAdamBlocks - 1, 256, 0, stream>>>(
-            d_wm_.p, d_wmm_.p, d_wmv_.p, d_gw_.p, m_off_[r][l], d.w_off[l], h.width[l + 1],
-            h.full_cols[l], d.pitch[l], l, h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v,
-            p_.duplicate_h, p_.duplicate_c, p_.learning_rate, p_.adam_b1, p_.adam_b2, 0, d_iter_.p,
-            0, d_tns_.p);
-        ms_adam_bias_kernel<R><<<1, 256, 0, stream>>>(
-            d_bias_.p + d.b_off[l], d_bm_.p + d.b_off[l], d_bv_.p + d.b_off[l], d_gb_.p + d.b_off[l],
-            h.width[l + 1], p_.learning_rate, p_.adam_b1, p_.adam_b2, 0, d_iter_.p, 0,
-            d_tns_.p + kAdamBlocks - 1);
-        CLS_CUDA(cudaMemcpyAsync(part.data(), d_tns_.p, sizeof(double) * kAdamBlocks,
-                                 cudaMemcpyDeviceToHost, stream));
-        CLS_CUDA(cudaStreamSynchronize(stream));
-        for (double q : part) s += q;
-      }
+    adam_device(iter, true, tns ? d_tns_.p : nullptr);
+    if (tns) {
+      CLS_CUDA(cudaMemcpyAsync(&tns_host_, d_tns_.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      *tns = tns_host_;
     }
-    return s;
   }
 
   void clear_adam() override {
@@ -978,7 +1047,7 @@ class SimImpl final : public SimBase {
       forward(steps, false, false);
       loss_device();
       backward(false);
-      if (with_adam) adam_device(-1, true);
+      if (with_adam) adam_device(-1, true, d_tns_.p);
     } catch (...) {
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(stream, &g);
@@ -1012,7 +1081,6 @@ class SimImpl final : public SimBase {
     if (cols) *cols = hr_[r].full_cols[l];
   }
 
-  static constexpr int kAdamBlocks = 129;
 
  private:
   std::vector<HostRobot> hr_;
@@ -1028,6 +1096,9 @@ class SimImpl final : public SimBase {
   std::vector<EnvDesc> ed_host_;
   std::vector<RobotDesc> rd_host_;
   std::vector<GemmTile> tiles_host_;
+  std::vector<OptSeg> opt_segs_, pack_segs_;
+  long long opt_total_ = 0, pack_total_ = 0;
+  double tns_host_ = 0;
   std::vector<std::vector<long long>> m_off_;
   bool keep_x_ = false, fwd_done_ = false, bwd_done_ = false, eval_ = false, per_env_ = false;
   bool graph_adam_ = false, capturing_ = false;
@@ -1039,14 +1110,24 @@ class SimImpl final : public SimBase {
   DevBuf<RobotDesc> d_robots_;
   DevBuf<EnvDesc> d_envs_;
   DevBuf<int> d_order_, d_queue_, d_inc_ptr_, d_spring_out_, d_status_, d_iter_;
-  DevBuf<int4> d_inc_i_;
-  DevBuf<V4<R>> d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_obsc_, d_xfull_,
+  DevBuf<int4> d_inc_i_, d_spr_i_, d_inc_p_;
+  DevBuf<V4<R>> d_spr_f_, d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_recvinc_, d_obsc_, d_xfull_,
       d_tv_, d_init_, d_adjx_, d_adjv_;
   DevBuf<R> d_w_, d_gw_, d_bias_, d_gb_, d_bm_, d_bv_, d_wm_, d_wmm_, d_wmv_, d_sin_, d_recin_,
       d_recz_, d_recdz_, d_obsh_, d_obsu_, d_obsr_, d_actfull_, d_th_, d_tc_, d_adjh_;
   DevBuf<unsigned char> d_head_;
+  DevBuf<unsigned long long> d_phase_;
+
+ public:
+  void phase_read(unsigned long long* out) override {
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    if (d_phase_.p) CLS_CUDA(cudaMemcpy(out, d_phase_.p, sizeof(unsigned long long) * 32, cudaMemcpyDeviceToHost));
+  }
+
+ private:
   DevBuf<double> d_lossenv_, d_stage_, d_tns_;
   DevBuf<GemmTile> d_tiles_;
+  DevBuf<OptSeg> d_opt_segs_, d_pack_segs_;
 };
 
 }  // namespace cls
@@ -1318,6 +1399,13 @@ int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset)
       for (int k = 0; k < cls::PK_COUNT; ++k) launches[k] = l[k];
   });
 }
+
+#ifdef CLS_PHASE_TIMERS
+// profiling builds only: per-phase clock totals (32 slots)
+int cls_phase_read(cls_sim* sim, unsigned long long* out) {
+  return guarded(sim, [&](cls::SimBase& s) { s.phase_read(out); });
+}
+#endif
 
 int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam) {
   return guarded(sim, [&](cls::SimBase& s) { s.graph_capture(steps, with_adam != 0); });

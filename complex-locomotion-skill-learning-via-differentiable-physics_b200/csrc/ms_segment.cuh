@@ -99,8 +99,8 @@ __device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
 // ---------------------------------------------------------------- forward
 // Advances every env from t_begin (state in checkpoint slot src_slot) through
 // t_end (exclusive), i.e. runs pre_advance/nn_input/forward/advance for each t.
-template <typename R>
-__global__ void __launch_bounds__(1024, 1)
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
 ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
   extern __shared__ __align__(256) char smem_raw[];
   __shared__ RobotDesc rb;
@@ -123,6 +123,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
     R hprev = 0;
     if ((mode & FWD_OBS) && t_begin > 0) hprev = a.obs_height[(size_t)(t_begin - 1) * a.n_envs + e];
     __syncthreads();
+    CLS_PHASE_START();
     for (int t = t_begin; t < t_end; ++t) {
       // -- checkpoints, records, trajectory
       if ((mode & FWD_CKPT) && t > t_begin && (t % a.K) == 0) {
@@ -150,6 +151,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
         c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
       }
       block_sum<R, 3>(c, s.red);
+      CLS_PHASE(a, 10);
       if (mode & FWD_OBS) {
         // compute_height / upper height (solver_mass_spring.py:158-173)
         R lo = R(10), hi = R(-10);
@@ -199,6 +201,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
         hprev = s.red[0];
         __syncthreads();
       }
+      CLS_PHASE(a, 11);
       // -- nn_input (taichi_env.py:149-183) in the compact column order
       {
         const int p0 = rb.pos_pad, nc = rb.n_c, pitch0 = rb.pitch[0];
@@ -218,6 +221,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
         }
       }
       __syncthreads();
+      CLS_PHASE(a, 12);
       // -- MLP (nn.py:130-146): z = W a, a' = act(z + b)
       R* out = nullptr;
       for (int l = 0; l < L; ++l) {
@@ -233,6 +237,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
         const int padto = (l + 1 < L) ? rb.pitch[l + 1] : ((nout + 3) & ~3);
         for (int q = nout + tid; q < padto; q += nt) y[q] = 0;
         __syncthreads();
+        CLS_PHASE(a, 13 + (l < 2 ? l : 2));
         out = y;
       }
       if ((mode & FWD_OBS) && a.act_full) {
@@ -240,10 +245,14 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
         for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
       }
       // -- apply_spring_force (gather form) then advance_toi
-      for (int i = tid; i < N; i += nt) s.vinc[i] = gather_vinc<R>(a, rb, i, s.xs, s.vs, out);
+      gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc,
+                         (mode & FWD_RECORD) ? a.rec_vinc + (size_t)(t - t_begin) * a.v_total + ed.v_off
+                                             : nullptr);
       __syncthreads();
+      CLS_PHASE(a, 16);
       for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
       __syncthreads();
+      CLS_PHASE(a, 17);
     }
     // state after the last processed step
     if (mode & FWD_OBS) {
@@ -359,62 +368,88 @@ __device__ __forceinline__ R seed_upper(const MsArgs<R>& a, int t, int e, R Br) 
 // -------------------------------------------------------------- spring adjoint
 // Accumulates, for vertex i, the adjoint of every incident spring's impulse:
 // d x_i, d v_i; for a-side entries also d actuation (-> gout).
+// Adjoint of apply_spring_force(t), one thread per spring: recompute the
+// spring's impulse, pull d v_inc of both endpoints, and push d x, d v into both
+// endpoints and d actuation into the spring's controller output with shared-
+// memory atomics (the reference scatters its forward with atomics too, so the
+// order of these sums is not fixed; they only change rounding).  Spring
+// records are fetched four at a time with the evict_last L2 policy.
 template <typename R>
-__device__ __forceinline__ void spring_adjoint_vertex(const MsArgs<R>& a, const RobotDesc& rb, int i,
-                                                      const V4<R>* xs, const V4<R>* vs,
-                                                      const V4<R>* gvinc, const R* outv, R* gout,
-                                                      R act_seed_scale, R act_lim, bool act_seed,
-                                                      R gxi[3], R gvi[3]) {
-  const int beg = a.inc_ptr[rb.ptr_off + i], end = a.inc_ptr[rb.ptr_off + i + 1];
-  for (int q = beg; q < end; ++q) {
-    const int4 ii = a.inc_i[rb.inc_off + q];
-    const V4<R> ff = a.inc_f[rb.inc_off + q];
-    const int o = ii.x;
-    const bool side_a = (ii.y == 0);
-    const V4<R> xa = side_a ? xs[i] : xs[o], xb = side_a ? xs[o] : xs[i];
-    const V4<R> va = side_a ? vs[i] : vs[o], vb = side_a ? vs[o] : vs[i];
-    const V4<R> ga = side_a ? gvinc[i] : gvinc[o], gb = side_a ? gvinc[o] : gvinc[i];
-    const R act = ii.w >= 0 ? outv[ii.w] : R(0);
-    // forward recompute
-    const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
-    const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
-    const R r8 = dsqrt<R>(n2 + R(1e-8));
-    const R length = r8 + R(1e-4);
-    const R target = ff.x * (R(1) + ff.z * act);
-    const R sc = a.dt * (length - target) * ff.y / length;
-    const R r = dsqrt<R>(n2), invlen = R(1) / r;
-    const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
-    const R dv0 = va.x - vb.x, dv1 = va.y - vb.y, dv2 = va.z - vb.z;
-    const R vrel = dv0 * n0 + dv1 * n1 + dv2 * nz;
-    // g_imp = g v_inc[b] - g v_inc[a]
-    const R gi0 = gb.x - ga.x, gi1 = gb.y - ga.y, gi2 = gb.z - ga.z;
-    const R gsc = gi0 * d0 + gi1 * d1 + gi2 * d2;
-    const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
-    const R cdv = a.dashpot * vrel;
-    R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
-    R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
-    const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
-    const R gr = -ginv / (r * r);
-    gd0 += gr * d0 / r; gd1 += gr * d1 / r; gd2 += gr * d2 / r;
-    const R glen = gsc * a.dt * ff.y * target / (length * length);
-    gd0 += glen * d0 / r8; gd1 += glen * d1 / r8; gd2 += glen * d2 / r8;
-    const R sgn = side_a ? R(1) : R(-1);
-    gxi[0] += sgn * gd0; gxi[1] += sgn * gd1; gxi[2] += sgn * gd2;
-    gvi[0] += sgn * gvrel * n0; gvi[1] += sgn * gvrel * n1; gvi[2] += sgn * gvrel * nz;
-    if (side_a && ii.w >= 0) {
-      const R gtarget = -gsc * a.dt * ff.y / length;
-      R gact = gtarget * ff.x * ff.z;
-      if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
-        if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
+__device__ __forceinline__ void spring_adjoint_all(const MsArgs<R>& a, const RobotDesc& rb,
+                                                   const V4<R>* xs, const V4<R>* vs,
+                                                   const V4<R>* gvinc, const R* outv, R* gout,
+                                                   V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
+                                                   bool act_seed) {
+  const unsigned long long pol = policy_evict_last();
+  const int4* ip = a.spr_i + rb.spr_off;
+  const V4<R>* fp = a.spr_f + rb.spr_off;
+  const int S = rb.n_s, nt = blockDim.x;
+  for (int s0 = threadIdx.x; s0 < S; s0 += 4 * nt) {
+    int4 iiv[4];
+    V4<R> ffv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = (s0 + u * nt < S) ? s0 + u * nt : s0;
+      iiv[u] = ldg_i4_hint(ip + q, pol);
+      ffv[u] = ldg4_hint<R>(fp + q, pol);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (s0 + u * nt >= S) break;
+      const int4 ii = iiv[u];
+      const V4<R> ff = ffv[u];
+      const int ia = ii.x, ib = ii.y;
+      const V4<R> xa = xs[ia], xb = xs[ib], va = vs[ia], vb = vs[ib];
+      const V4<R> ga = gvinc[ia], gb = gvinc[ib];
+      const R act = ii.z >= 0 ? outv[ii.z] : R(0);
+      // forward recompute (solver_mass_spring.py:89-103)
+      const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
+      const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
+      const R r8 = sqrt_s<R>(n2 + R(1e-8));
+      const R length = r8 + R(1e-4);
+      const R inv_length = rcp_s<R>(length);
+      const R target = ff.x * (R(1) + ff.z * act);
+      const R sc = a.dt * (length - target) * ff.y * inv_length;
+      const R invlen = rsqrt_s<R>(n2);
+      const R inv_r8 = rcp_s<R>(r8);
+      const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
+      const R dv0 = va.x - vb.x, dv1 = va.y - vb.y, dv2 = va.z - vb.z;
+      const R vrel = dv0 * n0 + dv1 * n1 + dv2 * nz;
+      // impulse enters v_inc[b] with +, v_inc[a] with -
+      const R gi0 = gb.x - ga.x, gi1 = gb.y - ga.y, gi2 = gb.z - ga.z;
+      const R gsc = gi0 * d0 + gi1 * d1 + gi2 * d2;
+      const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
+      const R cdv = a.dashpot * vrel;
+      const R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
+      R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
+      // invlen = 1 / r, r = |dist|:  d r = -d invlen / r^2, d dist += d r * dist / r
+      const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
+      const R gr_r = -ginv * invlen * invlen * invlen;
+      gd0 += gr_r * d0; gd1 += gr_r * d1; gd2 += gr_r * d2;
+      // sc = dt (length - target) k / length:  d length = d sc dt k target / length^2
+      const R glen = gsc * a.dt * ff.y * target * inv_length * inv_length;
+      const R glen_r8 = glen * inv_r8;
+      gd0 += glen_r8 * d0; gd1 += glen_r8 * d1; gd2 += glen_r8 * d2;
+      atomicAdd(&gx[ia].x, gd0); atomicAdd(&gx[ia].y, gd1); atomicAdd(&gx[ia].z, gd2);
+      atomicAdd(&gx[ib].x, -gd0); atomicAdd(&gx[ib].y, -gd1); atomicAdd(&gx[ib].z, -gd2);
+      const R h0 = gvrel * n0, h1 = gvrel * n1, h2 = gvrel * nz;
+      atomicAdd(&gv[ia].x, h0); atomicAdd(&gv[ia].y, h1); atomicAdd(&gv[ia].z, h2);
+      atomicAdd(&gv[ib].x, -h0); atomicAdd(&gv[ib].y, -h1); atomicAdd(&gv[ib].z, -h2);
+      if (ii.z >= 0) {
+        const R gtarget = -gsc * a.dt * ff.y * inv_length;
+        R gact = gtarget * ff.x * ff.z;
+        if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
+          if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
+        }
+        atomicAdd(gout + ii.z, gact);
       }
-      atomicAdd(gout + ii.w, gact);
     }
   }
 }
 
 // ---------------------------------------------------------------- reverse
-template <typename R>
-__global__ void __launch_bounds__(1024, 1)
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
 ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
   extern __shared__ __align__(256) char smem_raw[];
   __shared__ RobotDesc rb;
@@ -455,6 +490,8 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
     const R* wout = a.w + rb.w_off[L - 1];
     const R* bout = a.bias + rb.b_off[L - 1];
     const int nout = rb.n_out;
+    (void)wout;
+    CLS_PHASE_START();
     for (int t = t_end - 1; t >= t_begin; --t) {
       const int kk = t - t_begin;
       {
@@ -468,9 +505,14 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
         }
       }
       __syncthreads();
-      // v_inc[t] recompute (into gvinc as scratch)
-      for (int i = tid; i < N; i += nt) s.gvinc[i] = gather_vinc<R>(a, rb, i, s.xs, s.vs, s.bufA);
+      CLS_PHASE(a, 0);
+      // v_inc[t] as recorded by the recompute pass (into gvinc as scratch)
+      {
+        const V4<R>* rvi = a.rec_vinc + (size_t)kk * a.v_total + ed.v_off;
+        for (int i = tid; i < N; i += nt) s.gvinc[i] = rvi[i];
+      }
       __syncthreads();
+      CLS_PHASE(a, 1);
       // adjoint of advance_toi(t + 1)
       for (int i = tid; i < N; i += nt) {
         const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
@@ -513,25 +555,18 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
         s.gvinc[i] = gvi;
       }
       __syncthreads();
+      CLS_PHASE(a, 2);
       // adjoint of apply_spring_force(t)
       {
         const size_t o = (size_t)t * a.n_envs + e;
         const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < a.steps && a.th[o] < R(0.1 + 1e-4);
         const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
         const R act_scale = R(10) / R(a.steps) / Br / R(rb.n_s);
-        for (int i = tid; i < N; i += nt) {
-          R gxi[3] = {0, 0, 0}, gvi[3] = {0, 0, 0};
-          spring_adjoint_vertex<R>(a, rb, i, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, act_scale, lim,
-                                   act_seed, gxi, gvi);
-          V4<R> g = s.gx[i];
-          g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
-          s.gx[i] = g;
-          V4<R> h = s.gv[i];
-          h.x += gvi[0]; h.y += gvi[1]; h.z += gvi[2];
-          s.gv[i] = h;
-        }
+        spring_adjoint_all<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
+                              act_seed);
       }
       __syncthreads();
+      CLS_PHASE(a, 3);
       // adjoint of the MLP: output layer first
       {
         const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
@@ -543,6 +578,7 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
         }
       }
       __syncthreads();
+      CLS_PHASE(a, 4);
       for (int l = L - 1; l >= 1; --l) {
         const int nin = rb.width[l];
         dense_transposed<R>(a.w + rb.w_off[l], rb.pitch[l], rb.width[l + 1], nin, s.dz, s.part,
@@ -557,9 +593,11 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
         }
         __syncthreads();
       }
+      CLS_PHASE(a, 5);
       // first layer: only the position columns carry state dependence
       dense_transposed<R>(a.w + rb.w_off[0], rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
                           reinterpret_cast<V4<R>*>(s.bufA));
+      CLS_PHASE(a, 6);
       // adjoint of nn_input + compute_center + loss seeds at t
       {
         R gc[3] = {0, 0, 0};
@@ -580,6 +618,7 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
           s.gx[i] = g;
         }
       }
+      CLS_PHASE(a, 7);
       // adjoint of compute_height (running max of the lowest point) and upper height
       if (a.loss_mask & (LOSS_HEIGHT | LOSS_CRAWL)) {
         const R gh = seed_height<R>(a, t, e, Br) + hcarry;
@@ -610,6 +649,7 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
         }
       }
       __syncthreads();
+      CLS_PHASE(a, 8);
     }
     for (int i = tid; i < N; i += nt) {
       a.adj_x[ed.v_off + i] = s.gx[i];
@@ -855,77 +895,6 @@ __global__ void ms_pack_weights_kernel(const R* __restrict__ master, long long m
   }
 }
 
-// Adam on the reference-layout master weights (nn.py:184-191) with the
-// gradient read from the compact layout; also the per-block partial sums of
-// grad^2 over the full layout (Model.get_TNS, nn.py:173-182).
-template <typename R>
-__global__ void ms_adam_kernel(R* __restrict__ master, R* __restrict__ m, R* __restrict__ v,
-                               const R* __restrict__ gc, long long m_off, long long c_off, int rows,
-                               int n_in_full, int pitch, int layer, int N, int pos_pad, int n_sin,
-                               int dup_v, int dup_h, int dup_c, double lr, double b1, double b2,
-                               int iter, const int* iter_dev, int apply, double* tns_part) {
-  __shared__ double red[32];
-  if (iter < 0) iter = *iter_dev;
-  const double bc1 = 1.0 - pow(b1, (double)(iter + 1)), bc2 = 1.0 - pow(b2, (double)(iter + 1));
-  const long long total = (long long)rows * n_in_full;
-  double tns = 0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q / n_in_full), j = (int)(q % n_in_full);
-    int c = j;
-    if (layer == 0) c = full_to_compact(j, N, pos_pad, n_sin, dup_v, dup_h, dup_c);
-    const R g = c >= 0 ? gc[c_off + (long long)i * pitch + c] : R(0);
-    tns += (double)g * (double)g;
-    if (apply) {
-      const long long w = m_off + q;
-      const R mm = R(b1) * m[w] + R(1 - b1) * g;
-      const R vv = R(b2) * v[w] + R(1 - b2) * g * g;
-      m[w] = mm;
-      v[w] = vv;
-      const R mc = mm / R(bc1), vc = vv / R(bc2);
-      master[w] -= (R(lr) * mc) / (sqrt(vc) + R(1e-8));
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) tns += __shfl_xor_sync(0xffffffffu, tns, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tns;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    tns_part[blockIdx.x] = s;
-  }
-}
-
-// bias Adam (no column map)
-template <typename R>
-__global__ void ms_adam_bias_kernel(R* __restrict__ b, R* __restrict__ m, R* __restrict__ v,
-                                    const R* __restrict__ g, int n, double lr, double b1, double b2,
-                                    int iter, const int* iter_dev, int apply, double* tns_part) {
-  __shared__ double red[32];
-  if (iter < 0) iter = *iter_dev;
-  const double bc1 = 1.0 - pow(b1, (double)(iter + 1)), bc2 = 1.0 - pow(b2, (double)(iter + 1));
-  double tns = 0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const R gg = g[q];
-    tns += (double)gg * (double)gg;
-    if (apply) {
-      const R mm = R(b1) * m[q] + R(1 - b1) * gg;
-      const R vv = R(b2) * v[q] + R(1 - b2) * gg * gg;
-      m[q] = mm;
-      v[q] = vv;
-      b[q] -= (R(lr) * (mm / R(bc1))) / (sqrt(vv / R(bc2)) + R(1e-8));
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) tns += __shfl_xor_sync(0xffffffffu, tns, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tns;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    tns_part[blockIdx.x] = s;
-  }
-}
-
 // grads of the reference layout from the compact layout (for export)
 template <typename R>
 __global__ void ms_unpack_grad_kernel(const R* __restrict__ gc, long long c_off, int pitch, int rows,
@@ -972,6 +941,135 @@ __global__ void ms_v4_to_xyz_kernel(const V4<R>* __restrict__ in, double* __rest
        q += (long long)gridDim.x * blockDim.x) {
     const V4<R> r = in[q];
     out[3 * q] = r.x; out[3 * q + 1] = r.y; out[3 * q + 2] = r.z;
+  }
+}
+
+// ------------------------------------------------ whole-model optimiser step
+// Adam (Model.adam_update, nn.py:184-191) on the reference-layout master
+// weights, with the gradient read from the compact layout, plus the squared
+// gradient norm over the reference layout (Model.get_TNS, nn.py:173-182).
+// One launch updates every weight and bias tensor of every robot type.  The
+// tensors are laid end to end in a global element index; OptSeg describes one
+// tensor.  Each CTA takes a contiguous chunk of that index, finds its first
+// tensor by binary search and walks forward.
+struct OptSeg {
+  long long start;      // first global element index
+  long long m_off;      // offset in the master / moment arrays (reference layout)
+  long long c_off;      // offset in the compact gradient (weights) or gb (biases)
+  int rows, cols, pitch, layer;   // layer < 0: bias vector
+  int n_v, pos_pad;
+};
+
+__device__ __forceinline__ int find_seg(const OptSeg* segs, int n, long long q) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].start <= q) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+ms_adam_all_kernel(const OptSeg* __restrict__ segs, int n_segs, long long total, int chunk,
+                   R* __restrict__ wm, R* __restrict__ wmm, R* __restrict__ wmv,
+                   const R* __restrict__ gw, R* __restrict__ bias, R* __restrict__ bm,
+                   R* __restrict__ bv, const R* __restrict__ gb, int n_sin, int dup_v, int dup_h,
+                   int dup_c, double lr, double b1, double b2, int iter, const int* iter_dev,
+                   int apply, double* tns) {
+  __shared__ int s_seg;
+  __shared__ double red[8];
+  if (iter < 0) iter = *iter_dev;
+  const double bc1 = 1.0 - pow(b1, (double)(iter + 1)), bc2 = 1.0 - pow(b2, (double)(iter + 1));
+  const long long q0 = (long long)blockIdx.x * chunk;
+  if (q0 >= total) return;
+  if (threadIdx.x == 0) s_seg = find_seg(segs, n_segs, q0);
+  __syncthreads();
+  int sg = s_seg;
+  double acc = 0;
+  const long long q1 = q0 + chunk < total ? q0 + chunk : total;
+  for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+    while (sg + 1 < n_segs && segs[sg + 1].start <= q) ++sg;
+    const OptSeg& o = segs[sg];
+    const long long e = q - o.start;
+    R g;
+    R *w, *m, *v;
+    if (o.layer < 0) {
+      g = gb[o.c_off + e];
+      w = bias + o.m_off + e; m = bm + o.m_off + e; v = bv + o.m_off + e;
+    } else {
+      const int i = (int)(e / o.cols), j = (int)(e % o.cols);
+      int c = j;
+      if (o.layer == 0) c = full_to_compact(j, o.n_v, o.pos_pad, n_sin, dup_v, dup_h, dup_c);
+      g = c >= 0 ? gw[o.c_off + (long long)i * o.pitch + c] : R(0);
+      w = wm + o.m_off + e; m = wmm + o.m_off + e; v = wmv + o.m_off + e;
+    }
+    acc += (double)g * (double)g;
+    if (apply) {
+      const R mm = R(b1) * *m + R(1 - b1) * g;
+      const R vv = R(b2) * *v + R(1 - b2) * g * g;
+      *m = mm;
+      *v = vv;
+      *w -= (R(lr) * (mm / R(bc1))) / (sqrt(vv / R(bc2)) + R(1e-8));
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    if (tns) atomicAdd(tns, t);
+  }
+}
+
+// Compact weights of every robot and layer from the reference-layout master
+// (one launch; segments index the compact layout, rows x pitch each).
+template <typename R>
+__global__ void __launch_bounds__(256)
+ms_pack_all_kernel(const OptSeg* __restrict__ segs, int n_segs, long long total, int chunk,
+                   const R* __restrict__ master, R* __restrict__ wc, int n_sin, int dup_v,
+                   int dup_h, int dup_c) {
+  __shared__ int s_seg;
+  const long long q0 = (long long)blockIdx.x * chunk;
+  if (q0 >= total) return;
+  if (threadIdx.x == 0) s_seg = find_seg(segs, n_segs, q0);
+  __syncthreads();
+  int sg = s_seg;
+  const long long q1 = q0 + chunk < total ? q0 + chunk : total;
+  for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+    while (sg + 1 < n_segs && segs[sg + 1].start <= q) ++sg;
+    const OptSeg& o = segs[sg];
+    const long long e = q - o.start;
+    const int i = (int)(e / o.pitch), c = (int)(e % o.pitch);
+    const R* row = master + o.m_off + (long long)i * o.cols;
+    R s = 0;
+    const int N = o.n_v, pos_pad = o.pos_pad;
+    if (o.layer > 0) {
+      s = c < o.cols ? row[c] : R(0);
+    } else if (c < 3 * N) {
+      const int vtx = c / 3, d = c - 3 * vtx;
+      s = row[n_sin + 6 * vtx + d];
+    } else if (c >= pos_pad && c < pos_pad + n_sin) {
+      s = row[c - pos_pad];
+    } else if (c >= pos_pad + n_sin) {
+      const int g = c - pos_pad - n_sin;
+      const int base = n_sin + 6 * N;
+      int gi = 0;
+      if (dup_v > 0) {
+        if (g < 2)
+          for (int m = 0; m < dup_v; ++m) s += row[base + 2 * m + g];
+        gi = 2;
+      }
+      if (dup_h > 0) {
+        if (g == gi)
+          for (int m = 0; m < dup_h; ++m) s += row[base + 2 * dup_v + m];
+        gi += 1;
+      }
+      if (dup_c > 0 && g == gi)
+        for (int m = 0; m < dup_c; ++m) s += row[base + 2 * dup_v + dup_h + m];
+    }
+    wc[o.c_off + e] = s;
   }
 }
 

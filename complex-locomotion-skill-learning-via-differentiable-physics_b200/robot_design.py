@@ -68,7 +68,9 @@ class CubeLattice:
             return
         self._pairs.add((a, b))
         pa, pb = self.objects[a], self.objects[b]
-        length = math.sqrt(sum((pa[d] - pb[d]) ** 2 for d in range(3)))
+        # rest length = initial distance, evaluated as the reference does
+        # (power 0.5 of the squared sum, robot_design.py:346-348)
+        length = ((pa[0] - pb[0]) ** 2 + (pa[1] - pb[1]) ** 2 + (pa[2] - pb[2]) ** 2) ** 0.5
         self.springs.append([a, b, length, self.stiffness if stiffness is None else stiffness,
                              actuation])
 
@@ -133,7 +135,12 @@ def _robot_d(L, act, skeleton):   # spider, id 103 (:470-505)
     motor = lambda a, b: (a, b) in motors or (b, a) in motors  # noqa: E731
     for a, b in data["links"]:
         L.spring(a, b, act if motor(a, b) else 0.0)
-    for a, b in _SPIDER_MOTORS + _SPIDER_EXTRA:
+    # the reference walks its motor set (a set display of constant tuples)
+    # first; a set display of the same tuples iterates in the same
+    # hash-determined order
+    motor_set = {(9, 21), (36, 24), (29, 26), (14, 11), (14, 26), (10, 9), (29, 11), (25, 24),
+                 (25, 26), (36, 9), (21, 24), (10, 11)}
+    for a, b in list(motor_set) + _SPIDER_EXTRA:
         L.spring(a, b, act if motor(a, b) else 0.0)
 
 
@@ -177,14 +184,16 @@ def quadruped_lattice(stiffness=3e4, actuation=0.25, n_actuated=40):
     return objects, springs
 
 
-def spider_lattice(stiffness=3e4, actuation=0.2, legs_per_side=None):
-    """A 3 x 3 x 1 torso on eight 1 x 1 x 3 legs under its perimeter cells;
-    the 4 vertical edges of every leg cube are actuated (8 x 12 = 96)."""
+def spider_lattice(stiffness=3e4, actuation=0.2):
+    """A 3 x 3 x 1 torso (lattice layer y = 3) with eight 1 x 1 x 3 legs: vertical
+    columns of three cubes beside it, one cell apart from each other, whose
+    top cubes sit in the torso layer.  The 4 vertical edges of every leg cube
+    are actuated (8 legs x 3 cubes x 4 = 96 actuators)."""
     L = CubeLattice(stiffness, 0.0)
-    perimeter = [(i, k) for i in range(3) for k in range(3) if (i, k) != (1, 1)]
+    legs = [(-1, -1), (-1, 1), (-1, 3), (1, -1), (1, 3), (3, -1), (3, 1), (3, 3)]
     vertical = {("a", "b"), ("c", "d"), ("e", "f"), ("g", "h")}
-    for (i, k) in perimeter:
-        for j in range(3):
+    for (i, k) in legs:
+        for j in range(1, 4):
             ids = {c: L.point(i + _CORNER[c][0], j + _CORNER[c][1], k + _CORNER[c][2])
                    for c in _CORNER_ORDER}
             for p, q, _ in _SQUARE:
@@ -192,7 +201,9 @@ def spider_lattice(stiffness=3e4, actuation=0.2, legs_per_side=None):
     for i in range(3):
         for k in range(3):
             L.cube(i, 3, k, actuation=0.0)
-    return L.arrays()
+    objects, springs = L.arrays()
+    objects[:, 1] -= SPACING  # legs stand on the lattice origin height
+    return objects, springs
 
 
 def random_lattice(rng, n_vertices, stiffness=3e4, actuation=0.2, actuated_fraction=0.3):

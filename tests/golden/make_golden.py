@@ -160,6 +160,23 @@ def run_case(name, spec, ref_root, ti_shim):
     return out
 
 
+def robot_geometry(ref_root):
+    """objects / springs / faces of the five 3D robots from the reference's own
+    builder (multitask/robot_design.py:319-591)."""
+    from multitask.robot_design import RobotDesignMassSpring3D
+    out = {}
+    for name in ("sim_quad", "sim_x", "sim_y", "sim_spider", "sim_snake"):
+        builder = RobotDesignMassSpring3D.from_file("cfg3d/%s.json" % name)
+        objects, springs, faces = builder.build()
+        rid = builder.robot_id
+        out["objects_%d" % rid] = np.array(objects, dtype=np.float64)
+        out["springs_%d" % rid] = np.array(springs, dtype=np.float64)
+        out["faces_%d" % rid] = np.array(faces, dtype=np.int64)
+        out["stiffness_%d" % rid] = np.float64(builder.spring_stiffness)
+        out["actuation_%d" % rid] = np.float64(builder.spring_actuation)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -173,6 +190,9 @@ def main():
     out_dir = os.path.abspath(a.out)
     os.chdir(ref_root)  # the reference opens cfg3d/*.json relative to its root
     try:
+        geo = robot_geometry(ref_root)
+        np.savez_compressed(os.path.join(out_dir, "robots.npz"), **geo)
+        print("robots", sorted(k for k in geo if k.startswith("objects")))
         for name in a.cases:
             data = run_case(name, CASES[name], ref_root, ti_shim)
             np.savez_compressed(os.path.join(out_dir, name + ".npz"), **data)

@@ -79,12 +79,11 @@ def test_checkpoint_interval_does_not_change_gradients(K):
     b = batch_from_golden(g, precision=64, K=K)
     b.simulate(steps)
     gw = b.get_grads(0, 0)[0]
-    # the gather-form kernels are deterministic, so the recompute reproduces the
-    # first pass bit for bit and the adjoint chain through the states does not
-    # depend on K; weight gradients are summed per segment, so K only regroups
-    # that sum
-    np.testing.assert_array_equal(b.state_grads()[0], gx_ref)
-    assert rel_err(gw, gw_ref) < 1e-13
+    # the forward kernels are deterministic, so the recompute reproduces the
+    # first pass bit for bit; K only regroups the per-segment weight-gradient
+    # sums and the shared-memory atomics of the spring adjoint
+    assert rel_err(b.state_grads()[0], gx_ref) < 1e-12
+    assert rel_err(gw, gw_ref) < 1e-12
 
 
 def test_per_env_launch_equals_batched():
@@ -95,8 +94,8 @@ def test_per_env_launch_equals_batched():
     g1 = b.get_grads(0, 0)[0]
     l2 = b.simulate(steps, per_env=True)
     g2 = b.get_grads(0, 0)[0]
-    assert l1 == l2
-    np.testing.assert_array_equal(g1, g2)
+    assert l1 == l2          # deterministic forward: identical losses
+    assert rel_err(g2, g1) < 1e-5   # the adjoint's atomics only change rounding
 
 
 def test_eval_rollout_matches_golden():
