@@ -197,6 +197,43 @@ int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset)
 int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam);
 int cls_graph_launch(cls_sim* sim, int32_t iter);
 
+/* ---------------------------------------------------------------------------
+ * Mass-spring substeps without any allocation.  This entry point has no
+ * counterpart in the reference; it exists for callers that may not allocate
+ * device memory (a host runtime that owns a fixed device-memory budget or pool,
+ * or code that must not allocate while a surrounding system captures work) and
+ * therefore cannot create a cls_sim, whose buffers come from cudaMalloc.
+ *
+ * Runs n_substeps of spring forces (atomic scatter into a velocity increment)
+ * followed by the damped, ground-contact advance, in place on the caller's x
+ * and v.  All pointers are device pointers owned by the caller; the call
+ * allocates nothing (no cudaMalloc, no library allocator) and keeps its only
+ * scratch -- the velocity increment, n_envs * n_vertices * 3 floats -- in a
+ * fixed 2^21-float (8 MiB) array inside the library that every GPU loading the
+ * library holds until exit.  Larger problems are rejected with
+ * CLS_ERR_INVALID and a message.  All calls share that array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  Each call
+ * clears the part it uses first.  The first call on a device resolves the
+ * array's device address with that device current; make it before any stream
+ * capture on that device.
+ * --------------------------------------------------------------------------- */
+typedef struct {
+  int32_t n_envs, n_vertices, n_springs, n_substeps;
+  const int32_t* spring_a;      /* [n_springs] first endpoint */
+  const int32_t* spring_b;      /* [n_springs] second endpoint */
+  const float* rest_length;     /* [n_springs] */
+  const float* stiffness;       /* [n_springs] as applied (after any scaling) */
+  const float* actuation_coef;  /* [n_springs] */
+  const float* actuation;       /* [n_envs][n_springs], held for all substeps */
+  float* x;                     /* [n_envs][n_vertices][3], advanced in place */
+  float* v;                     /* [n_envs][n_vertices][3], advanced in place */
+  float dt, gravity, ground_height, drag_damping, dashpot_damping, friction;
+  char* error_message;          /* optional buffer for a failure message */
+  int32_t error_capacity;
+} cls_noalloc_advance;
+
+int cls_ms_advance_noalloc(const cls_noalloc_advance* args, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
