@@ -31,6 +31,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+adjoint env-substeps/s (batched uneven mass-spring)"
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+# divided by the algorithmic bytes of that launch, from one `ncu --set full`
+# capture of this workload at 128 robots x 100 substeps (the 512-robot workload
+# is too large to capture); the traffic reported below scales the full launch's
+# algorithmic bytes by it.
+TRAFFIC_RATIO = {"reverse": 8.620194e9 / 10.330433e9, "recompute": 8.787660e9 / 10.441533e9}
 UNIT = "env-substeps/s"
 
 
@@ -241,10 +247,9 @@ def run_ours(a):
     kernel_name = {"forward": "ms_forward_kernel (first pass)", "recompute": "ms_forward_kernel (recompute)",
                    "reverse": "ms_reverse_kernel"}[top]
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get(top)
+    if top in TRAFFIC_RATIO:
+        per_launch = alg[top] * (subs_total if top == "forward" else a.checkpoint)
+        traffic = TRAFFIC_RATIO[top] * per_launch
     roofline = {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": traffic,

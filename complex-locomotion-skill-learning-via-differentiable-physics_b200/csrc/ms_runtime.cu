@@ -649,17 +649,13 @@ class SimImpl final : public SimBase {
   }
 
   void weights_init(unsigned long long seed) override {
-    for (size_t r = 0; r < hr_.size(); ++r) {
-      const HostRobot& h = hr_[r];
-      for (int l = 0; l < L_; ++l) {
-        const long long n = (long long)h.width[l + 1] * h.full_cols[l];
-        timed(PK_OTHER, [&] {
-          ms_weights_init_kernel<R><<<blocks_for(n), 256, 0, stream>>>(
-              d_wm_.p, m_off_[r][l], n, h.full_cols[l], seed, (unsigned long long)(r * 16 + l));
-        });
-        pack_layer((int)r, l);
-      }
-    }
+    const int chunk = 256 * 16;
+    const int blocks = (int)((opt_total_ + chunk - 1) / chunk);
+    timed(PK_OTHER, [&] {
+      ms_weights_init_all_kernel<R><<<std::max(1, blocks), 256, 0, stream>>>(
+          d_opt_segs_.p, (int)opt_segs_.size(), opt_total_, chunk, d_wm_.p, seed);
+    });
+    pack_all();
     CLS_CUDA(cudaGetLastError());
   }
 

@@ -944,6 +944,17 @@ __global__ void ms_v4_to_xyz_kernel(const V4<R>* __restrict__ in, double* __rest
   }
 }
 
+// counter-based uniform in [0, 1): splitmix64 of (seed, stream, index)
+__device__ __forceinline__ double u01(unsigned long long seed, unsigned long long stream,
+                                      unsigned long long idx) {
+  unsigned long long z = seed * 0x9E3779B97F4A7C15ULL + stream * 0xD1B54A32D192ED03ULL + idx;
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
 // ------------------------------------------------ whole-model optimiser step
 // Adam (Model.adam_update, nn.py:184-191) on the reference-layout master
 // weights, with the gradient read from the compact layout, plus the squared
@@ -1074,25 +1085,29 @@ ms_pack_all_kernel(const OptSeg* __restrict__ segs, int n_segs, long long total,
 }
 
 // ------------------------------------------------- initialisation kernels
-// counter-based uniform in [0, 1): splitmix64 of (seed, stream, index)
-__device__ __forceinline__ double u01(unsigned long long seed, unsigned long long stream,
-                                      unsigned long long idx) {
-  unsigned long long z = seed * 0x9E3779B97F4A7C15ULL + stream * 0xD1B54A32D192ED03ULL + idx;
-  z += 0x9E3779B97F4A7C15ULL;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-  z ^= z >> 31;
-  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
-}
-
-// Model.weights_init (nn.py:59-67): W = (u * 2 - 1) * sqrt(6 / fan_in)
+// Model.weights_init (nn.py:59-67) for every weight tensor of every robot in
+// one launch: W = (u * 2 - 1) * sqrt(6 / fan_in), u uniform from a counter-
+// based stream keyed by (seed, tensor, element).  Bias segments are skipped
+// (the reference leaves biases untouched).
 template <typename R>
-__global__ void ms_weights_init_kernel(R* __restrict__ master, long long off, long long n, int fan_in,
-                                       unsigned long long seed, unsigned long long stream) {
-  const double q = sqrt(6.0 / fan_in);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    master[off + i] = (R)((u01(seed, stream, (unsigned long long)i) * 2 - 1) * q);
+__global__ void __launch_bounds__(256)
+ms_weights_init_all_kernel(const OptSeg* __restrict__ segs, int n_segs, long long total, int chunk,
+                           R* __restrict__ master, unsigned long long seed) {
+  __shared__ int s_seg;
+  const long long q0 = (long long)blockIdx.x * chunk;
+  if (q0 >= total) return;
+  if (threadIdx.x == 0) s_seg = find_seg(segs, n_segs, q0);
+  __syncthreads();
+  int sg = s_seg;
+  const long long q1 = q0 + chunk < total ? q0 + chunk : total;
+  for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+    while (sg + 1 < n_segs && segs[sg + 1].start <= q) ++sg;
+    const OptSeg& o = segs[sg];
+    if (o.layer < 0) continue;
+    const long long e = q - o.start;
+    const double scale = sqrt(6.0 / o.cols);
+    master[o.m_off + e] = (R)((u01(seed, (unsigned long long)sg, (unsigned long long)e) * 2 - 1) * scale);
+  }
 }
 
 // TaichiEnv.initialize_train, 3D branch (taichi_env.py:385-447): one pool of
