@@ -177,6 +177,50 @@ def robot_geometry(ref_root):
     return out
 
 
+def run_mpm_case(steps=24, B=2, seed=21):
+    """The reference's 2D MLS-MPM kernels (multitask/solver_mpm.py:60-165) on
+    its MPM robot design robot_design/robot_mpm_1.json.  The reference's env
+    cannot construct this solver (taichi_env.py:136 omits the config), so the
+    solver is constructed and stepped directly: clear_states, then per step
+    clear_grid, p2g, grid_op, g2p (advance_core's forward, :175-180)."""
+    from multitask.config_sim import ConfigSim
+    from multitask.solver_mpm import SolverMPM
+    from util import read_json
+    path = "cfg3d/sim_quad.json"
+    raw = read_json(path)
+    raw["robot"].update({"dim": 2, "simulator": "mpm", "solver": "mpm",
+                         "design_file": "robot_design/robot_mpm_1.json"})
+    raw["nn"]["batch_size"] = B
+    raw["process"]["max_steps"] = steps + 1
+    config = ConfigSim(raw, file_name=path, if_mkdir=False)
+    cfg = config.get_config()
+    solver = SolverMPM(config)
+    solver.initialize_robot()
+    objects = np.array(cfg["robot"]["objects"], dtype=np.float64) + np.array([0.35, 0.12])
+    for k in range(B):
+        solver.x.arr[0, k] = objects
+    rng = np.random.default_rng(seed)
+    act = rng.uniform(-1.0, 1.0, size=(steps + 1, B, 4))
+    solver.actuation.arr[:, :, :4] = act
+    solver.clear_states(steps + 1)
+    for f in range(steps):
+        solver.clear_grid()
+        solver.p2g(f)
+        solver.grid_op()
+        solver.g2p(f)
+    sim = cfg["simulator"]
+    return dict(
+        steps=np.int64(steps), B=np.int64(B), n_grid=np.int64(sim["mpm"]["n_grid"]),
+        dx=np.float64(sim["mpm"]["dx"]), inv_dx=np.float64(sim["mpm"]["inv_dx"]),
+        dt=np.float64(cfg["process"]["dt"]), gravity=np.float64(sim["gravity"]),
+        p_vol=np.float64(sim["p_vol"]), E=np.float64(sim["E"]), mu=np.float64(sim["mu"]),
+        la=np.float64(sim["la"]), act_strength=np.float64(sim["act_strength"]),
+        bound=np.int64(sim["bound"]), actuator_id=np.array(cfg["robot"]["springs"], dtype=np.int64),
+        objects=objects, actuation=act,
+        x=solver.x.to_numpy()[:steps + 1], v=solver.v.to_numpy()[:steps + 1],
+        C=solver.C.to_numpy()[:steps + 1], F=solver.F.to_numpy()[:steps + 1])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -190,6 +234,9 @@ def main():
     out_dir = os.path.abspath(a.out)
     os.chdir(ref_root)  # the reference opens cfg3d/*.json relative to its root
     try:
+        mpm = run_mpm_case()
+        np.savez_compressed(os.path.join(out_dir, "mpm2d_ref.npz"), **mpm)
+        print("mpm2d_ref x", mpm["x"].shape)
         geo = robot_geometry(ref_root)
         np.savez_compressed(os.path.join(out_dir, "robots.npz"), **geo)
         print("robots", sorted(k for k in geo if k.startswith("objects")))

@@ -113,6 +113,13 @@ class TiVec(np.ndarray):
     def outer_product(self, other):
         return np.outer(np.asarray(self), np.asarray(other)).view(TiVec)
 
+    def determinant(self):
+        return float(np.linalg.det(np.asarray(self)))
+
+    def __call__(self, *idx):
+        # old-style component access v(i) / m(i, j)
+        return np.asarray(self)[idx if len(idx) > 1 else idx[0]]
+
 
 def _vec(values):
     return np.array(values, dtype=np.float64).view(TiVec)
@@ -142,7 +149,27 @@ class Field:
     def _key(idx):
         if idx is None:
             return ()
+        if isinstance(idx, tuple):
+            out = []
+            for e in idx:
+                if isinstance(e, np.ndarray):
+                    out.extend(int(v) for v in np.asarray(e).ravel())
+                else:
+                    out.append(int(e))
+            return tuple(out)
         return idx
+
+    def __iter__(self):
+        # struct-for over all indices of the field
+        return itertools.product(*[range(s) for s in self.shape])
+
+    @property
+    def grad(self):
+        if getattr(self, "_grad", None) is None:
+            g = Field(self.dtype, n=self.n, m=self.m)
+            g._alloc(self.shape)
+            self._grad = g
+        return self._grad
 
     def __getitem__(self, idx):
         return self.arr[self._key(idx)]
@@ -257,8 +284,19 @@ def max(a, b):  # noqa: A001 - mirrors ti.max
 
 def cast(x, dtype):
     if dtype is i32:
-        return np.asarray(x).astype(np.int64)
-    return np.asarray(x).astype(np.float64)
+        return np.asarray(x).astype(np.int64).view(TiVec) if np.ndim(x) else int(x)
+    return np.asarray(x).astype(np.float64).view(TiVec) if np.ndim(x) else float(x)
+
+
+def polar_decompose(A, dt=None):
+    """2D polar decomposition in Taichi's closed form: R from
+    (A00 + A11, A10 - A01) normalised, S = R^T A."""
+    A = np.asarray(A)
+    x, y = A[0, 0] + A[1, 1], A[1, 0] - A[0, 1]
+    scale = 1.0 / np.sqrt(x * x + y * y)
+    c, s = x * scale, y * scale
+    r = np.array([[c, -s], [s, c]]).view(TiVec)
+    return r, (np.asarray(r).T @ A).view(TiVec)
 
 
 class _TapeCtx:
