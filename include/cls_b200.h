@@ -198,6 +198,75 @@ int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam);
 int cls_graph_launch(cls_sim* sim, int32_t iter);
 
 /* ---------------------------------------------------------------------------
+ * Differentiable MLS-MPM (multitask/solver_mpm.py).  The reference's solver is
+ * 2D (fixed-corotated, actuation along y) and unreachable from its env
+ * (taichi_env.py:136 constructs it without its config); these entry points run
+ * its algorithm in 2D or 3D, with per-particle fibre directions and a
+ * neo-Hookean option, and add the checkpointed reverse pass.
+ * --------------------------------------------------------------------------- */
+#define CLS_MPM_FIXED_COROTATED 0 /* reference model, 2D only */
+#define CLS_MPM_NEO_HOOKEAN 1
+
+typedef struct cls_mpm cls_mpm;
+
+/* Particle body: RobotDesignMPM.build output (multitask/robot_design.py:38-110):
+ * positions, actuator id per particle (-1 passive); fibre directions are new
+ * (NULL: the reference's e_y). */
+typedef struct {
+  int32_t dim;                  /* 2 or 3 */
+  int32_t n_particles;
+  const double* positions;      /* [n_particles][dim], inside the unit box */
+  const int32_t* muscle;        /* [n_particles] actuator index or -1 (NULL: all -1) */
+  const double* fibre;          /* [n_particles][dim] unit directions or NULL */
+  int32_t n_muscles;
+} cls_mpm_body;
+
+/* SolverMPM constants (multitask/solver_mpm.py:8-52, config_sim.py:123-129). */
+typedef struct {
+  int32_t max_steps;            /* trajectory length T */
+  int32_t n_grid;               /* simulator.mpm.n_grid (dx = 1 / n_grid) */
+  int32_t bound;                /* simulator.bound: sticky layer width in cells */
+  int32_t material;             /* CLS_MPM_* */
+  int32_t precision;            /* 32 or 64 */
+  int32_t checkpoint_every;     /* K */
+  double dt, gravity, p_vol, mu, la, act_strength, mass;
+} cls_mpm_params;
+
+/* Fills *p with the reference's 2D MPM constants (dt 1e-3, gravity -10,
+ * n_grid 32, bound 3, p_vol 1, mu = la = 40, act_strength 4, mass 1). */
+void cls_mpm_default_params(cls_mpm_params* p);
+/* Replaces SolverMPM.__init__ + initialize_robot (solver_mpm.py:7-58). */
+int cls_mpm_create(const cls_mpm_body* body, const cls_mpm_params* params, int32_t n_envs,
+                   cls_mpm** out);
+int cls_mpm_destroy(cls_mpm* sim);
+const char* cls_mpm_last_error(const cls_mpm* sim);
+int cls_mpm_set_stream(cls_mpm* sim, void* stream);
+/* x[0], v[0] ([n_envs][n_particles][dim]); C = 0 and F = I as clear_states
+ * does (solver_mpm.py:60-71). */
+int cls_mpm_set_state(cls_mpm* sim, const double* x0, const double* v0);
+/* actuation [T][n_envs][n_muscles] (the solver's actuation field). */
+int cls_mpm_set_actuation(cls_mpm* sim, const double* act);
+/* Centre-tracking loss sum_t w_t sum_env |c_t - target_t|^2 with c the
+ * particle-weighted centre: w [T+1], target [T+1][n_envs][dim], particle
+ * weights [n_particles] (NULL: uniform = compute_center, solver_mpm.py:167-173). */
+int cls_mpm_set_loss(cls_mpm* sim, const double* w, const double* target, const double* pw);
+/* steps x advance_core (clear_grid, p2g, grid_op, g2p; solver_mpm.py:175-180). */
+int cls_mpm_forward(cls_mpm* sim, int32_t steps);
+int cls_mpm_loss(cls_mpm* sim, double* loss);
+/* Reverse pass (advance_core_grad, solver_mpm.py:182-190, over checkpointed
+ * segments). */
+int cls_mpm_backward(cls_mpm* sim);
+int cls_mpm_get_final_state(cls_mpm* sim, double* x, double* v, double* C, double* F);
+/* d loss / d actuation [T][n_envs][n_muscles] and / d initial x, v, C, F. */
+int cls_mpm_get_grads(cls_mpm* sim, double* gact, double* gx0, double* gv0, double* gC0,
+                      double* gF0);
+/* centres [T+1][n_envs][dim] of the last rollout. */
+int cls_mpm_get_centers(cls_mpm* sim, double* centers);
+/* forward + backward of `steps` captured into a CUDA graph; replay. */
+int cls_mpm_graph_capture(cls_mpm* sim, int32_t steps);
+int cls_mpm_graph_launch(cls_mpm* sim);
+
+/* ---------------------------------------------------------------------------
  * Mass-spring substeps without any allocation.  This entry point has no
  * counterpart in the reference; it exists for callers that may not allocate
  * device memory (a host runtime that owns a fixed device-memory budget or pool,
