@@ -13,6 +13,13 @@ runs its own 512 robots (weak scaling, no data-path collective).
 ``--impl reference`` times the reference algorithm's CPU implementation (the
 project's FP64 restatement, all host cores) on a bounded sample of the same
 workload; the reference itself needs Taichi, which is not installed.
+
+``--config`` selects another workload for the same measurement (the default,
+``uneven``, is the headline line): ``quadruped`` (32 envs of the quadruped
+lattice, 1000 substeps, MLP 1x64), ``spider`` (4096 envs of the spider lattice,
+1000 substeps, MLP 2x256) or ``mpm`` (3D MLS-MPM legged body of 29,504
+particles on a 64^3 grid, 8 envs, 1000 substeps of dt 1e-4, neo-Hookean with
+16 fibre-actuated muscle groups, forward + checkpointed adjoint).
 """
 import argparse
 import json
@@ -30,7 +37,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "fwd+adjoint env-substeps/s (batched uneven mass-spring)"
+METRICS = {"uneven": "fwd+adjoint env-substeps/s (batched uneven mass-spring)",
+           "quadruped": "fwd+adjoint env-substeps/s (quadruped lattice, 32 envs)",
+           "spider": "fwd+adjoint env-substeps/s (spider lattice, 4096 envs)",
+           "mpm": "fwd+adjoint env-substeps/s (3D MLS-MPM legged body, 8 envs)"}
+DEFAULT_SUBSTEPS = {"uneven": 2000, "quadruped": 1000, "spider": 1000, "mpm": 1000}
+DEFAULT_ENVS = {"uneven": 512, "quadruped": 32, "spider": 4096, "mpm": 8}
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one launch
 # divided by the algorithmic bytes of that launch, from one `ncu --set full`
 # capture of this workload at 128 robots x 100 substeps (the 512-robot workload
@@ -46,14 +58,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--robots", type=int, default=512)
-    ap.add_argument("--substeps", type=int, default=2000)
+    ap.add_argument("--config", default="uneven", choices=sorted(METRICS))
+    ap.add_argument("--robots", "--envs", dest="robots", type=int, default=None,
+                    help="robots (uneven) or envs per GPU (default: the configuration's)")
+    ap.add_argument("--substeps", type=int, default=None)
     ap.add_argument("--checkpoint", type=int, default=50)
     ap.add_argument("--plain-sample", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: automatic)")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.robots is None:
+        a.robots = DEFAULT_ENVS[a.config]
+    if a.substeps is None:
+        a.substeps = DEFAULT_SUBSTEPS[a.config]
+    return a
 
 
 def dist_env():
@@ -62,12 +81,30 @@ def dist_env():
 
 
 def config_dict(a, n_gpus):
-    return {"workload": "batched uneven mass-spring: %d random lattices (50-2000 vertices, "
-                        "log-uniform; 30%% springs actuated) x %d substeps, checkpoint every %d, "
-                        "MLP 2x128 tanh, velocity+rotation loss, Adam" % (a.robots, a.substeps, a.checkpoint),
-            "robots_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
-            "parallelism": "env-sharded replicas x%d (no data-path collective)" % n_gpus,
-            "l2": "inputs larger than L2 (controller weights ~0.8 GB per GPU)"}
+    par = "env-sharded replicas x%d (no data-path collective)" % n_gpus
+    if a.config == "uneven":
+        return {"workload": "batched uneven mass-spring: %d random lattices (50-2000 vertices, "
+                            "log-uniform; 30%% springs actuated) x %d substeps, checkpoint every %d, "
+                            "MLP 2x128 tanh, velocity+rotation loss, Adam"
+                            % (a.robots, a.substeps, a.checkpoint),
+                "robots_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
+                "parallelism": par,
+                "l2": "inputs larger than L2 (controller weights ~0.8 GB per GPU)"}
+    if a.config in ("quadruped", "spider"):
+        shape = ("quadruped lattice (54 vertices, 323 springs, 40 actuated), MLP 1x64 tanh"
+                 if a.config == "quadruped" else
+                 "spider lattice (136 vertices, 732 springs, 96 actuated), MLP 2x256 tanh")
+        return {"workload": "%d envs of the %s x %d substeps, checkpoint every %d, "
+                            "velocity+rotation loss, Adam" % (a.robots, shape, a.substeps, a.checkpoint),
+                "envs_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
+                "parallelism": par,
+                "l2": "trajectory and checkpoints written every iteration exceed L2"}
+    return {"workload": "3D MLS-MPM: legged body of 29504 particles (8 per cell, 16 fibre-actuated "
+                        "muscle groups), 64^3 grid, neo-Hookean E=1e4 nu=0.3, dt 1e-4, %d envs x %d "
+                        "substeps, checkpoint every %d, centre loss" % (a.robots, a.substeps, a.checkpoint),
+            "envs_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
+            "parallelism": par,
+            "l2": "state trajectory checkpoints and per-step records exceed L2"}
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -114,7 +151,19 @@ def run_reference(a):
     if rank != 0:
         return
     from cls_b200 import workloads
-    robots = workloads.uneven_robots(a.robots, seed=0)
+    if a.config == "mpm":
+        return run_reference_mpm(a)
+    if a.config == "uneven":
+        robots = workloads.uneven_robots(a.robots, seed=0)
+    else:
+        from cls_b200 import robot_design
+        from cls_b200.batch import Robot
+        if a.config == "quadruped":
+            obj, spr = robot_design.quadruped_lattice()
+            robots = [Robot.actuated_outputs(obj, spr, hidden=[64])] * a.robots
+        else:
+            obj, spr = robot_design.spider_lattice()
+            robots = [Robot.actuated_outputs(obj, spr, hidden=[256, 256])] * a.robots
     cores = os.cpu_count() or 1
     vals = []
     sample = ""
@@ -123,7 +172,7 @@ def run_reference(a):
         if i >= a.warmup:
             vals.append(v)
     value = float(np.mean(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+    line = {"impl": "reference", "metric": METRICS[a.config], "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": config_dict(a, a.gpus),
@@ -180,6 +229,21 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ ours
+def make_ms_batch(a, n, seed, robots=None):
+    """The mass-spring batch of the selected configuration: (batch, robot list,
+    robot index of every env, (target velocities, target heights))."""
+    from cls_b200 import workloads
+    if a.config == "uneven":
+        b, robots, tt = workloads.uneven_batch(n_robots=n, steps=a.substeps, K=a.checkpoint,
+                                               seed=seed, robots=robots,
+                                               threads_per_block=a.threads)
+        return b, robots, list(range(len(robots))), tt
+    build = workloads.quadruped_batch if a.config == "quadruped" else workloads.spider_batch
+    b, robots, tt = build(n_envs=n, steps=a.substeps, K=a.checkpoint, seed=seed,
+                          threads_per_block=a.threads)
+    return b, robots, [0] * n, tt
+
+
 def run_ours(a):
     import torch
     rank, world, local = dist_env()
@@ -190,9 +254,7 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     import cls_b200
     from cls_b200 import workloads
-    b, robots, (tv, th) = workloads.uneven_batch(n_robots=a.robots, steps=a.substeps,
-                                                K=a.checkpoint, seed=1000 * rank,
-                                                threads_per_block=a.threads)
+    b, robots, env_robot, (tv, th) = make_ms_batch(a, a.robots, 1000 * rank)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     env_substeps = b.n_envs * (a.substeps - 1)
@@ -231,7 +293,7 @@ def run_ours(a):
           file=sys.stderr)
 
     # roofline of the dominant kernel (CUDA events around each launch above)
-    alg = workloads.algorithmic_bytes(robots, list(range(len(robots))))
+    alg = workloads.algorithmic_bytes(robots, env_robot)
     subs_total = a.substeps - 1
     kinds = {"forward": subs_total, "recompute": subs_total, "reverse": subs_total}
     top = max(kinds, key=lambda k: prof_ms[k])
@@ -259,8 +321,7 @@ def run_ours(a):
     # plain form: the same kernels, one robot per launch, on a bounded sample
     plain = None
     if rank == 0 and a.plain_sample > 0:
-        sub = robots[:a.plain_sample]
-        pb, _, _ = workloads.uneven_batch(robots=sub, steps=a.substeps, K=a.checkpoint, seed=7)
+        pb, _, sub, _ = make_ms_batch(a, min(a.plain_sample, a.robots), 7, robots=robots[:a.plain_sample])
         ps = torch.cuda.Stream()
         pb.set_stream(ps.cuda_stream)
         pb.simulate(a.substeps, per_env=True)
@@ -278,7 +339,7 @@ def run_ours(a):
         bms = e0.elapsed_time(e1)
         n_sub = len(sub) * (a.substeps - 1)
         plain = {"value": n_sub / (pms / 1e3), "unit": UNIT,
-                 "sample": "first %d robots of the workload, one robot per launch (same kernels)" % len(sub),
+                 "sample": "first %d envs of the workload, one env per launch (same kernels)" % len(sub),
                  "batched_same_sample": n_sub / (bms / 1e3),
                  "batched_full_over_plain": value / world / (n_sub / (pms / 1e3))}
         pb.close()
@@ -288,7 +349,7 @@ def run_ours(a):
     if a.e2e_steps > 0:
         x0 = torch.empty((b.n_vertices_total, 3), dtype=torch.float64).pin_memory()
         v0 = torch.zeros((b.n_vertices_total, 3), dtype=torch.float64).pin_memory()
-        x0.copy_(torch.from_numpy(np.concatenate([r.objects for r in robots])))
+        x0.copy_(torch.from_numpy(np.concatenate([robots[r].objects for r in env_robot])))
         tvh = torch.from_numpy(np.ascontiguousarray(tv)).pin_memory()
         thh = torch.from_numpy(np.ascontiguousarray(th)).pin_memory()
         loss_terms = torch.zeros(8, dtype=torch.float64).pin_memory()
@@ -324,12 +385,13 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        v, sample, wall = cpu_sample(robots, 11, n_robots=cores * 2, substeps=200, threads=cores)
+        v, sample, wall = cpu_sample([robots[r] for r in env_robot], 11, n_robots=cores * 2,
+                                     substeps=200, threads=cores)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": sample + "; wall %.1f s; reference Taichi not installed (no network)" % wall}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        line = {"metric": METRICS[a.config], "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded random lattices, targets and weights)",
@@ -343,10 +405,180 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------------------------- MPM
+def mpm_cpu_sample(a, seed, envs, substeps):
+    """Time the FP64 MPM oracle (OpenMP over envs, all host cores) on `envs`
+    envs of the workload body for `substeps` substeps, forward + loss +
+    backward."""
+    from oracle.mpm_oracle import MPMOracle
+    from cls_b200 import workloads
+    pos, mus, fib = workloads.legged_body()
+    E, nu = 1e4, 0.3
+    o = MPMOracle(pos, mus, envs, substeps, dim=3, n_grid=64, dt=1e-4, p_vol=1.0,
+                  mu=E / (2 * (1 + nu)), la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3,
+                  gravity=-10.0, bound=3, material="neo_hookean", fibre=fib, n_muscles=16)
+    rng = np.random.default_rng(seed)
+    o.act[...] = rng.uniform(-1, 1, o.act.shape)
+    o.loss_w[substeps] = 1.0
+    o.target[...] = pos.mean(axis=0) + np.array([0.05, 0.0, 0.0])
+    t0 = time.perf_counter()
+    o.run(substeps)
+    wall = time.perf_counter() - t0
+    return envs * substeps / wall, "%d envs x %d substeps of the workload body (forward+loss+backward, " \
+        "FP64, OpenMP over envs)" % (envs, substeps), wall
+
+
+def run_reference_mpm(a):
+    cores = os.cpu_count() or 1
+    vals, sample = [], ""
+    for i in range(a.warmup + a.steps):
+        v, sample, _ = mpm_cpu_sample(a, 100 + i, envs=cores, substeps=24)
+        if i >= a.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRICS[a.config], "value": value, "unit": UNIT,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config_dict(a, a.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample + "; the reference's MPM is 2D and needs Taichi "
+                                                "(not installed)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_mpm(a):
+    import ctypes
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import cls_b200
+    from cls_b200 import workloads
+    T = a.substeps
+    b, pos = workloads.mpm_batch(n_envs=a.robots, steps=T, K=a.checkpoint, seed=1000 * rank)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    env_substeps = b.E * T
+
+    # per-kernel profile of one iteration (events around every launch)
+    b.forward(T)
+    b.backward()
+    torch.cuda.synchronize()
+    b.profile(True)
+    b.profile_read(reset=True)
+    b.forward(T)
+    b.backward()
+    prof_ms, prof_n = b.profile_read(reset=True)
+    b.profile(False)
+
+    # timed: the captured forward + backward graph, one launch per iteration
+    b.graph_capture(T)
+    for _ in range(a.warmup):
+        b.graph_launch()
+    clk = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        b.graph_launch()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / a.steps
+    value = world * env_substeps / (ms_per_step / 1e3)
+    print("timed: %.1f ms/step, %.3e %s, kernels %s" % (ms_per_step, value, UNIT, prof_ms),
+          file=sys.stderr)
+
+    alg = workloads.mpm_algorithmic_bytes(pos, b.E, n_grid=64)
+    kinds = [k for k in alg if prof_n.get(k, 0) > 0]
+    top = max(kinds, key=lambda k: prof_ms[k])
+    achieved = alg[top] * prof_n[top] / (prof_ms[top] / 1e3) / 1e9
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    roofline = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                "share_of_step": prof_ms[top] / max(1e-9, sum(prof_ms.values())),
+                "kernel_ms": prof_ms, "launches": prof_n,
+                "per_kernel_frac": {k: alg[k] * prof_n[k] / (prof_ms[k] / 1e3) / 1e9 / peak
+                                    for k in kinds}}
+
+    # end to end through the C ABI with host buffers: initial state and
+    # actuation in, loss and actuation gradient out, every iteration
+    e2e = None
+    if a.e2e_steps > 0:
+        lib, h = b.lib, b.h
+        P = ctypes.POINTER(ctypes.c_double)
+        pd = lambda t: ctypes.cast(t.data_ptr(), P)  # noqa: E731
+        x0 = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(pos, (b.E,) + pos.shape))).pin_memory()
+        v0 = torch.zeros_like(x0).pin_memory()
+        act = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (T, b.E, b.M))).pin_memory()
+        gact = torch.zeros_like(act).pin_memory()
+        loss = ctypes.c_double()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            b._c(lib.cls_mpm_set_state(h, pd(x0), pd(v0)))
+            b._c(lib.cls_mpm_set_actuation(h, pd(act)))
+            b._c(lib.cls_mpm_forward(h, T))
+            b._c(lib.cls_mpm_loss(h, ctypes.byref(loss)))
+            b._c(lib.cls_mpm_backward(h))
+            b._c(lib.cls_mpm_get_grads(h, pd(gact), None, None, None, None))
+        e2e_s = (time.perf_counter() - t0) / a.e2e_steps
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * env_substeps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int((x0.numel() + v0.numel() + act.numel()) * 8),
+               "d2h_bytes_per_step": int(gact.numel() * 8 + 8),
+               "path": "cls_mpm_set_state/cls_mpm_set_actuation (pinned host) -> cls_mpm_forward "
+                       "-> cls_mpm_loss (D2H) -> cls_mpm_backward -> cls_mpm_get_grads (D2H)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        v, sample, wall = mpm_cpu_sample(a, 11, envs=cores, substeps=24)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": sample + "; wall %.1f s; the reference's MPM is 2D and needs Taichi" % wall}
+
+    if rank == 0:
+        line = {"metric": METRICS[a.config], "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded voxelised body and actuation)",
+                "config": config_dict(a, world), "clocks": clocks,
+                "gpu_launches": int(sum(prof_n.values())) * a.steps, "roofline": roofline,
+                "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    b.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "mpm":
+        run_mpm(a)
     else:
         run_ours(a)
 

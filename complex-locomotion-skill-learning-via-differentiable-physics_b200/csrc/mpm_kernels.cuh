@@ -1,15 +1,42 @@
 // mpm_kernels.cuh -- differentiable MLS-MPM substep (P2G, grid update, G2P)
 // and its hand-written adjoint, dimension-templated (2D / 3D).
 //
-// Follows the reference's multitask/solver_mpm.py (2D): p2g :83-124, grid_op
-// :126-144, g2p :146-165, advance_core_grad :182-190 (the adjoint of a step
-// rebuilds that step's grid from the particle state, then runs g2p^T,
-// grid_op^T, p2g^T).  Generalised to 3D, per-particle fibre directions
-// (actuation stress a * (F f)(F f)^T; the reference's is f = e_y) and the
-// compressible neo-Hookean Kirchhoff stress mu (F F^T - I) + lambda ln(J) I
-// next to the reference's fixed-corotated model (2D only, closed-form polar
-// decomposition).
+// Algorithm: the reference's multitask/solver_mpm.py (2D): p2g :83-124,
+// grid_op :126-144, g2p :146-165, advance_core_grad :182-190.  Generalised to
+// 3D, per-particle fibre directions (actuation stress a * (F f)(F f)^T; the
+// reference's is f = e_y) and the compressible neo-Hookean Kirchhoff stress
+// mu (F F^T - I) + lambda ln(J) I next to the reference's fixed-corotated
+// model (2D only, closed-form polar decomposition).
+//
+// Layout and kernels (B200):
+//  * particles are stored SoA (component planes of E*P values) in an internal
+//    order: Morton order of their initial cells, cut into chunks (one CTA
+//    each) of at most 256 particles that never leave one aligned group of
+//    4x4x2 cells (3D) or 8x8 cells (2D), so that a chunk's stencils cover a
+//    small box; inside a chunk the particles are interleaved so that the 32
+//    lanes of a warp hold particles of 32 different cells;
+//  * the grid is dense per env but blocked: blocks of 4^3 (3D) or 8^2 (2D)
+//    nodes, 64 nodes of 4 values (16 B in FP32) per block, so a block is one
+//    contiguous 1 KB run.  P2G keeps, per env, the box of the base cells it
+//    scattered from (one min/max atomic pair per warp); the grid kernels
+//    visit only the blocks under that box, and the accumulators are cleared
+//    by the grid kernel that consumes them;
+//  * scatters (P2G, G2P^T) go through a warp-private shared-memory tile over
+//    the box of the warp's stencils: with distinct base cells per lane, the
+//    lanes of one stencil offset write distinct nodes, so the warp adds with
+//    plain shared-memory read-modify-writes (a __syncwarp between offsets; a
+//    warp whose lanes share a base cell uses shared atomics instead), then
+//    flushes each touched node with one 16-byte vector atomic.  Gathers (G2P,
+//    P2G^T) read the grid through L1.  A warp whose box exceeds the tile falls
+//    back to global atomics;
+//  * forward: one fused particle kernel per substep does G2P of step f and
+//    P2G of step f + 1 (only x, F and the grid cross kernels; v and C are
+//    written when the step is recorded); reverse: one fused kernel does P2G^T
+//    and the loss seed of step f, then G2P^T of step f - 1 (only a_x and a_F
+//    cross kernels).
 #pragma once
+#include <climits>
+
 #include "cls_common.cuh"
 
 namespace cls {
@@ -17,25 +44,84 @@ namespace mpm {
 
 enum Material : int { FIXED_COROTATED = 0, NEO_HOOKEAN = 1 };
 
-template <typename R>
-struct Args {
-  int n_envs, P, M, n_grid, bound, material;
-  long long cells;                       // n_grid^D per env
-  R dx, inv_dx, dt, ks, mu, la, act_strength, gravity, mass;   // ks = dt p_vol 4 inv_dx^2
-  const int* muscle;                     // [P]
-  const R* fibre;                        // [P][D]
-  // state at step f and f + 1, [E][P][D] and [E][P][D][D]
-  const R* x; const R* v; const R* C; const R* F;
-  R* x1; R* v1; R* C1; R* F1;
-  const R* act;                          // [E][M] of step f
-  R* gm; R* gmv; R* gvo;                 // grid [E][cells], [E][cells][D] x 2
-  // adjoints of state f + 1 (a*) and of state f (n*)
-  const R* ax; const R* av; const R* aC; const R* aF;
-  R* nx; R* nv; R* nC; R* nF;
-  R* g_gvo; R* g_gv; R* g_gm;            // grid adjoints
-  R* gact;                               // [E][M] of step f
+constexpr int kChunk = 256;         // particles per CTA, one per thread
+constexpr int kWarps = kChunk / 32;
+constexpr int kTileDefault = 256;   // default warp tile capacity (nodes)
+constexpr int kMaxMuscles = 256;
+constexpr int kFwdPlanes = 4;       // P2G warp tile: momentum (3), mass
+constexpr int kAdjPlanes = 3;       // G2P^T warp tile: velocity adjoint (3)
+
+template <int D>
+struct Blk {
+  static constexpr int LOG = D == 3 ? 2 : 3;  // block side 4 (3D) or 8 (2D)
+  static constexpr int SIDE = 1 << LOG;
+  static constexpr int NODES = 64;
 };
 
+// Physical constants, body tables and grid geometry shared by all kernels.
+template <typename R>
+struct Phys {
+  int E, P, M, material, n_chunks, tile_cap;  // tile_cap: nodes per warp tile (<= 0: none)
+  int n_grid, nb, bound;                      // nodes per side, blocks per side
+  long long nblk;                             // blocks per env
+  long long EP;                               // E * P (plane stride)
+  R dx, inv_dx, dt, ks, mu, la, act_strength, gravity, mass;  // ks = dt p_vol 4 inv_dx^2
+  const int* muscle;                          // [P] internal order, -1 passive
+  const R* fibre;                             // [D][P]
+  const R* pw;                                // [P] particle weights of the centre
+  const int* chunk_start;                     // [n_chunks] first internal particle
+  const int* chunk_len;                       // [n_chunks] particles (<= kChunk)
+};
+
+// Forward particle kernel: G2P of step f (mode bit 1) and/or P2G of step g
+// (mode bit 2; g = f + 1 after G2P, else the state read from v_in / C_in).
+template <typename R>
+struct FwdArgs {
+  Phys<R> c;
+  const R* x_in;          // x_f (with G2P) or x_g (P2G only)
+  const V4<R>* gv;        // grid (velocity, mass) of step f
+  R* x_out;               // x_{f+1}
+  R* v_out;               // v_{f+1} or nullptr
+  R* C_out;               // C_{f+1} or nullptr
+  const R* v_in;          // v_g, C_g (P2G-only mode)
+  const R* C_in;
+  const R* F_in;          // F_g
+  R* F_out;               // F_{g+1} or nullptr
+  const R* act;           // [E][M] of step g
+  V4<R>* acc;             // (momentum, mass) accumulator of step g
+  int* bbox;              // [E][2 D] box of the base cells of step g (min, max)
+  R* csum;                // [E][D] pw-weighted position sums of the positions produced (or read)
+};
+
+// Reverse particle kernel: P2G^T of step f plus the loss seed of step f
+// (mode bit 1), then G2P^T of step h (mode bit 2; h = f - 1 after P2G^T, else
+// the first reverse step h = T - 1 whose x-adjoint is the seed of step T).
+template <typename R>
+struct AdjArgs {
+  Phys<R> c;
+  // P2G^T of step f
+  const R* x_f; const R* v_f; const R* C_f; const R* F_f;
+  const R* act_f;          // [E][M]
+  const V4<R>* ga;         // grid adjoint (d velocity, d mass) of step f
+  const R* ax_in;          // a_x(f) so far (G2P^T of step f applied)
+  const R* aF_in;          // a_F(f + 1)
+  R* gact;                 // d actuation [E][M] of step f (accumulated)
+  // loss seed of the state whose x-adjoint is completed here
+  R seed_w;                // w_t (0: none)
+  const R* csum;           // [E][D] pw-weighted position sums of that step
+  const R* target;         // [E][D]
+  R pw_sum;
+  // outputs of the last reverse step (no G2P^T follows)
+  R* out_ax; R* out_av; R* out_aC; R* out_aF;
+  // G2P^T of step h
+  const R* x_h;
+  const V4<R>* gv_h;       // grid of step h
+  V4<R>* gacc;             // d grid velocity accumulator of step h
+  R* ax_out;               // a_x(h) so far
+  R* aF_out;               // a_F(f) (zeros in the first reverse step)
+};
+
+// ------------------------------------------------------------ helpers
 template <typename R, int D>
 struct Kern {
   static constexpr int NN = D == 2 ? 9 : 27;
@@ -64,13 +150,6 @@ struct Kern {
     o[0] = q % 3;
     o[1] = (q / 3) % 3;
     if (D == 3) o[D - 1] = q / 9;
-  }
-
-  __device__ static long long cell(int n, const int base[D], const int o[D]) {
-    long long idx = 0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) idx = idx * n + (base[d] + o[d]);
-    return idx;
   }
 
   __device__ static R det(const R* A) {
@@ -108,14 +187,15 @@ struct Kern {
       }
   }
 
-  // Kirchhoff stress incl. actuation (solver_mpm.py:96-115)
-  __device__ static void stress(const Args<R>& a, const R* nF, int pidx, R act, R* tau) {
+  // Kirchhoff stress incl. actuation (solver_mpm.py:96-115); `am` is the
+  // actuation times its strength, `f` the fibre (active particles only).
+  __device__ static void stress(const Phys<R>& c, const R* nF, bool active, R am, const R* f, R* tau) {
     const R J = det(nF);
-    if (D == 2 && a.material == FIXED_COROTATED) {
+    if (D == 2 && c.material == FIXED_COROTATED) {
       const R xx = nF[0] + nF[3], yy = nF[2] - nF[1];
       const R sc = R(1) / dsqrt<R>(xx * xx + yy * yy);
-      const R c = xx * sc, s = yy * sc;
-      const R Rm[4] = {c, -s, s, c};
+      const R cs = xx * sc, s = yy * sc;
+      const R Rm[4] = {cs, -s, s, cs};
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -123,10 +203,10 @@ struct Kern {
           R acc = 0;
 #pragma unroll
           for (int q = 0; q < 2; ++q) acc += (nF[i * 2 + q] - Rm[i * 2 + q]) * nF[j * 2 + q];
-          tau[i * D + j] = R(2) * a.mu * acc;
+          tau[i * D + j] = R(2) * c.mu * acc;
         }
 #pragma unroll
-      for (int i = 0; i < 2; ++i) tau[i * D + i] += a.la * (J - R(1)) * J;
+      for (int i = 0; i < 2; ++i) tau[i * D + i] += c.la * (J - R(1)) * J;
     } else {
 #pragma unroll
       for (int i = 0; i < D; ++i)
@@ -135,14 +215,12 @@ struct Kern {
           R acc = 0;
 #pragma unroll
           for (int q = 0; q < D; ++q) acc += nF[i * D + q] * nF[j * D + q];
-          tau[i * D + j] = a.mu * (acc - (i == j ? R(1) : R(0)));
+          tau[i * D + j] = c.mu * (acc - (i == j ? R(1) : R(0)));
         }
 #pragma unroll
-      for (int i = 0; i < D; ++i) tau[i * D + i] += a.la * log(J);
+      for (int i = 0; i < D; ++i) tau[i * D + i] += c.la * log(J);
     }
-    if (a.muscle[pidx] >= 0) {
-      const R am = act * a.act_strength;
-      const R* f = a.fibre + (size_t)pidx * D;
+    if (active) {
       R u[D];
 #pragma unroll
       for (int i = 0; i < D; ++i) {
@@ -157,19 +235,20 @@ struct Kern {
     }
   }
 
-  // d tau / d nF (accumulated into gF) and d actuation (returned)
-  __device__ static R stress_adj(const Args<R>& a, const R* nF, int pidx, R act, const R* gt, R* gF) {
+  // d tau / d nF (accumulated into gF); returns d loss / d actuation
+  __device__ static R stress_adj(const Phys<R>& c, const R* nF, bool active, R am, const R* f,
+                                 const R* gt, R* gF) {
     const R J = det(nF);
     R cf[D * D];
     cof(nF, cf);
     R tr = 0;
 #pragma unroll
     for (int i = 0; i < D; ++i) tr += gt[i * D + i];
-    if (D == 2 && a.material == FIXED_COROTATED) {
+    if (D == 2 && c.material == FIXED_COROTATED) {
       const R xx = nF[0] + nF[3], yy = nF[2] - nF[1];
       const R r2 = xx * xx + yy * yy, r = dsqrt<R>(r2), r3 = r2 * r;
-      const R c = xx / r, s = yy / r;
-      const R Rm[4] = {c, -s, s, c};
+      const R cs = xx / r, s = yy / r;
+      const R Rm[4] = {cs, -s, s, cs};
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -180,7 +259,7 @@ struct Kern {
             acc += (gt[i * 2 + j] + gt[j * 2 + i]) * nF[j * 2 + q];
             acc2 += gt[j * 2 + i] * Rm[j * 2 + q];
           }
-          gF[i * 2 + q] += R(2) * a.mu * acc - R(2) * a.mu * acc2;
+          gF[i * 2 + q] += R(2) * c.mu * acc - R(2) * c.mu * acc2;
         }
       R gR[4];
 #pragma unroll
@@ -190,13 +269,13 @@ struct Kern {
           R acc = 0;
 #pragma unroll
           for (int j = 0; j < 2; ++j) acc += gt[i * 2 + j] * nF[j * 2 + q];
-          gR[i * 2 + q] = R(-2) * a.mu * acc;
+          gR[i * 2 + q] = R(-2) * c.mu * acc;
         }
       const R gc = gR[0] + gR[3], gs = -gR[1] + gR[2];
       const R gxx = gc * yy * yy / r3 - gs * xx * yy / r3;
       const R gyy = -gc * xx * yy / r3 + gs * xx * xx / r3;
       gF[0] += gxx; gF[3] += gxx; gF[2] += gyy; gF[1] -= gyy;
-      const R gJ = a.la * (R(2) * J - R(1)) * tr;
+      const R gJ = c.la * (R(2) * J - R(1)) * tr;
 #pragma unroll
       for (int e = 0; e < 4; ++e) gF[e] += gJ * cf[e];
     } else {
@@ -207,16 +286,14 @@ struct Kern {
           R acc = 0;
 #pragma unroll
           for (int j = 0; j < D; ++j) acc += (gt[i * D + j] + gt[j * D + i]) * nF[j * D + q];
-          gF[i * D + q] += a.mu * acc;
+          gF[i * D + q] += c.mu * acc;
         }
-      const R gJ = a.la * tr / J;
+      const R gJ = c.la * tr / J;
 #pragma unroll
       for (int e = 0; e < D * D; ++e) gF[e] += gJ * cf[e];
     }
     R gact = 0;
-    if (a.muscle[pidx] >= 0) {
-      const R am = act * a.act_strength;
-      const R* f = a.fibre + (size_t)pidx * D;
+    if (active) {
       R u[D];
 #pragma unroll
       for (int i = 0; i < D; ++i) {
@@ -238,298 +315,585 @@ struct Kern {
       for (int i = 0; i < D; ++i)
 #pragma unroll
         for (int q = 0; q < D; ++q) gF[i * D + q] += gu[i] * f[q];
-      gact = ga * a.act_strength;
+      gact = ga * c.act_strength;
     }
     return gact;
   }
+
+  // product weight of stencil node o and its gradient d w / d fx.  All 3^D
+  // stencil nodes lie inside the box of base cells (+2) that the grid
+  // kernels visit, so they hold finite values even where a weight is zero.
+  __device__ static R wgt(const R w[3][D], const int o[D]) {
+    R wt = 1;
+#pragma unroll
+    for (int d = 0; d < D; ++d) wt *= w[o[d]][d];
+    return wt;
+  }
+  __device__ static void dwgt(const R w[3][D], const R dw[3][D], const int o[D], R dwt[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      dwt[d] = dw[o[d]][d];
+#pragma unroll
+      for (int f = 0; f < D; ++f)
+        if (f != d) dwt[d] *= w[o[f]][f];
+    }
+  }
 };
 
+// blocked index of node I (per-dim coordinates) of env e
+template <typename R, int D>
+__device__ __forceinline__ long long node_index(const Phys<R>& c, int e, const int I[D]) {
+  constexpr int LOG = Blk<D>::LOG, SIDE = Blk<D>::SIDE;
+  long long blk = 0;
+  int loc = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    blk = blk * c.nb + (I[d] >> LOG);
+    loc = loc * SIDE + (I[d] & (SIDE - 1));
+  }
+  return ((long long)e * c.nblk + blk) * Blk<D>::NODES + loc;
+}
+
+template <typename R>
+__device__ __forceinline__ void red4(V4<R>* p, R x, R y, R z, R w);
+template <>
+__device__ __forceinline__ void red4<float>(V4<float>* p, float x, float y, float z, float w) {
+  atomicAdd(reinterpret_cast<float4*>(p), make_float4(x, y, z, w));
+}
+template <>
+__device__ __forceinline__ void red4<double>(V4<double>* p, double x, double y, double z, double w) {
+  atomicAdd(&p->x, x);
+  atomicAdd(&p->y, y);
+  atomicAdd(&p->z, z);
+  if (w != 0.0) atomicAdd(&p->w, w);
+}
+
+// The CTA's box of base cells, extended by the stencil (+2 per dim): the
+// nodes a CTA stages in shared memory.  n = 0 when the box exceeds the tile
+// capacity (global-atomic fallback).
+template <int D>
+struct Box {
+  int lo[D], ext[D], stride[D], n;
+  float rcp[D];
+  // tile index of base cell + 0 (add off() of a stencil offset)
+  __device__ __forceinline__ int index(const int base[D]) const {
+    int li = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) li += (base[d] - lo[d]) * stride[d];
+    return li;
+  }
+  __device__ __forceinline__ int off(const int o[D]) const {
+    int li = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) li += o[d] * stride[d];
+    return li;
+  }
+  // node coordinates of tile index li (li < n <= 4096: the float quotient is
+  // corrected to the exact one)
+  __device__ __forceinline__ void node(int li, int I[D]) const {
+#pragma unroll
+    for (int d = D - 1; d > 0; --d) {
+      int q = (int)(((float)li + 0.5f) * rcp[d]);
+      int r = li - q * ext[d];
+      if (r < 0) { --q; r += ext[d]; }
+      if (r >= ext[d]) { ++q; r -= ext[d]; }
+      I[d] = lo[d] + r;
+      li = q;
+    }
+    I[0] = lo[0] + li;
+  }
+};
+
+// the warp's box (all lanes call it); n = 0 when it exceeds the tile
+// capacity or no lane is valid
+template <typename R, int D>
+__device__ __forceinline__ Box<D> warp_box(const Phys<R>& c, bool valid, const int base[D]) {
+  Box<D> bx;
+  long long n = 1;
+  bool any = true;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int mn = __reduce_min_sync(0xffffffffu, valid ? base[d] : INT_MAX);
+    const int mx = __reduce_max_sync(0xffffffffu, valid ? base[d] : INT_MIN);
+    any = any && mn <= mx;
+    bx.lo[d] = mn;
+    bx.ext[d] = any ? mx - mn + 3 : 1;
+    bx.rcp[d] = 1.0f / (float)bx.ext[d];
+    n *= bx.ext[d];
+  }
+  int st = 1;
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    bx.stride[d] = st;
+    st *= bx.ext[d];
+  }
+  bx.n = (any && c.tile_cap > 0 && n <= c.tile_cap) ? (int)n : 0;
+  return bx;
+}
+
+// true when two valid lanes of the warp share a base cell (a hash collision
+// can only report a shared cell that is not there, which is safe)
+template <int D>
+__device__ __forceinline__ bool warp_dup_base(bool valid, const int base[D]) {
+  unsigned key = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) key = key * 4099u + (unsigned)base[d];
+  if (!valid) key = 0xffffffe0u | (threadIdx.x & 31);
+  const unsigned mm = __match_any_sync(0xffffffffu, key);
+  return __any_sync(0xffffffffu, __popc(mm) > 1);
+}
+
+// fold the warp's base cells into the env's box (lane 0: one atomic pair per dim)
+template <int D>
+__device__ __forceinline__ void warp_bbox(int* bbox, bool valid, const int base[D]) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int mn = __reduce_min_sync(0xffffffffu, valid ? base[d] : INT_MAX);
+    const int mx = __reduce_max_sync(0xffffffffu, valid ? base[d] : INT_MIN);
+    if ((threadIdx.x & 31) == 0 && mn <= mx) {
+      atomicMin(bbox + d, mn);
+      atomicMax(bbox + D + d, mx);
+    }
+  }
+}
+
+// add v to a warp-tile entry: plain read-modify-write when the warp's lanes
+// have distinct base cells (distinct entries per stencil offset), else atomic
+template <typename R>
+__device__ __forceinline__ void tile_add(R* p, R v, bool atomic) {
+  if (atomic) atomicAdd(p, v);
+  else *p += v;
+}
+
+// warp sum of D values, added to out[0..D) by lane 0
+template <typename R, int D>
+__device__ __forceinline__ void warp_sum_add(const R v[D], R* out) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    R s = v[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out + d, s);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ R ld(const R* p) { return __ldg(p); }
+
 // ------------------------------------------------------------------ forward
-// P2G (solver_mpm.py:83-124): scatter mass and APIC momentum with atomics;
-// optionally store F_{f+1}.
-template <typename R, int D>
-__global__ void p2g_kernel(Args<R> a, int write_F) {
+// G2P of step f (solver_mpm.py:146-165) fused with P2G of step f + 1
+// (solver_mpm.py:83-124); either half alone at the ends of a rollout.  The
+// 3^D stencil loops are unrolled so that the weights and tile offsets of a
+// node are compile-time selections.
+template <typename R, int D, int MODE, bool TILE>
+__global__ void __launch_bounds__(kChunk, 3) mpm_fwd_kernel(FwdArgs<R> a) {
   using K = Kern<R, D>;
-  const long long total = (long long)a.n_envs * a.P;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(q / a.P), p = (int)(q % a.P);
-    const R* xp = a.x + q * D;
-    const R* vp = a.v + q * D;
-    const R* Cp = a.C + q * D * D;
-    const R* Fp = a.F + q * D * D;
-    int base[D]; R fx[D], w[3][D], dw[3][D];
-    K::weights(xp, a.inv_dx, a.n_grid, base, fx, w, dw);
-    R nF[D * D], tau[D * D], aff[D * D];
-    K::new_F(Cp, Fp, a.dt, nF);
-    const int m = a.muscle[p];
-    const R act = m >= 0 ? a.act[(size_t)e * a.M + m] : R(0);
-    K::stress(a, nF, p, act, tau);
+  extern __shared__ __align__(16) unsigned char mpm_smem[];
+  const Phys<R>& c = a.c;
+  const int cap = c.tile_cap > 0 ? c.tile_cap : 1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  R* wt_tile = reinterpret_cast<R*>(mpm_smem) + (size_t)wid * kFwdPlanes * cap;  // [kFwdPlanes][cap]
+  const int e = blockIdx.x / c.n_chunks, ch = blockIdx.x % c.n_chunks;
+  const bool valid = (int)threadIdx.x < c.chunk_len[ch];
+  const int p = c.chunk_start[ch] + (valid ? (int)threadIdx.x : 0);
+  const long long q = (long long)e * c.P + p;
+  const long long EP = c.EP;
+  R x[D], v[D], Cm[D * D];
 #pragma unroll
-    for (int i = 0; i < D * D; ++i) aff[i] = -a.ks * tau[i] + a.mass * Cp[i];
-    if (write_F) {
+  for (int d = 0; d < D; ++d) x[d] = ld(a.x_in + d * EP + q);
+  int base[D];
+  R fx[D], w[3][D], dw[3][D];
+
+  if (MODE & 1) {
+    K::weights(x, c.inv_dx, c.n_grid, base, fx, w, dw);
 #pragma unroll
-      for (int i = 0; i < D * D; ++i) a.F1[q * D * D + i] = nF[i];
+    for (int i = 0; i < D; ++i) v[i] = 0;
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) Cm[i] = 0;
+    if (valid) {
+      const V4<R>* gv = a.gv + (size_t)e * c.nblk * Blk<D>::NODES;
+#pragma unroll
+      for (int nq = 0; nq < K::NN; ++nq) {
+        int o[D];
+        K::offs(nq, o);
+        const R wt = K::wgt(w, o);
+        int I[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
+        const V4<R> gg = ldg4(gv + node_index<R, D>(c, 0, I));
+        R g[D];
+        g[0] = gg.x;
+        g[1] = gg.y;
+        if (D == 3) g[D - 1] = gg.z;
+        const R s4 = R(4) * wt * c.inv_dx;
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          v[i] += wt * g[i];
+#pragma unroll
+          for (int j = 0; j < D; ++j) Cm[i * D + j] += s4 * g[i] * ((R)o[j] - fx[j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        x[i] += c.dt * v[i];
+        a.x_out[i * EP + q] = x[i];
+        if (a.v_out) a.v_out[i * EP + q] = v[i];
+      }
+      if (a.C_out) {
+#pragma unroll
+        for (int i = 0; i < D * D; ++i) a.C_out[i * EP + q] = Cm[i];
+      }
     }
-    R* gm = a.gm + (size_t)e * a.cells;
-    R* gmv = a.gmv + (size_t)e * a.cells * D;
-#pragma unroll 1
+  } else {
+#pragma unroll
+    for (int i = 0; i < D; ++i) v[i] = ld(a.v_in + i * EP + q);
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) Cm[i] = ld(a.C_in + i * EP + q);
+  }
+  if (a.csum) {
+    R s[D];
+    const R pwv = valid ? ld(c.pw + p) : R(0);
+#pragma unroll
+    for (int d = 0; d < D; ++d) s[d] = pwv * x[d];
+    warp_sum_add<R, D>(s, a.csum + (long long)e * D);
+  }
+  if (!(MODE & 2)) return;
+
+  // P2G of the state (x, v, Cm, F_in)
+  K::weights(x, c.inv_dx, c.n_grid, base, fx, w, dw);
+  R aff[D * D];  // affine momentum matrix times dx
+  {
+    R F[D * D], nF[D * D], tau[D * D];
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) F[i] = ld(a.F_in + i * EP + q);
+    K::new_F(Cm, F, c.dt, nF);
+    const int m = valid ? ld(c.muscle + p) : -1;
+    R f[D];
+    R am = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) f[d] = 0;
+    if (m >= 0) {
+      am = ld(a.act + (long long)e * c.M + m) * c.act_strength;
+#pragma unroll
+      for (int d = 0; d < D; ++d) f[d] = ld(c.fibre + (long long)d * c.P + p);
+    }
+    K::stress(c, nF, m >= 0, am, f, tau);
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) aff[i] = (-c.ks * tau[i] + c.mass * Cm[i]) * c.dx;
+    if (a.F_out && valid) {
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) a.F_out[i * EP + q] = nF[i];
+    }
+  }
+  warp_bbox<D>(a.bbox + (size_t)e * 2 * D, valid, base);
+  Box<D> bx;
+  bx.n = 0;
+  if (TILE) bx = warp_box<R, D>(c, valid, base);
+  const bool dup = bx.n ? warp_dup_base<D>(valid, base) : false;
+  if (bx.n) {
+    for (int li = lane; li < bx.n; li += 32) {
+      wt_tile[li] = 0;
+      wt_tile[cap + li] = 0;
+      wt_tile[2 * cap + li] = 0;
+      wt_tile[3 * cap + li] = 0;
+    }
+    __syncwarp();
+  }
+  {
+    // every lane runs the offsets so that the warp can sync between them
+    const int li0 = bx.index(base);
+    R mv[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) mv[i] = c.mass * v[i];
+#pragma unroll
     for (int nq = 0; nq < K::NN; ++nq) {
       int o[D];
       K::offs(nq, o);
-      R wt = 1, dpos[D];
+      const R wt = K::wgt(w, o);
+      if (valid) {
+        R mom[3] = {0, 0, 0};
 #pragma unroll
-      for (int d = 0; d < D; ++d) { wt *= w[o[d]][d]; dpos[d] = ((R)o[d] - fx[d]) * a.dx; }
-      const long long c = K::cell(a.n_grid, base, o);
+        for (int i = 0; i < D; ++i) {
+          R s = mv[i];
 #pragma unroll
-      for (int i = 0; i < D; ++i) {
-        R mom = a.mass * vp[i];
+          for (int j = 0; j < D; ++j) s += aff[i * D + j] * ((R)o[j] - fx[j]);
+          mom[i] = wt * s;
+        }
+        if (bx.n) {
+          const int li = li0 + bx.off(o);
+          tile_add(wt_tile + li, mom[0], dup);
+          tile_add(wt_tile + cap + li, mom[1], dup);
+          if (D == 3) tile_add(wt_tile + 2 * cap + li, mom[2], dup);
+          tile_add(wt_tile + 3 * cap + li, wt * c.mass, dup);
+        } else {
+          int I[D];
 #pragma unroll
-        for (int j = 0; j < D; ++j) mom += aff[i * D + j] * dpos[j];
-        atomicAdd(gmv + c * D + i, wt * mom);
+          for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
+          red4<R>(a.acc + node_index<R, D>(c, e, I), mom[0], mom[1], mom[2], wt * c.mass);
+        }
       }
-      atomicAdd(gm + c, wt * a.mass);
+      if (bx.n) __syncwarp();
+    }
+  }
+  if (bx.n) {
+    __syncwarp();
+    for (int li = lane; li < bx.n; li += 32) {
+      const R m = wt_tile[3 * cap + li];
+      if (m == R(0)) continue;  // no particle weight on this node
+      int I[D];
+      bx.node(li, I);
+      red4<R>(a.acc + node_index<R, D>(c, e, I), wt_tile[li], wt_tile[cap + li],
+              D == 3 ? wt_tile[2 * cap + li] : R(0), m);
     }
   }
 }
 
-// grid_op (solver_mpm.py:126-144): velocity, gravity on axis 1, sticky walls
+// Node n (0 <= n < count) of the blocks under env e's box of base cells
+// (+2 per dim); returns false past the last node.
 template <typename R, int D>
-__global__ void grid_op_kernel(Args<R> a) {
-  const long long total = (long long)a.n_envs * a.cells;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    long long r = q % a.cells;
+__device__ __forceinline__ bool box_node(const Phys<R>& c, const int* bb, long long n, int I[D], long long* node) {
+  constexpr int LOG = Blk<D>::LOG, SIDE = Blk<D>::SIDE;
+  int blo[D], bext[D];
+  long long nb = 1;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    if (bb[d] > bb[D + d]) return false;  // no particle
+    blo[d] = bb[d] >> LOG;
+    bext[d] = ((bb[D + d] + 2) >> LOG) - blo[d] + 1;
+    nb *= bext[d];
+  }
+  if (n >= nb * Blk<D>::NODES) return false;
+  long long bi = n / Blk<D>::NODES;
+  int loc = (int)(n % Blk<D>::NODES);
+  int b[D];
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    b[d] = blo[d] + (int)(bi % bext[d]);
+    bi /= bext[d];
+  }
+  long long blk = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) blk = blk * c.nb + b[d];
+  int l = loc;
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    I[d] = b[d] * SIDE + (l & (SIDE - 1));
+    l >>= LOG;
+  }
+  *node = blk * Blk<D>::NODES + loc;
+  return true;
+}
+
+// grid_op (solver_mpm.py:126-144) over the blocks under each env's box:
+// velocity, gravity on axis 1, sticky walls.  Consumes (and clears) the
+// accumulator, stores (velocity, mass) for G2P and the reverse pass, and
+// resets the next step's boxes.  Grid: (x, E).
+template <typename R, int D>
+__global__ void __launch_bounds__(256) mpm_grid_kernel(Phys<R> c, V4<R>* acc, V4<R>* gv, const int* bbox,
+                                                       int* bbox_next) {
+  const int e = blockIdx.y;
+  int bb[2 * D];
+#pragma unroll
+  for (int d = 0; d < 2 * D; ++d) bb[d] = bbox[e * 2 * D + d];
+  const size_t goff = (size_t)e * c.nblk * Blk<D>::NODES;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;; n += (long long)gridDim.x * blockDim.x) {
+    int I[D];
+    long long node;
+    if (!box_node<R, D>(c, bb, n, I, &node)) break;
     bool wall = false;
 #pragma unroll
-    for (int d = D - 1; d >= 0; --d) {
-      const int I = (int)(r % a.n_grid);
-      r /= a.n_grid;
-      wall |= (I < a.bound || I > a.n_grid - a.bound);
+    for (int d = 0; d < D; ++d) wall |= (I[d] < c.bound || I[d] > c.n_grid - c.bound);
+    const V4<R> s = acc[goff + node];
+    const R inv_m = R(1) / (s.w + R(1e-10));
+    V4<R> o;
+    o.x = inv_m * s.x;
+    o.y = inv_m * s.y + c.dt * c.gravity;
+    o.z = D == 3 ? inv_m * s.z : R(0);
+    if (wall) {
+      o.x = 0;
+      o.y = 0;
+      o.z = 0;
     }
-    const R inv_m = R(1) / (a.gm[q] + R(1e-10));
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      R vo = inv_m * a.gmv[q * D + i];
-      if (i == 1) vo += a.dt * a.gravity;
-      a.gvo[q * D + i] = wall ? R(0) : vo;
-    }
+    o.w = s.w;
+    gv[goff + node] = o;
+    acc[goff + node] = V4<R>{0, 0, 0, 0};
   }
+  if (bbox_next && blockIdx.x == 0 && threadIdx.x < 2 * D)
+    bbox_next[e * 2 * D + threadIdx.x] = threadIdx.x < D ? INT_MAX : INT_MIN;
 }
 
-// G2P (solver_mpm.py:146-165)
+// grid_op^T over the blocks under each env's box: consumes (and clears) the
+// velocity adjoint accumulator; writes (d velocity before the update, d mass).
 template <typename R, int D>
-__global__ void g2p_kernel(Args<R> a) {
-  using K = Kern<R, D>;
-  const long long total = (long long)a.n_envs * a.P;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(q / a.P);
-    const R* xp = a.x + q * D;
-    int base[D]; R fx[D], w[3][D], dw[3][D];
-    K::weights(xp, a.inv_dx, a.n_grid, base, fx, w, dw);
-    R nv[D], nC[D * D];
+__global__ void __launch_bounds__(256) mpm_grid_adj_kernel(Phys<R> c, V4<R>* gacc, const V4<R>* gv,
+                                                           V4<R>* ga, const int* bbox) {
+  const int e = blockIdx.y;
+  int bb[2 * D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) nv[i] = 0;
-#pragma unroll
-    for (int i = 0; i < D * D; ++i) nC[i] = 0;
-    const R* gvo = a.gvo + (size_t)e * a.cells * D;
-#pragma unroll 1
-    for (int nq = 0; nq < K::NN; ++nq) {
-      int o[D];
-      K::offs(nq, o);
-      R wt = 1, dpos[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) { wt *= w[o[d]][d]; dpos[d] = (R)o[d] - fx[d]; }
-      const long long c = K::cell(a.n_grid, base, o);
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        const R g = gvo[c * D + i];
-        nv[i] += wt * g;
-#pragma unroll
-        for (int j = 0; j < D; ++j) nC[i * D + j] += R(4) * wt * g * dpos[j] * a.inv_dx;
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      a.v1[q * D + i] = nv[i];
-      a.x1[q * D + i] = xp[i] + a.dt * nv[i];
-    }
-#pragma unroll
-    for (int i = 0; i < D * D; ++i) a.C1[q * D * D + i] = nC[i];
-  }
-}
-
-// ------------------------------------------------------------------ adjoint
-// G2P^T: scatter d grid velocity (atomics); write the x, v-independent parts
-// of the state-f adjoint (n* are overwritten here, accumulated by P2G^T).
-template <typename R, int D>
-__global__ void g2p_adj_kernel(Args<R> a) {
-  using K = Kern<R, D>;
-  const long long total = (long long)a.n_envs * a.P;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(q / a.P);
-    const R* xp = a.x + q * D;
-    int base[D]; R fx[D], w[3][D], dw[3][D];
-    K::weights(xp, a.inv_dx, a.n_grid, base, fx, w, dw);
-    R gvt[D], gfx[D];
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      gvt[i] = a.av[q * D + i] + a.dt * a.ax[q * D + i];
-      gfx[i] = 0;
-    }
-    const R* gC1 = a.aC + q * D * D;
-    const R* gvo = a.gvo + (size_t)e * a.cells * D;
-    R* ggvo = a.g_gvo + (size_t)e * a.cells * D;
-#pragma unroll 1
-    for (int nq = 0; nq < K::NN; ++nq) {
-      int o[D];
-      K::offs(nq, o);
-      R wt = 1, dpos[D], dwt[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) { wt *= w[o[d]][d]; dpos[d] = (R)o[d] - fx[d]; }
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        dwt[d] = dw[o[d]][d];
-#pragma unroll
-        for (int f = 0; f < D; ++f)
-          if (f != d) dwt[d] *= w[o[f]][f];
-      }
-      const long long c = K::cell(a.n_grid, base, o);
-      R gw = 0;
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        R gGC = 0;
-#pragma unroll
-        for (int j = 0; j < D; ++j) gGC += gC1[i * D + j] * dpos[j];
-        const R g = gvo[c * D + i];
-        atomicAdd(ggvo + c * D + i, wt * gvt[i] + R(4) * a.inv_dx * wt * gGC);
-        gw += gvt[i] * g + R(4) * a.inv_dx * g * gGC;
-      }
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        R acc = 0;
-#pragma unroll
-        for (int i = 0; i < D; ++i) acc += gC1[i * D + j] * gvo[c * D + i];
-        gfx[j] -= R(4) * a.inv_dx * wt * acc;
-      }
-#pragma unroll
-      for (int d = 0; d < D; ++d) gfx[d] += gw * dwt[d];
-    }
-#pragma unroll
-    for (int d = 0; d < D; ++d) a.nx[q * D + d] = a.ax[q * D + d] + gfx[d] * a.inv_dx;
-  }
-}
-
-// grid_op^T
-template <typename R, int D>
-__global__ void grid_op_adj_kernel(Args<R> a) {
-  const long long total = (long long)a.n_envs * a.cells;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    long long r = q % a.cells;
+  for (int d = 0; d < 2 * D; ++d) bb[d] = bbox[e * 2 * D + d];
+  const size_t goff = (size_t)e * c.nblk * Blk<D>::NODES;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;; n += (long long)gridDim.x * blockDim.x) {
+    int I[D];
+    long long node;
+    if (!box_node<R, D>(c, bb, n, I, &node)) break;
     bool wall = false;
 #pragma unroll
-    for (int d = D - 1; d >= 0; --d) {
-      const int I = (int)(r % a.n_grid);
-      r /= a.n_grid;
-      wall |= (I < a.bound || I > a.n_grid - a.bound);
+    for (int d = 0; d < D; ++d) wall |= (I[d] < c.bound || I[d] > c.n_grid - c.bound);
+    const V4<R> g = gacc[goff + node];
+    const V4<R> s = gv[goff + node];
+    const R inv_m = R(1) / (s.w + R(1e-10));
+    V4<R> o{0, 0, 0, 0};
+    if (!wall) {
+      // velocity before the update: v - dt g e_1 (momentum / mass)
+      const R vy = s.y - c.dt * c.gravity;
+      o.x = g.x * inv_m;
+      o.y = g.y * inv_m;
+      o.z = D == 3 ? g.z * inv_m : R(0);
+      o.w = -(g.x * s.x + g.y * vy + (D == 3 ? g.z * s.z : R(0))) * inv_m;
     }
-    R gmass = 0;
-    const R inv_m = R(1) / (a.gm[q] + R(1e-10));
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      const R g = wall ? R(0) : a.g_gvo[q * D + i];
-      a.g_gv[q * D + i] = g * inv_m;
-      gmass -= g * a.gmv[q * D + i] * inv_m * inv_m;
-    }
-    a.g_gm[q] = gmass;
+    ga[goff + node] = o;
+    gacc[goff + node] = V4<R>{0, 0, 0, 0};
   }
 }
 
-// P2G^T (and the adjoint of F_{f+1} = (I + dt C) F): gather grid adjoints,
-// finish the state-f adjoint, accumulate d actuation.
-template <typename R, int D>
-__global__ void p2g_adj_kernel(Args<R> a) {
+// ------------------------------------------------------------------ reverse
+// P2G^T of step f + seed of step f (mode bit 1), then G2P^T of step h (mode
+// bit 2).  Adjoint of solver_mpm.py:83-124 and :146-165.
+template <typename R, int D, int MODE, bool TILE>
+__global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
   using K = Kern<R, D>;
-  const long long total = (long long)a.n_envs * a.P;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(q / a.P), p = (int)(q % a.P);
-    const R* xp = a.x + q * D;
-    const R* vp = a.v + q * D;
-    const R* Cp = a.C + q * D * D;
-    const R* Fp = a.F + q * D * D;
-    int base[D]; R fx[D], w[3][D], dw[3][D];
-    K::weights(xp, a.inv_dx, a.n_grid, base, fx, w, dw);
-    R nFm[D * D], tau[D * D], aff[D * D];
-    K::new_F(Cp, Fp, a.dt, nFm);
-    const int m = a.muscle[p];
-    const R act = m >= 0 ? a.act[(size_t)e * a.M + m] : R(0);
-    K::stress(a, nFm, p, act, tau);
+  extern __shared__ __align__(16) unsigned char mpm_smem[];
+  const Phys<R>& c = a.c;
+  const int cap = c.tile_cap > 0 ? c.tile_cap : 1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  R* wt_tile = reinterpret_cast<R*>(mpm_smem) + (size_t)wid * kAdjPlanes * cap;  // [kAdjPlanes][cap]
+  const int e = blockIdx.x / c.n_chunks, ch = blockIdx.x % c.n_chunks;
+  const bool valid = (int)threadIdx.x < c.chunk_len[ch];
+  const int p = c.chunk_start[ch] + (valid ? (int)threadIdx.x : 0);
+  const long long q = (long long)e * c.P + p;
+  const long long EP = c.EP;
+  const size_t goff = (size_t)e * c.nblk * Blk<D>::NODES;
+  int base[D];
+  R fx[D], w[3][D], dw[3][D];
+  R ax[D], av[D], aC[D * D];
+
+  if (MODE & 1) {
+    R x[D], vp[D];
 #pragma unroll
-    for (int i = 0; i < D * D; ++i) aff[i] = -a.ks * tau[i] + a.mass * Cp[i];
-    R gaff[D * D], gfx[D], gvp[D];
+    for (int d = 0; d < D; ++d) {
+      x[d] = ld(a.x_f + d * EP + q);
+      vp[d] = ld(a.v_f + d * EP + q);
+    }
+    K::weights(x, c.inv_dx, c.n_grid, base, fx, w, dw);
+    const int m = valid ? ld(c.muscle + p) : -1;
+    R f[D], am = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) f[d] = 0;
+    if (m >= 0) {
+      am = ld(a.act_f + (long long)e * c.M + m) * c.act_strength;
+#pragma unroll
+      for (int d = 0; d < D; ++d) f[d] = ld(c.fibre + (long long)d * c.P + p);
+    }
+    R aff[D * D];  // affine momentum matrix times dx
+    {
+      R Cp[D * D], Fp[D * D], nF[D * D], tau[D * D];
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) {
+        Cp[i] = ld(a.C_f + i * EP + q);
+        Fp[i] = ld(a.F_f + i * EP + q);
+      }
+      K::new_F(Cp, Fp, c.dt, nF);
+      K::stress(c, nF, m >= 0, am, f, tau);
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) aff[i] = (-c.ks * tau[i] + c.mass * Cp[i]) * c.dx;
+    }
+    R gaff[D * D], gfx[D];  // gaff: d loss / d (affine matrix times dx)
 #pragma unroll
     for (int i = 0; i < D * D; ++i) gaff[i] = 0;
 #pragma unroll
-    for (int i = 0; i < D; ++i) { gfx[i] = 0; gvp[i] = 0; }
-    const R* ggv = a.g_gv + (size_t)e * a.cells * D;
-    const R* ggm = a.g_gm + (size_t)e * a.cells;
-#pragma unroll 1
-    for (int nq = 0; nq < K::NN; ++nq) {
-      int o[D];
-      K::offs(nq, o);
-      R wt = 1, dpos[D], dwt[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) { wt *= w[o[d]][d]; dpos[d] = ((R)o[d] - fx[d]) * a.dx; }
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        dwt[d] = dw[o[d]][d];
-#pragma unroll
-        for (int f = 0; f < D; ++f)
-          if (f != d) dwt[d] *= w[o[f]][f];
-      }
-      const long long c = K::cell(a.n_grid, base, o);
-      R gg[D];
-#pragma unroll
-      for (int i = 0; i < D; ++i) gg[i] = ggv[c * D + i];
-      R gw = ggm[c] * a.mass;
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        R mom = a.mass * vp[i];
-#pragma unroll
-        for (int j = 0; j < D; ++j) mom += aff[i * D + j] * dpos[j];
-        gw += gg[i] * mom;
-        gvp[i] += wt * a.mass * gg[i];
-#pragma unroll
-        for (int j = 0; j < D; ++j) gaff[i * D + j] += wt * gg[i] * dpos[j];
-      }
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        R acc = 0;
-#pragma unroll
-        for (int i = 0; i < D; ++i) acc += aff[i * D + j] * gg[i];
-        gfx[j] -= wt * acc * a.dx;
-      }
-#pragma unroll
-      for (int d = 0; d < D; ++d) gfx[d] += gw * dwt[d];
+    for (int i = 0; i < D; ++i) {
+      gfx[i] = 0;
+      av[i] = 0;
     }
-    R gtau[D * D], gnF[D * D];
+    if (valid) {
 #pragma unroll
-    for (int i = 0; i < D * D; ++i) {
-      gtau[i] = -a.ks * gaff[i];
-      gnF[i] = a.aF[q * D * D + i];
+      for (int nq = 0; nq < K::NN; ++nq) {
+        int o[D];
+        K::offs(nq, o);
+        const R wt = K::wgt(w, o);
+        R dwt[D], dp[D], gg[D];
+        K::dwgt(w, dw, o, dwt);
+        int I[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          dp[d] = (R)o[d] - fx[d];
+          I[d] = base[d] + o[d];
+        }
+        const V4<R> g4 = ldg4(a.ga + goff + node_index<R, D>(c, 0, I));
+        gg[0] = g4.x;
+        gg[1] = g4.y;
+        if (D == 3) gg[D - 1] = g4.z;
+        R gw = g4.w * c.mass;
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          R mom = c.mass * vp[i];
+#pragma unroll
+          for (int j = 0; j < D; ++j) mom += aff[i * D + j] * dp[j];
+          gw += gg[i] * mom;
+          av[i] += wt * c.mass * gg[i];
+          const R wg = wt * gg[i];
+#pragma unroll
+          for (int j = 0; j < D; ++j) gaff[i * D + j] += wg * dp[j];
+        }
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          R acc = 0;
+#pragma unroll
+          for (int i = 0; i < D; ++i) acc += aff[i * D + j] * gg[i];
+          gfx[j] -= wt * acc;
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) gfx[d] += gw * dwt[d];
+      }
     }
-    const R ga = K::stress_adj(a, nFm, p, act, gtau, gnF);
-    if (m >= 0 && ga != R(0)) atomicAdd(a.gact + (size_t)e * a.M + m, ga);
-    // state-f adjoint: x (nx already holds the G2P^T part), v, C, F
+    // stress adjoint: reload C, F (cheaper than keeping them live)
+    R Cp[D * D], Fp[D * D], gnF[D * D], gact;
+    {
+      R nF[D * D], gtau[D * D];
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) {
+        Cp[i] = ld(a.C_f + i * EP + q);
+        Fp[i] = ld(a.F_f + i * EP + q);
+        gtau[i] = -c.ks * c.dx * gaff[i];
+        gnF[i] = valid ? ld(a.aF_in + i * EP + q) : R(0);
+      }
+      K::new_F(Cp, Fp, c.dt, nF);
+      gact = K::stress_adj(c, nF, m >= 0, am, f, gtau, gnF);
+    }
+    // d actuation: warp-aggregated when the warp's particles share a muscle
+    {
+      const unsigned full = 0xffffffffu;
+      const int m0 = __shfl_sync(full, m, 0);
+      R* ga_e = a.gact + (long long)e * c.M;
+      if (__all_sync(full, m == m0)) {
+        R s = gact;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
+        if (lane == 0 && m0 >= 0) atomicAdd(ga_e + m0, s);
+      } else if (m >= 0) {
+        atomicAdd(ga_e + m, gact);
+      }
+    }
+    // complete the state-f adjoint (+ loss seed of step f)
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      a.nx[q * D + d] += gfx[d] * a.inv_dx;
-      a.nv[q * D + d] = gvp[d];
+      R s = 0;
+      if (a.seed_w != R(0) && valid)
+        s = R(2) * a.seed_w * (ld(a.csum + (long long)e * D + d) / a.pw_sum - ld(a.target + (long long)e * D + d)) *
+            ld(c.pw + p) / a.pw_sum;
+      ax[d] = (valid ? ld(a.ax_in + d * EP + q) : R(0)) + gfx[d] * c.inv_dx + s;
     }
+    R* aF_dst = (MODE & 2) ? a.aF_out : a.out_aF;
 #pragma unroll
     for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -538,52 +902,138 @@ __global__ void p2g_adj_kernel(Args<R> a) {
 #pragma unroll
         for (int k = 0; k < D; ++k) {
           accC += gnF[i * D + k] * Fp[j * D + k];
-          accF += ((k == i ? R(1) : R(0)) + a.dt * Cp[k * D + i]) * gnF[k * D + j];
+          accF += ((k == i ? R(1) : R(0)) + c.dt * Cp[k * D + i]) * gnF[k * D + j];
         }
-        a.nC[q * D * D + i * D + j] = a.mass * gaff[i * D + j] + a.dt * accC;
-        a.nF[q * D * D + i * D + j] = accF;
+        aC[i * D + j] = c.mass * c.dx * gaff[i * D + j] + c.dt * accC;
+        if (valid) aF_dst[(i * D + j) * EP + q] = accF;
       }
+    if (!(MODE & 2)) {
+      if (valid) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          a.out_ax[d * EP + q] = ax[d];
+          a.out_av[d * EP + q] = av[d];
+        }
+#pragma unroll
+        for (int i = 0; i < D * D; ++i) a.out_aC[i * EP + q] = aC[i];
+      }
+      return;
+    }
+  } else {
+    // first reverse step: a_x(T) is the loss seed of step T, a_v = a_C = 0
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      ax[d] = 0;
+      av[d] = 0;
+      if (a.seed_w != R(0) && valid)
+        ax[d] = R(2) * a.seed_w * (ld(a.csum + (long long)e * D + d) / a.pw_sum - ld(a.target + (long long)e * D + d)) *
+                ld(c.pw + p) / a.pw_sum;
+    }
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) aC[i] = 0;
+    if (valid) {
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) a.aF_out[i * EP + q] = 0;
+    }
+  }
+
+  // G2P^T of step h: gather the grid velocity of step h through L1, scatter
+  // the velocity adjoint through the warp tile
+  R xh[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) xh[d] = ld(a.x_h + d * EP + q);
+  K::weights(xh, c.inv_dx, c.n_grid, base, fx, w, dw);
+  Box<D> bx;
+  bx.n = 0;
+  if (TILE) bx = warp_box<R, D>(c, valid, base);
+  const bool dup = bx.n ? warp_dup_base<D>(valid, base) : false;
+  if (bx.n) {
+    for (int li = lane; li < bx.n; li += 32) {
+      wt_tile[li] = 0;
+      wt_tile[cap + li] = 0;
+      wt_tile[2 * cap + li] = 0;
+    }
+    __syncwarp();
+  }
+  {
+    R gvt[D], gfx[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      gvt[i] = av[i] + c.dt * ax[i];
+      gfx[i] = 0;
+    }
+    const R s4 = R(4) * c.inv_dx;
+    const int li0 = bx.index(base);
+#pragma unroll
+    for (int nq = 0; nq < K::NN; ++nq) {
+      int o[D];
+      K::offs(nq, o);
+      const R wt = K::wgt(w, o);
+      if (valid) {
+        R dwt[D], dp[D], g[D];
+        K::dwgt(w, dw, o, dwt);
+        int I[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          dp[d] = (R)o[d] - fx[d];
+          I[d] = base[d] + o[d];
+        }
+        const long long gidx = node_index<R, D>(c, e, I);
+        const V4<R> g4 = ldg4(a.gv_h + gidx);
+        g[0] = g4.x;
+        g[1] = g4.y;
+        if (D == 3) g[D - 1] = g4.z;
+        R gw = 0, sc[3] = {0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          R gGC = 0;
+#pragma unroll
+          for (int j = 0; j < D; ++j) gGC += aC[i * D + j] * dp[j];
+          sc[i] = wt * (gvt[i] + s4 * gGC);
+          gw += g[i] * (gvt[i] + s4 * gGC);
+        }
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          R acc = 0;
+#pragma unroll
+          for (int i = 0; i < D; ++i) acc += aC[i * D + j] * g[i];
+          gfx[j] -= s4 * wt * acc;
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) gfx[d] += gw * dwt[d];
+        if (bx.n) {
+          const int li = li0 + bx.off(o);
+          tile_add(wt_tile + li, sc[0], dup);
+          tile_add(wt_tile + cap + li, sc[1], dup);
+          if (D == 3) tile_add(wt_tile + 2 * cap + li, sc[2], dup);
+        } else {
+          red4<R>(a.gacc + gidx, sc[0], sc[1], sc[2], R(0));
+        }
+      }
+      if (bx.n) __syncwarp();
+    }
+    if (valid) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) a.ax_out[d * EP + q] = ax[d] + gfx[d] * c.inv_dx;
+    }
+  }
+  if (bx.n) {
+    __syncwarp();
+    for (int li = lane; li < bx.n; li += 32) {
+      const R s0 = wt_tile[li], s1 = wt_tile[cap + li], s2 = D == 3 ? wt_tile[2 * cap + li] : R(0);
+      if (s0 == R(0) && s1 == R(0) && s2 == R(0)) continue;
+      int I[D];
+      bx.node(li, I);
+      red4<R>(a.gacc + node_index<R, D>(c, e, I), s0, s1, s2, R(0));
+    }
   }
 }
 
-// weighted centre of every env: c = sum pw x / sum pw  (one block per env)
-template <typename R, int D>
-__global__ void center_kernel(const R* __restrict__ x, const R* __restrict__ pw, R pw_sum, int P,
-                              R* __restrict__ out) {
-  __shared__ R red[32 * 3];
-  const int e = blockIdx.x;
-  R s[3] = {0, 0, 0};
-  for (int p = threadIdx.x; p < P; p += blockDim.x) {
-    const R wgt = pw[p];
-#pragma unroll
-    for (int d = 0; d < D; ++d) s[d] += wgt * x[((size_t)e * P + p) * D + d];
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int d = 0; d < D; ++d)
-    for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
-  if (lane == 0)
-    for (int d = 0; d < D; ++d) red[d * 32 + wid] = s[d];
-  __syncthreads();
-  if (threadIdx.x < D) {
-    R acc = 0;
-    for (int w2 = 0; w2 < nw; ++w2) acc += red[threadIdx.x * 32 + w2];
-    out[(size_t)e * D + threadIdx.x] = acc / pw_sum;
-  }
-}
-
-// loss seed at step t: a_x += 2 w (c - target) pw / sum pw
-template <typename R, int D>
-__global__ void seed_kernel(R* __restrict__ ax, const R* __restrict__ center, const R* __restrict__ target,
-                            const R* __restrict__ pw, R weight, R pw_sum, int n_envs, int P) {
-  const long long total = (long long)n_envs * P;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(q / P), p = (int)(q % P);
-#pragma unroll
-    for (int d = 0; d < D; ++d)
-      ax[q * D + d] += R(2) * weight * (center[(size_t)e * D + d] - target[(size_t)e * D + d]) * pw[p] / pw_sum;
-  }
+// empty boxes (min = INT_MAX, max = INT_MIN) for n_env envs
+template <int D>
+__global__ void mpm_bbox_reset_kernel(int* bbox, int n_env) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_env * 2 * D) bbox[i] = (i % (2 * D)) < D ? INT_MAX : INT_MIN;
 }
 
 }  // namespace mpm

@@ -1,17 +1,24 @@
 // mpm_runtime.cu -- cls_mpm_* C ABI: MLS-MPM episodes with checkpointed
-// reverse passes (forward keeps a checkpoint every K steps; the reverse pass
-// recomputes each segment, then for every step rebuilds its grid and runs the
-// adjoint kernels, as the reference's advance_core_grad does per step).
+// reverse passes.  The first pass keeps the particle state every K steps; the
+// reverse pass recomputes each segment's states and grids into a record (two
+// records, alternating by segment), then runs one grid-adjoint and one fused
+// particle-adjoint launch per step.  The reference's advance_core_grad
+// (solver_mpm.py:182-190) rebuilds a step's grid before its adjoint; here the
+// grid recorded by the recompute is reused.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <numeric>
 #include <string>
 #include <vector>
 
 #include "../../include/cls_b200.h"
+#include "cls_profile.cuh"
 #include "mpm_kernels.cuh"
 
 namespace cls {
@@ -65,10 +72,17 @@ class MpmBase {
   virtual void centers(double* c) = 0;
   virtual void graph_capture(int steps) = 0;
   virtual void graph_launch() = 0;
+  virtual void profile_enable(bool on) = 0;
+  virtual void profile_read(double* ms, long long* launches, bool reset) = 0;
 };
+
+// launch categories of the per-kernel profile (CLS_MPM_PROFILE_KINDS)
+enum MpmKind : int { MK_PFWD = 0, MK_PREC, MK_GRID, MK_PADJ, MK_GADJ, MK_OTHER, MK_COUNT };
 
 template <typename R, int D>
 class MpmImpl final : public MpmBase {
+  using V = V4<R>;
+
  public:
   MpmImpl(const cls_mpm_body& b, const cls_mpm_params& p, int n_envs) : p_(p) {
     E_ = n_envs;
@@ -77,33 +91,60 @@ class MpmImpl final : public MpmBase {
     T_ = p.max_steps;
     K_ = std::max(1, p.checkpoint_every);
     n_grid_ = p.n_grid;
-    cells_ = 1;
-    for (int d = 0; d < D; ++d) cells_ *= n_grid_;
-    const size_t EP = (size_t)E_ * P_;
+    MPM_REQUIRE(M_ <= kMaxMuscles, "at most 256 muscle groups");
+    MPM_REQUIRE(E_ <= 65535, "at most 65535 envs per handle");
+    MPM_REQUIRE((long long)E_ * P_ < (1LL << 31) / (D * D), "too many particles");
+    tile_cap_ = p.tile_nodes > 0 ? p.tile_nodes : 0;
+    MPM_REQUIRE(tile_cap_ <= 1024, "tile_nodes must be at most 1024");
+    nb_ = (n_grid_ + Blk<D>::SIDE - 1) / Blk<D>::SIDE;
+    nblk_ = 1;
+    for (int d = 0; d < D; ++d) nblk_ *= nb_;
+    MPM_REQUIRE((long long)E_ * nblk_ < (1LL << 31), "grid too large");
+    slots_ = std::max(K_, 2);
     n_ckpt_ = (T_ + K_ - 1) / K_ + 1;
-    ck_x_.alloc(n_ckpt_ * EP * D); ck_v_.alloc(n_ckpt_ * EP * D);
-    ck_C_.alloc(n_ckpt_ * EP * D * D); ck_F_.alloc(n_ckpt_ * EP * D * D);
-    rc_x_.alloc((K_ + 1) * EP * D); rc_v_.alloc((K_ + 1) * EP * D);
-    rc_C_.alloc((K_ + 1) * EP * D * D); rc_F_.alloc((K_ + 1) * EP * D * D);
+    build_order(b);
+    n_chunks_ = (int)chunk_start_h_.size();
+    MPM_REQUIRE((long long)E_ * n_chunks_ < (1LL << 31), "too many particle chunks");
+
+    const size_t EP = (size_t)E_ * P_, VX = EP * D, VM = EP * D * D;
+    const size_t nodes = (size_t)E_ * nblk_ * Blk<D>::NODES;
+    ck_x_.alloc(n_ckpt_ * VX); ck_v_.alloc(n_ckpt_ * VX);
+    ck_C_.alloc(n_ckpt_ * VM); ck_F_.alloc(n_ckpt_ * VM);
     for (int s = 0; s < 2; ++s) {
-      ax_[s].alloc(EP * D); av_[s].alloc(EP * D); aC_[s].alloc(EP * D * D); aF_[s].alloc(EP * D * D);
+      X_[s].alloc(VX); Fw_[s].alloc(VM);
+      RX_[s].alloc(K_ * VX); RV_[s].alloc(K_ * VX); RC_[s].alloc(K_ * VM); RF_[s].alloc(K_ * VM);
+      AX_[s].alloc(VX); AF_[s].alloc(VM);
+      gv_[s].alloc(slots_ * nodes);
     }
-    fin_x_.alloc(EP * D); fin_v_.alloc(EP * D); fin_C_.alloc(EP * D * D); fin_F_.alloc(EP * D * D);
-    gm_.alloc((size_t)E_ * cells_); gmv_.alloc((size_t)E_ * cells_ * D); gvo_.alloc((size_t)E_ * cells_ * D);
-    g_gvo_.alloc((size_t)E_ * cells_ * D); g_gv_.alloc((size_t)E_ * cells_ * D); g_gm_.alloc((size_t)E_ * cells_);
+    bboxes_.alloc((size_t)2 * slots_ * E_ * 2 * D);
+    acc_.alloc(nodes); gacc_.alloc(nodes); ga_.alloc(nodes);
+    fin_x_.alloc(VX); fin_v_.alloc(VX); fin_C_.alloc(VM); fin_F_.alloc(VM);
+    out_ax_.alloc(VX); out_av_.alloc(VX); out_aC_.alloc(VM); out_aF_.alloc(VM);
     act_.alloc((size_t)T_ * E_ * M_); gact_.alloc((size_t)T_ * E_ * M_);
-    center_.alloc((size_t)(T_ + 1) * E_ * D);
+    csum_.alloc((size_t)(T_ + 1) * E_ * D);
     target_.alloc((size_t)(T_ + 1) * E_ * D);
     muscle_.alloc(P_); fibre_.alloc((size_t)P_ * D); pw_.alloc(P_);
-    stage_.alloc(std::max<size_t>({(size_t)T_ * E_ * M_, EP * D * D, (size_t)(T_ + 1) * E_ * D, (size_t)P_ * D}));
-    std::vector<int> mus(b.muscle ? b.muscle : nullptr, b.muscle ? b.muscle + P_ : nullptr);
-    if (mus.empty()) mus.assign(P_, -1);
-    for (int m : mus) MPM_REQUIRE(m >= -1 && m < M_, "muscle index out of range");
+    chunk_start_.alloc(n_chunks_); chunk_len_.alloc(n_chunks_);
+    MPM_CUDA(cudaMemcpy(chunk_start_.p, chunk_start_h_.data(), sizeof(int) * n_chunks_, cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(chunk_len_.p, chunk_len_h_.data(), sizeof(int) * n_chunks_, cudaMemcpyHostToDevice));
+    // accumulators and flags start (and stay, between steps) zero; the grid
+    // buffers start zero so that unvisited nodes hold finite values
+    MPM_CUDA(cudaMemset(acc_.p, 0, sizeof(V) * nodes));
+    MPM_CUDA(cudaMemset(gacc_.p, 0, sizeof(V) * nodes));
+    MPM_CUDA(cudaMemset(ga_.p, 0, sizeof(V) * nodes));
+    for (int s = 0; s < 2; ++s) MPM_CUDA(cudaMemset(gv_[s].p, 0, sizeof(V) * slots_ * nodes));
+
+    std::vector<int> mus(P_, -1);
+    for (int i = 0; i < P_; ++i) {
+      const int m = b.muscle ? b.muscle[perm_[i]] : -1;
+      MPM_REQUIRE(m >= -1 && m < M_, "muscle index out of range");
+      mus[i] = m;
+    }
     MPM_CUDA(cudaMemcpy(muscle_.p, mus.data(), sizeof(int) * P_, cudaMemcpyHostToDevice));
     std::vector<R> fib((size_t)P_ * D, R(0));
-    for (int q = 0; q < P_; ++q)
+    for (int i = 0; i < P_; ++i)
       for (int d = 0; d < D; ++d)
-        fib[(size_t)q * D + d] = b.fibre ? (R)b.fibre[(size_t)q * D + d] : (d == 1 ? R(1) : R(0));
+        fib[(size_t)d * P_ + i] = b.fibre ? (R)b.fibre[(size_t)perm_[i] * D + d] : (d == 1 ? R(1) : R(0));
     MPM_CUDA(cudaMemcpy(fibre_.p, fib.data(), sizeof(R) * fib.size(), cudaMemcpyHostToDevice));
     std::vector<R> pw(P_, R(1));
     pw_sum_ = P_;
@@ -111,6 +152,17 @@ class MpmImpl final : public MpmBase {
     loss_w_.assign(T_ + 1, 0.0);
     MPM_CUDA(cudaMemset(act_.p, 0, sizeof(R) * act_.n));
     MPM_CUDA(cudaMemset(target_.p, 0, sizeof(R) * target_.n));
+    // shared-memory opt-in for the tile
+    fwd_smem_ = tile_cap_ > 0 ? (size_t)kWarps * kFwdPlanes * tile_cap_ * sizeof(R) : 0;
+    adj_smem_ = tile_cap_ > 0 ? (size_t)kWarps * kAdjPlanes * tile_cap_ * sizeof(R) : 0;
+    if (tile_cap_ > 0) {
+      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
+      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
+      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
+    }
     // initial state: body positions in every env, v = C = 0, F = I
     std::vector<double> x0(EP * D), v0(EP * D, 0.0);
     for (int e = 0; e < E_; ++e)
@@ -124,158 +176,300 @@ class MpmImpl final : public MpmBase {
     if (graph_) cudaGraphDestroy(graph_);
   }
 
-  Args<R> base_args() const {
-    Args<R> a;
+  // Internal particle order: Morton order of the initial cells (ties by
+  // position), cut into chunks of at most kChunk (below); inside a chunk the
+  // i-th particle of every cell comes first, so that a warp's lanes sit in
+  // different cells.
+  void build_order(const cls_mpm_body& b) {
+    std::vector<unsigned long long> key(P_);
+    std::map<unsigned long long, int> cells;
+    for (int u = 0; u < P_; ++u) {
+      unsigned long long k = 0;
+      int cc[D];
+      for (int d = 0; d < D; ++d) {
+        const double c = std::floor(b.positions[(size_t)u * D + d] * n_grid_);
+        cc[d] = (int)std::min<double>(std::max<double>(c, 0.0), n_grid_ - 1);
+      }
+      for (int bit = 20; bit >= 0; --bit)
+        for (int d = 0; d < D; ++d) k = (k << 1) | ((cc[d] >> bit) & 1);
+      key[u] = k;
+      cells[k] += 1;
+    }
+    std::vector<int> order(P_);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+      if (key[a] != key[c]) return key[a] < key[c];
+      for (int d = 0; d < D; ++d) {
+        const double pa = b.positions[(size_t)a * D + d], pc = b.positions[(size_t)c * D + d];
+        if (pa != pc) return pa < pc;
+      }
+      return false;
+    });
+    const int per_cell = std::max(1, std::min(8, (int)std::lround((double)P_ / (double)cells.size())));
+    // chunks: aligned Morton groups of 32 cells (4x4x2) in 3D or 64 cells
+    // (8x8) in 2D, split at kChunk particles.  With the interleave below, the
+    // warps of a full group each hold one particle of every cell, so their
+    // lanes have distinct base cells and a compact stencil box.
+    const int group_shift = D == 3 ? 5 : 6;
+    chunk_start_h_.clear();
+    chunk_len_h_.clear();
+    for (int i = 0; i < P_;) {
+      const unsigned long long g = key[order[i]] >> group_shift;
+      int j = i;
+      while (j < P_ && j - i < kChunk && (key[order[j]] >> group_shift) == g) ++j;
+      chunk_start_h_.push_back(i);
+      chunk_len_h_.push_back(j - i);
+      i = j;
+    }
+    perm_.resize(P_);
+    for (size_t ch = 0; ch < chunk_start_h_.size(); ++ch) {
+      const int c0 = chunk_start_h_[ch], len = chunk_len_h_[ch];
+      std::vector<int> pos(len);
+      std::iota(pos.begin(), pos.end(), 0);
+      std::stable_sort(pos.begin(), pos.end(), [&](int a, int c) { return a % per_cell < c % per_cell; });
+      for (int t = 0; t < len; ++t) perm_[c0 + t] = order[c0 + pos[t]];
+    }
+  }
+
+  Phys<R> phys() const {
+    Phys<R> c;
+    std::memset(&c, 0, sizeof(c));
+    c.E = E_; c.P = P_; c.M = M_; c.material = p_.material; c.n_chunks = n_chunks_; c.tile_cap = tile_cap_;
+    c.n_grid = n_grid_; c.nb = nb_; c.bound = p_.bound; c.nblk = nblk_; c.EP = (long long)E_ * P_;
+    c.dx = (R)(1.0 / n_grid_); c.inv_dx = (R)n_grid_; c.dt = (R)p_.dt;
+    c.ks = (R)(p_.dt * p_.p_vol * 4.0 * n_grid_ * n_grid_);
+    c.mu = (R)p_.mu; c.la = (R)p_.la; c.act_strength = (R)p_.act_strength;
+    c.gravity = (R)p_.gravity; c.mass = (R)p_.mass;
+    c.muscle = muscle_.p; c.fibre = fibre_.p; c.pw = pw_.p;
+    c.chunk_start = chunk_start_.p; c.chunk_len = chunk_len_.p;
+    return c;
+  }
+
+  size_t VX() const { return (size_t)E_ * P_ * D; }
+  size_t VM() const { return (size_t)E_ * P_ * D * D; }
+  size_t NODES() const { return (size_t)E_ * nblk_ * Blk<D>::NODES; }
+
+  // checkpoint s, record slot k of record r, work buffers
+  R* ckx(int s) { return ck_x_.p + (size_t)s * VX(); }
+  R* ckv(int s) { return ck_v_.p + (size_t)s * VX(); }
+  R* ckC(int s) { return ck_C_.p + (size_t)s * VM(); }
+  R* ckF(int s) { return ck_F_.p + (size_t)s * VM(); }
+  V* gv(int r, int k) { return gv_[r].p + (size_t)k * NODES(); }
+  int* bbox(int r, int k) { return bboxes_.p + ((size_t)r * slots_ + k) * E_ * 2 * D; }
+  // state of step t0(s) + k of segment s (slot 0 is the checkpoint)
+  R* rx(int s, int k) { return k == 0 ? ckx(s) : RX_[s % 2].p + (size_t)k * VX(); }
+  R* rv(int s, int k) { return k == 0 ? ckv(s) : RV_[s % 2].p + (size_t)k * VX(); }
+  R* rC(int s, int k) { return k == 0 ? ckC(s) : RC_[s % 2].p + (size_t)k * VM(); }
+  R* rF(int s, int k) { return k == 0 ? ckF(s) : RF_[s % 2].p + (size_t)k * VM(); }
+  // first pass: x and F of step g (checkpoint steps live in the checkpoints)
+  R* fx(int g) { return g % K_ == 0 ? ckx(g / K_) : X_[g % 2].p; }
+  R* fF(int g) { return g % K_ == 0 ? ckF(g / K_) : Fw_[g % 2].p; }
+  const R* act(int g) const { return act_.p + (size_t)g * E_ * M_; }
+
+  int particle_grid() const { return E_ * n_chunks_; }
+
+  template <typename F>
+  void timed(int kind, F&& f) {
+    MPM_CUDA(prof_.run(kind, stream, std::forward<F>(f)));
+  }
+
+  template <bool TILE>
+  void fwd_t(int mode, const FwdArgs<R>& a) {
+    if (mode == 1) mpm_fwd_kernel<R, D, 1, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+    else if (mode == 2) mpm_fwd_kernel<R, D, 2, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+    else mpm_fwd_kernel<R, D, 3, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+  }
+  template <bool TILE>
+  void adj_t(int mode, const AdjArgs<R>& a) {
+    if (mode == 1) mpm_adj_kernel<R, D, 1, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+    else if (mode == 2) mpm_adj_kernel<R, D, 2, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+    else mpm_adj_kernel<R, D, 3, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+  }
+  void launch_fwd(int mode, const FwdArgs<R>& a, int kind) {
+    timed(kind, [&] {
+      if (tile_cap_ > 0) fwd_t<true>(mode, a);
+      else fwd_t<false>(mode, a);
+    });
+  }
+  void launch_adj(int mode, const AdjArgs<R>& a) {
+    timed(MK_PADJ, [&] {
+      if (tile_cap_ > 0) adj_t<true>(mode, a);
+      else adj_t<false>(mode, a);
+    });
+  }
+  dim3 grid_dims() const { return dim3((unsigned)std::max(1, 148 * 4 / E_), (unsigned)E_); }
+  void launch_grid(V* gvo, int r, int k, int* bbox_next) {
+    const Phys<R> c = phys();
+    timed(MK_GRID, [&] {
+      mpm_grid_kernel<R, D><<<grid_dims(), 256, 0, stream>>>(c, acc_.p, gvo, bbox(r, k), bbox_next);
+    });
+  }
+  void reset_bbox(int r, int k) {
+    timed(MK_OTHER, [&] {
+      mpm_bbox_reset_kernel<D><<<(E_ * 2 * D + 255) / 256, 256, 0, stream>>>(bbox(r, k), E_);
+    });
+  }
+
+  FwdArgs<R> fwd_args() const {
+    FwdArgs<R> a;
     std::memset(&a, 0, sizeof(a));
-    a.n_envs = E_; a.P = P_; a.M = M_; a.n_grid = n_grid_; a.bound = p_.bound; a.material = p_.material;
-    a.cells = cells_;
-    a.dx = (R)(1.0 / n_grid_); a.inv_dx = (R)n_grid_; a.dt = (R)p_.dt;
-    a.ks = (R)(p_.dt * p_.p_vol * 4.0 * n_grid_ * n_grid_);
-    a.mu = (R)p_.mu; a.la = (R)p_.la; a.act_strength = (R)p_.act_strength;
-    a.gravity = (R)p_.gravity; a.mass = (R)p_.mass;
-    a.muscle = muscle_.p; a.fibre = fibre_.p;
-    a.gm = gm_.p; a.gmv = gmv_.p; a.gvo = gvo_.p;
-    a.g_gvo = g_gvo_.p; a.g_gv = g_gv_.p; a.g_gm = g_gm_.p;
+    a.c = phys();
+    a.acc = acc_.p;
     return a;
   }
 
-  size_t EP() const { return (size_t)E_ * P_; }
-  static int blocks(long long n) { return (int)std::max<long long>(1, std::min<long long>(148 * 32, (n + 255) / 256)); }
-
-  // one forward step from (x, v, C, F) to (x1, v1, C1, F1)
-  void step(const R* x, const R* v, const R* C, const R* F, R* x1, R* v1, R* C1, R* F1, int f, bool write_F) {
-    Args<R> a = base_args();
-    a.x = x; a.v = v; a.C = C; a.F = F; a.x1 = x1; a.v1 = v1; a.C1 = C1; a.F1 = F1;
-    a.act = act_.p + (size_t)f * E_ * M_;
-    MPM_CUDA(cudaMemsetAsync(gm_.p, 0, sizeof(R) * gm_.n, stream));
-    MPM_CUDA(cudaMemsetAsync(gmv_.p, 0, sizeof(R) * gmv_.n, stream));
-    p2g_kernel<R, D><<<blocks(EP()), 256, 0, stream>>>(a, write_F ? 1 : 0);
-    grid_op_kernel<R, D><<<blocks((long long)E_ * cells_), 256, 0, stream>>>(a);
-    if (x1) g2p_kernel<R, D><<<blocks(EP()), 256, 0, stream>>>(a);
-    launches_ += x1 ? 3 : 2;
-  }
-
-  void center_at(const R* x, int t) {
-    center_kernel<R, D><<<E_, 256, 0, stream>>>(x, pw_.p, (R)pw_sum_, P_, center_.p + (size_t)t * E_ * D);
-    launches_ += 1;
-  }
-
-  R* slot(Buf<R>& b, size_t per, int i) { return b.p + per * i; }
-
+  // ---------------------------------------------------------------- forward
   void forward(int steps) override {
     MPM_REQUIRE(steps >= 1 && steps <= T_, "steps must be in [1, max_steps]");
     steps_ = steps;
-    const size_t px = EP() * D, pm = EP() * D * D;
-    // working states live in the record buffers' slots 0 and 1 (ping-pong);
-    // checkpoint slot 0 holds the initial state
-    MPM_CUDA(cudaMemcpyAsync(slot(rc_x_, px, 0), ck_x_.p, sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(slot(rc_v_, px, 0), ck_v_.p, sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(slot(rc_C_, pm, 0), ck_C_.p, sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(slot(rc_F_, pm, 0), ck_F_.p, sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-    int cur = 0;
-    for (int f = 0; f < steps; ++f) {
-      const int nx = 1 - cur;
-      if (f > 0 && f % K_ == 0) {
-        const int s = f / K_;
-        MPM_CUDA(cudaMemcpyAsync(slot(ck_x_, px, s), slot(rc_x_, px, cur), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-        MPM_CUDA(cudaMemcpyAsync(slot(ck_v_, px, s), slot(rc_v_, px, cur), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-        MPM_CUDA(cudaMemcpyAsync(slot(ck_C_, pm, s), slot(rc_C_, pm, cur), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-        MPM_CUDA(cudaMemcpyAsync(slot(ck_F_, pm, s), slot(rc_F_, pm, cur), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-      }
-      center_at(slot(rc_x_, px, cur), f);
-      step(slot(rc_x_, px, cur), slot(rc_v_, px, cur), slot(rc_C_, pm, cur), slot(rc_F_, pm, cur),
-           slot(rc_x_, px, nx), slot(rc_v_, px, nx), slot(rc_C_, pm, nx), slot(rc_F_, pm, nx), f, true);
-      cur = nx;
+    const size_t cslab = (size_t)E_ * D;
+    timed(MK_OTHER, [&] { cudaMemsetAsync(csum_.p, 0, sizeof(R) * (steps + 1) * cslab, stream); });
+    reset_bbox(0, 0);
+    {  // P2G of step 0
+      FwdArgs<R> a = fwd_args();
+      a.x_in = ckx(0); a.v_in = ckv(0); a.C_in = ckC(0); a.F_in = ckF(0);
+      a.F_out = steps > 1 ? fF(1) : fin_F_.p;
+      a.act = act(0);
+      a.bbox = bbox(0, 0);
+      a.csum = csum_.p;
+      launch_fwd(2, a, MK_PFWD);
     }
-    center_at(slot(rc_x_, px, cur), steps);
-    final_slot_ = cur;
-    // keep the final state outside the record buffers
-    MPM_CUDA(cudaMemcpyAsync(fin_x_.p, slot(rc_x_, px, cur), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(fin_v_.p, slot(rc_v_, px, cur), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(fin_C_.p, slot(rc_C_, pm, cur), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-    MPM_CUDA(cudaMemcpyAsync(fin_F_.p, slot(rc_F_, pm, cur), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
+    launch_grid(gv(0, 0), 0, 0, steps > 1 ? bbox(0, 1) : nullptr);
+    for (int f = 0; f + 1 < steps; ++f) {
+      const int g = f + 1;
+      FwdArgs<R> a = fwd_args();
+      a.x_in = fx(f);
+      a.gv = gv(0, f % 2);
+      a.x_out = fx(g);
+      if (g % K_ == 0) { a.v_out = ckv(g / K_); a.C_out = ckC(g / K_); }
+      a.F_in = fF(g);
+      a.F_out = g + 1 <= steps - 1 ? fF(g + 1) : fin_F_.p;
+      a.act = act(g);
+      a.bbox = bbox(0, g % 2);
+      a.csum = csum_.p + (size_t)g * cslab;
+      launch_fwd(3, a, MK_PFWD);
+      launch_grid(gv(0, g % 2), 0, g % 2, g + 1 <= steps - 1 ? bbox(0, f % 2) : nullptr);
+    }
+    {  // G2P of the last step
+      FwdArgs<R> a = fwd_args();
+      a.x_in = fx(steps - 1);
+      a.gv = gv(0, (steps - 1) % 2);
+      a.x_out = fin_x_.p; a.v_out = fin_v_.p; a.C_out = fin_C_.p;
+      a.csum = csum_.p + (size_t)steps * cslab;
+      launch_fwd(1, a, MK_PFWD);
+    }
     MPM_CUDA(cudaGetLastError());
     fwd_done_ = true;
+    bwd_done_ = false;
+  }
+
+  // states and grids of segment s recomputed into its record (record s % 2)
+  void recompute(int s) {
+    const int r = s % 2, t0 = s * K_, len = std::min(K_, steps_ - t0);
+    reset_bbox(r, 0);
+    {
+      FwdArgs<R> a = fwd_args();
+      a.x_in = rx(s, 0); a.v_in = rv(s, 0); a.C_in = rC(s, 0); a.F_in = rF(s, 0);
+      a.F_out = len > 1 ? rF(s, 1) : nullptr;
+      a.act = act(t0);
+      a.bbox = bbox(r, 0);
+      launch_fwd(2, a, MK_PREC);
+    }
+    launch_grid(gv(r, 0), r, 0, len > 1 ? bbox(r, 1) : nullptr);
+    for (int k = 0; k + 1 < len; ++k) {
+      FwdArgs<R> a = fwd_args();
+      a.x_in = rx(s, k);
+      a.gv = gv(r, k);
+      a.x_out = rx(s, k + 1); a.v_out = rv(s, k + 1); a.C_out = rC(s, k + 1);
+      a.F_in = rF(s, k + 1);
+      a.F_out = k + 2 < len ? rF(s, k + 2) : nullptr;
+      a.act = act(t0 + k + 1);
+      a.bbox = bbox(r, k + 1);
+      launch_fwd(3, a, MK_PREC);
+      launch_grid(gv(r, k + 1), r, k + 1, k + 2 < len ? bbox(r, k + 2) : nullptr);
+    }
   }
 
   double loss() override {
     MPM_REQUIRE(fwd_done_, "cls_mpm_loss before a forward rollout");
     std::vector<R> c((size_t)(steps_ + 1) * E_ * D), tg((size_t)(steps_ + 1) * E_ * D);
-    MPM_CUDA(cudaMemcpyAsync(c.data(), center_.p, sizeof(R) * c.size(), cudaMemcpyDeviceToHost, stream));
+    MPM_CUDA(cudaMemcpyAsync(c.data(), csum_.p, sizeof(R) * c.size(), cudaMemcpyDeviceToHost, stream));
     MPM_CUDA(cudaMemcpyAsync(tg.data(), target_.p, sizeof(R) * tg.size(), cudaMemcpyDeviceToHost, stream));
     MPM_CUDA(cudaStreamSynchronize(stream));
     double L = 0;
     for (int t = 0; t <= steps_; ++t) {
       if (loss_w_[t] == 0.0) continue;
       for (size_t q = 0; q < (size_t)E_ * D; ++q) {
-        const double e = (double)c[(size_t)t * E_ * D + q] - (double)tg[(size_t)t * E_ * D + q];
+        const double e = (double)(c[(size_t)t * E_ * D + q] / (R)pw_sum_) - (double)tg[(size_t)t * E_ * D + q];
         L += loss_w_[t] * e * e;
       }
     }
     return L;
   }
 
-  void seed(R* ax, int t) {
-    if (loss_w_[t] == 0.0) return;
-    seed_kernel<R, D><<<blocks(EP()), 256, 0, stream>>>(ax, center_.p + (size_t)t * E_ * D,
-                                                       target_.p + (size_t)t * E_ * D, pw_.p,
-                                                       (R)loss_w_[t], (R)pw_sum_, E_, P_);
-    launches_ += 1;
-  }
-
+  // ---------------------------------------------------------------- reverse
   void backward() override {
     MPM_REQUIRE(fwd_done_, "cls_mpm_backward before a forward rollout");
-    const size_t px = EP() * D, pm = EP() * D * D;
-    int a = 0;  // adjoint buffers: a = state t + 1, 1 - a = state t
-    MPM_CUDA(cudaMemsetAsync(ax_[a].p, 0, sizeof(R) * px, stream));
-    MPM_CUDA(cudaMemsetAsync(av_[a].p, 0, sizeof(R) * px, stream));
-    MPM_CUDA(cudaMemsetAsync(aC_[a].p, 0, sizeof(R) * pm, stream));
-    MPM_CUDA(cudaMemsetAsync(aF_[a].p, 0, sizeof(R) * pm, stream));
-    MPM_CUDA(cudaMemsetAsync(gact_.p, 0, sizeof(R) * gact_.n, stream));
-    seed(ax_[a].p, steps_);
-    const int n_seg = (steps_ + K_ - 1) / K_;
-    for (int s = n_seg - 1; s >= 0; --s) {
-      const int t0 = s * K_, t1 = std::min(t0 + K_, steps_);
-      // recompute the segment's states into record slots 0 .. t1 - t0 - 1
-      MPM_CUDA(cudaMemcpyAsync(slot(rc_x_, px, 0), slot(ck_x_, px, s), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-      MPM_CUDA(cudaMemcpyAsync(slot(rc_v_, px, 0), slot(ck_v_, px, s), sizeof(R) * px, cudaMemcpyDeviceToDevice, stream));
-      MPM_CUDA(cudaMemcpyAsync(slot(rc_C_, pm, 0), slot(ck_C_, pm, s), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-      MPM_CUDA(cudaMemcpyAsync(slot(rc_F_, pm, 0), slot(ck_F_, pm, s), sizeof(R) * pm, cudaMemcpyDeviceToDevice, stream));
-      for (int f = t0; f < t1 - 1; ++f) {
-        const int k = f - t0;
-        step(slot(rc_x_, px, k), slot(rc_v_, px, k), slot(rc_C_, pm, k), slot(rc_F_, pm, k),
-             slot(rc_x_, px, k + 1), slot(rc_v_, px, k + 1), slot(rc_C_, pm, k + 1), slot(rc_F_, pm, k + 1),
-             f, true);
-      }
-      for (int f = t1 - 1; f >= t0; --f) {
-        const int k = f - t0;
-        const R* x = slot(rc_x_, px, k);
-        const R* v = slot(rc_v_, px, k);
-        const R* C = slot(rc_C_, pm, k);
-        const R* F = slot(rc_F_, pm, k);
-        step(x, v, C, F, nullptr, nullptr, nullptr, nullptr, f, false);  // grid of step f
-        Args<R> ar = base_args();
-        ar.x = x; ar.v = v; ar.C = C; ar.F = F;
-        ar.act = act_.p + (size_t)f * E_ * M_;
-        ar.gact = gact_.p + (size_t)f * E_ * M_;
-        ar.ax = ax_[a].p; ar.av = av_[a].p; ar.aC = aC_[a].p; ar.aF = aF_[a].p;
-        ar.nx = ax_[1 - a].p; ar.nv = av_[1 - a].p; ar.nC = aC_[1 - a].p; ar.nF = aF_[1 - a].p;
-        MPM_CUDA(cudaMemsetAsync(g_gvo_.p, 0, sizeof(R) * g_gvo_.n, stream));
-        g2p_adj_kernel<R, D><<<blocks(EP()), 256, 0, stream>>>(ar);
-        grid_op_adj_kernel<R, D><<<blocks((long long)E_ * cells_), 256, 0, stream>>>(ar);
-        p2g_adj_kernel<R, D><<<blocks(EP()), 256, 0, stream>>>(ar);
-        launches_ += 3;
-        a = 1 - a;
-        seed(ax_[a].p, f);
+    const int steps = steps_;
+    const int n_seg = (steps + K_ - 1) / K_;
+    const Phys<R> c = phys();
+    auto seed = [&](AdjArgs<R>& a, int t) {
+      a.seed_w = (R)loss_w_[t];
+      a.csum = csum_.p + (size_t)t * E_ * D;
+      a.target = target_.p + (size_t)t * E_ * D;
+      a.pw_sum = (R)pw_sum_;
+    };
+    auto g2pT = [&](AdjArgs<R>& a, int h) {
+      const int sh = h / K_, kh = h - sh * K_;
+      a.x_h = rx(sh, kh);
+      a.gv_h = gv(sh % 2, kh);
+      a.gacc = gacc_.p;
+    };
+    timed(MK_OTHER, [&] { cudaMemsetAsync(gact_.p, 0, sizeof(R) * gact_.n, stream); });
+    recompute(n_seg - 1);
+    int cur = 0;
+    {  // G2P^T of the last step, seeded by the loss at step `steps`
+      AdjArgs<R> a;
+      std::memset(&a, 0, sizeof(a));
+      a.c = c;
+      seed(a, steps);
+      g2pT(a, steps - 1);
+      a.ax_out = AX_[0].p; a.aF_out = AF_[0].p;
+      launch_adj(2, a);
+    }
+    for (int f = steps - 1; f >= 0; --f) {
+      const int s = f / K_, k = f - s * K_;
+      if (f >= 1 && k == 0) recompute(s - 1);
+      timed(MK_GADJ, [&] {
+        mpm_grid_adj_kernel<R, D><<<grid_dims(), 256, 0, stream>>>(c, gacc_.p, gv(s % 2, k), ga_.p,
+                                                                   bbox(s % 2, k));
+      });
+      AdjArgs<R> a;
+      std::memset(&a, 0, sizeof(a));
+      a.c = c;
+      a.x_f = rx(s, k); a.v_f = rv(s, k); a.C_f = rC(s, k); a.F_f = rF(s, k);
+      a.act_f = act(f);
+      a.ga = ga_.p;
+      a.ax_in = AX_[cur].p; a.aF_in = AF_[cur].p;
+      a.gact = gact_.p + (size_t)f * E_ * M_;
+      seed(a, f);
+      if (f >= 1) {
+        g2pT(a, f - 1);
+        a.ax_out = AX_[1 - cur].p; a.aF_out = AF_[1 - cur].p;
+        launch_adj(3, a);
+        cur = 1 - cur;
+      } else {
+        a.out_ax = out_ax_.p; a.out_av = out_av_.p; a.out_aC = out_aC_.p; a.out_aF = out_aF_.p;
+        launch_adj(1, a);
       }
     }
-    adj_slot_ = a;
     MPM_CUDA(cudaGetLastError());
     bwd_done_ = true;
   }
 
   void graph_capture(int steps) override {
     MPM_REQUIRE(stream != nullptr, "graph capture needs a non-default stream");
+    MPM_REQUIRE(!prof_.on, "disable profiling before graph capture");
     if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
     if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
     MPM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -298,8 +492,30 @@ class MpmImpl final : public MpmBase {
   }
 
   // ------------------------------------------------------------------- I/O
+  // user layout [E][P][comps] (double) <-> planes [comps][E][P_internal] (R)
+  void up_planes(const double* h, R* d, int comps) {
+    const size_t EP = (size_t)E_ * P_;
+    std::vector<R> tmp(EP * comps);
+    for (int e = 0; e < E_; ++e)
+      for (int i = 0; i < P_; ++i) {
+        const double* src = h + ((size_t)e * P_ + perm_[i]) * comps;
+        for (int k = 0; k < comps; ++k) tmp[(size_t)k * EP + (size_t)e * P_ + i] = (R)src[k];
+      }
+    MPM_CUDA(cudaMemcpyAsync(d, tmp.data(), sizeof(R) * tmp.size(), cudaMemcpyHostToDevice, stream));
+    MPM_CUDA(cudaStreamSynchronize(stream));
+  }
+  void down_planes(const R* d, double* h, int comps) {
+    const size_t EP = (size_t)E_ * P_;
+    std::vector<R> tmp(EP * comps);
+    MPM_CUDA(cudaMemcpyAsync(tmp.data(), d, sizeof(R) * tmp.size(), cudaMemcpyDeviceToHost, stream));
+    MPM_CUDA(cudaStreamSynchronize(stream));
+    for (int e = 0; e < E_; ++e)
+      for (int i = 0; i < P_; ++i) {
+        double* dst = h + ((size_t)e * P_ + perm_[i]) * comps;
+        for (int k = 0; k < comps; ++k) dst[k] = (double)tmp[(size_t)k * EP + (size_t)e * P_ + i];
+      }
+  }
   void up(const double* h, R* d, size_t n) {
-    MPM_REQUIRE(n <= stage_.n, "staging too small");
     std::vector<R> tmp(n);
     for (size_t i = 0; i < n; ++i) tmp[i] = (R)h[i];
     MPM_CUDA(cudaMemcpyAsync(d, tmp.data(), sizeof(R) * n, cudaMemcpyHostToDevice, stream));
@@ -313,68 +529,85 @@ class MpmImpl final : public MpmBase {
   }
 
   void set_state(const double* x0, const double* v0) override {
-    const size_t px = EP() * D, pm = EP() * D * D;
     MPM_REQUIRE(x0 != nullptr, "x0 required");
-    up(x0, ck_x_.p, px);
-    if (v0) up(v0, ck_v_.p, px);
-    else MPM_CUDA(cudaMemsetAsync(ck_v_.p, 0, sizeof(R) * px, stream));
-    MPM_CUDA(cudaMemsetAsync(ck_C_.p, 0, sizeof(R) * pm, stream));
-    std::vector<double> eye(pm, 0.0);
-    for (size_t q = 0; q < EP(); ++q)
-      for (int d = 0; d < D; ++d) eye[q * D * D + d * D + d] = 1.0;
-    up(eye.data(), ck_F_.p, pm);
+    up_planes(x0, ckx(0), D);
+    if (v0) up_planes(v0, ckv(0), D);
+    else MPM_CUDA(cudaMemsetAsync(ckv(0), 0, sizeof(R) * VX(), stream));
+    MPM_CUDA(cudaMemsetAsync(ckC(0), 0, sizeof(R) * VM(), stream));
+    std::vector<R> eye(VM(), R(0));
+    for (int d = 0; d < D; ++d)
+      for (size_t q = 0; q < (size_t)E_ * P_; ++q) eye[(size_t)(d * D + d) * E_ * P_ + q] = R(1);
+    MPM_CUDA(cudaMemcpyAsync(ckF(0), eye.data(), sizeof(R) * eye.size(), cudaMemcpyHostToDevice, stream));
+    MPM_CUDA(cudaStreamSynchronize(stream));
     fwd_done_ = bwd_done_ = false;
   }
 
-  void set_actuation(const double* act) override { up(act, act_.p, (size_t)T_ * E_ * M_); }
+  void set_actuation(const double* act_h) override { up(act_h, act_.p, (size_t)T_ * E_ * M_); }
 
   void set_loss(const double* w, const double* target, const double* pw) override {
     if (w) loss_w_.assign(w, w + T_ + 1);
     if (target) up(target, target_.p, (size_t)(T_ + 1) * E_ * D);
     if (pw) {
-      up(pw, pw_.p, P_);
+      std::vector<double> pi(P_);
       pw_sum_ = 0;
-      for (int q = 0; q < P_; ++q) pw_sum_ += pw[q];
+      for (int i = 0; i < P_; ++i) {
+        pi[i] = pw[perm_[i]];
+        pw_sum_ += pw[i];
+      }
       MPM_REQUIRE(pw_sum_ > 0, "particle weights must have a positive sum");
+      up(pi.data(), pw_.p, P_);
     }
   }
 
   void final_state(double* x, double* v, double* C, double* F) override {
     MPM_REQUIRE(fwd_done_, "no rollout yet");
-    const size_t px = EP() * D, pm = EP() * D * D;
-    if (x) down(fin_x_.p, x, px);
-    if (v) down(fin_v_.p, v, px);
-    if (C) down(fin_C_.p, C, pm);
-    if (F) down(fin_F_.p, F, pm);
+    if (x) down_planes(fin_x_.p, x, D);
+    if (v) down_planes(fin_v_.p, v, D);
+    if (C) down_planes(fin_C_.p, C, D * D);
+    if (F) down_planes(fin_F_.p, F, D * D);
   }
 
   void grads(double* gact, double* gx0, double* gv0, double* gC0, double* gF0) override {
     MPM_REQUIRE(bwd_done_, "no reverse pass yet");
-    const size_t px = EP() * D, pm = EP() * D * D;
     if (gact) down(gact_.p, gact, (size_t)T_ * E_ * M_);
-    if (gx0) down(ax_[adj_slot_].p, gx0, px);
-    if (gv0) down(av_[adj_slot_].p, gv0, px);
-    if (gC0) down(aC_[adj_slot_].p, gC0, pm);
-    if (gF0) down(aF_[adj_slot_].p, gF0, pm);
+    if (gx0) down_planes(out_ax_.p, gx0, D);
+    if (gv0) down_planes(out_av_.p, gv0, D);
+    if (gC0) down_planes(out_aC_.p, gC0, D * D);
+    if (gF0) down_planes(out_aF_.p, gF0, D * D);
   }
 
-  void centers(double* c) override { down(center_.p, c, (size_t)(T_ + 1) * E_ * D); }
+  void centers(double* c) override {
+    down(csum_.p, c, (size_t)(T_ + 1) * E_ * D);
+    for (size_t i = 0; i < (size_t)(T_ + 1) * E_ * D; ++i) c[i] /= pw_sum_;
+  }
 
-  long long launches_ = 0;
+  void profile_enable(bool on) override {
+    MPM_CUDA(prof_.collect(stream));
+    prof_.on = on;
+  }
+  void profile_read(double* ms, long long* launches, bool reset) override {
+    MPM_CUDA(prof_.collect(stream));
+    prof_.read(ms, launches, reset);
+  }
 
  private:
   cls_mpm_params p_;
-  int E_ = 0, P_ = 0, M_ = 1, T_ = 0, K_ = 1, n_grid_ = 0, steps_ = 0, final_slot_ = 0, adj_slot_ = 0;
-  long long cells_ = 0;
-  size_t n_ckpt_ = 0;
+  int E_ = 0, P_ = 0, M_ = 1, T_ = 0, K_ = 1, n_grid_ = 0, nb_ = 0, n_chunks_ = 0, slots_ = 2;
+  int tile_cap_ = 0, steps_ = 0;
+  long long nblk_ = 0;
+  size_t n_ckpt_ = 0, fwd_smem_ = 0, adj_smem_ = 0;
   double pw_sum_ = 1;
   std::vector<double> loss_w_;
+  std::vector<int> perm_;  // internal particle -> user particle
+  std::vector<int> chunk_start_h_, chunk_len_h_;
   bool fwd_done_ = false, bwd_done_ = false;
-  Buf<R> ck_x_, ck_v_, ck_C_, ck_F_, rc_x_, rc_v_, rc_C_, rc_F_;
-  Buf<R> ax_[2], av_[2], aC_[2], aF_[2];
-  Buf<R> gm_, gmv_, gvo_, g_gvo_, g_gv_, g_gm_, act_, gact_, center_, target_, fibre_, pw_, stage_;
-  Buf<int> muscle_;
-  Buf<R> fin_x_, fin_v_, fin_C_, fin_F_;
+  Buf<R> ck_x_, ck_v_, ck_C_, ck_F_;
+  Buf<R> X_[2], Fw_[2], RX_[2], RV_[2], RC_[2], RF_[2], AX_[2], AF_[2];
+  Buf<V> gv_[2], acc_, gacc_, ga_;
+  Buf<int> bboxes_, muscle_, chunk_start_, chunk_len_;
+  Buf<R> fin_x_, fin_v_, fin_C_, fin_F_, out_ax_, out_av_, out_aC_, out_aF_;
+  Buf<R> act_, gact_, csum_, target_, fibre_, pw_;
+  EventProfile<MK_COUNT> prof_;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
 };
@@ -509,6 +742,14 @@ int cls_mpm_graph_capture(cls_mpm* s, int32_t steps) {
 }
 int cls_mpm_graph_launch(cls_mpm* s) {
   return mguard(s, [&](cls::mpm::MpmBase& b) { b.graph_launch(); });
+}
+int cls_mpm_profile_enable(cls_mpm* s, int32_t on) {
+  return mguard(s, [&](cls::mpm::MpmBase& b) { b.profile_enable(on != 0); });
+}
+int cls_mpm_profile_read(cls_mpm* s, double* ms, int64_t* launches, int32_t reset) {
+  return mguard(s, [&](cls::mpm::MpmBase& b) {
+    b.profile_read(ms, reinterpret_cast<long long*>(launches), reset != 0);
+  });
 }
 
 }  // extern "C"

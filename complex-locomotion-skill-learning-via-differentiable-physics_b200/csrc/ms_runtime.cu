@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/cls_b200.h"
+#include "cls_profile.cuh"
 #include "ms_segment.cuh"
 
 namespace cls {
@@ -68,17 +69,7 @@ struct HostRobot {
 // launch categories for the per-kernel CUDA-event profile
 enum ProfKind : int { PK_FWD = 0, PK_RECOMP, PK_REV, PK_WGRAD, PK_LOSS, PK_ADAM, PK_OTHER, PK_COUNT };
 
-struct Profiler {
-  bool on = false;
-  std::vector<cudaEvent_t> ev;    // pairs (start, stop)
-  std::vector<int> kind;
-  size_t used = 0;
-  double ms[PK_COUNT] = {0};
-  long long launches[PK_COUNT] = {0};
-  ~Profiler() {
-    for (cudaEvent_t e : ev) cudaEventDestroy(e);
-  }
-};
+using Profiler = EventProfile<PK_COUNT>;
 
 class SimBase {
  public:
@@ -599,37 +590,10 @@ class SimImpl final : public SimBase {
   // run one kernel launch, counted and (when profiling) bracketed by events
   template <typename F>
   void timed(int kind, F&& f) {
-    prof_.launches[kind] += 1;
-    if (!prof_.on) {
-      f();
-      return;
-    }
-    if (prof_.used + 2 > prof_.ev.size()) {
-      for (int q = 0; q < 64; ++q) {
-        cudaEvent_t e;
-        CLS_CUDA(cudaEventCreate(&e));
-        prof_.ev.push_back(e);
-      }
-    }
-    cudaEvent_t a = prof_.ev[prof_.used], b = prof_.ev[prof_.used + 1];
-    prof_.used += 2;
-    prof_.kind.push_back(kind);
-    CLS_CUDA(cudaEventRecord(a, stream));
-    f();
-    CLS_CUDA(cudaEventRecord(b, stream));
+    CLS_CUDA(prof_.run(kind, stream, std::forward<F>(f)));
   }
 
-  void profile_collect() {
-    if (prof_.used == 0) return;
-    CLS_CUDA(cudaStreamSynchronize(stream));
-    for (size_t q = 0; q < prof_.kind.size(); ++q) {
-      float t = 0;
-      CLS_CUDA(cudaEventElapsedTime(&t, prof_.ev[2 * q], prof_.ev[2 * q + 1]));
-      prof_.ms[prof_.kind[q]] += t;
-    }
-    prof_.kind.clear();
-    prof_.used = 0;
-  }
+  void profile_collect() { CLS_CUDA(prof_.collect(stream)); }
 
   void profile_enable(bool on) override {
     CLS_REQUIRE(!capturing_, "profiling cannot be switched during graph capture");
@@ -639,13 +603,7 @@ class SimImpl final : public SimBase {
 
   void profile_read(double* ms, long long* launches, bool reset) override {
     profile_collect();
-    for (int k = 0; k < PK_COUNT; ++k) {
-      if (ms) ms[k] = prof_.ms[k];
-      if (launches) launches[k] = prof_.launches[k];
-    }
-    if (reset) {
-      for (int k = 0; k < PK_COUNT; ++k) { prof_.ms[k] = 0; prof_.launches[k] = 0; }
-    }
+    prof_.read(ms, launches, reset);
   }
 
   void weights_init(unsigned long long seed) override {

@@ -23,7 +23,8 @@ class MPMBody(ctypes.Structure):
 class MPMParams(ctypes.Structure):
     _fields_ = [("max_steps", _i32), ("n_grid", _i32), ("bound", _i32), ("material", _i32),
                 ("precision", _i32), ("checkpoint_every", _i32), ("dt", _d), ("gravity", _d),
-                ("p_vol", _d), ("mu", _d), ("la", _d), ("act_strength", _d), ("mass", _d)]
+                ("p_vol", _d), ("mu", _d), ("la", _d), ("act_strength", _d), ("mass", _d),
+                ("tile_nodes", _i32)]
 
 
 _SIGS = {
@@ -44,7 +45,12 @@ _SIGS = {
     "cls_mpm_get_centers": (_i32, [ctypes.c_void_p, P_D]),
     "cls_mpm_graph_capture": (_i32, [ctypes.c_void_p, _i32]),
     "cls_mpm_graph_launch": (_i32, [ctypes.c_void_p]),
+    "cls_mpm_profile_enable": (_i32, [ctypes.c_void_p, _i32]),
+    "cls_mpm_profile_read": (_i32, [ctypes.c_void_p, P_D, ctypes.POINTER(ctypes.c_int64), _i32]),
 }
+
+# categories of cls_mpm_profile_read
+PROFILE_KINDS = ["particle", "particle_recompute", "grid", "particle_adj", "grid_adj", "other"]
 
 
 def _lib():
@@ -174,3 +180,16 @@ class MPMBatch:
 
     def graph_launch(self):
         self._c(self.lib.cls_mpm_graph_launch(self.h))
+
+    def profile(self, on=True):
+        self._c(self.lib.cls_mpm_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self, reset=False):
+        """Per-category device milliseconds and launch counts since the last reset."""
+        n = len(PROFILE_KINDS)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        self._c(self.lib.cls_mpm_profile_read(self.h, _capi.ptr(ms),
+                                              cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                              1 if reset else 0))
+        return dict(zip(PROFILE_KINDS, ms.tolist())), dict(zip(PROFILE_KINDS, cnt.tolist()))

@@ -125,3 +125,110 @@ def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4):
         out["recompute"] += wbytes + springs + 32 * N + widths[0] * dtype_bytes + rows
         out["reverse"] += wbytes + springs + 32 * N + 2 * rows + 2 * traj
     return out
+
+
+def legged_body(n_grid=64, ppc=2, torso=(24, 8, 14), leg=(5, 10, 5), origin_cells=(18, 4, 25)):
+    """Voxelised legged body for the 3D MPM configuration: a torso box on four
+    legs, ppc^3 particles per cell at cell-centred sub-positions.  Each leg is
+    split into 4 muscle groups (front/back half x upper/lower half) = 16 groups
+    with vertical fibres; the torso is passive.  Returns positions [P][3],
+    muscle [P], fibre [P][3]."""
+    dx = 1.0 / n_grid
+    ox, oy, oz = origin_cells
+    pts, mus = [], []
+
+    def add_box(c0, size, muscle_of):
+        for i in range(size[0]):
+            for j in range(size[1]):
+                for k in range(size[2]):
+                    m = muscle_of(i, j, k)
+                    for a in range(ppc):
+                        for b in range(ppc):
+                            for c in range(ppc):
+                                pts.append(((c0[0] + i + (a + 0.5) / ppc) * dx,
+                                            (c0[1] + j + (b + 0.5) / ppc) * dx,
+                                            (c0[2] + k + (c + 0.5) / ppc) * dx))
+                                mus.append(m)
+
+    lx, ly, lz = leg
+    tx, ty, tz = torso
+    corners = [(0, 0), (tx - lx, 0), (0, tz - lz), (tx - lx, tz - lz)]
+    for li, (cx, cz) in enumerate(corners):
+        add_box((ox + cx, oy, oz + cz), leg,
+                lambda i, j, k, li=li: 4 * li + (0 if i < lx // 2 else 1) + (0 if j < ly // 2 else 2))
+    add_box((ox, oy + ly, oz), torso, lambda i, j, k: -1)
+    pos = np.array(pts)
+    fib = np.zeros_like(pos)
+    fib[:, 1] = 1.0
+    return pos, np.array(mus, dtype=np.int32), fib
+
+
+def mpm_batch(n_envs=8, steps=1000, K=50, seed=0, precision=32, n_grid=64, **over):
+    """3D MLS-MPM configuration: legged body on a 64^3 grid, neo-Hookean
+    (E = 1e4, nu = 0.3), 16 fibre-actuated muscle groups driven by seeded
+    sinusoids, dt = 1e-4, sticky walls and floor; the loss tracks the body's
+    centre towards a point 0.05 ahead at the last step."""
+    from . import mpm as mpm_mod
+    pos, mus, fib = legged_body(n_grid=n_grid)
+    E, nu = 1e4, 0.3
+    mu, la = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    b = mpm_mod.MPMBatch(pos, mus, n_envs, dim=3, fibre=fib, n_muscles=16, max_steps=steps,
+                         n_grid=n_grid, bound=3, material="neo_hookean", precision=precision,
+                         checkpoint_every=K, dt=1e-4, gravity=-10.0, p_vol=1.0, mu=mu, la=la,
+                         act_strength=1e3, mass=1.0, **over)
+    rng = np.random.default_rng(seed)
+    t = np.arange(steps)[:, None, None] * 1e-4
+    freq = rng.uniform(2.0, 6.0, size=(1, n_envs, 16))
+    phase = rng.uniform(0, 2 * np.pi, size=(1, n_envs, 16))
+    b.set_actuation(np.sin(2 * np.pi * freq * t + phase))
+    w = np.zeros(steps + 1)
+    w[steps] = 1.0
+    c0 = pos.mean(axis=0)
+    target = np.broadcast_to(c0 + np.array([0.05, 0.0, 0.0]), (steps + 1, n_envs, 3)).copy()
+    b.set_loss(w, target)
+    return b, pos
+
+
+def mpm_touched_nodes(pos, n_grid=64):
+    """Grid nodes inside the 3^D quadratic B-spline stencil of at least one
+    particle at positions `pos` [P][D]."""
+    base = np.floor(pos * n_grid - 0.5).astype(np.int64)
+    D = pos.shape[1]
+    offs = np.stack(np.meshgrid(*([np.arange(3)] * D), indexing="ij"), -1).reshape(-1, D)
+    nodes = (base[:, None, :] + offs[None, :, :]).reshape(-1, D)
+    key = np.zeros(len(nodes), dtype=np.int64)
+    for d in range(D):
+        key = key * n_grid + nodes[:, d]
+    return int(np.unique(key).size)
+
+
+def mpm_algorithmic_bytes(pos, n_envs, n_grid=64, dtype_bytes=4):
+    """Compulsory DRAM bytes of ONE launch of each MPM kernel over the batch
+    (FP32, 3D; P particles and G touched grid nodes per env; grid nodes are
+    16-byte (velocity, mass) / (momentum, mass) records):
+
+      particle:            G2P of step f + P2G of step f+1: read x, F, muscle
+                           id, fibre, centre weight (68 P), write x, F (48 P);
+                           gather the staged grid (16 G), flush the tile (16 G)
+      particle_recompute:  the same + v, C of the recorded step (48 P)
+      grid:                read the accumulator (16 G), write (velocity, mass)
+                           (16 G), clear the accumulator (16 G)
+      particle_adj:        P2G^T of step f + G2P^T of step f-1: read x, v, C, F
+                           of step f, muscle id, fibre, weight (116 P), a_x and
+                           a_F in (48 P), x of step f-1 (12 P); write a_x, a_F
+                           (48 P); grid adjoint and grid gathers (32 G), flush
+                           of the velocity adjoint (16 G)
+      grid_adj:            read the adjoint accumulator and the grid (32 G),
+                           write the grid adjoint (16 G), clear (16 G)
+    """
+    P, D = pos.shape
+    G = mpm_touched_nodes(pos, n_grid)
+    s = dtype_bytes / 4.0
+    per_env = {
+        "particle": 116 * P + 32 * G,
+        "particle_recompute": 164 * P + 32 * G,
+        "grid": 48 * G,
+        "particle_adj": 224 * P + 48 * G,
+        "grid_adj": 64 * G,
+    }
+    return {k: v * s * n_envs for k, v in per_env.items()}

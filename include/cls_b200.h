@@ -230,6 +230,9 @@ typedef struct {
   int32_t precision;            /* 32 or 64 */
   int32_t checkpoint_every;     /* K */
   double dt, gravity, p_vol, mu, la, act_strength, mass;
+  int32_t tile_nodes;           /* > 0: scatter through a warp-private shared-memory tile
+                                   of this many grid nodes (at most 1024); 0 (default)
+                                   or < 0: 16-byte vector atomics straight to the grid */
 } cls_mpm_params;
 
 /* Fills *p with the reference's 2D MPM constants (dt 1e-3, gravity -10,
@@ -265,6 +268,15 @@ int cls_mpm_get_centers(cls_mpm* sim, double* centers);
 /* forward + backward of `steps` captured into a CUDA graph; replay. */
 int cls_mpm_graph_capture(cls_mpm* sim, int32_t steps);
 int cls_mpm_graph_launch(cls_mpm* sim);
+/* Per-kernel CUDA-event timing on the handle's stream (no counterpart in the
+ * reference).  Categories: 0 particle kernel of the first pass (G2P of step f
+ * fused with P2G of step f+1), 1 the same kernel in the reverse pass's
+ * recompute, 2 grid update, 3 particle adjoint (P2G^T of step f fused with
+ * G2P^T of step f-1), 4 grid adjoint, 5 other (centre and actuation-gradient
+ * reductions, list resets).  ms / launches have CLS_MPM_PROFILE_KINDS entries. */
+#define CLS_MPM_PROFILE_KINDS 6
+int cls_mpm_profile_enable(cls_mpm* sim, int32_t on);
+int cls_mpm_profile_read(cls_mpm* sim, double* ms, int64_t* launches, int32_t reset);
 
 /* ---------------------------------------------------------------------------
  * Mass-spring substeps without any allocation.  This entry point has no

@@ -67,8 +67,11 @@ def test_mpm2d_gradients_match_oracle(material, precision):
     b.close()
 
 
-@pytest.mark.parametrize("precision", [64, 32])
-def test_mpm3d_neo_hookean_fibre_matches_oracle(precision):
+@pytest.mark.parametrize("precision,tile", [(64, 0), (32, 0), (64, 256), (32, 256), (64, 48)])
+def test_mpm3d_neo_hookean_fibre_matches_oracle(precision, tile):
+    """tile 0: vector atomics straight to the grid (default); 256: warp-private
+    shared-memory scatter tiles; 48: a capacity that some warps' boxes exceed
+    (mixed tiled / global)."""
     from cls_b200.mpm import MPMBatch
     rng = np.random.default_rng(1)
     pts, musc, fib = body3d(rng)
@@ -85,7 +88,7 @@ def test_mpm3d_neo_hookean_fibre_matches_oracle(precision):
     o.target[...] = 0.45
     L = o.run(steps)
     b = MPMBatch(pts, musc, B, fibre=fib, n_muscles=4, max_steps=steps, material="neo_hookean",
-                 precision=precision, checkpoint_every=5, mass=1.0, **kw)
+                 precision=precision, checkpoint_every=5, mass=1.0, tile_nodes=tile, **kw)
     b.set_state(np.broadcast_to(pts, (B,) + pts.shape), o.v[0])
     b.set_actuation(o.act)
     b.set_loss(o.loss_w, o.target, pw)
