@@ -89,6 +89,11 @@ _SIGS = {
     "cls_profile_read": (c_int32, [ctypes.c_void_p, P_D, ctypes.POINTER(ctypes.c_int64), c_int32]),
     "cls_graph_capture": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
     "cls_graph_launch": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_serve_reset_env": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D, P_D, P_D, P_D]),
+    "cls_serve_forward": (c_int32, [ctypes.c_void_p, P_I, P_I]),
+    "cls_serve_backward": (c_int32, [ctypes.c_void_p, P_I, P_I]),
+    "cls_serve_loss": (c_int32, [ctypes.c_void_p, P_I, P_D]),
+    "cls_serve_env_state": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D]),
 }
 
 

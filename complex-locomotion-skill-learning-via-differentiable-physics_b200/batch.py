@@ -187,6 +187,42 @@ class MassSpringBatch:
         self._c(fn(self.h, steps, ctypes.byref(out)))
         return out.value
 
+    # ----------------------------------------------------------------- serving
+    def serve_reset_env(self, env, x0, v0=None, target_v=None, target_h=None, target_c=None):
+        """Restart env `env` with its own initial state and targets (one env's
+        [T] columns); other envs are untouched."""
+        n = self.robots[self.env_robot[env]].n_vertices
+        x0 = self._f64(x0, (n, 3))
+        v0 = None if v0 is None else self._f64(v0, (n, 3))
+        tv = None if target_v is None else self._f64(target_v, (self.T, 3))
+        th = None if target_h is None else self._f64(target_h, (self.T,))
+        tc = None if target_c is None else self._f64(target_c, (self.T,))
+        self._c(self.lib.cls_serve_reset_env(self.h, env, ptr(x0), ptr(v0), ptr(tv), ptr(th), ptr(tc)))
+
+    @staticmethod
+    def _i32(a, shape):
+        return np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(shape))
+
+    def serve_forward(self, windows, steps):
+        w, s = self._i32(windows, (self.n_envs, 4)), self._i32(steps, (self.n_envs,))
+        self._c(self.lib.cls_serve_forward(self.h, ptr(w, _capi.P_I), ptr(s, _capi.P_I)))
+
+    def serve_backward(self, windows, steps):
+        w, s = self._i32(windows, (self.n_envs, 4)), self._i32(steps, (self.n_envs,))
+        self._c(self.lib.cls_serve_backward(self.h, ptr(w, _capi.P_I), ptr(s, _capi.P_I)))
+
+    def serve_loss(self, steps):
+        s = self._i32(steps, (self.n_envs,))
+        env = np.zeros((8, self.n_envs))
+        self._c(self.lib.cls_serve_loss(self.h, ptr(s, _capi.P_I), ptr(env)))
+        return env
+
+    def serve_env_state(self, env):
+        n = self.robots[self.env_robot[env]].n_vertices
+        x, v = np.zeros((n, 3)), np.zeros((n, 3))
+        self._c(self.lib.cls_serve_env_state(self.h, env, ptr(x), ptr(v)))
+        return x, v
+
     def adam_step(self, it):
         tns = ctypes.c_double()
         self._c(self.lib.cls_adam_step(self.h, it, ctypes.byref(tns)))

@@ -13,8 +13,8 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libcls_b200.so")
 SOURCES = ["ms_runtime.cu", "mpm_runtime.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-         "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def _inputs():
@@ -34,14 +34,28 @@ def needs_build():
 
 
 def build(force=False, verbose=False):
-    """Compile every CUDA source into one shared library (sm_100a only)."""
+    """Compile every CUDA source (in parallel, one nvcc per file) and link
+    them into one shared library (sm_100a only)."""
     if not force and not needs_build():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     nvcc = os.environ.get("NVCC", "nvcc")
+    objs = [os.path.join(OBJ_DIR, os.path.basename(s)[:-3] + ".o") for s in srcs]
+
+    def compile_one(src_obj):
+        src, obj = src_obj
+        cmd = [nvcc, *ARCH, *FLAGS, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        list(ex.map(compile_one, zip(srcs, objs)))
     tmp = LIB + ".tmp"
-    cmd = [nvcc, *ARCH, *FLAGS, "-o", tmp, *srcs]
+    cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd)

@@ -70,6 +70,10 @@ struct MsArgs {
   const RobotDesc* robots;
   const EnvDesc* envs;
   const int* order;                  // env processing order (largest first)
+  // per-env windows (serving): win[e] = {t_begin, t_end, source checkpoint,
+  // first reverse segment}; nullptr: the launch's own arguments for all envs
+  const int4* win;
+  const int* env_steps;              // per-env episode steps (nullptr: steps)
   int* queue;                        // work-queue counter, zeroed before each launch
   const int* inc_ptr;                // CSR row pointers (relative to inc_off)
   const int4* inc_i;                 // {other vertex, side (0: a, 1: b), spring, out index}

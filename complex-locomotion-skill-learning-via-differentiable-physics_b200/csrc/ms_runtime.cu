@@ -100,6 +100,13 @@ class SimBase {
   virtual void sizes(int* ne, int* nv, int* T) const = 0;
   virtual void phase_read(unsigned long long* out) = 0;
   virtual void layer_shape(int r, int l, int* rows, int* cols) const = 0;
+  // serving: per-env windows over envs at different episode times
+  virtual void serve_reset_env(int ue, const double* x0, const double* v0, const double* tv,
+                               const double* th, const double* tc) = 0;
+  virtual void serve_forward(const int* win, const int* steps) = 0;
+  virtual void serve_backward(const int* win, const int* steps) = 0;
+  virtual void serve_loss(const int* steps, double* env) = 0;
+  virtual void serve_env_state(int ue, double* x, double* v) = 0;
 };
 
 template <typename R>
@@ -407,6 +414,13 @@ class SimImpl final : public SimBase {
                         cudaMemcpyHostToDevice));
     n_queue_ = (size_t)(1 + 2 * n_seg_max) * E;
     d_queue_.alloc(n_queue_);
+    d_win_.alloc(E);
+    d_env_steps_.alloc(E);
+    d_sorder_.alloc(E);
+    d_squeue_.alloc(2);
+    d_stiles_.alloc(std::max<size_t>(1, tiles_host_.size()));
+    inv_perm_.assign(E, 0);
+    for (int ie = 0; ie < E; ++ie) inv_perm_[perm_[ie]] = ie;
     size_t stage = std::max<size_t>((size_t)T_ * E * 3, (size_t)V_ * 3);
     stage = std::max<size_t>(stage, (size_t)moff);
     stage = std::max<size_t>(stage, (size_t)boff);
@@ -970,6 +984,186 @@ class SimImpl final : public SimBase {
     if (v) get_vstate(d_finv_.p, v);
   }
 
+  // ------------------------------------------------------------- serving
+  // A served batch advances envs that sit at different times of their own
+  // episodes: every launch takes a window {t_begin, t_end, source checkpoint,
+  // first reverse segment} per env (user order; t_begin >= t_end: idle) and
+  // per-env episode steps.  Envs keep their state, targets, observables and
+  // checkpoints in their own regions, so admitting an env (serve_reset_env)
+  // touches no other env.
+  int ienv(int ue) const {
+    CLS_REQUIRE(ue >= 0 && ue < E_, "env index out of range");
+    return inv_perm_[ue];
+  }
+
+  void serve_reset_env(int ue, const double* x0, const double* v0, const double* tv, const double* th,
+                       const double* tc) override {
+    const int ie = ienv(ue);
+    const EnvDesc& ed = ed_host_[ie];
+    const int N = rd_host_[ed.robot].n_v;
+    CLS_REQUIRE(x0 != nullptr, "x0 is required");
+    std::vector<V4<R>> xs(N), vs(N);
+    for (int i = 0; i < N; ++i) {
+      xs[i].x = (R)x0[3 * i]; xs[i].y = (R)x0[3 * i + 1]; xs[i].z = (R)x0[3 * i + 2]; xs[i].w = 0;
+      vs[i].x = v0 ? (R)v0[3 * i] : R(0); vs[i].y = v0 ? (R)v0[3 * i + 1] : R(0);
+      vs[i].z = v0 ? (R)v0[3 * i + 2] : R(0); vs[i].w = 0;
+    }
+    CLS_CUDA(cudaMemcpyAsync(d_ckx_.p + ed.v_off, xs.data(), sizeof(V4<R>) * N, cudaMemcpyHostToDevice, stream));
+    CLS_CUDA(cudaMemcpyAsync(d_init_.p + ed.v_off, xs.data(), sizeof(V4<R>) * N, cudaMemcpyHostToDevice, stream));
+    CLS_CUDA(cudaMemcpyAsync(d_ckv_.p + ed.v_off, vs.data(), sizeof(V4<R>) * N, cudaMemcpyHostToDevice, stream));
+    // targets: one column of the [T][E] arrays
+    std::vector<V4<R>> tvv(T_);
+    std::vector<R> thv(T_), tcv(T_);
+    for (int t = 0; t < T_; ++t) {
+      tvv[t].x = tv ? (R)tv[3 * t] : R(0); tvv[t].y = tv ? (R)tv[3 * t + 1] : R(0);
+      tvv[t].z = tv ? (R)tv[3 * t + 2] : R(0); tvv[t].w = 0;
+      thv[t] = th ? (R)th[t] : R(0);
+      tcv[t] = tc ? (R)tc[t] : R(0);
+    }
+    CLS_CUDA(cudaMemcpy2DAsync(d_tv_.p + ie, sizeof(V4<R>) * E_, tvv.data(), sizeof(V4<R>), sizeof(V4<R>), T_,
+                               cudaMemcpyHostToDevice, stream));
+    CLS_CUDA(cudaMemcpy2DAsync(d_th_.p + ie, sizeof(R) * E_, thv.data(), sizeof(R), sizeof(R), T_,
+                               cudaMemcpyHostToDevice, stream));
+    CLS_CUDA(cudaMemcpy2DAsync(d_tc_.p + ie, sizeof(R) * E_, tcv.data(), sizeof(R), sizeof(R), T_,
+                               cudaMemcpyHostToDevice, stream));
+    // observables and trajectories of the env start at zero, as after the
+    // whole-batch clears of cls_forward
+    CLS_CUDA(cudaMemset2DAsync(d_obsc_.p + ie, sizeof(V4<R>) * E_, 0, sizeof(V4<R>), T_, stream));
+    CLS_CUDA(cudaMemset2DAsync(d_obsh_.p + ie, sizeof(R) * E_, 0, sizeof(R), T_, stream));
+    CLS_CUDA(cudaMemset2DAsync(d_obsu_.p + ie, sizeof(R) * E_, 0, sizeof(R), T_, stream));
+    CLS_CUDA(cudaMemset2DAsync(d_obsr_.p + ie, sizeof(R) * E_, 0, sizeof(R), T_, stream));
+    if (d_xfull_.p)
+      CLS_CUDA(cudaMemset2DAsync(d_xfull_.p + ed.v_off, sizeof(V4<R>) * V_, 0, sizeof(V4<R>) * N, T_, stream));
+    if (d_actfull_.p) {
+      const int zt = z_total_[L_ - 1], no = rd_host_[ed.robot].n_out;
+      CLS_CUDA(cudaMemset2DAsync(d_actfull_.p + ed.z_off[L_ - 1], sizeof(R) * zt, 0, sizeof(R) * no, T_, stream));
+    }
+    CLS_CUDA(cudaStreamSynchronize(stream));  // host staging vectors go out of scope
+  }
+
+  // windows and steps (user order) -> internal tables; returns the active count
+  int serve_prepare(const int* win, const int* steps) {
+    CLS_REQUIRE(win != nullptr && steps != nullptr, "windows and steps are required");
+    std::vector<int4> w(E_);
+    std::vector<int> st(E_);
+    std::vector<int> order;
+    for (int ie = 0; ie < E_; ++ie) {
+      const int ue = perm_[ie];
+      w[ie] = make_int4(win[4 * ue], win[4 * ue + 1], win[4 * ue + 2], win[4 * ue + 3]);
+      st[ie] = steps[ue];
+      if (w[ie].x < w[ie].y) {
+        CLS_REQUIRE(st[ie] >= 2 && st[ie] <= T_, "episode steps out of range");
+        CLS_REQUIRE(w[ie].x >= 0 && w[ie].y <= st[ie] - 1, "a window lies in [0, steps - 1)");
+        CLS_REQUIRE(w[ie].y - w[ie].x <= K_, "a window spans at most checkpoint_every steps");
+        CLS_REQUIRE(w[ie].z >= 0 && w[ie].z < (int)n_ckpt_ && w[ie].x == w[ie].z * K_,
+                    "a window starts at its source checkpoint (t_begin = checkpoint * checkpoint_every)");
+      }
+    }
+    for (int ie : order_host_)
+      if (w[ie].x < w[ie].y) order.push_back(ie);
+    CLS_CUDA(cudaMemcpyAsync(d_win_.p, w.data(), sizeof(int4) * E_, cudaMemcpyHostToDevice, stream));
+    CLS_CUDA(cudaMemcpyAsync(d_env_steps_.p, st.data(), sizeof(int) * E_, cudaMemcpyHostToDevice, stream));
+    if (!order.empty())
+      CLS_CUDA(cudaMemcpyAsync(d_sorder_.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice,
+                               stream));
+    serve_win_h_ = w;
+    serve_order_h_ = order;
+    CLS_CUDA(cudaStreamSynchronize(stream));  // host tables go out of scope
+    return (int)order.size();
+  }
+
+  MsArgs<R> serve_args(int n) {
+    MsArgs<R> a = args(T_);
+    a.win = d_win_.p;
+    a.env_steps = d_env_steps_.p;
+    a.order = d_sorder_.p;
+    a.n_items = n;
+    return a;
+  }
+
+  void serve_forward(const int* win, const int* steps) override {
+    const int n = serve_prepare(win, steps);
+    if (n == 0) return;
+    CLS_CUDA(cudaMemsetAsync(d_squeue_.p, 0, sizeof(int) * 2, stream));
+    MsArgs<R> a = serve_args(n);
+    a.queue = d_squeue_.p;
+    timed(PK_FWD, [&] {
+      fwd_fn()<<<grid_for(n), threads_, fwd_smem_, stream>>>(a, 0, 0, FWD_CKPT | FWD_OBS | FWD_CKEND, 0);
+    });
+    CLS_CUDA(cudaGetLastError());
+  }
+
+  void serve_backward(const int* win, const int* steps) override {
+    const int n = serve_prepare(win, steps);
+    if (n == 0) return;
+    // a robot's weight gradients restart with its env's first reverse segment
+    std::vector<int> active_robot(rd_host_.size(), 0);
+    for (int ie : serve_order_h_) {
+      const int r = ed_host_[ie].robot;
+      CLS_REQUIRE(rd_host_[r].n_env == 1, "served envs need a robot (controller) of their own");
+      active_robot[r] = 1;
+      if (serve_win_h_[ie].w) {
+        const RobotDesc& d = rd_host_[r];
+        const long long w0 = d.w_off[0];
+        const long long w1 = d.w_off[L_ - 1] + (long long)d.pitch[L_ - 1] * d.width[L_];
+        const int b0 = d.b_off[0], b1 = d.b_off[L_ - 1] + d.width[L_];
+        CLS_CUDA(cudaMemsetAsync(d_gw_.p + w0, 0, sizeof(R) * (w1 - w0), stream));
+        CLS_CUDA(cudaMemsetAsync(d_gb_.p + b0, 0, sizeof(R) * (b1 - b0), stream));
+      }
+    }
+    std::vector<GemmTile> tiles;
+    for (const GemmTile& t : tiles_host_)
+      if (active_robot[t.robot]) tiles.push_back(t);
+    CLS_CUDA(cudaMemsetAsync(d_squeue_.p, 0, sizeof(int) * 2, stream));
+    MsArgs<R> a = serve_args(n);
+    a.queue = d_squeue_.p;
+    timed(PK_RECOMP, [&] { fwd_fn()<<<grid_for(n), threads_, fwd_smem_, stream>>>(a, 0, 0, FWD_RECORD, 0); });
+    a.queue = d_squeue_.p + 1;
+    timed(PK_REV, [&] { rev_fn()<<<grid_for(n), threads_, rev_smem_, stream>>>(a, 0, 0, 0); });
+    if (!tiles.empty()) {
+      CLS_CUDA(cudaMemcpyAsync(d_stiles_.p, tiles.data(), sizeof(GemmTile) * tiles.size(), cudaMemcpyHostToDevice,
+                               stream));
+      timed(PK_WGRAD, [&] {
+        ms_wgrad_kernel<R><<<(int)tiles.size(), 256, 0, stream>>>(a, d_stiles_.p, 0, d_gw_.p, d_gb_.p);
+      });
+      CLS_CUDA(cudaStreamSynchronize(stream));  // tile list goes out of scope
+    }
+    CLS_CUDA(cudaGetLastError());
+    bwd_done_ = true;  // served robots' gradients are readable (cls_get_grads)
+  }
+
+  void serve_loss(const int* steps, double* env) override {
+    CLS_REQUIRE(steps != nullptr, "steps are required");
+    std::vector<int> st(E_);
+    for (int ie = 0; ie < E_; ++ie) {
+      st[ie] = steps[perm_[ie]];
+      CLS_REQUIRE(st[ie] >= 2 && st[ie] <= T_, "episode steps out of range");
+    }
+    CLS_CUDA(cudaMemcpyAsync(d_env_steps_.p, st.data(), sizeof(int) * E_, cudaMemcpyHostToDevice, stream));
+    MsArgs<R> a = args(T_);
+    a.env_steps = d_env_steps_.p;
+    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p); });
+    CLS_CUDA(cudaGetLastError());
+    std::vector<double> raw((size_t)E_ * 8);
+    CLS_CUDA(cudaMemcpyAsync(raw.data(), d_lossenv_.p, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    loss_from_raw(raw, nullptr, env);
+  }
+
+  void serve_env_state(int ue, double* x, double* v) override {
+    const int ie = ienv(ue);
+    const EnvDesc& ed = ed_host_[ie];
+    const int N = rd_host_[ed.robot].n_v;
+    std::vector<V4<R>> xs(N), vs(N);
+    CLS_CUDA(cudaMemcpyAsync(xs.data(), d_finx_.p + ed.v_off, sizeof(V4<R>) * N, cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaMemcpyAsync(vs.data(), d_finv_.p + ed.v_off, sizeof(V4<R>) * N, cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    for (int i = 0; i < N; ++i) {
+      if (x) { x[3 * i] = (double)xs[i].x; x[3 * i + 1] = (double)xs[i].y; x[3 * i + 2] = (double)xs[i].z; }
+      if (v) { v[3 * i] = (double)vs[i].x; v[3 * i + 1] = (double)vs[i].y; v[3 * i + 2] = (double)vs[i].z; }
+    }
+  }
+
   void state_grads(double* gx, double* gv) override {
     CLS_REQUIRE(bwd_done_, "state gradients requested before cls_backward");
     if (gx) get_vstate(d_adjx_.p, gx);
@@ -1050,6 +1244,11 @@ class SimImpl final : public SimBase {
   std::vector<EnvDesc> ed_host_;
   std::vector<RobotDesc> rd_host_;
   std::vector<GemmTile> tiles_host_;
+  std::vector<int> inv_perm_, serve_order_h_;
+  std::vector<int4> serve_win_h_;
+  DevBuf<int4> d_win_;
+  DevBuf<int> d_env_steps_, d_sorder_, d_squeue_;
+  DevBuf<GemmTile> d_stiles_;
   std::vector<OptSeg> opt_segs_, pack_segs_;
   long long opt_total_ = 0, pack_total_ = 0;
   double tns_host_ = 0;
@@ -1280,6 +1479,23 @@ int cls_loss(cls_sim* sim, double* terms, double* env) {
 
 int cls_backward(cls_sim* sim) {
   return guarded(sim, [&](cls::SimBase& s) { s.backward(false); });
+}
+
+int cls_serve_reset_env(cls_sim* sim, int32_t env, const double* x0, const double* v0, const double* tv,
+                        const double* th, const double* tc) {
+  return guarded(sim, [&](cls::SimBase& s) { s.serve_reset_env(env, x0, v0, tv, th, tc); });
+}
+int cls_serve_forward(cls_sim* sim, const int32_t* windows, const int32_t* steps) {
+  return guarded(sim, [&](cls::SimBase& s) { s.serve_forward(windows, steps); });
+}
+int cls_serve_backward(cls_sim* sim, const int32_t* windows, const int32_t* steps) {
+  return guarded(sim, [&](cls::SimBase& s) { s.serve_backward(windows, steps); });
+}
+int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* env) {
+  return guarded(sim, [&](cls::SimBase& s) { s.serve_loss(steps, env); });
+}
+int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v) {
+  return guarded(sim, [&](cls::SimBase& s) { s.serve_env_state(env, x, v); });
 }
 
 int cls_simulate(cls_sim* sim, int32_t steps, double* loss) {

@@ -5,7 +5,13 @@
 
 namespace cls {
 
-enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4 };
+enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4, FWD_CKEND = 8 };
+
+// episode steps of env e (per-env in served batches)
+template <typename R>
+__device__ __forceinline__ int steps_of(const MsArgs<R>& a, int e) {
+  return a.env_steps ? a.env_steps[e] : a.steps;
+}
 
 // sum of M values over the block, deterministic; red must hold 32*M entries
 template <typename R, int M>
@@ -101,7 +107,7 @@ __device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
 // t_end (exclusive), i.e. runs pre_advance/nn_input/forward/advance for each t.
 template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
-ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
+ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0) {
   extern __shared__ __align__(256) char smem_raw[];
   __shared__ RobotDesc rb;
   __shared__ EnvDesc ed;
@@ -112,6 +118,11 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
     const int item = next_item(a, &s_item);
     if (item >= a.n_items) break;
     const int e = a.order[item];
+    int t_begin = t_begin0, t_end = t_end0, src_slot = src_slot0;
+    if (a.win) {
+      const int4 w = a.win[e];
+      t_begin = w.x; t_end = w.y; src_slot = w.z;
+    }
     load_descs(a, e, rb, ed);
     const int N = rb.n_v, L = rb.n_layers;
     const R invN = R(1) / R(N);
@@ -255,6 +266,11 @@ ms_forward_kernel(MsArgs<R> a, int t_begin, int t_end, int mode, int src_slot) {
       CLS_PHASE(a, 17);
     }
     // state after the last processed step
+    if ((mode & FWD_CKEND) && t_end % a.K == 0 && t_end > t_begin) {
+      V4<R>* cx = a.ckpt_x + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
+      V4<R>* cv = a.ckpt_v + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
+      for (int i = tid; i < N; i += nt) { cx[i] = s.xs[i]; cv[i] = s.vs[i]; }
+    }
     if (mode & FWD_OBS) {
       for (int i = tid; i < N; i += nt) {
         a.fin_x[ed.v_off + i] = s.xs[i];
@@ -278,7 +294,7 @@ __device__ __forceinline__ V4<R> obs_c(const MsArgs<R>& a, int t, int e) {
 // d loss / d center[t] from the velocity loss (taichi_env.py:185-211)
 template <typename R>
 __device__ __forceinline__ void seed_center_velocity(const MsArgs<R>& a, int t, int e, R Br, R g[3]) {
-  const int rp = a.run_period, tp = a.turn_period, st = a.steps;
+  const int rp = a.run_period, tp = a.turn_period, st = steps_of(a, e);
   const R sc = R(2) * R(100) / R(st) / Br;
   if (t >= rp && t % tp > rp && t <= st && t < a.T) {
     const V4<R> c1 = obs_c(a, t, e), c0 = obs_c(a, t - rp, e);
@@ -301,7 +317,7 @@ template <typename R>
 __device__ __forceinline__ void seed_x_rotation_pose(const MsArgs<R>& a, const RobotDesc& rb,
                                                      const EnvDesc& ed, int t, int e, int i,
                                                      const V4<R>& xi, R Br, R gxi[3], R gc[3]) {
-  const int rp = a.run_period, tp = a.turn_period, st = a.steps;
+  const int rp = a.run_period, tp = a.turn_period, st = steps_of(a, e);
   if (a.loss_mask & LOSS_ROTATION) {
     const R k = R(2) / R(40) / R(st);
     if (t >= 1 && t % tp > rp && t <= st && t < a.T) {
@@ -346,7 +362,7 @@ __device__ __forceinline__ void seed_x_rotation_pose(const MsArgs<R>& a, const R
 template <typename R>
 __device__ __forceinline__ R seed_height(const MsArgs<R>& a, int t, int e, R Br) {
   if (!(a.loss_mask & LOSS_HEIGHT)) return 0;
-  const int jp = a.jump_period, st = a.steps;
+  const int jp = a.jump_period, st = steps_of(a, e);
   const size_t o = (size_t)t * a.n_envs + e;
   if (t >= 1 && t <= st && t < a.T && t % jp == jp - 1 && a.th[o] > R(0.1 + 1e-6))
     return R(2) * (a.obs_height[o] - a.th[o]) * R(100) / R(st / jp) / Br;
@@ -356,7 +372,7 @@ __device__ __forceinline__ R seed_height(const MsArgs<R>& a, int t, int e, R Br)
 template <typename R>
 __device__ __forceinline__ R seed_upper(const MsArgs<R>& a, int t, int e, R Br) {
   if (!(a.loss_mask & LOSS_CRAWL)) return 0;
-  const int st = a.steps;
+  const int st = steps_of(a, e);
   const size_t o = (size_t)t * a.n_envs + e;
   if (t >= 1 && t <= st && t < a.T && a.tc[o] > R(1 - 1e-4)) {
     const R d = a.obs_upper[o] - R(0.1);
@@ -450,7 +466,7 @@ __device__ __forceinline__ void spring_adjoint_all(const MsArgs<R>& a, const Rob
 // ---------------------------------------------------------------- reverse
 template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
-ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
+ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
   extern __shared__ __align__(256) char smem_raw[];
   __shared__ RobotDesc rb;
   __shared__ EnvDesc ed;
@@ -462,6 +478,11 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
     const int item = next_item(a, &s_item);
     if (item >= a.n_items) break;
     const int e = a.order[item];
+    int t_begin = t_begin0, t_end = t_end0, last_seg = last_seg0;
+    if (a.win) {
+      const int4 w = a.win[e];
+      t_begin = w.x; t_end = w.y; last_seg = w.w;
+    }
     load_descs(a, e, rb, ed);
     const int N = rb.n_v, L = rb.n_layers;
     const R Br = R(rb.n_env);
@@ -559,9 +580,10 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin, int t_end, int last_seg) {
       // adjoint of apply_spring_force(t)
       {
         const size_t o = (size_t)t * a.n_envs + e;
-        const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < a.steps && a.th[o] < R(0.1 + 1e-4);
+        const int st_e = steps_of(a, e);
+        const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
         const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
-        const R act_scale = R(10) / R(a.steps) / Br / R(rb.n_s);
+        const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
         spring_adjoint_all<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
                               act_seed);
       }
@@ -671,7 +693,7 @@ __global__ void ms_loss_kernel(MsArgs<R> a, double* out) {
   __shared__ double red[32 * 8];
   const EnvDesc ed = a.envs[e];
   const RobotDesc& rb = a.robots[ed.robot];
-  const int N = rb.n_v, st = a.steps, rp = a.run_period, tp = a.turn_period, jp = a.jump_period;
+  const int N = rb.n_v, st = steps_of(a, e), rp = a.run_period, tp = a.turn_period, jp = a.jump_period;
   const double Br = rb.n_env;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   acc[7] = 0.0;
@@ -765,6 +787,10 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
   const int M = rb.width[l + 1], Ncol = rb.width[l], pitch = rb.pitch[l];
   const int nb = rb.n_env;
   const EnvDesc& e0 = a.envs[rb.env_first];
+  if (a.win) {  // served batches: one env per robot, its own window
+    const int4 w = a.win[rb.env_first];
+    kseg = w.y > w.x ? w.y - w.x : 0;
+  }
   const int rows = kseg * nb;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   R acc[4][4];

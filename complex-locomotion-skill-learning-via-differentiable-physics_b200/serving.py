@@ -1,0 +1,432 @@
+"""Request loop: continuous batching of rollout requests on resident env slots.
+
+The reference has no serving path; it trains one batch at a time
+(multitask/diffphy_trainer.py:219-256).  Here a ``Server`` keeps a pool of
+env slots on the GPU and folds rollout requests into the running batch:
+
+* a request names a registered robot type, an episode length (``steps``), a
+  target seed and whether it wants weight gradients (forward + adjoint) or
+  the forward rollout only (controller evaluation);
+* it is admitted when a slot of its type is free and its HBM footprint fits
+  the remaining budget; admission restarts that slot alone
+  (``cls_serve_reset_env``), so the other slots keep running;
+* every tick advances each active slot through its own window of at most
+  ``checkpoint_every`` substeps in ONE launch per pool (``cls_serve_forward``),
+  and each slot in its reverse pass through one checkpointed segment
+  (``cls_serve_backward``); requests that arrive meanwhile join at the next
+  tick;
+* a finished request returns its losses (``cls_serve_loss``), final state and,
+  for gradient queries, the weight gradients of its slot's controller.
+
+Each slot owns a controller (a robot entry of the batch), so a slot's weight
+gradients are its request's alone, and a request's result does not depend on
+what else is in the batch.  Robot types are grouped into pools by controller
+depth (one batch per depth, each on its own CUDA stream, so the pools' work
+overlaps on the device).
+
+The scheduling is separate from the GPU backend (``SlotBackend``): the tests
+drive the scheduler with a fake backend on the CPU.
+"""
+import math
+import time
+import zlib
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+
+@dataclass
+class RobotType:
+    """A registered robot type: geometry + controller shape (``batch.Robot``)
+    and its controller weights [(W, b) per layer] (None: seeded init)."""
+    robot: object
+    weights: Optional[list] = None
+
+
+@dataclass
+class Request:
+    kind: str                 # robot type name
+    steps: int                # episode steps (cls_forward's `steps`, >= 2)
+    grad: bool = False        # forward + adjoint (weight gradients) or forward only
+    seed: int = 0             # seeds the targets (target velocity / height)
+    arrival: float = 0.0      # seconds, on the server's clock
+    x0: Optional[np.ndarray] = None   # initial state [n_v][3] (None: the robot's objects)
+    rid: int = -1
+
+
+@dataclass
+class Result:
+    rid: int
+    kind: str
+    steps: int
+    grad: bool
+    loss: float
+    loss_terms: Dict[str, float]
+    final_x: np.ndarray
+    grads: Optional[list]
+    arrival: float
+    admitted: float
+    done: float
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+LOSS_SLOTS = ("total", "velocity", "height", "pose", "rotation", "weight", "actuation", "crawl")
+
+
+def request_targets(seed, T, steps, turn_period, lo=-0.1, hi=0.1):
+    """Targets of one request, drawn from its seed: target velocity (vx, 0, vz)
+    and height ~ U(lo, hi), one draw per turn period (held for the period)."""
+    rng = np.random.default_rng(seed)
+    n_blocks = T // turn_period + 1
+    d = rng.uniform(lo, hi, size=(n_blocks, 3))
+    idx = np.arange(T) // turn_period
+    tv = np.zeros((T, 3))
+    tv[:, 0] = d[idx, 0]
+    tv[:, 2] = d[idx, 1]
+    return tv, d[idx, 2].copy()
+
+
+def footprint_bytes(robot, steps, grad, K, dtype_bytes=4):
+    """HBM bytes a request keeps resident while it is served: state and
+    checkpoints, its trajectory and observables, targets, controller
+    weights (x3 with gradient and optimiser-sized buffers) and, for
+    gradient queries, the per-segment records of its reverse pass."""
+    n = robot.n_vertices
+    widths = [3 * n + 11] + list(robot.hidden) + [robot.n_outputs or robot.n_springs]
+    params = sum(widths[i] * widths[i + 1] + widths[i + 1] for i in range(len(widths) - 1))
+    ckpt = 2 * 16 * n * (steps // K + 2)
+    traj = 16 * n * steps + 32 * steps + 24 * steps
+    w = params * dtype_bytes * (3 if grad else 1)
+    rec = K * (48 * n + 8 * sum(widths[1:]) + 4 * widths[0]) if grad else 0
+    return int(ckpt + traj + w + rec)
+
+
+class SlotBackend:
+    """GPU backend of one pool: a ``MassSpringBatch`` whose envs are the
+    slots, each with a robot entry (controller) of its own."""
+
+    def __init__(self, slot_types: Sequence[str], types: Dict[str, RobotType], params, stream=None,
+                 weights_seed=0):
+        from .batch import MassSpringBatch
+        self.slot_types = list(slot_types)
+        robots = [types[k].robot for k in self.slot_types]
+        self.batch = MassSpringBatch(robots, list(range(len(robots))), params)
+        if stream is not None:
+            self.batch.set_stream(stream)
+        self.T = self.batch.T
+        self.K = int(params.checkpoint_every)
+        self.turn_period = int(params.turn_period)
+        self.loaded = [None] * len(robots)   # type whose weights a slot holds
+        for e, k in enumerate(self.slot_types):
+            if types[k].weights is None:
+                types[k].weights = self._type_weights(e, k, weights_seed)
+            self.load_weights(e, k, types[k].weights)
+
+    def _type_weights(self, slot, kind, seed):
+        """Weights of a type without given ones: U(-1, 1) sqrt(6 / fan_in), zero
+        bias (multitask/nn.py:59-67), drawn from (seed, type name) so that every
+        slot and every server holds the same controller for the type."""
+        rng = np.random.default_rng([seed, zlib.crc32(kind.encode())])
+        out = []
+        for l in range(self.batch.n_layers(slot)):
+            rows, cols = self.batch.layer_shape(slot, l)
+            out.append(((rng.random((rows, cols)) * 2 - 1) * math.sqrt(6.0 / cols), np.zeros(rows)))
+        return out
+
+    def load_weights(self, slot, kind, weights):
+        if weights is not None:
+            for l, (W, b) in enumerate(weights):
+                self.batch.set_weights(slot, l, W, b)
+        self.loaded[slot] = kind
+
+    def reset(self, slot, req: Request, robot):
+        x0 = robot.objects if req.x0 is None else req.x0
+        tv, th = request_targets(req.seed, self.T, req.steps, self.turn_period)
+        self.batch.serve_reset_env(slot, x0, None, tv, th)
+
+    def forward(self, windows, steps):
+        self.batch.serve_forward(windows, steps)
+
+    def backward(self, windows, steps):
+        self.batch.serve_backward(windows, steps)
+
+    def loss(self, steps):
+        return self.batch.serve_loss(steps)
+
+    def final_x(self, slot):
+        return self.batch.serve_env_state(slot)[0]
+
+    def grads(self, slot):
+        return [self.batch.get_grads(slot, l) for l in range(self.batch.n_layers(slot))]
+
+    def sync(self):
+        self.batch.synchronize()
+
+    def close(self):
+        self.batch.close()
+
+
+class _Slot:
+    __slots__ = ("kind", "req", "phase", "pos", "seg", "loss", "terms", "fx", "admitted", "bytes")
+
+    def __init__(self, kind):
+        self.kind = kind
+        self.req = None
+        self.phase = "free"     # free | fwd | rev
+        self.pos = 0            # forward: next step to run
+        self.seg = 0            # reverse: next segment to run
+        self.loss = None
+        self.terms = None
+        self.fx = None
+        self.admitted = 0.0
+        self.bytes = 0
+
+
+class Pool:
+    """Slots of robot types with one controller depth, served by one backend."""
+
+    def __init__(self, slot_types, backend, K, T):
+        self.slots = [_Slot(k) for k in slot_types]
+        self.backend = backend
+        self.K = K
+        self.T = T
+
+    def free_slot(self, kind):
+        for i, s in enumerate(self.slots):
+            if s.phase == "free" and s.kind == kind:
+                return i
+        return -1
+
+    def busy(self):
+        return any(s.phase != "free" for s in self.slots)
+
+    def windows(self):
+        """Forward and reverse window tables for this tick ({t_begin, t_end,
+        checkpoint, first} per slot) and the per-slot episode steps."""
+        n, K = len(self.slots), self.K
+        fw = np.zeros((n, 4), dtype=np.int32)
+        bw = np.zeros((n, 4), dtype=np.int32)
+        steps = np.full(n, 2, dtype=np.int32)
+        any_f = any_b = False
+        for i, s in enumerate(self.slots):
+            if s.phase == "free":
+                continue
+            st = s.req.steps
+            steps[i] = st
+            t_last = st - 1          # the first pass runs steps [0, steps - 1)
+            if s.phase == "fwd":
+                t0 = s.pos
+                fw[i] = (t0, min(t0 + K, t_last), t0 // K, 0)
+                any_f = True
+            else:
+                n_seg = (t_last + K - 1) // K
+                t0 = s.seg * K
+                bw[i] = (t0, min(t0 + K, t_last), s.seg, 1 if s.seg == n_seg - 1 else 0)
+                any_b = True
+        return fw if any_f else None, bw if any_b else None, steps
+
+
+class Server:
+    """Continuous-batching request loop over resident env slots.
+
+    types:      {name: RobotType}
+    slots:      {name: number of slots of that type}
+    params:     ``batch.default_params`` of the served batches (max_steps is
+                the longest episode; checkpoint_every the tick length)
+    hbm_budget: bytes of request footprints admitted at once (None: no limit
+                beyond the slots)
+    """
+
+    def __init__(self, types: Dict[str, RobotType], slots: Dict[str, int], params, hbm_budget=None,
+                 backend_factory=None, streams=True, clock=time.perf_counter):
+        self.types = types
+        self.K = int(params.checkpoint_every)
+        self.T = int(params.max_steps)
+        self.hbm_budget = hbm_budget
+        self.used_bytes = 0
+        self.clock = clock
+        self.t0 = clock()
+        self.queue: List[Request] = []
+        self.results: List[Result] = []
+        self.next_rid = 0
+        self.substeps_done = 0
+        self.ticks = 0
+        by_depth: Dict[int, List[str]] = {}
+        for name, n in slots.items():
+            depth = len(types[name].robot.hidden)
+            by_depth.setdefault(depth, []).extend([name] * n)
+        self.pools: List[Pool] = []
+        for depth in sorted(by_depth):
+            slot_types = by_depth[depth]
+            if backend_factory is not None:
+                backend = backend_factory(slot_types, types, params)
+            else:
+                stream = None
+                if streams:
+                    import torch
+                    self._keep_streams = getattr(self, "_keep_streams", [])
+                    st = torch.cuda.Stream()
+                    self._keep_streams.append(st)
+                    stream = st.cuda_stream
+                backend = SlotBackend(slot_types, types, params, stream=stream)
+            self.pools.append(Pool(slot_types, backend, self.K, self.T))
+
+    def now(self):
+        return self.clock() - self.t0
+
+    def close(self):
+        for p in self.pools:
+            p.backend.close()
+
+    # ---------------------------------------------------------------- requests
+    def submit(self, req: Request) -> int:
+        if req.kind not in self.types:
+            raise KeyError("unknown robot type %r" % req.kind)
+        if not 2 <= req.steps <= self.T:
+            raise ValueError("steps must be in [2, %d]" % self.T)
+        req.rid = self.next_rid
+        self.next_rid += 1
+        self.queue.append(req)
+        return req.rid
+
+    def footprint(self, req):
+        return footprint_bytes(self.types[req.kind].robot, req.steps, req.grad, self.K)
+
+    def _admit(self):
+        """FIFO admission: a request waits for a free slot of its type and for
+        HBM budget; later requests of other types may pass it."""
+        waiting = []
+        for req in self.queue:
+            fp = self.footprint(req)
+            if self.hbm_budget is not None and self.used_bytes + fp > self.hbm_budget:
+                waiting.append(req)
+                continue
+            placed = False
+            for pool in self.pools:
+                i = pool.free_slot(req.kind)
+                if i < 0:
+                    continue
+                s = pool.slots[i]
+                if pool.backend.loaded[i] != req.kind:
+                    pool.backend.load_weights(i, req.kind, self.types[req.kind].weights)
+                pool.backend.reset(i, req, self.types[req.kind].robot)
+                s.req, s.phase, s.pos, s.seg = req, "fwd", 0, 0
+                s.admitted, s.bytes = self.now(), fp
+                self.used_bytes += fp
+                placed = True
+                break
+            if not placed:
+                waiting.append(req)
+        self.queue = waiting
+
+    # -------------------------------------------------------------------- tick
+    def tick(self) -> List[Result]:
+        """Admit what fits, advance every active slot by one window, return
+        the requests that finished."""
+        self._admit()
+        plans = []
+        for pool in self.pools:
+            fw, bw, steps = pool.windows()
+            if fw is not None:
+                pool.backend.forward(fw, steps)
+            if bw is not None:
+                pool.backend.backward(bw, steps)
+            plans.append((fw, bw, steps))
+        done = []
+        for pool, (fw, bw, steps) in zip(self.pools, plans):
+            if fw is None and bw is None:
+                continue
+            pool.backend.sync()
+            fwd_finished = []
+            for i, s in enumerate(pool.slots):
+                if s.phase == "fwd":
+                    self.substeps_done += int(fw[i, 1] - fw[i, 0])
+                    s.pos = int(fw[i, 1])
+                    if s.pos >= s.req.steps - 1:
+                        fwd_finished.append(i)
+                elif s.phase == "rev":
+                    s.seg -= 1
+            if fwd_finished:
+                env = pool.backend.loss(steps)
+                for i in fwd_finished:
+                    s = pool.slots[i]
+                    s.terms = dict(zip(LOSS_SLOTS, env[:, i].tolist()))
+                    s.loss = s.terms["total"]
+                    s.fx = pool.backend.final_x(i)
+                    if s.req.grad:
+                        t_last = s.req.steps - 1
+                        s.phase, s.seg = "rev", (t_last + self.K - 1) // self.K - 1
+                    else:
+                        done.append(self._finish(pool, i, None))
+            for i, s in enumerate(pool.slots):
+                if s.phase == "rev" and s.seg < 0:
+                    done.append(self._finish(pool, i, pool.backend.grads(i)))
+        self.ticks += 1
+        self.results.extend(done)
+        return done
+
+    def _finish(self, pool, i, grads):
+        s = pool.slots[i]
+        r = Result(rid=s.req.rid, kind=s.req.kind, steps=s.req.steps, grad=s.req.grad, loss=s.loss,
+                   loss_terms=s.terms, final_x=s.fx, grads=grads, arrival=s.req.arrival,
+                   admitted=s.admitted, done=self.now())
+        self.used_bytes -= s.bytes
+        s.req, s.phase, s.bytes = None, "free", 0
+        return r
+
+    def busy(self):
+        return bool(self.queue) or any(p.busy() for p in self.pools)
+
+    def drain(self):
+        while self.busy():
+            self.tick()
+        return self.results
+
+    # ------------------------------------------------------------ open loop
+    def run(self, requests: Sequence[Request], max_seconds=None):
+        """Serve requests at their arrival times (seconds from now); returns
+        the results and latency / throughput statistics."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        self.t0 = self.clock()
+        k = 0
+        while k < len(reqs) or self.busy():
+            t = self.now()
+            while k < len(reqs) and reqs[k].arrival <= t:
+                self.submit(reqs[k])
+                k += 1
+            if self.busy():
+                self.tick()
+            elif k < len(reqs):
+                time.sleep(max(0.0, min(reqs[k].arrival - t, 0.01)))
+            if max_seconds is not None and self.now() > max_seconds:
+                break
+        return self.results, self.stats()
+
+    def stats(self):
+        lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
+        wall = max(self.now(), 1e-9)
+        return {"requests": len(self.results), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+                "env_substeps_per_s": self.substeps_done / wall, "ticks": self.ticks,
+                "wall_s": wall}
+
+
+def poisson_requests(rng, rate, duration, kinds, p_kinds, steps_lo=100, steps_hi=2000, p_grad=0.2):
+    """Open-loop arrivals: Poisson at `rate` per second over `duration`
+    seconds, robot types drawn with probabilities p_kinds, episode steps
+    U{steps_lo..steps_hi}, a fraction p_grad of gradient queries."""
+    out = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        k = kinds[int(rng.choice(len(kinds), p=p_kinds))]
+        out.append(Request(kind=k, steps=int(rng.integers(steps_lo, steps_hi + 1)),
+                           grad=bool(rng.random() < p_grad), seed=int(rng.integers(1 << 30)),
+                           arrival=t))
+    return out

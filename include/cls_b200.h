@@ -198,6 +198,35 @@ int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam);
 int cls_graph_launch(cls_sim* sim, int32_t iter);
 
 /* ---------------------------------------------------------------------------
+ * Serving: one handle as a pool of env slots at different times of their own
+ * episodes.  The reference has no serving path; these calls let a request
+ * loop (serving.py) fold rollout requests into a running batch: a slot is
+ * (re)started with cls_serve_reset_env, and every launch advances each slot
+ * through its own window.  Each slot needs a robot (controller) of its own,
+ * so that its weight gradients are its own.
+ *
+ * windows: [n_envs][4] int32 in user env order, {t_begin, t_end, checkpoint,
+ * first}: the env runs steps [t_begin, t_end) of its episode from checkpoint
+ * `checkpoint` (t_begin = checkpoint * checkpoint_every, t_end - t_begin <=
+ * checkpoint_every); t_begin >= t_end leaves the env idle.  `first` marks the
+ * first (last-in-time) reverse segment of an env's reverse pass.
+ * steps: [n_envs] episode steps of each env (the `steps` of cls_forward).
+ * --------------------------------------------------------------------------- */
+/* Initial state x0 (v0 may be NULL: zero) [n_v][3] and targets tv [T][3],
+ * th [T], tc [T] (NULL: zero) of one env; clears its observables. */
+int cls_serve_reset_env(cls_sim* sim, int32_t env, const double* x0, const double* v0, const double* tv,
+                        const double* th, const double* tc);
+/* First-pass substeps of every env's window (checkpoints at window ends). */
+int cls_serve_forward(cls_sim* sim, const int32_t* windows, const int32_t* steps);
+/* One reverse segment per env window (recompute + adjoint + weight
+ * gradients); an env's robot gradients restart at its `first` segment. */
+int cls_serve_backward(cls_sim* sim, const int32_t* windows, const int32_t* steps);
+/* Per-env losses [8][n_envs] (cls_loss's loss_env layout) with per-env steps. */
+int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* loss_env);
+/* State at the end of the env's last forward window, [n_v][3] each. */
+int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v);
+
+/* ---------------------------------------------------------------------------
  * Differentiable MLS-MPM (multitask/solver_mpm.py).  The reference's solver is
  * 2D (fixed-corotated, actuation along y) and unreachable from its env
  * (taichi_env.py:136 constructs it without its config); these entry points run

@@ -1,0 +1,165 @@
+"""Request-loop scheduling on the CPU with a fake backend: window tables per
+tick (they must reproduce the windows of cls_forward / cls_backward),
+folding of late requests into running launches, admission by slots and by
+HBM footprint, and the open-loop arrival generator."""
+import itertools
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from cls_b200 import robot_design
+from cls_b200.batch import Robot
+from cls_b200.serving import (Request, RobotType, Server, footprint_bytes, poisson_requests)
+
+
+class FakeBackend:
+    """Records every launch; losses and gradients are functions of the request."""
+
+    def __init__(self, slot_types, types, params):
+        self.slot_types = list(slot_types)
+        self.loaded = [k for k in slot_types]
+        self.req = [None] * len(slot_types)
+        self.calls = []
+
+    def load_weights(self, slot, kind, weights):
+        self.loaded[slot] = kind
+
+    def reset(self, slot, req, robot):
+        self.req[slot] = req
+        self.calls.append(("reset", slot, req.rid))
+
+    def forward(self, windows, steps):
+        self.calls.append(("forward", windows.copy(), steps.copy()))
+
+    def backward(self, windows, steps):
+        self.calls.append(("backward", windows.copy(), steps.copy()))
+
+    def loss(self, steps):
+        env = np.zeros((8, len(self.slot_types)))
+        for i, r in enumerate(self.req):
+            if r is not None:
+                env[0, i] = r.seed + 0.5 * steps[i]
+        return env
+
+    def final_x(self, slot):
+        return np.zeros((1, 3))
+
+    def grads(self, slot):
+        return [("grad-of", self.req[slot].rid)]
+
+    def sync(self):
+        pass
+
+    def close(self):
+        pass
+
+
+def _robots():
+    obj, spr = robot_design.quadruped_lattice()
+    quad = Robot.actuated_outputs(obj, spr, hidden=[64])
+    rng = np.random.default_rng(0)
+    o2, s2 = robot_design.random_lattice(rng, 120)
+    lat = Robot.actuated_outputs(o2, s2, hidden=[128, 128])
+    return {"quad": RobotType(quad), "lattice": RobotType(lat)}
+
+
+def _server(slots, K=50, T=2000, budget=None):
+    params = SimpleNamespace(checkpoint_every=K, max_steps=T, turn_period=500)
+    ticks = itertools.count()
+    clock = lambda: next(ticks) * 1e-3  # noqa: E731
+    return Server(_robots(), slots, params, hbm_budget=budget,
+                  backend_factory=lambda st, types, p: FakeBackend(st, types, p), clock=clock)
+
+
+def _windows_of(backend, slot, kind):
+    return [tuple(c[1][slot]) for c in backend.calls if c[0] == kind and c[1][slot][0] < c[1][slot][1]]
+
+
+@pytest.mark.parametrize("steps,K", [(1000, 50), (137, 50), (2, 50), (51, 50), (52, 50), (300, 7)])
+def test_windows_reproduce_forward_and_backward_segments(steps, K):
+    srv = _server({"quad": 1}, K=K)
+    srv.submit(Request(kind="quad", steps=steps, grad=True, seed=3))
+    res = srv.drain()
+    assert len(res) == 1 and res[0].grads == [("grad-of", 0)]
+    be = srv.pools[0].backend
+    t_last = steps - 1
+    fwd = _windows_of(be, 0, "forward")
+    exp_f = [(t, min(t + K, t_last), t // K, 0) for t in range(0, t_last, K)]
+    assert fwd == exp_f
+    n_seg = (t_last + K - 1) // K
+    exp_b = [(s * K, min(s * K + K, t_last), s, int(s == n_seg - 1)) for s in range(n_seg - 1, -1, -1)]
+    assert _windows_of(be, 0, "backward") == exp_b
+    assert res[0].loss == pytest.approx(3 + 0.5 * steps)
+
+
+def test_late_request_is_folded_into_running_launches():
+    srv = _server({"quad": 2, "lattice": 1})
+    srv.submit(Request(kind="quad", steps=1000, seed=1))
+    for _ in range(4):
+        srv.tick()
+    srv.submit(Request(kind="quad", steps=400, seed=2))
+    srv.submit(Request(kind="lattice", steps=300, seed=3))
+    srv.tick()
+    # the quad pool's next launch advances the first request at t = 200 and
+    # starts the second at t = 0 in the same launch
+    quad_pool = [p for p in srv.pools if p.slots[0].kind == "quad"][0]
+    last = [c for c in quad_pool.backend.calls if c[0] == "forward"][-1][1]
+    assert tuple(last[0][:2]) == (200, 250) and tuple(last[1][:2]) == (0, 50)
+    res = {r.rid: r for r in srv.drain()}
+    assert sorted(res) == [0, 1, 2]
+    assert res[1].done < res[0].done      # the short late request finishes first
+
+
+def test_admission_waits_for_slots_and_lets_other_types_pass():
+    srv = _server({"quad": 1, "lattice": 1})
+    a = srv.submit(Request(kind="quad", steps=500))
+    b = srv.submit(Request(kind="quad", steps=200))
+    c = srv.submit(Request(kind="lattice", steps=200))
+    srv.tick()
+    active = {s.req.rid for p in srv.pools for s in p.slots if s.req is not None}
+    assert active == {a, c} and [r.rid for r in srv.queue] == [b]
+    res = srv.drain()
+    order = [r.rid for r in sorted(res, key=lambda r: r.done)]
+    assert order.index(a) < order.index(b)
+
+
+def test_admission_by_hbm_footprint():
+    types = _robots()
+    fp = footprint_bytes(types["quad"].robot, 1000, False, 50)
+    srv = _server({"quad": 4}, budget=int(1.5 * fp))
+    ids = [srv.submit(Request(kind="quad", steps=1000)) for _ in range(3)]
+    srv.tick()
+    active = [s.req.rid for s in srv.pools[0].slots if s.req is not None]
+    assert active == [ids[0]] and srv.used_bytes == fp
+    res = srv.drain()
+    assert len(res) == 3 and srv.used_bytes == 0
+    done = sorted(res, key=lambda r: r.done)
+    assert [r.rid for r in done] == ids           # one at a time, in order
+    with pytest.raises(ValueError):
+        srv.submit(Request(kind="quad", steps=5000))
+
+
+def test_poisson_requests_statistics():
+    rng = np.random.default_rng(7)
+    reqs = poisson_requests(rng, 200.0, 50.0, ["a", "b"], [0.25, 0.75])
+    assert abs(len(reqs) / 50.0 - 200.0) < 200.0 * 0.05
+    gaps = np.diff([r.arrival for r in reqs])
+    assert abs(gaps.mean() - 1 / 200.0) < 0.05 / 200.0
+    steps = np.array([r.steps for r in reqs])
+    assert steps.min() >= 100 and steps.max() <= 2000
+    assert abs(np.mean([r.grad for r in reqs]) - 0.2) < 0.03
+    assert abs(np.mean([r.kind == "a" for r in reqs]) - 0.25) < 0.03
+
+
+def test_stats_report_percentiles():
+    srv = _server({"quad": 2})
+    for k in range(6):
+        srv.submit(Request(kind="quad", steps=60 + 40 * k))
+    srv.drain()
+    st = srv.stats()
+    lat = sorted(r.latency for r in srv.results)
+    assert st["requests"] == 6
+    assert st["p50_ms"] == pytest.approx(np.percentile(lat, 50) * 1e3)
+    assert st["p99_ms"] == pytest.approx(np.percentile(lat, 99) * 1e3)
+    assert st["env_substeps_per_s"] > 0

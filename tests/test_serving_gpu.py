@@ -1,0 +1,114 @@
+"""Served requests on the GPU: a request's result is the same alone and in a
+mix that folds other requests into the running launches, and both equal the
+plain one-env batch (cls_forward + cls_loss + cls_backward) of the same robot,
+weights and targets.  Losses within rel 1e-6 (the first pass is
+deterministic), weight gradients within rel 1e-5 (the reverse pass adds
+spring adjoints with shared-memory atomics); FP64 at 1e-10."""
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _types(precision):
+    from cls_b200 import robot_design
+    from cls_b200.batch import Robot
+    from cls_b200.serving import RobotType
+    obj, spr = robot_design.quadruped_lattice()
+    types = {"quad": RobotType(Robot.actuated_outputs(obj, spr, hidden=[64]))}
+    rng = np.random.default_rng(5)
+    for name, n in (("lat120", 120), ("lat300", 300)):
+        o2, s2 = robot_design.random_lattice(rng, n)
+        types[name] = RobotType(Robot.actuated_outputs(o2, s2, hidden=[64, 64]))
+    return types
+
+
+def _params(T, precision):
+    from cls_b200 import workloads
+    from cls_b200.batch import default_params
+    return default_params(**workloads._params(T, 50, precision=precision))
+
+
+def _requests():
+    from cls_b200.serving import Request
+    return [Request("quad", 300, grad=True, seed=11), Request("lat120", 260, grad=False, seed=12),
+            Request("lat300", 400, grad=True, seed=13), Request("quad", 120, grad=False, seed=14),
+            Request("lat120", 333, grad=True, seed=15), Request("lat300", 75, grad=False, seed=16)]
+
+
+def _serve(types, params, reqs, slots, stagger):
+    from cls_b200.serving import Server
+    srv = Server(types, slots, params)
+    try:
+        ids = []
+        for k, r in enumerate(reqs):
+            ids.append(srv.submit(r))
+            if stagger and k % 2 == 1:
+                srv.tick()
+                srv.tick()
+        res = {r.rid: r for r in srv.drain()}
+        return [res[i] for i in ids]
+    finally:
+        srv.close()
+
+
+def _plain(types, params, req):
+    from cls_b200.batch import MassSpringBatch
+    from cls_b200.serving import request_targets
+    rt = types[req.kind]
+    b = MassSpringBatch([rt.robot], [0], params)
+    try:
+        for l, (W, bias) in enumerate(rt.weights):
+            b.set_weights(0, l, W, bias)
+        tv, th = request_targets(req.seed, b.T, req.steps, params.turn_period)
+        b.set_targets(tv[:, None, :], th[:, None])
+        b.forward(req.steps)
+        terms, _ = b.loss()
+        grads = None
+        if req.grad:
+            b.backward()
+            grads = [b.get_grads(0, l) for l in range(b.n_layers(0))]
+        x, _ = b.final_state()
+        return terms["total"], grads, x
+    finally:
+        b.close()
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_served_results_same_alone_in_mix_and_as_plain_batch(precision):
+    import copy
+    types = _types(precision)
+    params = _params(400, precision)
+    tl, tg = (1e-6, 1e-5) if precision == 32 else (1e-10, 1e-10)
+    mix = _serve(types, params, _requests(), {"quad": 2, "lat120": 2, "lat300": 2}, stagger=True)
+    # the mix made the types' controllers; alone-runs reuse them
+    for req, got in zip(_requests(), mix):
+        alone = _serve(types, params, [copy.copy(req)], {req.kind: 1}, stagger=False)[0]
+        ref_loss, ref_grads, ref_x = _plain(types, params, req)
+        assert got.loss == pytest.approx(alone.loss, rel=tl, abs=1e-12)
+        assert got.loss == pytest.approx(ref_loss, rel=tl, abs=1e-12)
+        assert rel_err(got.final_x, ref_x) < tl
+        if req.grad:
+            for (gW, gb), (aW, ab), (rW, rb) in zip(got.grads, alone.grads, ref_grads):
+                assert rel_err(gW, aW) < tg and rel_err(gW, rW) < tg
+                assert rel_err(gb, ab) < tg and rel_err(gb, rb) < tg
+        else:
+            assert got.grads is None
+
+
+def test_open_loop_run_reports_latency():
+    from cls_b200.serving import Server, poisson_requests
+    types = _types(32)
+    params = _params(400, 32)
+    rng = np.random.default_rng(3)
+    reqs = poisson_requests(rng, 100.0, 0.2, list(types), [0.4, 0.3, 0.3], steps_lo=50, steps_hi=400)
+    srv = Server(types, {"quad": 4, "lat120": 4, "lat300": 4}, params)
+    try:
+        res, st = srv.run(reqs)
+    finally:
+        srv.close()
+    assert len(res) == len(reqs) and st["requests"] == len(reqs)
+    assert 0 < st["p50_ms"] <= st["p99_ms"]
+    assert all(np.isfinite(r.loss) for r in res)
