@@ -40,9 +40,12 @@ sys.path.insert(0, ROOT)
 METRICS = {"uneven": "fwd+adjoint env-substeps/s (batched uneven mass-spring)",
            "quadruped": "fwd+adjoint env-substeps/s (quadruped lattice, 32 envs)",
            "spider": "fwd+adjoint env-substeps/s (spider lattice, 4096 envs)",
-           "mpm": "fwd+adjoint env-substeps/s (3D MLS-MPM legged body, 8 envs)"}
-DEFAULT_SUBSTEPS = {"uneven": 2000, "quadruped": 1000, "spider": 1000, "mpm": 1000}
-DEFAULT_ENVS = {"uneven": 512, "quadruped": 32, "spider": 4096, "mpm": 8}
+           "mpm": "fwd+adjoint env-substeps/s (3D MLS-MPM legged body, 8 envs)",
+           "serve": "served env-substeps/s of Poisson rollout requests (p50/p99 latency beside)"}
+DEFAULT_SUBSTEPS = {"uneven": 2000, "quadruped": 1000, "spider": 1000, "mpm": 1000, "serve": 2000}
+DEFAULT_ENVS = {"uneven": 512, "quadruped": 32, "spider": 4096, "mpm": 8, "serve": 32}
+SERVE_RATE = 200.0          # requests per second
+SERVE_SECONDS_PER_STEP = 2.0  # seconds of arrivals per bench step
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one launch
 # divided by the algorithmic bytes of that launch, from one `ncu --set full`
 # capture of this workload at 128 robots x 100 substeps (the 512-robot workload
@@ -67,6 +70,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: automatic)")
+    ap.add_argument("--tick-segments", type=int, default=4,
+                    help="serve: checkpoint segments a tick advances every request by")
     a = ap.parse_args()
     if a.robots is None:
         a.robots = DEFAULT_ENVS[a.config]
@@ -99,6 +104,17 @@ def config_dict(a, n_gpus):
                 "envs_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
                 "parallelism": par,
                 "l2": "trajectory and checkpoints written every iteration exceed L2"}
+    if a.config == "serve":
+        return {"workload": "serving: Poisson rollout requests at %.0f/s over %.0f s; robot mix quadruped "
+                            "25%% (MLP 1x64), spider 25%% (MLP 2x256), random lattices of 100/300/800/1500 "
+                            "vertices 50%% (MLP 2x128); episodes U{100..2000} substeps; 80%% forward-only "
+                            "evaluation, 20%% forward+adjoint gradient queries; %d slots per robot type, "
+                            "ticks of %d substeps" % (SERVE_RATE, a.steps * SERVE_SECONDS_PER_STEP,
+                                                        a.robots, a.checkpoint * a.tick_segments),
+                "slots_per_type": a.robots, "rate_per_s": SERVE_RATE,
+                "arrival_seconds": a.steps * SERVE_SECONDS_PER_STEP, "checkpoint_every": a.checkpoint,
+                "parallelism": "independent servers x%d (no data-path collective)" % n_gpus,
+                "l2": "per-slot trajectories and checkpoints of all resident requests exceed L2"}
     return {"workload": "3D MLS-MPM: legged body of 29504 particles (8 per cell, 16 fibre-actuated "
                         "muscle groups), 64^3 grid, neo-Hookean E=1e4 nu=0.3, dt 1e-4, %d envs x %d "
                         "substeps, checkpoint every %d, centre loss" % (a.robots, a.substeps, a.checkpoint),
@@ -153,6 +169,8 @@ def run_reference(a):
     from cls_b200 import workloads
     if a.config == "mpm":
         return run_reference_mpm(a)
+    if a.config == "serve":
+        return run_reference_serve(a)
     if a.config == "uneven":
         robots = workloads.uneven_robots(a.robots, seed=0)
     else:
@@ -573,12 +591,178 @@ def run_mpm(a):
         torch.distributed.destroy_process_group()
 
 
+# ----------------------------------------------------------------- serving
+def serve_oracle_sample(types, reqs, threads, cap=200):
+    """Time the FP64 oracle on requests of the serving mix (episodes capped
+    at `cap` substeps): forward + loss, and the reverse pass for gradient
+    queries; one request per worker thread."""
+    from oracle.ms_oracle import MassSpringOracle
+    from cls_b200.serving import request_targets
+
+    def one(req):
+        rb = types[req.kind].robot
+        T = min(req.steps, cap)
+        o = MassSpringOracle(rb.objects, rb.springs, 1, T, n_sin=8, dup_v=1, dup_h=1, dup_c=0,
+                             hidden=list(rb.hidden), dt=2e-3, gravity=-9.8, ground=0.0,
+                             drag=-math.log(0.99) / 2e-3, dashpot=0.1, friction=0.5,
+                             spring_omega=2 * math.pi / 2e-3 / 100, run_period=100,
+                             turn_period=500, jump_period=500, act_hidden="tanh", act_out="tanh",
+                             out_index=rb.spring_output, n_out=rb.n_outputs,
+                             loss=("velocity", "rotation"), n_threads=1)
+        wr = np.random.default_rng(req.seed)
+        for l in range(o.L):
+            o.W[l][...] = (wr.random(o.W[l].shape) * 2 - 1) * math.sqrt(6 / o.W[l].shape[1])
+        o.set_initial_state(rb.objects)
+        tv, th = request_targets(req.seed, T, T, 500)
+        o.set_targets(tv[:, None, :], th[:, None])
+        t0 = time.perf_counter()
+        if req.grad:
+            o.run(T)
+        else:
+            o.forward(T)
+            o.compute_loss(T)
+        return time.perf_counter() - t0, T - 1
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        res = list(ex.map(one, reqs))
+    wall = time.perf_counter() - t0
+    n = sum(k for _, k in res)
+    return n / wall, "%d requests of the serving mix, episodes capped at %d substeps (FP64; forward + " \
+        "loss, + reverse pass for gradient queries)" % (len(reqs), cap), wall
+
+
+def run_reference_serve(a):
+    from cls_b200 import workloads
+    from cls_b200.serving import poisson_requests
+    types, kinds, probs = workloads.serving_types()
+    cores = os.cpu_count() or 1
+    vals, sample = [], ""
+    for i in range(a.warmup + a.steps):
+        reqs = poisson_requests(np.random.default_rng(100 + i), SERVE_RATE, 2.0 * cores / SERVE_RATE,
+                                kinds, probs)[:2 * cores]
+        v, sample, _ = serve_oracle_sample(types, reqs, cores)
+        if i >= a.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRICS[a.config], "value": value, "unit": UNIT,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config_dict(a, a.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample + "; requests run back to back on the host cores (no "
+                                                "request loop); reference Taichi not installed"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_serve(a):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from cls_b200 import workloads
+    from cls_b200.batch import default_params
+    from cls_b200.serving import Server, poisson_requests
+    types, kinds, probs = workloads.serving_types()
+    params = default_params(**workloads._params(a.substeps, a.checkpoint))
+    srv = Server(types, {k: a.robots for k in kinds}, params, tick_segments=a.tick_segments)
+    # warm-up: a short burst of requests (kernels loaded, slots exercised)
+    warm = poisson_requests(np.random.default_rng(77 + rank), SERVE_RATE, 0.5 * a.warmup, kinds, probs,
+                            steps_hi=400)
+    srv.run(warm)
+    srv.results, srv.substeps_done, srv.ticks = [], 0, 0
+    for p in srv.pools:
+        p.backend.batch.profile(True)
+        p.backend.batch.profile_read(reset=True)
+    reqs = poisson_requests(np.random.default_rng(1000 * rank + 1), SERVE_RATE,
+                            a.steps * SERVE_SECONDS_PER_STEP, kinds, probs)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    res, st = srv.run(reqs)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    kern_ms, launches = {}, {}
+    for p in srv.pools:
+        ms, n = p.backend.batch.profile_read(reset=True)
+        for k in ms:
+            kern_ms[k] = kern_ms.get(k, 0.0) + ms[k]
+            launches[k] = launches.get(k, 0) + n[k]
+    wall = st["wall_s"]
+    substeps = st["env_substeps_per_s"] * wall
+    if world > 1:
+        t = torch.tensor([wall, substeps], device="cuda", dtype=torch.float64)
+        w = t.clone()
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        wall, substeps = float(w[0].item()), float(t[1].item())
+    value = substeps / wall
+    # roofline of the first-pass kernel: algorithmic bytes of the served
+    # forward substeps over its device time
+    fwd_bytes = 0.0
+    for r in res:
+        per = workloads.algorithmic_bytes([types[r.kind].robot], [0])["forward"]
+        fwd_bytes += per * (r.steps - 1)
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    # the pools' streams run concurrently, so per-launch event times overlap:
+    # the forward kernel's achieved rate is taken over the run's wall time
+    # (a lower bound)
+    achieved = fwd_bytes / wall / 1e9
+    roofline = {"kernel": "ms_forward_kernel (served windows)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": None, "basis": "algorithmic first-pass bytes of the served requests / wall time",
+                "kernel_ms_overlapping_streams": kern_ms, "launches": launches}
+    n_req = max(1, len(res))
+    h2d = sum(types[r.kind].robot.n_vertices * 24 + params.max_steps * 40 for r in res) / n_req
+    d2h = sum(types[r.kind].robot.n_vertices * 24 + 64 * a.robots * len(types) +
+              (sum(W.size + b.size for W, b in r.grads) * 8 if r.grads else 0) for r in res) / n_req
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        sample = [r for r in reqs[:4 * cores]]
+        v, desc, w = serve_oracle_sample(types, sample, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": desc + "; wall %.1f s; reference Taichi not installed" % w}
+    if rank == 0:
+        line = {"metric": METRICS[a.config], "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": wall * 1e3 / a.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Poisson arrivals, robots, targets and controllers)",
+                "config": config_dict(a, world), "clocks": clocks,
+                "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"]},
+                "requests": st["requests"], "ticks": st["ticks"],
+                "gpu_launches": int(sum(launches.values())), "roofline": roofline,
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(h2d * len(res) / a.steps),
+                        "d2h_bytes_per_step": int(d2h * len(res) / a.steps),
+                        "path": "Server.run: requests -> cls_serve_reset_env (host targets/state) -> "
+                                "cls_serve_forward / cls_serve_backward ticks -> cls_serve_loss, "
+                                "cls_serve_env_state, cls_get_grads (host results)"},
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    srv.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.config == "mpm":
         run_mpm(a)
+    elif a.config == "serve":
+        run_serve(a)
     else:
         run_ours(a)
 

@@ -71,6 +71,57 @@ enum ProfKind : int { PK_FWD = 0, PK_RECOMP, PK_REV, PK_WGRAD, PK_LOSS, PK_ADAM,
 
 using Profiler = EventProfile<PK_COUNT>;
 
+// Pinned host -> device staging ring for small per-launch tables: slot k's
+// host bytes are reused only after the event recorded behind its last copy
+// has completed, so uploads never block on the stream.
+struct StageRing {
+  static constexpr int kSlots = 32;
+  size_t bytes = 0;
+  unsigned char* host = nullptr;
+  unsigned char* dev = nullptr;
+  cudaEvent_t ev[kSlots] = {};
+  bool used[kSlots] = {};
+  int next = 0;
+  cudaError_t init(size_t b) {
+    bytes = (b + 255) & ~size_t(255);
+    cudaError_t r = cudaMallocHost(&host, bytes * kSlots);
+    if (r != cudaSuccess) return r;
+    r = cudaMalloc(&dev, bytes * kSlots);
+    if (r != cudaSuccess) return r;
+    for (int k = 0; k < kSlots; ++k) {
+      r = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+      if (r != cudaSuccess) return r;
+    }
+    return cudaSuccess;
+  }
+  ~StageRing() {
+    for (int k = 0; k < kSlots; ++k)
+      if (ev[k]) cudaEventDestroy(ev[k]);
+    if (host) cudaFreeHost(host);
+    if (dev) cudaFree(dev);
+  }
+  // host and device addresses of the next free slot
+  cudaError_t acquire(unsigned char** h, unsigned char** d, int* slot) {
+    const int k = next;
+    next = (next + 1) % kSlots;
+    if (used[k]) {
+      const cudaError_t r = cudaEventSynchronize(ev[k]);
+      if (r != cudaSuccess) return r;
+    }
+    *h = host + (size_t)k * bytes;
+    *d = dev + (size_t)k * bytes;
+    *slot = k;
+    return cudaSuccess;
+  }
+  cudaError_t upload(int slot, size_t n, cudaStream_t s) {
+    cudaError_t r = cudaMemcpyAsync(dev + (size_t)slot * bytes, host + (size_t)slot * bytes, n,
+                                    cudaMemcpyHostToDevice, s);
+    if (r != cudaSuccess) return r;
+    used[slot] = true;
+    return cudaEventRecord(ev[slot], s);
+  }
+};
+
 class SimBase {
  public:
   virtual ~SimBase() = default;
@@ -414,11 +465,9 @@ class SimImpl final : public SimBase {
                         cudaMemcpyHostToDevice));
     n_queue_ = (size_t)(1 + 2 * n_seg_max) * E;
     d_queue_.alloc(n_queue_);
-    d_win_.alloc(E);
     d_env_steps_.alloc(E);
     d_sorder_.alloc(E);
     d_squeue_.alloc(2);
-    d_stiles_.alloc(std::max<size_t>(1, tiles_host_.size()));
     inv_perm_.assign(E, 0);
     for (int ie = 0; ie < E; ++ie) inv_perm_[perm_[ie]] = ie;
     size_t stage = std::max<size_t>((size_t)T_ * E * 3, (size_t)V_ * 3);
@@ -674,7 +723,7 @@ class SimImpl final : public SimBase {
 
   void loss_device() {
     MsArgs<R> a = args(steps_);
-    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p); });
+    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p, nullptr); });
     CLS_CUDA(cudaGetLastError());
   }
 
@@ -1041,12 +1090,17 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaStreamSynchronize(stream));  // host staging vectors go out of scope
   }
 
-  // windows and steps (user order) -> internal tables; returns the active count
-  int serve_prepare(const int* win, const int* steps) {
+  // windows and steps (user order) -> internal tables in one staging slot
+  // (int4 windows [E], int steps [E], int order [E]); returns the active
+  // count; the slot's device address is left in serve_stage_.
+  int serve_prepare(const int* win, const int* steps, bool reverse) {
     CLS_REQUIRE(win != nullptr && steps != nullptr, "windows and steps are required");
-    std::vector<int4> w(E_);
-    std::vector<int> st(E_);
-    std::vector<int> order;
+    std::vector<int4>& w = serve_w_tmp_;
+    std::vector<int>& st = serve_st_tmp_;
+    std::vector<int>& order = serve_order_h_;
+    w.assign(E_, make_int4(0, 0, 0, 0));
+    st.assign(E_, 0);
+    order.clear();
     for (int ie = 0; ie < E_; ++ie) {
       const int ue = perm_[ie];
       w[ie] = make_int4(win[4 * ue], win[4 * ue + 1], win[4 * ue + 2], win[4 * ue + 3]);
@@ -1054,35 +1108,42 @@ class SimImpl final : public SimBase {
       if (w[ie].x < w[ie].y) {
         CLS_REQUIRE(st[ie] >= 2 && st[ie] <= T_, "episode steps out of range");
         CLS_REQUIRE(w[ie].x >= 0 && w[ie].y <= st[ie] - 1, "a window lies in [0, steps - 1)");
-        CLS_REQUIRE(w[ie].y - w[ie].x <= K_, "a window spans at most checkpoint_every steps");
+        CLS_REQUIRE(!reverse || w[ie].y - w[ie].x <= K_, "a reverse window spans one checkpoint segment");
         CLS_REQUIRE(w[ie].z >= 0 && w[ie].z < (int)n_ckpt_ && w[ie].x == w[ie].z * K_,
                     "a window starts at its source checkpoint (t_begin = checkpoint * checkpoint_every)");
       }
     }
     for (int ie : order_host_)
       if (w[ie].x < w[ie].y) order.push_back(ie);
-    CLS_CUDA(cudaMemcpyAsync(d_win_.p, w.data(), sizeof(int4) * E_, cudaMemcpyHostToDevice, stream));
-    CLS_CUDA(cudaMemcpyAsync(d_env_steps_.p, st.data(), sizeof(int) * E_, cudaMemcpyHostToDevice, stream));
-    if (!order.empty())
-      CLS_CUDA(cudaMemcpyAsync(d_sorder_.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice,
-                               stream));
+    if (!stage_.host) CLS_CUDA(stage_.init(stage_bytes()));
+    unsigned char *h, *d;
+    int slot;
+    CLS_CUDA(stage_.acquire(&h, &d, &slot));
+    std::memcpy(h, w.data(), sizeof(int4) * E_);
+    std::memcpy(h + sizeof(int4) * E_, st.data(), sizeof(int) * E_);
+    std::memcpy(h + (sizeof(int4) + sizeof(int)) * E_, order.data(), sizeof(int) * order.size());
+    CLS_CUDA(stage_.upload(slot, (sizeof(int4) + 2 * sizeof(int)) * E_, stream));
+    serve_stage_ = d;
     serve_win_h_ = w;
-    serve_order_h_ = order;
-    CLS_CUDA(cudaStreamSynchronize(stream));  // host tables go out of scope
     return (int)order.size();
+  }
+
+  size_t stage_bytes() const {
+    return std::max((sizeof(int4) + 2 * sizeof(int)) * (size_t)E_,
+                    sizeof(GemmTile) * std::max<size_t>(1, tiles_host_.size()));
   }
 
   MsArgs<R> serve_args(int n) {
     MsArgs<R> a = args(T_);
-    a.win = d_win_.p;
-    a.env_steps = d_env_steps_.p;
-    a.order = d_sorder_.p;
+    a.win = reinterpret_cast<const int4*>(serve_stage_);
+    a.env_steps = reinterpret_cast<const int*>(serve_stage_ + sizeof(int4) * E_);
+    a.order = reinterpret_cast<const int*>(serve_stage_ + (sizeof(int4) + sizeof(int)) * E_);
     a.n_items = n;
     return a;
   }
 
   void serve_forward(const int* win, const int* steps) override {
-    const int n = serve_prepare(win, steps);
+    const int n = serve_prepare(win, steps, false);
     if (n == 0) return;
     CLS_CUDA(cudaMemsetAsync(d_squeue_.p, 0, sizeof(int) * 2, stream));
     MsArgs<R> a = serve_args(n);
@@ -1094,7 +1155,7 @@ class SimImpl final : public SimBase {
   }
 
   void serve_backward(const int* win, const int* steps) override {
-    const int n = serve_prepare(win, steps);
+    const int n = serve_prepare(win, steps, true);
     if (n == 0) return;
     // a robot's weight gradients restart with its env's first reverse segment
     std::vector<int> active_robot(rd_host_.size(), 0);
@@ -1121,12 +1182,15 @@ class SimImpl final : public SimBase {
     a.queue = d_squeue_.p + 1;
     timed(PK_REV, [&] { rev_fn()<<<grid_for(n), threads_, rev_smem_, stream>>>(a, 0, 0, 0); });
     if (!tiles.empty()) {
-      CLS_CUDA(cudaMemcpyAsync(d_stiles_.p, tiles.data(), sizeof(GemmTile) * tiles.size(), cudaMemcpyHostToDevice,
-                               stream));
+      unsigned char *h, *d;
+      int slot;
+      CLS_CUDA(stage_.acquire(&h, &d, &slot));
+      std::memcpy(h, tiles.data(), sizeof(GemmTile) * tiles.size());
+      CLS_CUDA(stage_.upload(slot, sizeof(GemmTile) * tiles.size(), stream));
+      const GemmTile* dt = reinterpret_cast<const GemmTile*>(d);
       timed(PK_WGRAD, [&] {
-        ms_wgrad_kernel<R><<<(int)tiles.size(), 256, 0, stream>>>(a, d_stiles_.p, 0, d_gw_.p, d_gb_.p);
+        ms_wgrad_kernel<R><<<(int)tiles.size(), 256, 0, stream>>>(a, dt, 0, d_gw_.p, d_gb_.p);
       });
-      CLS_CUDA(cudaStreamSynchronize(stream));  // tile list goes out of scope
     }
     CLS_CUDA(cudaGetLastError());
     bwd_done_ = true;  // served robots' gradients are readable (cls_get_grads)
@@ -1134,16 +1198,25 @@ class SimImpl final : public SimBase {
 
   void serve_loss(const int* steps, double* env) override {
     CLS_REQUIRE(steps != nullptr, "steps are required");
-    std::vector<int> st(E_);
+    std::vector<int> st(E_), list;
     for (int ie = 0; ie < E_; ++ie) {
       st[ie] = steps[perm_[ie]];
+      if (st[ie] <= 0) continue;  // not requested
       CLS_REQUIRE(st[ie] >= 2 && st[ie] <= T_, "episode steps out of range");
+      list.push_back(ie);
     }
-    CLS_CUDA(cudaMemcpyAsync(d_env_steps_.p, st.data(), sizeof(int) * E_, cudaMemcpyHostToDevice, stream));
-    MsArgs<R> a = args(T_);
-    a.env_steps = d_env_steps_.p;
-    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p); });
-    CLS_CUDA(cudaGetLastError());
+    CLS_CUDA(cudaMemsetAsync(d_lossenv_.p, 0, sizeof(double) * E_ * 8, stream));
+    if (!list.empty()) {
+      CLS_CUDA(cudaMemcpyAsync(d_env_steps_.p, st.data(), sizeof(int) * E_, cudaMemcpyHostToDevice, stream));
+      CLS_CUDA(cudaMemcpyAsync(d_sorder_.p, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice,
+                               stream));
+      MsArgs<R> a = args(T_);
+      a.env_steps = d_env_steps_.p;
+      timed(PK_LOSS, [&] {
+        ms_loss_kernel<R><<<(int)list.size(), 256, 0, stream>>>(a, d_lossenv_.p, d_sorder_.p);
+      });
+      CLS_CUDA(cudaGetLastError());
+    }
     std::vector<double> raw((size_t)E_ * 8);
     CLS_CUDA(cudaMemcpyAsync(raw.data(), d_lossenv_.p, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, stream));
     CLS_CUDA(cudaStreamSynchronize(stream));
@@ -1244,11 +1317,11 @@ class SimImpl final : public SimBase {
   std::vector<EnvDesc> ed_host_;
   std::vector<RobotDesc> rd_host_;
   std::vector<GemmTile> tiles_host_;
-  std::vector<int> inv_perm_, serve_order_h_;
-  std::vector<int4> serve_win_h_;
-  DevBuf<int4> d_win_;
+  std::vector<int> inv_perm_, serve_order_h_, serve_st_tmp_;
+  std::vector<int4> serve_win_h_, serve_w_tmp_;
   DevBuf<int> d_env_steps_, d_sorder_, d_squeue_;
-  DevBuf<GemmTile> d_stiles_;
+  StageRing stage_;
+  unsigned char* serve_stage_ = nullptr;
   std::vector<OptSeg> opt_segs_, pack_segs_;
   long long opt_total_ = 0, pack_total_ = 0;
   double tns_host_ = 0;

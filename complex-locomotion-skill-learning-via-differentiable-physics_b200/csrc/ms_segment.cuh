@@ -687,8 +687,8 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
 // out[e * 8 + slot]: raw sums (reference's loss_x, not multiplied by B);
 // slot 7 holds the env's max height seen by the height loss.
 template <typename R>
-__global__ void ms_loss_kernel(MsArgs<R> a, double* out) {
-  const int e = blockIdx.x;
+__global__ void ms_loss_kernel(MsArgs<R> a, double* out, const int* envs) {
+  const int e = envs ? envs[blockIdx.x] : (int)blockIdx.x;  // envs: the listed envs only
   if (e >= a.n_envs) return;
   __shared__ double red[32 * 8];
   const EnvDesc ed = a.envs[e];

@@ -20,9 +20,10 @@ env slots on the GPU and folds rollout requests into the running batch:
 
 Each slot owns a controller (a robot entry of the batch), so a slot's weight
 gradients are its request's alone, and a request's result does not depend on
-what else is in the batch.  Robot types are grouped into pools by controller
-depth (one batch per depth, each on its own CUDA stream, so the pools' work
-overlaps on the device).
+what else is in the batch.  Each robot type is a pool (one batch on its own
+CUDA stream) that ticks at its own pace, so a small robot's requests are not
+held to a large robot's substep time, and the pools' work overlaps on the
+device.
 
 The scheduling is separate from the GPU backend (``SlotBackend``): the tests
 drive the scheduler with a fake backend on the CPU.
@@ -115,8 +116,9 @@ class SlotBackend:
         self.slot_types = list(slot_types)
         robots = [types[k].robot for k in self.slot_types]
         self.batch = MassSpringBatch(robots, list(range(len(robots))), params)
+        self.stream = stream          # a torch.cuda.Stream (or None: default stream)
         if stream is not None:
-            self.batch.set_stream(stream)
+            self.batch.set_stream(stream.cuda_stream)
         self.T = self.batch.T
         self.K = int(params.checkpoint_every)
         self.turn_period = int(params.turn_period)
@@ -166,6 +168,10 @@ class SlotBackend:
     def sync(self):
         self.batch.synchronize()
 
+    def query(self):
+        """True when the pool's stream has finished its work."""
+        return self.stream.query() if self.stream is not None else True
+
     def close(self):
         self.batch.close()
 
@@ -187,13 +193,17 @@ class _Slot:
 
 
 class Pool:
-    """Slots of robot types with one controller depth, served by one backend."""
+    """The slots of one robot type, served by one backend (one batch on its
+    own stream).  A pool advances by ticks: launch() issues one tick's
+    windows, complete() collects its effects once the stream is done."""
 
-    def __init__(self, slot_types, backend, K, T):
+    def __init__(self, slot_types, backend, K, T, rounds):
         self.slots = [_Slot(k) for k in slot_types]
         self.backend = backend
         self.K = K
         self.T = T
+        self.rounds = rounds
+        self.plan = None          # the tick in flight
 
     def free_slot(self, kind):
         for i, s in enumerate(self.slots):
@@ -202,49 +212,117 @@ class Pool:
         return -1
 
     def busy(self):
-        return any(s.phase != "free" for s in self.slots)
+        return self.plan is not None or any(s.phase != "free" for s in self.slots)
 
-    def windows(self):
-        """Forward and reverse window tables for this tick ({t_begin, t_end,
-        checkpoint, first} per slot) and the per-slot episode steps."""
-        n, K = len(self.slots), self.K
-        fw = np.zeros((n, 4), dtype=np.int32)
-        bw = np.zeros((n, 4), dtype=np.int32)
-        steps = np.full(n, 2, dtype=np.int32)
-        any_f = any_b = False
+    def steps(self):
+        st = np.full(len(self.slots), 2, dtype=np.int32)
         for i, s in enumerate(self.slots):
-            if s.phase == "free":
-                continue
-            st = s.req.steps
-            steps[i] = st
-            t_last = st - 1          # the first pass runs steps [0, steps - 1)
+            if s.phase != "free":
+                st[i] = s.req.steps
+        return st
+
+    def forward_windows(self, span):
+        """Forward window table of this tick ({t_begin, t_end, checkpoint, 0}
+        per slot): `span` substeps from each forward-phase slot's position."""
+        fw = np.zeros((len(self.slots), 4), dtype=np.int32)
+        any_f = False
+        for i, s in enumerate(self.slots):
             if s.phase == "fwd":
-                t0 = s.pos
-                fw[i] = (t0, min(t0 + K, t_last), t0 // K, 0)
+                t0, t_last = s.pos, s.req.steps - 1   # the first pass runs steps [0, steps - 1)
+                fw[i] = (t0, min(t0 + span, t_last), t0 // self.K, 0)
                 any_f = True
-            else:
+        return fw if any_f else None
+
+    def reverse_windows(self, r):
+        """Reverse window table of round r of this tick: segment seg - r of
+        each reverse-phase slot ({t_begin, t_end, segment, first})."""
+        K = self.K
+        bw = np.zeros((len(self.slots), 4), dtype=np.int32)
+        any_b = False
+        for i, s in enumerate(self.slots):
+            if s.phase == "rev" and s.seg - r >= 0:
+                t_last = s.req.steps - 1
                 n_seg = (t_last + K - 1) // K
-                t0 = s.seg * K
-                bw[i] = (t0, min(t0 + K, t_last), s.seg, 1 if s.seg == n_seg - 1 else 0)
+                seg = s.seg - r
+                bw[i] = (seg * K, min(seg * K + K, t_last), seg, 1 if seg == n_seg - 1 else 0)
                 any_b = True
-        return fw if any_f else None, bw if any_b else None, steps
+        return bw if any_b else None
+
+    def launch(self):
+        """Issue one tick (forward windows of rounds * K substeps, `rounds`
+        reverse segments); False when no slot is active."""
+        steps = self.steps()
+        fw = self.forward_windows(self.rounds * self.K)
+        if fw is not None:
+            self.backend.forward(fw, steps)
+        any_b = False
+        for r in range(self.rounds):
+            bw = self.reverse_windows(r)
+            if bw is None:
+                break
+            self.backend.backward(bw, steps)
+            any_b = True
+        if fw is None and not any_b:
+            return False
+        self.plan = (fw, steps)
+        return True
+
+    def ready(self):
+        return self.plan is not None and self.backend.query()
+
+    def complete(self, server):
+        """Effects of the tick in flight: positions, finished first passes
+        (losses), finished requests.  Returns the finished requests."""
+        fw, steps = self.plan
+        self.plan = None
+        self.backend.sync()
+        done, fwd_finished = [], []
+        for i, s in enumerate(self.slots):
+            if s.phase == "fwd":
+                server.substeps_done += int(fw[i, 1] - fw[i, 0])
+                s.pos = int(fw[i, 1])
+                if s.pos >= s.req.steps - 1:
+                    fwd_finished.append(i)
+            elif s.phase == "rev":
+                s.seg -= self.rounds
+        if fwd_finished:
+            lsteps = np.zeros_like(steps)
+            lsteps[fwd_finished] = steps[fwd_finished]
+            env = self.backend.loss(lsteps)
+            for i in fwd_finished:
+                s = self.slots[i]
+                s.terms = dict(zip(LOSS_SLOTS, env[:, i].tolist()))
+                s.loss = s.terms["total"]
+                s.fx = self.backend.final_x(i)
+                if s.req.grad:
+                    t_last = s.req.steps - 1
+                    s.phase, s.seg = "rev", (t_last + self.K - 1) // self.K - 1
+                else:
+                    done.append(server._finish(self, i, None))
+        for i, s in enumerate(self.slots):
+            if s.phase == "rev" and s.seg < 0:
+                done.append(server._finish(self, i, self.backend.grads(i)))
+        return done
 
 
 class Server:
     """Continuous-batching request loop over resident env slots.
 
-    types:      {name: RobotType}
-    slots:      {name: number of slots of that type}
-    params:     ``batch.default_params`` of the served batches (max_steps is
-                the longest episode; checkpoint_every the tick length)
-    hbm_budget: bytes of request footprints admitted at once (None: no limit
-                beyond the slots)
+    types:         {name: RobotType}
+    slots:         {name: number of slots of that type}; each type is a pool
+                   (one batch on its own CUDA stream) that ticks at its own pace
+    params:        ``batch.default_params`` of the served batches (max_steps
+                   is the longest episode, checkpoint_every the segment length)
+    hbm_budget:    bytes of request footprints admitted at once (None: no
+                   limit beyond the slots)
+    tick_segments: checkpoint segments a tick advances every request by
     """
 
     def __init__(self, types: Dict[str, RobotType], slots: Dict[str, int], params, hbm_budget=None,
-                 backend_factory=None, streams=True, clock=time.perf_counter):
+                 backend_factory=None, streams=True, clock=time.perf_counter, tick_segments=1):
         self.types = types
         self.K = int(params.checkpoint_every)
+        self.rounds = max(1, int(tick_segments))
         self.T = int(params.max_steps)
         self.hbm_budget = hbm_budget
         self.used_bytes = 0
@@ -255,25 +333,20 @@ class Server:
         self.next_rid = 0
         self.substeps_done = 0
         self.ticks = 0
-        by_depth: Dict[int, List[str]] = {}
-        for name, n in slots.items():
-            depth = len(types[name].robot.hidden)
-            by_depth.setdefault(depth, []).extend([name] * n)
         self.pools: List[Pool] = []
-        for depth in sorted(by_depth):
-            slot_types = by_depth[depth]
+        self._streams = []
+        for name, n in slots.items():
+            slot_types = [name] * n
             if backend_factory is not None:
                 backend = backend_factory(slot_types, types, params)
             else:
                 stream = None
                 if streams:
                     import torch
-                    self._keep_streams = getattr(self, "_keep_streams", [])
-                    st = torch.cuda.Stream()
-                    self._keep_streams.append(st)
-                    stream = st.cuda_stream
+                    stream = torch.cuda.Stream()
+                    self._streams.append(stream)
                 backend = SlotBackend(slot_types, types, params, stream=stream)
-            self.pools.append(Pool(slot_types, backend, self.K, self.T))
+            self.pools.append(Pool(slot_types, backend, self.K, self.T, self.rounds))
 
     def now(self):
         return self.clock() - self.t0
@@ -296,9 +369,9 @@ class Server:
     def footprint(self, req):
         return footprint_bytes(self.types[req.kind].robot, req.steps, req.grad, self.K)
 
-    def _admit(self):
-        """FIFO admission: a request waits for a free slot of its type and for
-        HBM budget; later requests of other types may pass it."""
+    def _admit(self, pools):
+        """FIFO admission into idle pools: a request waits for a free slot of
+        its type and for HBM budget; later requests may pass it."""
         waiting = []
         for req in self.queue:
             fp = self.footprint(req)
@@ -306,7 +379,7 @@ class Server:
                 waiting.append(req)
                 continue
             placed = False
-            for pool in self.pools:
+            for pool in pools:
                 i = pool.free_slot(req.kind)
                 if i < 0:
                     continue
@@ -325,46 +398,15 @@ class Server:
 
     # -------------------------------------------------------------------- tick
     def tick(self) -> List[Result]:
-        """Admit what fits, advance every active slot by one window, return
-        the requests that finished."""
-        self._admit()
-        plans = []
+        """One synchronous round: admit what fits, launch a tick in every pool,
+        wait for them and return the requests that finished."""
+        self._admit(self.pools)
         for pool in self.pools:
-            fw, bw, steps = pool.windows()
-            if fw is not None:
-                pool.backend.forward(fw, steps)
-            if bw is not None:
-                pool.backend.backward(bw, steps)
-            plans.append((fw, bw, steps))
+            pool.launch()
         done = []
-        for pool, (fw, bw, steps) in zip(self.pools, plans):
-            if fw is None and bw is None:
-                continue
-            pool.backend.sync()
-            fwd_finished = []
-            for i, s in enumerate(pool.slots):
-                if s.phase == "fwd":
-                    self.substeps_done += int(fw[i, 1] - fw[i, 0])
-                    s.pos = int(fw[i, 1])
-                    if s.pos >= s.req.steps - 1:
-                        fwd_finished.append(i)
-                elif s.phase == "rev":
-                    s.seg -= 1
-            if fwd_finished:
-                env = pool.backend.loss(steps)
-                for i in fwd_finished:
-                    s = pool.slots[i]
-                    s.terms = dict(zip(LOSS_SLOTS, env[:, i].tolist()))
-                    s.loss = s.terms["total"]
-                    s.fx = pool.backend.final_x(i)
-                    if s.req.grad:
-                        t_last = s.req.steps - 1
-                        s.phase, s.seg = "rev", (t_last + self.K - 1) // self.K - 1
-                    else:
-                        done.append(self._finish(pool, i, None))
-            for i, s in enumerate(pool.slots):
-                if s.phase == "rev" and s.seg < 0:
-                    done.append(self._finish(pool, i, pool.backend.grads(i)))
+        for pool in self.pools:
+            if pool.plan is not None:
+                done.extend(pool.complete(self))
         self.ticks += 1
         self.results.extend(done)
         return done
@@ -387,9 +429,12 @@ class Server:
         return self.results
 
     # ------------------------------------------------------------ open loop
-    def run(self, requests: Sequence[Request], max_seconds=None):
-        """Serve requests at their arrival times (seconds from now); returns
-        the results and latency / throughput statistics."""
+    def run(self, requests: Sequence[Request], max_seconds=None, poll=2e-4):
+        """Serve requests at their arrival times (seconds from now), every
+        pool ticking at its own pace: a pool whose tick is done collects its
+        results, takes in waiting requests and launches its next tick while
+        the other pools' ticks are still on the GPU.  Returns the results and
+        latency / throughput statistics."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         self.t0 = self.clock()
         k = 0
@@ -398,10 +443,22 @@ class Server:
             while k < len(reqs) and reqs[k].arrival <= t:
                 self.submit(reqs[k])
                 k += 1
-            if self.busy():
-                self.tick()
-            elif k < len(reqs):
-                time.sleep(max(0.0, min(reqs[k].arrival - t, 0.01)))
+            progressed = False
+            for pool in self.pools:
+                if pool.plan is not None:
+                    if not pool.ready():
+                        continue
+                    self.results.extend(pool.complete(self))
+                    progressed = True
+                self._admit([pool])
+                if pool.launch():
+                    self.ticks += 1
+                    progressed = True
+            if not progressed:
+                if self.busy():
+                    time.sleep(poll)
+                elif k < len(reqs):
+                    time.sleep(max(0.0, min(reqs[k].arrival - self.now(), 0.01)))
             if max_seconds is not None and self.now() > max_seconds:
                 break
         return self.results, self.stats()

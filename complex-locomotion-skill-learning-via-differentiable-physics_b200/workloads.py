@@ -232,3 +232,24 @@ def mpm_algorithmic_bytes(pos, n_envs, n_grid=64, dtype_bytes=4):
         "grid_adj": 64 * G,
     }
     return {k: v * s * n_envs for k, v in per_env.items()}
+
+
+def serving_types(seed=0, lattice_sizes=(100, 300, 800, 1500)):
+    """Robot types of the serving workload (the training configurations'
+    robots): the quadruped lattice (MLP 1x64), the spider lattice (MLP
+    2x256) and random lattices of the uneven batch (MLP 2x128), with the
+    request mix: quadruped 25 %, spider 25 %, lattices 50 % (equal shares).
+    Controllers are drawn per type by the server."""
+    from .serving import RobotType
+    types = {}
+    obj, spr = robot_design.quadruped_lattice()
+    types["quadruped"] = RobotType(Robot.actuated_outputs(obj, spr, hidden=[64]))
+    obj, spr = robot_design.spider_lattice()
+    types["spider"] = RobotType(Robot.actuated_outputs(obj, spr, hidden=[256, 256]))
+    rng = np.random.default_rng(seed)
+    for n in lattice_sizes:
+        o, s = robot_design.random_lattice(rng, n)
+        types["lattice%d" % n] = RobotType(Robot.actuated_outputs(o, s, hidden=[128, 128]))
+    kinds = list(types)
+    p = [0.25, 0.25] + [0.5 / len(lattice_sizes)] * len(lattice_sizes)
+    return types, kinds, p

@@ -207,9 +207,10 @@ int cls_graph_launch(cls_sim* sim, int32_t iter);
  *
  * windows: [n_envs][4] int32 in user env order, {t_begin, t_end, checkpoint,
  * first}: the env runs steps [t_begin, t_end) of its episode from checkpoint
- * `checkpoint` (t_begin = checkpoint * checkpoint_every, t_end - t_begin <=
- * checkpoint_every); t_begin >= t_end leaves the env idle.  `first` marks the
- * first (last-in-time) reverse segment of an env's reverse pass.
+ * `checkpoint` (t_begin = checkpoint * checkpoint_every, t_end <= steps - 1;
+ * a reverse window spans one checkpoint segment); t_begin >= t_end leaves the
+ * env idle.  `first` marks the first (last-in-time) reverse segment of an
+ * env's reverse pass.
  * steps: [n_envs] episode steps of each env (the `steps` of cls_forward).
  * --------------------------------------------------------------------------- */
 /* Initial state x0 (v0 may be NULL: zero) [n_v][3] and targets tv [T][3],
@@ -221,7 +222,8 @@ int cls_serve_forward(cls_sim* sim, const int32_t* windows, const int32_t* steps
 /* One reverse segment per env window (recompute + adjoint + weight
  * gradients); an env's robot gradients restart at its `first` segment. */
 int cls_serve_backward(cls_sim* sim, const int32_t* windows, const int32_t* steps);
-/* Per-env losses [8][n_envs] (cls_loss's loss_env layout) with per-env steps. */
+/* Per-env losses [8][n_envs] (cls_loss's loss_env layout) with per-env steps;
+ * envs with steps <= 0 are skipped (zeros). */
 int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* loss_env);
 /* State at the end of the env's last forward window, [n_v][3] each. */
 int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v);

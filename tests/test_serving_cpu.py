@@ -38,7 +38,7 @@ class FakeBackend:
     def loss(self, steps):
         env = np.zeros((8, len(self.slot_types)))
         for i, r in enumerate(self.req):
-            if r is not None:
+            if r is not None and steps[i] > 0:
                 env[0, i] = r.seed + 0.5 * steps[i]
         return env
 
@@ -50,6 +50,9 @@ class FakeBackend:
 
     def sync(self):
         pass
+
+    def query(self):
+        return True
 
     def close(self):
         pass
@@ -64,11 +67,11 @@ def _robots():
     return {"quad": RobotType(quad), "lattice": RobotType(lat)}
 
 
-def _server(slots, K=50, T=2000, budget=None):
+def _server(slots, K=50, T=2000, budget=None, rounds=1):
     params = SimpleNamespace(checkpoint_every=K, max_steps=T, turn_period=500)
     ticks = itertools.count()
     clock = lambda: next(ticks) * 1e-3  # noqa: E731
-    return Server(_robots(), slots, params, hbm_budget=budget,
+    return Server(_robots(), slots, params, hbm_budget=budget, tick_segments=rounds,
                   backend_factory=lambda st, types, p: FakeBackend(st, types, p), clock=clock)
 
 
@@ -76,16 +79,17 @@ def _windows_of(backend, slot, kind):
     return [tuple(c[1][slot]) for c in backend.calls if c[0] == kind and c[1][slot][0] < c[1][slot][1]]
 
 
-@pytest.mark.parametrize("steps,K", [(1000, 50), (137, 50), (2, 50), (51, 50), (52, 50), (300, 7)])
-def test_windows_reproduce_forward_and_backward_segments(steps, K):
-    srv = _server({"quad": 1}, K=K)
+@pytest.mark.parametrize("steps,K,rounds", [(1000, 50, 1), (137, 50, 1), (2, 50, 1), (51, 50, 1),
+                                            (52, 50, 1), (300, 7, 1), (1000, 50, 4), (333, 7, 3)])
+def test_windows_reproduce_forward_and_backward_segments(steps, K, rounds):
+    srv = _server({"quad": 1}, K=K, rounds=rounds)
     srv.submit(Request(kind="quad", steps=steps, grad=True, seed=3))
     res = srv.drain()
     assert len(res) == 1 and res[0].grads == [("grad-of", 0)]
     be = srv.pools[0].backend
     t_last = steps - 1
     fwd = _windows_of(be, 0, "forward")
-    exp_f = [(t, min(t + K, t_last), t // K, 0) for t in range(0, t_last, K)]
+    exp_f = [(t, min(t + rounds * K, t_last), t // K, 0) for t in range(0, t_last, rounds * K)]
     assert fwd == exp_f
     n_seg = (t_last + K - 1) // K
     exp_b = [(s * K, min(s * K + K, t_last), s, int(s == n_seg - 1)) for s in range(n_seg - 1, -1, -1)]
@@ -163,3 +167,16 @@ def test_stats_report_percentiles():
     assert st["p50_ms"] == pytest.approx(np.percentile(lat, 50) * 1e3)
     assert st["p99_ms"] == pytest.approx(np.percentile(lat, 99) * 1e3)
     assert st["env_substeps_per_s"] > 0
+
+
+def test_open_loop_run_serves_every_request_with_independent_pools():
+    srv = _server({"quad": 2, "lattice": 2}, rounds=2)
+    rng = np.random.default_rng(4)
+    reqs = poisson_requests(rng, 2000.0, 0.02, ["quad", "lattice"], [0.5, 0.5], steps_lo=50, steps_hi=500)
+    res, st = srv.run(reqs)
+    assert sorted(r.rid for r in res) == list(range(len(reqs)))
+    assert st["requests"] == len(reqs) and all(r.latency >= 0 for r in res)
+    assert all(r.done >= r.admitted >= r.arrival - 1e-9 for r in res)
+    # the pools ticked independently: both launched
+    for p in srv.pools:
+        assert any(c[0] == "forward" for c in p.backend.calls)

@@ -38,9 +38,9 @@ def _requests():
             Request("lat120", 333, grad=True, seed=15), Request("lat300", 75, grad=False, seed=16)]
 
 
-def _serve(types, params, reqs, slots, stagger):
+def _serve(types, params, reqs, slots, stagger, rounds=1):
     from cls_b200.serving import Server
-    srv = Server(types, slots, params)
+    srv = Server(types, slots, params, tick_segments=rounds)
     try:
         ids = []
         for k, r in enumerate(reqs):
@@ -76,13 +76,16 @@ def _plain(types, params, req):
         b.close()
 
 
-@pytest.mark.parametrize("precision", [32, 64])
-def test_served_results_same_alone_in_mix_and_as_plain_batch(precision):
+@pytest.mark.parametrize("precision,rounds", [(32, 1), (64, 1), (32, 3)])
+def test_served_results_same_alone_in_mix_and_as_plain_batch(precision, rounds):
+    """rounds: checkpoint segments per tick (forward windows of rounds * K
+    substeps, rounds reverse segments per tick)."""
     import copy
     types = _types(precision)
     params = _params(400, precision)
     tl, tg = (1e-6, 1e-5) if precision == 32 else (1e-10, 1e-10)
-    mix = _serve(types, params, _requests(), {"quad": 2, "lat120": 2, "lat300": 2}, stagger=True)
+    mix = _serve(types, params, _requests(), {"quad": 2, "lat120": 2, "lat300": 2}, stagger=True,
+                 rounds=rounds)
     # the mix made the types' controllers; alone-runs reuse them
     for req, got in zip(_requests(), mix):
         alone = _serve(types, params, [copy.copy(req)], {req.kind: 1}, stagger=False)[0]
