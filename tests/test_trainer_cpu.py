@@ -1,0 +1,81 @@
+"""cfg3d loader (derived keys, robot build), scripted evaluation targets and
+the reference weight-pickle layout, on the CPU."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import load_golden
+
+
+def golden_config(g, **extra):
+    """A cfg3d-schema config with the golden run's settings."""
+    spr = g["springs"]
+    cfg = {
+        "train": {"name": "golden", "save_dir": "unused", "task": [str(s) for s in g["loss_names"]]},
+        "validation": {"velocity": [0.0], "height": [0.0]},
+        "robot": {"dim": 3, "robot_id": int(g["robot_id"]), "simulator": "mass_spring",
+                  "design_file": "unused", "control_length": 1, "name": "golden", "id": int(g["robot_id"]),
+                  "spring_stiffness": float(spr[:, 3].max()), "spring_actuation": float(spr[:, 4].max()),
+                  "solver": "mass_spring"},
+        "process": {"max_steps": int(g["T"]), "evaluate_max_steps": 60, "vis_interval": 256,
+                    "output_vis_interval": 8, "run_period": int(g["run_period"]),
+                    "jump_period": int(g["jump_period"]), "turn_period": int(g["turn_period"]),
+                    "max_speed": float(g["max_speed"]), "max_height": float(g["max_height"]), "dt": 0.01},
+        "simulator": {"mpm": {"n_grid": 32}, "ground_height": float(g["ground"]), "gravity": -9.8,
+                      "drag_damping": float(g["drag"]), "dash_damping": 0.2, "p_vol": 1, "E": 40, "mu": 40,
+                      "la": 40, "act_strength": 4, "bound": 3, "coeff": 5},
+        "nn": {"n_sin_waves": int(g["n_sin"]), "n_hidden": int(g["n_hidden"]), "duplicate_v": int(g["dup_v"]),
+               "duplicate_h": int(g["dup_h"]), "duplicate_c": int(g["dup_c"]), "batch_size": int(g["B"]),
+               "max_reset_step": 4, "optimizer": "adam", "learning_rate": 3e-4, "adam_b1": 0.9,
+               "adam_b2": 0.9},
+    }
+    cfg.update(extra)
+    return cfg
+
+
+@pytest.mark.parametrize("case", ["quad_ref", "x_all_losses"])
+def test_load_config_derives_the_reference_keys(case):
+    from cls_b200.trainer import load_config
+    g = load_golden(case)
+    cfg = load_config(golden_config(g), seed=5)
+    assert np.array_equal(np.asarray(cfg["robot"]["objects"]), g["objects"])
+    assert np.array_equal(np.asarray(cfg["robot"]["springs"]), g["springs"])
+    pr, sim, nn = cfg["process"], cfg["simulator"], cfg["nn"]
+    assert pr["dt"] == 0.004 and sim["gravity"] == -1.8 and sim["dashpot_damping"] == 0.1
+    assert pr["dt"] == float(g["dt"]) and sim["gravity"] == float(g["gravity"])
+    assert pr["spring_omega"] == pytest.approx(2 * math.pi / 0.004 / pr["run_period"])
+    assert pr["spring_omega"] == pytest.approx(float(g["spring_omega"]))
+    N = len(g["objects"])
+    assert nn["n_input_states"] == nn["n_sin_waves"] + 6 * N + 2 * nn["duplicate_v"] + nn["duplicate_h"] \
+        + nn["duplicate_c"]
+    assert nn["n_input_states"] == g["input_state"].shape[-1]
+    assert nn["adam_a"] == nn["learning_rate"] and cfg["train"]["random_seed"] == 5
+    ov = load_config(golden_config(g), overrides={"simulator": {"friction": 0.5}, "process": {"dt": 0.002}})
+    assert ov["simulator"]["friction"] == 0.5 and ov["process"]["dt"] == 0.002
+    with pytest.raises(NotImplementedError):
+        c = golden_config(g)
+        c["robot"]["simulator"] = "mpm"
+        load_config(c)
+
+
+def test_script_targets_phases():
+    from cls_b200.trainer import script_targets
+    tv, th = script_targets(6100, 6000, 0.08)
+    assert tuple(tv[0, [0, 2]]) == (-0.08, 0.0) and tuple(tv[1500, [0, 2]]) == (0.0, 0.08)
+    assert tuple(tv[2500, [0, 2]]) == (0.08, 0.0) and tuple(tv[3999, [0, 2]]) == (0.0, -0.08)
+    assert th[4500] == -1.0 and th[5999] == 1.0 and th[6000] == 0.0
+    assert np.all(tv[4000:, :] == 0) and np.all(th[:4000] == 0)
+
+
+def test_reference_pickle_layout_roundtrip():
+    from cls_b200.trainer import from_reference_list, to_reference_list
+    rng = np.random.default_rng(0)
+    layers = [(rng.normal(size=(64, 838)), rng.normal(size=64)), (rng.normal(size=(272, 64)), rng.normal(size=272))]
+    lst = to_reference_list(layers)
+    assert [a.shape for a in lst] == [(64, 838), (272, 64), (64,), (272,)]
+    back = from_reference_list(lst)
+    for (W, b), (W2, b2) in zip(layers, back):
+        assert np.array_equal(W, W2) and np.array_equal(b, b2)
+    with pytest.raises(ValueError):
+        to_reference_list(layers + layers)
