@@ -394,12 +394,16 @@ class SimImpl final : public SimBase {
                     " bytes needed, " + std::to_string(rev_cap) + " available)");
     CLS_CUDA(cudaFuncSetAttribute(fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_cap));
     CLS_CUDA(cudaFuncSetAttribute(rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_cap));
-    // GEMM tiles (per robot, per layer)
+    // GEMM tiles (per robot, per layer); a robot shared by many envs splits
+    // its K = envs x substeps rows over several CTAs (about 2048 rows each)
     for (int r = 0; r < nr; ++r) {
       if (count[r] == 0) continue;
+      const long long rows = (long long)K_ * count[r];
+      const int nsplit = (int)std::max<long long>(1, std::min<long long>(64, rows / 2048));
       for (int l = 0; l < L_; ++l)
         for (int i0 = 0; i0 < hr_[r].width[l + 1]; i0 += 64)
-          for (int j0 = 0; j0 < hr_[r].width[l]; j0 += 64) tiles_host_.push_back({r, l, i0, j0});
+          for (int j0 = 0; j0 < hr_[r].width[l]; j0 += 64)
+            for (int sp = 0; sp < nsplit; ++sp) tiles_host_.push_back({r, l, i0, j0, sp, nsplit});
     }
     // device allocations
     const int n_seg_max = (T_ - 1 + K_ - 1) / K_ + 1;

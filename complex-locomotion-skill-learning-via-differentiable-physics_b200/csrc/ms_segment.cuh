@@ -773,6 +773,7 @@ __global__ void ms_loss_kernel(MsArgs<R> a, double* out, const int* envs) {
 // computes a 64 x 64 tile; 256 threads, 4 x 4 outputs each.
 struct GemmTile {
   int robot, layer, i0, j0;
+  int split, nsplit;  // split-K: this tile sums rows [rows*split/nsplit, rows*(split+1)/nsplit)
 };
 
 template <typename R>
@@ -792,6 +793,8 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
     kseg = w.y > w.x ? w.y - w.x : 0;
   }
   const int rows = kseg * nb;
+  const int row_lo = (int)((long long)rows * tl.split / tl.nsplit);
+  const int row_hi = (int)((long long)rows * (tl.split + 1) / tl.nsplit);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   R acc[4][4];
 #pragma unroll
@@ -800,12 +803,12 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
     for (int q = 0; q < 4; ++q) acc[p][q] = 0;
   R bacc[4] = {0, 0, 0, 0};
   const R* biasp = (l > 0) ? a.bias + rb.b_off[l - 1] : nullptr;
-  for (int r0 = 0; r0 < rows; r0 += TK) {
+  for (int r0 = row_lo; r0 < row_hi; r0 += TK) {
     for (int q = threadIdx.x; q < TK * TM; q += 256) {
       const int rr = q / TM, ii = q % TM;
       const int rho = r0 + rr, i = tl.i0 + ii;
       R va = 0, vb = 0;
-      if (rho < rows) {
+      if (rho < row_hi) {
         const int k = rho / nb, b = rho - k * nb;
         if (i < M)
           va = a.rec_dz[a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * M + i];
@@ -841,6 +844,7 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
     __syncthreads();
   }
   R* W = gw + rb.w_off[l];
+  const bool split = tl.nsplit > 1;  // several CTAs add into this tile
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
     const int i = tl.i0 + ty * 4 + p;
@@ -848,9 +852,15 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int j = tl.j0 + tx * 4 + q;
-      if (j < Ncol) W[(size_t)i * pitch + j] += acc[p][q];
+      if (j < Ncol) {
+        if (split) atomicAdd(W + (size_t)i * pitch + j, acc[p][q]);
+        else W[(size_t)i * pitch + j] += acc[p][q];
+      }
     }
-    if (tl.j0 == 0 && tx == 0) gb[rb.b_off[l] + i] += bacc[p];
+    if (tl.j0 == 0 && tx == 0) {
+      if (split) atomicAdd(gb + rb.b_off[l] + i, bacc[p]);
+      else gb[rb.b_off[l] + i] += bacc[p];
+    }
   }
 }
 
