@@ -106,9 +106,11 @@ def load(build_if_missing=True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing and _build.needs_build():
-        _build.build()
-    path = _build.LIB
+    path = os.environ.get("CLS_B200_LIBRARY")  # an alternative build of the same library
+    if not path:
+        if build_if_missing and _build.needs_build():
+            _build.build()
+        path = _build.LIB
     if not os.path.exists(path):
         raise ClsError("CUDA library %s is missing; run build.py" % path)
     lib = ctypes.CDLL(path)

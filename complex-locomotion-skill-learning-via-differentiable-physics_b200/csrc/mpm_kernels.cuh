@@ -10,10 +10,8 @@
 //
 // Layout and kernels (B200):
 //  * particles are stored SoA (component planes of E*P values) in an internal
-//    order: Morton order of their initial cells, cut into chunks (one CTA
-//    each) of at most 256 particles that never leave one aligned group of
-//    4x4x2 cells (3D) or 8x8 cells (2D), so that a chunk's stencils cover a
-//    small box; inside a chunk the particles are interleaved so that the 32
+//    order: Morton order of their initial cells, cut into chunks of 256 (one
+//    CTA each); inside a chunk the particles are interleaved so that the 32
 //    lanes of a warp hold particles of 32 different cells;
 //  * the grid is dense per env but blocked: blocks of 4^3 (3D) or 8^2 (2D)
 //    nodes, 64 nodes of 4 values (16 B in FP32) per block, so a block is one
@@ -44,12 +42,24 @@ namespace mpm {
 
 enum Material : int { FIXED_COROTATED = 0, NEO_HOOKEAN = 1 };
 
+// occupancy targets of the particle kernels (CTAs per SM for the register
+// budget); compile-time tuning knobs
+#ifndef CLS_MPM_FWD_MIN_BLOCKS
+#define CLS_MPM_FWD_MIN_BLOCKS 3
+#endif
+#ifndef CLS_MPM_ADJ_MIN_BLOCKS
+#define CLS_MPM_ADJ_MIN_BLOCKS 2
+#endif
+
 constexpr int kChunk = 256;         // particles per CTA, one per thread
 constexpr int kWarps = kChunk / 32;
 constexpr int kTileDefault = 256;   // default warp tile capacity (nodes)
 constexpr int kMaxMuscles = 256;
-constexpr int kFwdPlanes = 4;       // P2G warp tile: momentum (3), mass
-constexpr int kAdjPlanes = 3;       // G2P^T warp tile: velocity adjoint (3)
+constexpr int kFwdPlanes = 4;       // staged grid velocity (3) / P2G scatter: momentum (3), mass
+constexpr int kAdjPlanes = 6;       // staged grid adjoint (4) / staged velocity (3) + velocity adjoint (3)
+// particle-kernel variants (template bitmask): stage the grid a warp gathers
+// from in shared memory, scatter through a warp tile
+constexpr int kStageGather = 1, kScatterTile = 2;
 
 template <int D>
 struct Blk {
@@ -356,9 +366,14 @@ __device__ __forceinline__ long long node_index(const Phys<R>& c, int e, const i
 
 template <typename R>
 __device__ __forceinline__ void red4(V4<R>* p, R x, R y, R z, R w);
+// 16-byte vector reduction without a return value (PTX red.global.add.v4.f32,
+// sm_90+): the issuing thread does not wait for the L2 round trip
 template <>
 __device__ __forceinline__ void red4<float>(V4<float>* p, float x, float y, float z, float w) {
-  atomicAdd(reinterpret_cast<float4*>(p), make_float4(x, y, z, w));
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
+               :
+               : "l"(p), "f"(x), "f"(y), "f"(z), "f"(w)
+               : "memory");
 }
 template <>
 __device__ __forceinline__ void red4<double>(V4<double>* p, double x, double y, double z, double w) {
@@ -457,6 +472,23 @@ __device__ __forceinline__ void warp_bbox(int* bbox, bool valid, const int base[
   }
 }
 
+// stage the grid records under a warp's box into planes [0, NP) of the warp
+// tile (component c of node li at tile[c * cap + li]); all lanes call it
+template <typename R, int D, int NP>
+__device__ __forceinline__ void warp_stage(const Phys<R>& c, const V4<R>* grid, const Box<D>& bx, R* tile,
+                                           int cap) {
+  for (int li = (int)(threadIdx.x & 31); li < bx.n; li += 32) {
+    int I[D];
+    bx.node(li, I);
+    const V4<R> g = ldg4(grid + node_index<R, D>(c, 0, I));
+    tile[li] = g.x;
+    if (NP > 1) tile[cap + li] = g.y;
+    if (NP > 2) tile[2 * cap + li] = g.z;
+    if (NP > 3) tile[3 * cap + li] = g.w;
+  }
+  __syncwarp();
+}
+
 // add v to a warp-tile entry: plain read-modify-write when the warp's lanes
 // have distinct base cells (distinct entries per stencil offset), else atomic
 template <typename R>
@@ -485,8 +517,8 @@ __device__ __forceinline__ R ld(const R* p) { return __ldg(p); }
 // (solver_mpm.py:83-124); either half alone at the ends of a rollout.  The
 // 3^D stencil loops are unrolled so that the weights and tile offsets of a
 // node are compile-time selections.
-template <typename R, int D, int MODE, bool TILE>
-__global__ void __launch_bounds__(kChunk, 3) mpm_fwd_kernel(FwdArgs<R> a) {
+template <typename R, int D, int MODE, int SM>
+__global__ void __launch_bounds__(kChunk, CLS_MPM_FWD_MIN_BLOCKS) mpm_fwd_kernel(FwdArgs<R> a) {
   using K = Kern<R, D>;
   extern __shared__ __align__(16) unsigned char mpm_smem[];
   const Phys<R>& c = a.c;
@@ -510,21 +542,34 @@ __global__ void __launch_bounds__(kChunk, 3) mpm_fwd_kernel(FwdArgs<R> a) {
     for (int i = 0; i < D; ++i) v[i] = 0;
 #pragma unroll
     for (int i = 0; i < D * D; ++i) Cm[i] = 0;
+    const V4<R>* gv = a.gv + (size_t)e * c.nblk * Blk<D>::NODES;
+    Box<D> gbx;
+    gbx.n = 0;
+    if (SM & kStageGather) {
+      gbx = warp_box<R, D>(c, valid, base);
+      if (gbx.n) warp_stage<R, D, D>(c, gv, gbx, wt_tile, cap);
+    }
     if (valid) {
-      const V4<R>* gv = a.gv + (size_t)e * c.nblk * Blk<D>::NODES;
+      const int li0 = gbx.index(base);
 #pragma unroll
       for (int nq = 0; nq < K::NN; ++nq) {
         int o[D];
         K::offs(nq, o);
         const R wt = K::wgt(w, o);
-        int I[D];
-#pragma unroll
-        for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
-        const V4<R> gg = ldg4(gv + node_index<R, D>(c, 0, I));
         R g[D];
-        g[0] = gg.x;
-        g[1] = gg.y;
-        if (D == 3) g[D - 1] = gg.z;
+        if (gbx.n) {
+          const int li = li0 + gbx.off(o);
+#pragma unroll
+          for (int i = 0; i < D; ++i) g[i] = wt_tile[i * cap + li];
+        } else {
+          int I[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
+          const V4<R> gg = ldg4(gv + node_index<R, D>(c, 0, I));
+          g[0] = gg.x;
+          g[1] = gg.y;
+          if (D == 3) g[D - 1] = gg.z;
+        }
         const R s4 = R(4) * wt * c.inv_dx;
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -588,9 +633,10 @@ __global__ void __launch_bounds__(kChunk, 3) mpm_fwd_kernel(FwdArgs<R> a) {
   warp_bbox<D>(a.bbox + (size_t)e * 2 * D, valid, base);
   Box<D> bx;
   bx.n = 0;
-  if (TILE) bx = warp_box<R, D>(c, valid, base);
+  if (SM & kScatterTile) bx = warp_box<R, D>(c, valid, base);
   const bool dup = bx.n ? warp_dup_base<D>(valid, base) : false;
   if (bx.n) {
+    __syncwarp();  // the staged gather is no longer read
     for (int li = lane; li < bx.n; li += 32) {
       wt_tile[li] = 0;
       wt_tile[cap + li] = 0;
@@ -759,8 +805,8 @@ __global__ void __launch_bounds__(256) mpm_grid_adj_kernel(Phys<R> c, V4<R>* gac
 // ------------------------------------------------------------------ reverse
 // P2G^T of step f + seed of step f (mode bit 1), then G2P^T of step h (mode
 // bit 2).  Adjoint of solver_mpm.py:83-124 and :146-165.
-template <typename R, int D, int MODE, bool TILE>
-__global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
+template <typename R, int D, int MODE, int SM>
+__global__ void __launch_bounds__(kChunk, CLS_MPM_ADJ_MIN_BLOCKS) mpm_adj_kernel(AdjArgs<R> a) {
   using K = Kern<R, D>;
   extern __shared__ __align__(16) unsigned char mpm_smem[];
   const Phys<R>& c = a.c;
@@ -815,25 +861,39 @@ __global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
       gfx[i] = 0;
       av[i] = 0;
     }
+    Box<D> gbx;
+    gbx.n = 0;
+    if (SM & kStageGather) {
+      gbx = warp_box<R, D>(c, valid, base);
+      if (gbx.n) warp_stage<R, D, 4>(c, a.ga + goff, gbx, wt_tile, cap);
+    }
     if (valid) {
+      const int li0 = gbx.index(base);
 #pragma unroll
       for (int nq = 0; nq < K::NN; ++nq) {
         int o[D];
         K::offs(nq, o);
         const R wt = K::wgt(w, o);
-        R dwt[D], dp[D], gg[D];
+        R dwt[D], dp[D], gg[D], ggm;
         K::dwgt(w, dw, o, dwt);
-        int I[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          dp[d] = (R)o[d] - fx[d];
-          I[d] = base[d] + o[d];
+        for (int d = 0; d < D; ++d) dp[d] = (R)o[d] - fx[d];
+        if (gbx.n) {
+          const int li = li0 + gbx.off(o);
+#pragma unroll
+          for (int i = 0; i < D; ++i) gg[i] = wt_tile[i * cap + li];
+          ggm = wt_tile[3 * cap + li];
+        } else {
+          int I[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
+          const V4<R> g4 = ldg4(a.ga + goff + node_index<R, D>(c, 0, I));
+          gg[0] = g4.x;
+          gg[1] = g4.y;
+          if (D == 3) gg[D - 1] = g4.z;
+          ggm = g4.w;
         }
-        const V4<R> g4 = ldg4(a.ga + goff + node_index<R, D>(c, 0, I));
-        gg[0] = g4.x;
-        gg[1] = g4.y;
-        if (D == 3) gg[D - 1] = g4.z;
-        R gw = g4.w * c.mass;
+        R gw = ggm * c.mass;
 #pragma unroll
         for (int i = 0; i < D; ++i) {
           R mom = c.mass * vp[i];
@@ -943,17 +1003,24 @@ __global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
 #pragma unroll
   for (int d = 0; d < D; ++d) xh[d] = ld(a.x_h + d * EP + q);
   K::weights(xh, c.inv_dx, c.n_grid, base, fx, w, dw);
+  // planes 0..2: the staged grid velocity; planes 3..5: the scatter tile
   Box<D> bx;
   bx.n = 0;
-  if (TILE) bx = warp_box<R, D>(c, valid, base);
-  const bool dup = bx.n ? warp_dup_base<D>(valid, base) : false;
+  if (SM & (kStageGather | kScatterTile)) bx = warp_box<R, D>(c, valid, base);
+  const bool stage = (SM & kStageGather) && bx.n;
+  const bool tile = (SM & kScatterTile) && bx.n;
+  const bool dup = tile ? warp_dup_base<D>(valid, base) : false;
   if (bx.n) {
-    for (int li = lane; li < bx.n; li += 32) {
-      wt_tile[li] = 0;
-      wt_tile[cap + li] = 0;
-      wt_tile[2 * cap + li] = 0;
+    __syncwarp();  // the P2G^T staging is no longer read
+    if (stage) warp_stage<R, D, D>(c, a.gv_h + goff, bx, wt_tile, cap);
+    if (tile) {
+      for (int li = lane; li < bx.n; li += 32) {
+        wt_tile[3 * cap + li] = 0;
+        wt_tile[4 * cap + li] = 0;
+        wt_tile[5 * cap + li] = 0;
+      }
+      __syncwarp();
     }
-    __syncwarp();
   }
   {
     R gvt[D], gfx[D];
@@ -979,10 +1046,16 @@ __global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
           I[d] = base[d] + o[d];
         }
         const long long gidx = node_index<R, D>(c, e, I);
-        const V4<R> g4 = ldg4(a.gv_h + gidx);
-        g[0] = g4.x;
-        g[1] = g4.y;
-        if (D == 3) g[D - 1] = g4.z;
+        const int li = li0 + bx.off(o);
+        if (stage) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) g[i] = wt_tile[i * cap + li];
+        } else {
+          const V4<R> g4 = ldg4(a.gv_h + gidx);
+          g[0] = g4.x;
+          g[1] = g4.y;
+          if (D == 3) g[D - 1] = g4.z;
+        }
         R gw = 0, sc[3] = {0, 0, 0};
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -1001,26 +1074,25 @@ __global__ void __launch_bounds__(kChunk, 2) mpm_adj_kernel(AdjArgs<R> a) {
         }
 #pragma unroll
         for (int d = 0; d < D; ++d) gfx[d] += gw * dwt[d];
-        if (bx.n) {
-          const int li = li0 + bx.off(o);
-          tile_add(wt_tile + li, sc[0], dup);
-          tile_add(wt_tile + cap + li, sc[1], dup);
-          if (D == 3) tile_add(wt_tile + 2 * cap + li, sc[2], dup);
+        if (tile) {
+          tile_add(wt_tile + 3 * cap + li, sc[0], dup);
+          tile_add(wt_tile + 4 * cap + li, sc[1], dup);
+          if (D == 3) tile_add(wt_tile + 5 * cap + li, sc[2], dup);
         } else {
           red4<R>(a.gacc + gidx, sc[0], sc[1], sc[2], R(0));
         }
       }
-      if (bx.n) __syncwarp();
+      if (tile) __syncwarp();
     }
     if (valid) {
 #pragma unroll
       for (int d = 0; d < D; ++d) a.ax_out[d * EP + q] = ax[d] + gfx[d] * c.inv_dx;
     }
   }
-  if (bx.n) {
+  if (tile) {
     __syncwarp();
     for (int li = lane; li < bx.n; li += 32) {
-      const R s0 = wt_tile[li], s1 = wt_tile[cap + li], s2 = D == 3 ? wt_tile[2 * cap + li] : R(0);
+      const R s0 = wt_tile[3 * cap + li], s1 = wt_tile[4 * cap + li], s2 = D == 3 ? wt_tile[5 * cap + li] : R(0);
       if (s0 == R(0) && s1 == R(0) && s2 == R(0)) continue;
       int I[D];
       bx.node(li, I);

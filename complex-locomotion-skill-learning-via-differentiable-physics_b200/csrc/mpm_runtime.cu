@@ -94,8 +94,11 @@ class MpmImpl final : public MpmBase {
     MPM_REQUIRE(M_ <= kMaxMuscles, "at most 256 muscle groups");
     MPM_REQUIRE(E_ <= 65535, "at most 65535 envs per handle");
     MPM_REQUIRE((long long)E_ * P_ < (1LL << 31) / (D * D), "too many particles");
+    // warp tiles (staged gathers and scatter tiles) only with tile_nodes > 0:
+    // both measured slower than L1 gathers and direct vector reductions
+    MPM_REQUIRE(p.tile_nodes <= 1024, "tile_nodes must be at most 1024");
+    sm_mode_ = p.tile_nodes > 0 ? (kStageGather | kScatterTile) : 0;
     tile_cap_ = p.tile_nodes > 0 ? p.tile_nodes : 0;
-    MPM_REQUIRE(tile_cap_ <= 1024, "tile_nodes must be at most 1024");
     nb_ = (n_grid_ + Blk<D>::SIDE - 1) / Blk<D>::SIDE;
     nblk_ = 1;
     for (int d = 0; d < D; ++d) nblk_ *= nb_;
@@ -155,14 +158,7 @@ class MpmImpl final : public MpmBase {
     // shared-memory opt-in for the tile
     fwd_smem_ = tile_cap_ > 0 ? (size_t)kWarps * kFwdPlanes * tile_cap_ * sizeof(R) : 0;
     adj_smem_ = tile_cap_ > 0 ? (size_t)kWarps * kAdjPlanes * tile_cap_ * sizeof(R) : 0;
-    if (tile_cap_ > 0) {
-      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
-      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
-      MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
-      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
-      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
-      MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
-    }
+    set_smem_attrs<kStageGather | kScatterTile>();
     // initial state: body positions in every env, v = C = 0, F = I
     std::vector<double> x0(EP * D), v0(EP * D, 0.0);
     for (int e = 0; e < E_; ++e)
@@ -206,17 +202,23 @@ class MpmImpl final : public MpmBase {
       return false;
     });
     const int per_cell = std::max(1, std::min(8, (int)std::lround((double)P_ / (double)cells.size())));
-    // chunks: aligned Morton groups of 32 cells (4x4x2) in 3D or 64 cells
-    // (8x8) in 2D, split at kChunk particles.  With the interleave below, the
-    // warps of a full group each hold one particle of every cell, so their
-    // lanes have distinct base cells and a compact stencil box.
+    // chunks of at most kChunk particles; with the interleave below, the
+    // warps of a full chunk each hold particles of distinct cells.  Default:
+    // plain runs in Morton order (every thread of a CTA busy); with
+    // CLS_MPM_CHUNK_GROUPS a chunk stays inside one aligned Morton group of 32
+    // (3D) or 64 (2D) cells (compact boxes for the shared-memory tiles, but
+    // about 60 % of the threads busy on a voxelised body)
+#ifndef CLS_MPM_CHUNK_GROUPS
+#define CLS_MPM_CHUNK_GROUPS 0
+#endif
+    const bool grouped = CLS_MPM_CHUNK_GROUPS != 0;
     const int group_shift = D == 3 ? 5 : 6;
     chunk_start_h_.clear();
     chunk_len_h_.clear();
     for (int i = 0; i < P_;) {
       const unsigned long long g = key[order[i]] >> group_shift;
       int j = i;
-      while (j < P_ && j - i < kChunk && (key[order[j]] >> group_shift) == g) ++j;
+      while (j < P_ && j - i < kChunk && (!grouped || (key[order[j]] >> group_shift) == g)) ++j;
       chunk_start_h_.push_back(i);
       chunk_len_h_.push_back(j - i);
       i = j;
@@ -273,28 +275,37 @@ class MpmImpl final : public MpmBase {
     MPM_CUDA(prof_.run(kind, stream, std::forward<F>(f)));
   }
 
-  template <bool TILE>
-  void fwd_t(int mode, const FwdArgs<R>& a) {
-    if (mode == 1) mpm_fwd_kernel<R, D, 1, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
-    else if (mode == 2) mpm_fwd_kernel<R, D, 2, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
-    else mpm_fwd_kernel<R, D, 3, TILE><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+  template <int SM>
+  void set_smem_attrs() {
+    MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 1, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+    MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 2, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+    MPM_CUDA(cudaFuncSetAttribute(mpm_fwd_kernel<R, D, 3, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem_));
+    MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 1, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
+    MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 2, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
+    MPM_CUDA(cudaFuncSetAttribute(mpm_adj_kernel<R, D, 3, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_));
   }
-  template <bool TILE>
+  template <int SM>
+  void fwd_t(int mode, const FwdArgs<R>& a) {
+    if (mode == 1) mpm_fwd_kernel<R, D, 1, SM><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+    else if (mode == 2) mpm_fwd_kernel<R, D, 2, SM><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+    else mpm_fwd_kernel<R, D, 3, SM><<<particle_grid(), kChunk, fwd_smem_, stream>>>(a);
+  }
+  template <int SM>
   void adj_t(int mode, const AdjArgs<R>& a) {
-    if (mode == 1) mpm_adj_kernel<R, D, 1, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
-    else if (mode == 2) mpm_adj_kernel<R, D, 2, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
-    else mpm_adj_kernel<R, D, 3, TILE><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+    if (mode == 1) mpm_adj_kernel<R, D, 1, SM><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+    else if (mode == 2) mpm_adj_kernel<R, D, 2, SM><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
+    else mpm_adj_kernel<R, D, 3, SM><<<particle_grid(), kChunk, adj_smem_, stream>>>(a);
   }
   void launch_fwd(int mode, const FwdArgs<R>& a, int kind) {
     timed(kind, [&] {
-      if (tile_cap_ > 0) fwd_t<true>(mode, a);
-      else fwd_t<false>(mode, a);
+      if (sm_mode_ == 0) fwd_t<0>(mode, a);
+      else fwd_t<kStageGather | kScatterTile>(mode, a);
     });
   }
   void launch_adj(int mode, const AdjArgs<R>& a) {
     timed(MK_PADJ, [&] {
-      if (tile_cap_ > 0) adj_t<true>(mode, a);
-      else adj_t<false>(mode, a);
+      if (sm_mode_ == 0) adj_t<0>(mode, a);
+      else adj_t<kStageGather | kScatterTile>(mode, a);
     });
   }
   dim3 grid_dims() const { return dim3((unsigned)std::max(1, 148 * 4 / E_), (unsigned)E_); }
@@ -593,7 +604,7 @@ class MpmImpl final : public MpmBase {
  private:
   cls_mpm_params p_;
   int E_ = 0, P_ = 0, M_ = 1, T_ = 0, K_ = 1, n_grid_ = 0, nb_ = 0, n_chunks_ = 0, slots_ = 2;
-  int tile_cap_ = 0, steps_ = 0;
+  int tile_cap_ = 0, sm_mode_ = 0, steps_ = 0;
   long long nblk_ = 0;
   size_t n_ckpt_ = 0, fwd_smem_ = 0, adj_smem_ = 0;
   double pw_sum_ = 1;

@@ -261,9 +261,10 @@ typedef struct {
   int32_t precision;            /* 32 or 64 */
   int32_t checkpoint_every;     /* K */
   double dt, gravity, p_vol, mu, la, act_strength, mass;
-  int32_t tile_nodes;           /* > 0: scatter through a warp-private shared-memory tile
-                                   of this many grid nodes (at most 1024); 0 (default)
-                                   or < 0: 16-byte vector atomics straight to the grid */
+  int32_t tile_nodes;           /* > 0: warp-private shared-memory tiles of this many grid
+                                   nodes (at most 1024) for the gathers and scatters; 0
+                                   (default) or < 0: gathers through L1 and 16-byte vector
+                                   reductions straight to the grid */
 } cls_mpm_params;
 
 /* Fills *p with the reference's 2D MPM constants (dt 1e-3, gravity -10,

@@ -67,11 +67,12 @@ def test_mpm2d_gradients_match_oracle(material, precision):
     b.close()
 
 
-@pytest.mark.parametrize("precision,tile", [(64, 0), (32, 0), (64, 256), (32, 256), (64, 48)])
+@pytest.mark.parametrize("precision,tile", [(64, 0), (32, 0), (64, 256), (32, 256), (64, 48), (64, -1),
+                                            (32, -1)])
 def test_mpm3d_neo_hookean_fibre_matches_oracle(precision, tile):
-    """tile 0: vector atomics straight to the grid (default); 256: warp-private
-    shared-memory scatter tiles; 48: a capacity that some warps' boxes exceed
-    (mixed tiled / global)."""
+    """tile 0 / -1: L1 gathers and vector reductions straight to the grid
+    (default); 256: warp-private tiles for gathers and scatters; 48: a capacity
+    that some warps' boxes exceed (mixed tiled / global)."""
     from cls_b200.mpm import MPMBatch
     rng = np.random.default_rng(1)
     pts, musc, fib = body3d(rng)
