@@ -21,7 +21,8 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
 ACT = {"sin": 0, "tanh": 1}
 LOSS_BITS = {"velocity": 1, "height": 2, "pose": 4, "actuation": 8,
              "rotation": 16, "crawl": 32}
-PROFILE_KINDS = ("forward", "recompute", "reverse", "wgrad", "loss", "adam", "other")
+PROFILE_KINDS = ("forward", "recompute", "reverse", "wgrad", "loss", "adam", "other", "ctrl_gemm",
+                 "ctrl_gemm_adj")
 LOSS_SLOTS = ("total", "velocity", "height", "pose", "rotation", "weight",
               "actuation", "crawl")
 
@@ -89,6 +90,8 @@ _SIGS = {
     "cls_profile_read": (c_int32, [ctypes.c_void_p, P_D, ctypes.POINTER(ctypes.c_int64), c_int32]),
     "cls_graph_capture": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
     "cls_graph_launch": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_set_controller_path": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_controller_batched": (c_int32, [ctypes.c_void_p, P_I]),
     "cls_serve_reset_env": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D, P_D, P_D, P_D]),
     "cls_serve_forward": (c_int32, [ctypes.c_void_p, P_I, P_I]),
     "cls_serve_backward": (c_int32, [ctypes.c_void_p, P_I, P_I]),

@@ -256,6 +256,20 @@ class MassSpringBatch:
     def graph_launch(self, it=0):
         self._c(self.lib.cls_graph_launch(self.h, it))
 
+    CONTROLLER_PATHS = {"auto": 0, "per_env": 1, "batched": 2}
+
+    def set_controller_path(self, path):
+        """'auto' (batched when every robot type has >= 256 envs), 'per_env'
+        (the controller inside the fused segment kernels) or 'batched' (one
+        tensor-core GEMM per layer over all envs of a type)."""
+        self._c(self.lib.cls_set_controller_path(self.h, self.CONTROLLER_PATHS[path]))
+
+    @property
+    def controller_batched(self):
+        on = np.zeros(1, dtype=np.int32)
+        self._c(self.lib.cls_controller_batched(self.h, on.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return bool(on[0])
+
     # ----------------------------------------------------------------- outputs
     def observables(self):
         T, E = self.T, self.n_envs

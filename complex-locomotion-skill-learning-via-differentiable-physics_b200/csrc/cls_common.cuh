@@ -18,7 +18,7 @@ enum LossSlot : int { LS_VEL = 0, LS_HEIGHT = 1, LS_POSE = 2, LS_ROT = 3, LS_WEI
                       LS_ACT = 5, LS_CRAWL = 6, LS_COUNT = 7 };
 
 // error bits written to the device status word
-enum ErrBit : int { ERR_NONFINITE = 1, ERR_SMEM = 2, ERR_CONFIG = 4 };
+enum ErrBit : int { ERR_NONFINITE = 1, ERR_SMEM = 2, ERR_CONFIG = 4, ERR_TIMEOUT = 8 };
 
 // 4-wide vector, 16 B (float) / 32 B (double) aligned, for vectorised state I/O
 template <typename R>

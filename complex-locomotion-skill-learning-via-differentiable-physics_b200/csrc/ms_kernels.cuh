@@ -37,6 +37,8 @@ struct RobotDesc {
   int pitch[kMaxLayers];             // row pitch (elements, multiple of 4) of layer l
   long long w_off[kMaxLayers];       // compact weight offsets (elements)
   int b_off[kMaxLayers];             // bias offsets
+  long long wt_off[kMaxLayers];      // transposed compact weights (batched controller)
+  int wt_pitch[kMaxLayers];          // row pitch of W_l^T: width[l + 1] padded to 4
   int n_env;                         // envs of this type: B in the loss normalisation
   int env_first;                     // envs are sorted by type
   int rot_idx[4];                    // heading vertices for robot 100
@@ -103,6 +105,9 @@ struct MsArgs {
   const V4<R>* init_obj;             // [v_total] initial_objects per env (pose loss)
   // adjoint carries between segments
   V4<R>* adj_x; V4<R>* adj_v; R* adj_h;
+  // batched controller: state between step launches, d input positions
+  // [v_total][3], transposed compact weights
+  V4<R>* live_x; V4<R>* live_v; R* din; const R* wt;
   // status
   int* status;
   // per-phase clock totals, only written by builds with CLS_PHASE_TIMERS

@@ -9,11 +9,12 @@
 #include <memory>
 #include <numeric>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cls_b200.h"
 #include "cls_profile.cuh"
-#include "ms_segment.cuh"
+#include "ms_dense.cuh"
 
 namespace cls {
 
@@ -67,7 +68,12 @@ struct HostRobot {
 };
 
 // launch categories for the per-kernel CUDA-event profile
-enum ProfKind : int { PK_FWD = 0, PK_RECOMP, PK_REV, PK_WGRAD, PK_LOSS, PK_ADAM, PK_OTHER, PK_COUNT };
+enum ProfKind : int {
+  PK_FWD = 0, PK_RECOMP, PK_REV, PK_WGRAD, PK_LOSS, PK_ADAM, PK_OTHER,
+  PK_CGEMM,      // batched controller: forward GEMMs (first pass and recompute)
+  PK_CGEMM_ADJ,  // batched controller: adjoint GEMMs
+  PK_COUNT
+};
 
 using Profiler = EventProfile<PK_COUNT>;
 
@@ -158,6 +164,9 @@ class SimBase {
   virtual void serve_backward(const int* win, const int* steps) = 0;
   virtual void serve_loss(const int* steps, double* env) = 0;
   virtual void serve_env_state(int ue, double* x, double* v) = 0;
+  // controller path: 0 auto, 1 per env (fused segment kernels), 2 batched
+  virtual void set_controller_path(int path) = 0;
+  virtual bool controller_batched() const = 0;
 };
 
 template <typename R>
@@ -167,6 +176,7 @@ class SimImpl final : public SimBase {
           const cls_sim_params& p)
       : hr_(robots), p_(p) {
     build(env_robot);
+    set_controller_path(0);
   }
   ~SimImpl() override {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
@@ -196,7 +206,7 @@ class SimImpl final : public SimBase {
     std::vector<int> spring_out;
     std::vector<int4> spr_i;
     std::vector<V4<R>> spr_f;
-    long long woff = 0, moff = 0;
+    long long woff = 0, moff = 0, wtoff = 0;
     int boff = 0;
     nmax_ = 0;
     int p0max = 4, dmax = 4, amax = 4, omax = 4;
@@ -219,9 +229,19 @@ class SimImpl final : public SimBase {
         woff += (long long)d.pitch[l] * h.width[l + 1];
         woff = (woff + 7) & ~7LL;  // keep every row block 32-byte aligned
         d.b_off[l] = boff;
-        boff += h.width[l + 1];
+        boff += round4(h.width[l + 1]);
         m_off_[r][l] = moff;
         moff += (long long)h.width[l + 1] * h.full_cols[l];
+        d.wt_pitch[l] = round4(h.width[l + 1]);
+        d.wt_off[l] = wtoff;
+        wtoff += (long long)d.wt_pitch[l] * h.width[l];
+        wtoff = (wtoff + 7) & ~7LL;
+        TransSeg tsg{};
+        tsg.w_off = d.w_off[l]; tsg.wt_off = d.wt_off[l];
+        tsg.rows = h.width[l + 1]; tsg.cols = h.width[l]; tsg.pitch = d.pitch[l]; tsg.wt_pitch = d.wt_pitch[l];
+        tsg.tile0 = n_ttiles_;
+        n_ttiles_ += ((tsg.rows + 31) / 32) * ((tsg.cols + 31) / 32);
+        tsegs_.push_back(tsg);
       }
       int rid[4] = {45, 46, 34, 36};
       for (int q = 0; q < 4; ++q) d.rot_idx[q] = rid[q];
@@ -323,11 +343,13 @@ class SimImpl final : public SimBase {
       d.robot = r;
       d.v_off = voff;
       voff += hr_[r].n_v;
+      // per-env rows padded to 16 bytes (the batched controller's GEMMs read
+      // them as float4)
       d.in_off = inoff;
-      inoff += hr_[r].n_c;
+      inoff += round4(hr_[r].n_c);
       for (int l = 0; l < L_; ++l) {
         d.z_off[l] = zoff[l];
-        zoff[l] += hr_[r].width[l + 1];
+        zoff[l] += round4(hr_[r].width[l + 1]);
       }
       if (first[r] < 0) first[r] = ie;
       count[r]++;
@@ -420,6 +442,7 @@ class SimImpl final : public SimBase {
     d_spr_f_.alloc(std::max<size_t>(1, spr_f.size()));
     d_w_.alloc(woff);
     d_gw_.alloc(woff);
+    wt_total_ = wtoff;
     d_bias_.alloc(boff);
     d_gb_.alloc(boff);
     d_bm_.alloc(boff);
@@ -630,6 +653,10 @@ class SimImpl final : public SimBase {
     a.adj_h = d_adjh_.p;
     a.status = d_status_.p;
     a.phase = d_phase_.p;
+    a.live_x = d_livex_.p;
+    a.live_v = d_livev_.p;
+    a.din = d_din_.p;
+    a.wt = d_wt_.p;
     return a;
   }
 
@@ -716,13 +743,158 @@ class SimImpl final : public SimBase {
     const int t_end = eval ? steps + 1 : steps - 1;
     MsArgs<R> a = args(steps);
     qslot_ = 0;
-    each_launch(per_env, a, qslot_, [&](const MsArgs<R>& b, int grid) {
-      timed(PK_FWD, [&] {
-        fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
+    if (dense_ && !per_env) {
+      dense_pass(a, 0, t_end, FWD_CKPT | FWD_OBS, 0, true, PK_FWD);
+    } else {
+      each_launch(per_env, a, qslot_, [&](const MsArgs<R>& b, int grid) {
+        timed(PK_FWD, [&] {
+          fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
+        });
       });
-    });
+    }
     CLS_CUDA(cudaGetLastError());
     fwd_done_ = true;
+  }
+
+
+  // ------------------------------------------------- batched controller
+  // Robot types with at least this many envs take the batched path when the
+  // controller path is automatic.
+  static constexpr int kAutoDenseEnvs = 256;
+
+  bool controller_batched() const override { return dense_; }
+
+  void set_controller_path(int path) override {
+    CLS_REQUIRE(path >= 0 && path <= 2, "controller path: 0 automatic, 1 per env, 2 batched");
+    CLS_REQUIRE(!capturing_, "the controller path cannot change during graph capture");
+    bool want = path == 2;
+    if (path == 0) {
+      want = true;
+      for (const RobotDesc& d : rd_host_)
+        if (d.n_env > 0 && d.n_env < kAutoDenseEnvs) want = false;
+    }
+    if (want && !d_wt_.p) enable_dense();
+    dense_ = want;
+    fwd_done_ = bwd_done_ = false;
+  }
+
+  void enable_dense() {
+    constexpr bool f32 = std::is_same<R, float>::value;
+    const int tm = f32 ? umma::TM : kSimtTile, tn = f32 ? kDenseTN : kSimtTile;
+    jobs_h_.clear();
+    for (int l = 0; l < L_; ++l) {
+      jf_off_[l] = (int)jobs_h_.size();
+      for (int r = 0; r < (int)hr_.size(); ++r) {
+        if (rd_host_[r].n_env == 0 || l >= hr_[r].n_layers) continue;
+        for (int m0 = 0; m0 < rd_host_[r].n_env; m0 += tm)
+          for (int n0 = 0; n0 < hr_[r].width[l + 1]; n0 += tn) jobs_h_.push_back({r, l, m0, n0});
+      }
+      jf_cnt_[l] = (int)jobs_h_.size() - jf_off_[l];
+    }
+    for (int l = 0; l < L_; ++l) {
+      jb_off_[l] = (int)jobs_h_.size();
+      for (int r = 0; r < (int)hr_.size(); ++r) {
+        if (rd_host_[r].n_env == 0 || l >= hr_[r].n_layers) continue;
+        const int ncol = l > 0 ? hr_[r].width[l] : 3 * hr_[r].n_v;
+        for (int m0 = 0; m0 < rd_host_[r].n_env; m0 += tm)
+          for (int n0 = 0; n0 < ncol; n0 += tn) jobs_h_.push_back({r, l, m0, n0});
+      }
+      jb_cnt_[l] = (int)jobs_h_.size() - jb_off_[l];
+    }
+    d_jobs_.alloc(std::max<size_t>(1, jobs_h_.size()));
+    CLS_CUDA(cudaMemcpy(d_jobs_.p, jobs_h_.data(), sizeof(DenseJob) * jobs_h_.size(), cudaMemcpyHostToDevice));
+    d_tsegs_.alloc(std::max<size_t>(1, tsegs_.size()));
+    CLS_CUDA(cudaMemcpy(d_tsegs_.p, tsegs_.data(), sizeof(TransSeg) * tsegs_.size(), cudaMemcpyHostToDevice));
+    d_livex_.alloc(V_);
+    d_livev_.alloc(V_);
+    d_din_.alloc((size_t)3 * V_);
+    d_wt_.alloc(std::max<long long>(1, wt_total_));
+    CLS_CUDA(cudaMemset(d_wt_.p, 0, sizeof(R) * d_wt_.n));
+    // step kernels: one CTA per env, no controller inside
+    int nv = 0;
+    for (const HostRobot& h : hr_) nv = std::max(nv, h.n_v);
+    dense_threads_ = nv <= 192 ? 128 : (nv <= 768 ? 256 : 512);
+    dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_dmax_, smem_p0max_);
+    drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, dense_threads_);
+    int dev = 0, optin = 0;
+    CLS_CUDA(cudaGetDevice(&dev));
+    CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{}, ra{};
+    CLS_CUDA(cudaFuncGetAttributes(&fa, dense_fwd_fn()));
+    CLS_CUDA(cudaFuncGetAttributes(&ra, dense_rev_fn()));
+    CLS_REQUIRE(dfwd_smem_ + fa.sharedSizeBytes <= (size_t)optin && drev_smem_ + ra.sharedSizeBytes <= (size_t)optin,
+                "robot too large for the batched controller's step kernels");
+    CLS_CUDA(cudaFuncSetAttribute(dense_fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)optin - fa.sharedSizeBytes)));
+    CLS_CUDA(cudaFuncSetAttribute(dense_rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)optin - ra.sharedSizeBytes)));
+    if constexpr (f32) {
+      const int sm = (int)umma::Shape<kDenseTN>::kSmemBytes;
+      CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+      CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    }
+    transpose_weights();
+    CLS_CUDA(cudaStreamSynchronize(stream));
+  }
+
+  using DFwdFn = void (*)(MsArgs<R>, int, int, int, int, int, int, int);
+  using DRevFn = void (*)(MsArgs<R>, int, int, int, int, int);
+  DFwdFn dense_fwd_fn() const {
+    return dense_threads_ <= 128 ? ms_step_fwd_kernel<R, 128>
+                                 : (dense_threads_ <= 256 ? ms_step_fwd_kernel<R, 256> : ms_step_fwd_kernel<R, 512>);
+  }
+  DRevFn dense_rev_fn() const {
+    return dense_threads_ <= 128 ? ms_step_rev_kernel<R, 128>
+                                 : (dense_threads_ <= 256 ? ms_step_rev_kernel<R, 256> : ms_step_rev_kernel<R, 512>);
+  }
+
+  // one layer's GEMM over all batched envs (record slot kslot)
+  void ctrl_gemm(const MsArgs<R>& a, bool bwd, int l, int kslot) {
+    const int cnt = bwd ? jb_cnt_[l] : jf_cnt_[l];
+    if (cnt == 0) return;
+    const DenseJob* jobs = d_jobs_.p + (bwd ? jb_off_[l] : jf_off_[l]);
+    timed(bwd ? PK_CGEMM_ADJ : PK_CGEMM, [&] {
+      if constexpr (std::is_same<R, float>::value) {
+        const size_t sm = umma::Shape<kDenseTN>::kSmemBytes;
+        if (bwd) ms_ctrl_gemm_tc_kernel<1><<<cnt, umma::kThreads, sm, stream>>>(a, jobs, kslot);
+        else ms_ctrl_gemm_tc_kernel<0><<<cnt, umma::kThreads, sm, stream>>>(a, jobs, kslot);
+      } else {
+        if (bwd) ms_ctrl_gemm_simt_kernel<R, 1><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
+        else ms_ctrl_gemm_simt_kernel<R, 0><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
+      }
+    });
+  }
+
+  // forward over [t_first, t_end): a step launch per substep boundary and the
+  // controller's GEMMs in between.  Record slots: t mod K for the first pass
+  // (the controller's records are only scratch there), t - t_first for a
+  // segment recompute.
+  void dense_pass(const MsArgs<R>& a, int t_first, int t_end, int mode, int src_slot, bool first_pass,
+                  int kind) {
+    for (int t = t_first; t <= t_end; ++t) {
+      const int k_prev = t > t_first ? (first_pass ? (t - 1) % K_ : t - 1 - t_first) : 0;
+      const int k_cur = t < t_end ? (first_pass ? t % K_ : t - t_first) : 0;
+      timed(kind, [&] {
+        dense_fwd_fn()<<<E_, dense_threads_, dfwd_smem_, stream>>>(a, t, t_first, t_end, mode, src_slot, k_prev,
+                                                                    k_cur);
+      });
+      if (t < t_end)
+        for (int l = 0; l < L_; ++l) ctrl_gemm(a, false, l, k_cur);
+    }
+  }
+
+  // reverse of segment [t0, t1): step launches from t1 - 1 down to t0 - 1,
+  // the controller's adjoint GEMMs after each launch that ends in dZ
+  void dense_reverse(const MsArgs<R>& a, int t0, int t1, bool last) {
+    for (int t = t1 - 1; t >= t0 - 1; --t) {
+      const int t_post = (t + 1 < t1) ? t + 1 : -1;
+      const int t_pre = (t >= t0) ? t : -1;
+      timed(PK_REV, [&] {
+        dense_rev_fn()<<<E_, dense_threads_, drev_smem_, stream>>>(a, t_post, t_pre, t0, t1, last ? 1 : 0);
+      });
+      if (t_pre >= 0)
+        for (int l = L_ - 1; l >= 0; --l) ctrl_gemm(a, true, l, t_pre - t0);
+    }
   }
 
   void loss_device() {
@@ -775,16 +947,21 @@ class SimImpl final : public SimBase {
     int qslot = qslot_;
     for (int s = n_seg - 1; s >= 0; --s) {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
-      each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
-        timed(PK_RECOMP, [&] {
-          fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+      if (dense_ && !per_env) {
+        dense_pass(a, t0, t1, FWD_RECORD, s, false, PK_RECOMP);
+        dense_reverse(a, t0, t1, s == n_seg - 1);
+      } else {
+        each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
+          timed(PK_RECOMP, [&] {
+            fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+          });
         });
-      });
-      each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
-        timed(PK_REV, [&] {
-          rev_fn()<<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
+        each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
+          timed(PK_REV, [&] {
+            rev_fn()<<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
+          });
         });
-      });
+      }
       if (!tiles_host_.empty())
         timed(PK_WGRAD, [&] {
           ms_wgrad_kernel<R><<<(int)tiles_host_.size(), 256, 0, stream>>>(a, d_tiles_.p, t1 - t0,
@@ -819,6 +996,17 @@ class SimImpl final : public SimBase {
           d_pack_segs_.p, (int)pack_segs_.size(), pack_total_, chunk, d_wm_.p, d_w_.p,
           p_.n_sin_waves, p_.duplicate_v, p_.duplicate_h, p_.duplicate_c);
     });
+    transpose_weights();
+  }
+
+  // W_l^T of every layer for the batched controller's adjoint GEMMs (only
+  // once the batched path has been enabled)
+  void transpose_weights() {
+    if (!d_wt_.p || n_ttiles_ == 0) return;
+    timed(PK_ADAM, [&] {
+      ms_transpose_weights_kernel<R><<<n_ttiles_, 256, 0, stream>>>(d_w_.p, d_wt_.p, d_tsegs_.p,
+                                                                    (int)tsegs_.size());
+    });
   }
 
   void adam(int iter, double* tns) override {
@@ -848,6 +1036,7 @@ class SimImpl final : public SimBase {
           d_wm_.p, m_off_[r][l], h.width[l + 1], h.full_cols[l], d_w_.p, d.w_off[l], d.pitch[l], l,
           h.n_v, h.pos_pad, p_.n_sin_waves, p_.duplicate_v, p_.duplicate_h, p_.duplicate_c);
     });
+    transpose_weights();
   }
 
   // ---------------------------------------------------------------- I/O
@@ -1257,6 +1446,10 @@ class SimImpl final : public SimBase {
         err = "non-finite state detected";
         return CLS_ERR_NONFINITE;
       }
+      if (st & ERR_TIMEOUT) {
+        err = "a tensor-core GEMM's wait for its MMAs timed out";
+        return CLS_ERR_CUDA;
+      }
     }
     return CLS_OK;
   }
@@ -1347,6 +1540,18 @@ class SimImpl final : public SimBase {
       d_recz_, d_recdz_, d_obsh_, d_obsu_, d_obsr_, d_actfull_, d_th_, d_tc_, d_adjh_;
   DevBuf<unsigned char> d_head_;
   DevBuf<unsigned long long> d_phase_;
+  // batched controller path
+  bool dense_ = false;
+  int dense_threads_ = 128, n_ttiles_ = 0;
+  size_t dfwd_smem_ = 0, drev_smem_ = 0;
+  long long wt_total_ = 0;
+  std::vector<TransSeg> tsegs_;
+  std::vector<DenseJob> jobs_h_;
+  int jf_off_[kMaxLayers] = {0}, jf_cnt_[kMaxLayers] = {0}, jb_off_[kMaxLayers] = {0}, jb_cnt_[kMaxLayers] = {0};
+  DevBuf<DenseJob> d_jobs_;
+  DevBuf<TransSeg> d_tsegs_;
+  DevBuf<V4<R>> d_livex_, d_livev_;
+  DevBuf<R> d_din_, d_wt_;
 
  public:
   void phase_read(unsigned long long* out) override {
@@ -1660,6 +1865,16 @@ int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam) {
 
 int cls_graph_launch(cls_sim* sim, int32_t iter) {
   return guarded(sim, [&](cls::SimBase& s) { s.graph_launch(iter); });
+}
+
+int cls_set_controller_path(cls_sim* sim, int32_t path) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_controller_path(path); });
+}
+
+int cls_controller_batched(const cls_sim* sim, int32_t* on) {
+  if (!sim || !sim->impl || !on) return CLS_ERR_INVALID;
+  *on = sim->impl->controller_batched() ? 1 : 0;
+  return CLS_OK;
 }
 
 }  // extern "C"

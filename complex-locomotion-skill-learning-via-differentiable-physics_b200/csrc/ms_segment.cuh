@@ -103,6 +103,161 @@ __device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
 }
 
 // ---------------------------------------------------------------- forward
+// The two halves of one substep around the controller, shared by the fused
+// segment kernel (MLP in between, per env) and the batched-controller step
+// kernels (MLP as tensor-core GEMMs over all envs of a robot type).
+
+// Substep t up to the controller input: checkpoint / records / trajectory of
+// x(t), compute_center / compute_height / compute_rotation
+// (solver_mass_spring.py:150-192) into the observables, nn_input
+// (taichi_env.py:149-183) into s.ain (compact column order, zero padded to
+// pitch 0).  The input row is recorded at slot kslot when `rec_in` (FWD_RECORD
+// or the batched path, which also records the zero padding).  hprev: running
+// height of t - 1, updated to t.
+template <typename R>
+__device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                        const FwdSmem<R>& s, int e, int t, int t_begin, int mode,
+                                        int kslot, bool rec_in, bool rec_pad, R& hprev) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int N = rb.n_v;
+  const R invN = R(1) / R(N);
+  if ((mode & FWD_CKPT) && t > t_begin && (t % a.K) == 0) {
+    V4<R>* cx = a.ckpt_x + (size_t)(t / a.K) * a.v_total + ed.v_off;
+    V4<R>* cv = a.ckpt_v + (size_t)(t / a.K) * a.v_total + ed.v_off;
+    bool bad = false;
+    for (int i = tid; i < N; i += nt) {
+      cx[i] = s.xs[i]; cv[i] = s.vs[i];
+      bad |= !(finite(s.xs[i].x) && finite(s.xs[i].y) && finite(s.xs[i].z));
+    }
+    if (bad) atomicOr(a.status, ERR_NONFINITE);
+  }
+  if (mode & FWD_RECORD) {
+    V4<R>* rx = a.rec_x + (size_t)kslot * a.v_total + ed.v_off;
+    V4<R>* rv = a.rec_v + (size_t)kslot * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) { rx[i] = s.xs[i]; rv[i] = s.vs[i]; }
+  }
+  if ((mode & FWD_OBS) && a.x_full) {
+    V4<R>* xf = a.x_full + (size_t)t * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
+  }
+  // -- compute_center (solver_mass_spring.py:150-156): sum of x / n
+  R c[3] = {0, 0, 0};
+  for (int i = tid; i < N; i += nt) {
+    c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
+  }
+  block_sum<R, 3>(c, s.red);
+  if (mode & FWD_OBS) {
+    // compute_height / upper height (solver_mass_spring.py:158-173)
+    R lo = R(10), hi = R(-10);
+    for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
+    int li = 0, hiidx = 0;
+    block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+    block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+    // compute_rotation (solver_mass_spring.py:175-192)
+    R rot;
+    if (rb.robot_id == 100) {
+      R d0 = 0, d2 = 0;
+      if (tid == 0) {
+        const V4<R> p = s.xs[rb.rot_idx[0]], q = s.xs[rb.rot_idx[1]];
+        const V4<R> u = s.xs[rb.rot_idx[2]], w = s.xs[rb.rot_idx[3]];
+        d0 = p.x + q.x - u.x - w.x;
+        d2 = p.z + q.z - u.z - w.z;
+      }
+      rot = datan2<R>(d2, d0);
+    } else {
+      unsigned char* hd = a.head + ed.v_off;
+      if (t == 0) {
+        for (int i = tid; i < N; i += nt) hd[i] = (s.xs[i].x < c[0]) ? 1 : 0;
+        __syncthreads();
+      }
+      R hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int i = tid; i < N; i += nt) {
+        const V4<R> p = s.xs[i];
+        if (hd[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
+        else { hs[4] += p.x; hs[5] += p.y; hs[6] += p.z; hs[7] += R(1); }
+      }
+      block_sum<R, 8>(hs, s.red);
+      const R d0 = -hs[0] * hs[7] + hs[4] * hs[3];
+      const R d2 = -hs[2] * hs[7] + hs[6] * hs[3];
+      rot = datan2<R>(d2, d0);
+    }
+    if (tid == 0) {
+      const size_t o = (size_t)t * a.n_envs + e;
+      V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
+      a.obs_center[o] = cc;
+      const R h = (t % a.jump_period == 0) ? lo : fmax(hprev, lo);
+      a.obs_height[o] = h;
+      a.obs_upper[o] = hi;
+      a.obs_rot[o] = rot;
+      s.red[0] = h;
+    }
+    __syncthreads();
+    hprev = s.red[0];
+    __syncthreads();
+  }
+  // -- nn_input (taichi_env.py:149-183) in the compact column order
+  {
+    const int p0 = rb.pos_pad, nc = rb.n_c, pitch0 = rb.pitch[0];
+    const int nrec = rec_pad ? pitch0 : nc;
+    R* rin = rec_in ? a.rec_in + (size_t)kslot * a.in_total + ed.in_off : nullptr;
+    for (int q = tid; q < pitch0; q += nt) {
+      R val = 0;
+      if (q < 3 * N) {
+        const int i = q / 3, d = q - 3 * (q / 3);
+        val = (comp(s.xs[i], d) - c[d]) / R(0.2);
+      } else if (q >= p0 && q < p0 + a.n_sin) {
+        val = a.sin_table[(size_t)t * a.n_sin + (q - p0)];
+      } else if (q >= p0 + a.n_sin && q < nc) {
+        val = goal_value<R>(a, q - p0 - a.n_sin, (size_t)t * a.n_envs + e);
+      }
+      s.ain[q] = val;
+      if (rin && q < nrec) rin[q] = val;
+    }
+  }
+  __syncthreads();
+}
+
+// Substep t after the controller: actuation record, apply_spring_force
+// (gather form) with the controller outputs `out`, advance_toi.
+template <typename R>
+__device__ __forceinline__ void fwd_post(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                         const FwdSmem<R>& s, int t, int mode, int kslot, const R* out) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int N = rb.n_v, L = rb.n_layers;
+  if ((mode & FWD_OBS) && a.act_full) {
+    R* af = a.act_full + (size_t)t * a.z_total[L - 1] + ed.z_off[L - 1];
+    for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
+  }
+  gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc,
+                     (mode & FWD_RECORD) ? a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off : nullptr);
+  __syncthreads();
+  for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
+  __syncthreads();
+}
+
+// State after the last processed step of a range ending at t_end.
+template <typename R>
+__device__ __forceinline__ void fwd_finish(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                           const FwdSmem<R>& s, int t_begin, int t_end, int mode) {
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
+  if ((mode & FWD_CKEND) && t_end % a.K == 0 && t_end > t_begin) {
+    V4<R>* cx = a.ckpt_x + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
+    V4<R>* cv = a.ckpt_v + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) { cx[i] = s.xs[i]; cv[i] = s.vs[i]; }
+  }
+  if (mode & FWD_OBS) {
+    for (int i = tid; i < N; i += nt) {
+      a.fin_x[ed.v_off + i] = s.xs[i];
+      a.fin_v[ed.v_off + i] = s.vs[i];
+    }
+    if (a.x_full && t_end < a.T) {
+      V4<R>* xf = a.x_full + (size_t)t_end * a.v_total + ed.v_off;
+      for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
+    }
+  }
+  __syncthreads();
+}
+
 // Advances every env from t_begin (state in checkpoint slot src_slot) through
 // t_end (exclusive), i.e. runs pre_advance/nn_input/forward/advance for each t.
 template <typename R, int MAXT>
@@ -125,7 +280,6 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
     }
     load_descs(a, e, rb, ed);
     const int N = rb.n_v, L = rb.n_layers;
-    const R invN = R(1) / R(N);
     {
       const V4<R>* cx = a.ckpt_x + (size_t)src_slot * a.v_total + ed.v_off;
       const V4<R>* cv = a.ckpt_v + (size_t)src_slot * a.v_total + ed.v_off;
@@ -136,152 +290,30 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
     __syncthreads();
     CLS_PHASE_START();
     for (int t = t_begin; t < t_end; ++t) {
-      // -- checkpoints, records, trajectory
-      if ((mode & FWD_CKPT) && t > t_begin && (t % a.K) == 0) {
-        V4<R>* cx = a.ckpt_x + (size_t)(t / a.K) * a.v_total + ed.v_off;
-        V4<R>* cv = a.ckpt_v + (size_t)(t / a.K) * a.v_total + ed.v_off;
-        bool bad = false;
-        for (int i = tid; i < N; i += nt) {
-          cx[i] = s.xs[i]; cv[i] = s.vs[i];
-          bad |= !(finite(s.xs[i].x) && finite(s.xs[i].y) && finite(s.xs[i].z));
-        }
-        if (bad) atomicOr(a.status, ERR_NONFINITE);
-      }
-      if (mode & FWD_RECORD) {
-        V4<R>* rx = a.rec_x + (size_t)(t - t_begin) * a.v_total + ed.v_off;
-        V4<R>* rv = a.rec_v + (size_t)(t - t_begin) * a.v_total + ed.v_off;
-        for (int i = tid; i < N; i += nt) { rx[i] = s.xs[i]; rv[i] = s.vs[i]; }
-      }
-      if ((mode & FWD_OBS) && a.x_full) {
-        V4<R>* xf = a.x_full + (size_t)t * a.v_total + ed.v_off;
-        for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
-      }
-      // -- compute_center (solver_mass_spring.py:150-156): sum of x / n
-      R c[3] = {0, 0, 0};
-      for (int i = tid; i < N; i += nt) {
-        c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
-      }
-      block_sum<R, 3>(c, s.red);
+      const int kk = t - t_begin;
+      fwd_pre<R>(a, rb, ed, s, e, t, t_begin, mode, kk, (mode & FWD_RECORD) != 0, false, hprev);
       CLS_PHASE(a, 10);
-      if (mode & FWD_OBS) {
-        // compute_height / upper height (solver_mass_spring.py:158-173)
-        R lo = R(10), hi = R(-10);
-        for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
-        int li = 0, hiidx = 0;
-        block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
-        block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
-        // compute_rotation (solver_mass_spring.py:175-192)
-        R rot;
-        if (rb.robot_id == 100) {
-          R d0 = 0, d2 = 0;
-          if (tid == 0) {
-            const V4<R> p = s.xs[rb.rot_idx[0]], q = s.xs[rb.rot_idx[1]];
-            const V4<R> u = s.xs[rb.rot_idx[2]], w = s.xs[rb.rot_idx[3]];
-            d0 = p.x + q.x - u.x - w.x;
-            d2 = p.z + q.z - u.z - w.z;
-          }
-          rot = datan2<R>(d2, d0);
-        } else {
-          unsigned char* hd = a.head + ed.v_off;
-          if (t == 0) {
-            for (int i = tid; i < N; i += nt) hd[i] = (s.xs[i].x < c[0]) ? 1 : 0;
-            __syncthreads();
-          }
-          R hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-          for (int i = tid; i < N; i += nt) {
-            const V4<R> p = s.xs[i];
-            if (hd[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
-            else { hs[4] += p.x; hs[5] += p.y; hs[6] += p.z; hs[7] += R(1); }
-          }
-          block_sum<R, 8>(hs, s.red);
-          const R d0 = -hs[0] * hs[7] + hs[4] * hs[3];
-          const R d2 = -hs[2] * hs[7] + hs[6] * hs[3];
-          rot = datan2<R>(d2, d0);
-        }
-        if (tid == 0) {
-          const size_t o = (size_t)t * a.n_envs + e;
-          V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
-          a.obs_center[o] = cc;
-          const R h = (t % a.jump_period == 0) ? lo : fmax(hprev, lo);
-          a.obs_height[o] = h;
-          a.obs_upper[o] = hi;
-          a.obs_rot[o] = rot;
-          s.red[0] = h;
-        }
-        __syncthreads();
-        hprev = s.red[0];
-        __syncthreads();
-      }
-      CLS_PHASE(a, 11);
-      // -- nn_input (taichi_env.py:149-183) in the compact column order
-      {
-        const int p0 = rb.pos_pad, nc = rb.n_c, pitch0 = rb.pitch[0];
-        for (int q = tid; q < pitch0; q += nt) {
-          R val = 0;
-          if (q < 3 * N) {
-            const int i = q / 3, d = q - 3 * (q / 3);
-            val = (comp(s.xs[i], d) - c[d]) / R(0.2);
-          } else if (q >= p0 && q < p0 + a.n_sin) {
-            val = a.sin_table[(size_t)t * a.n_sin + (q - p0)];
-          } else if (q >= p0 + a.n_sin && q < nc) {
-            val = goal_value<R>(a, q - p0 - a.n_sin, (size_t)t * a.n_envs + e);
-          }
-          s.ain[q] = val;
-          if ((mode & FWD_RECORD) && q < nc)
-            a.rec_in[(size_t)(t - t_begin) * a.in_total + ed.in_off + q] = val;
-        }
-      }
-      __syncthreads();
-      CLS_PHASE(a, 12);
       // -- MLP (nn.py:130-146): z = W a, a' = act(z + b)
       R* out = nullptr;
       for (int l = 0; l < L; ++l) {
         const R* in = (l == 0) ? s.ain : ((l & 1) ? s.buf0 : s.buf1);
         R* y = (l & 1) ? s.buf1 : s.buf0;
         const int nout = rb.width[l + 1];
-        R* zrec = (mode & FWD_RECORD)
-                      ? a.rec_z + a.z_base[l] + (size_t)(t - t_begin) * a.z_total[l] + ed.z_off[l]
-                      : nullptr;
+        R* zrec = (mode & FWD_RECORD) ? a.rec_z + a.z_base[l] + (size_t)kk * a.z_total[l] + ed.z_off[l]
+                                      : nullptr;
         dense_forward<R>(a.w + rb.w_off[l], rb.pitch[l], nout, a.bias + rb.b_off[l], in, y, zrec,
                          l == L - 1 ? a.act_out : a.act_hidden);
         // zero the padding up to the next layer's pitch
         const int padto = (l + 1 < L) ? rb.pitch[l + 1] : ((nout + 3) & ~3);
         for (int q = nout + tid; q < padto; q += nt) y[q] = 0;
         __syncthreads();
-        CLS_PHASE(a, 13 + (l < 2 ? l : 2));
         out = y;
       }
-      if ((mode & FWD_OBS) && a.act_full) {
-        R* af = a.act_full + (size_t)t * a.z_total[L - 1] + ed.z_off[L - 1];
-        for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
-      }
-      // -- apply_spring_force (gather form) then advance_toi
-      gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc,
-                         (mode & FWD_RECORD) ? a.rec_vinc + (size_t)(t - t_begin) * a.v_total + ed.v_off
-                                             : nullptr);
-      __syncthreads();
+      CLS_PHASE(a, 13);
+      fwd_post<R>(a, rb, ed, s, t, mode, kk, out);
       CLS_PHASE(a, 16);
-      for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
-      __syncthreads();
-      CLS_PHASE(a, 17);
     }
-    // state after the last processed step
-    if ((mode & FWD_CKEND) && t_end % a.K == 0 && t_end > t_begin) {
-      V4<R>* cx = a.ckpt_x + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
-      V4<R>* cv = a.ckpt_v + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
-      for (int i = tid; i < N; i += nt) { cx[i] = s.xs[i]; cv[i] = s.vs[i]; }
-    }
-    if (mode & FWD_OBS) {
-      for (int i = tid; i < N; i += nt) {
-        a.fin_x[ed.v_off + i] = s.xs[i];
-        a.fin_v[ed.v_off + i] = s.vs[i];
-      }
-      if (a.x_full && t_end < a.T) {
-        V4<R>* xf = a.x_full + (size_t)t_end * a.v_total + ed.v_off;
-        for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
-      }
-    }
-    __syncthreads();
+    fwd_finish<R>(a, rb, ed, s, t_begin, t_end, mode);
   }
 }
 
@@ -464,6 +496,205 @@ __device__ __forceinline__ void spring_adjoint_all(const MsArgs<R>& a, const Rob
 }
 
 // ---------------------------------------------------------------- reverse
+// The two halves of the adjoint of substep t around the controller, shared
+// by the fused segment kernel and the batched-controller step kernels.
+
+// Adjoint of substep t up to the controller outputs: x(t), v(t) from the
+// records (slot kslot), advance_toi adjoint, spring-force adjoint, then
+// dz of the output layer (recorded, and left in s.dz).
+template <typename R>
+__device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                        const RevSmem<R>& s, int e, int t, int kslot) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int N = rb.n_v, L = rb.n_layers;
+  const R Br = R(rb.n_env);
+  const R* bout = a.bias + rb.b_off[L - 1];
+  const int nout = rb.n_out;
+  const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kslot * a.z_total[L - 1] + ed.z_off[L - 1];
+  {
+    const V4<R>* rx = a.rec_x + (size_t)kslot * a.v_total + ed.v_off;
+    const V4<R>* rv = a.rec_v + (size_t)kslot * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; }
+    for (int o = tid; o < nout; o += nt) {
+      s.bufA[o] = act_f<R>(a.act_out, zl[o] + bout[o]);
+      s.bufB[o] = 0;
+    }
+  }
+  __syncthreads();
+  // v_inc[t] as recorded by the recompute pass (into gvinc as scratch)
+  {
+    const V4<R>* rvi = a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) s.gvinc[i] = rvi[i];
+  }
+  __syncthreads();
+  // adjoint of advance_toi(t + 1)
+  for (int i = tid; i < N; i += nt) {
+    const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
+    const V4<R> gx1 = s.gx[i], gv1 = s.gv[i];
+    R ov0 = a.drag_s * v.x + vi.x;
+    R ov1 = a.drag_s * v.y + a.dt * a.gravity + vi.y;
+    R ov2 = a.drag_s * v.z + vi.z;
+    R nv0 = ov0, nv1 = ov1, nv2 = ov2, toi = 0, f = 0;
+    const R nx1 = x.y + a.dt * ov1;
+    const bool hit = (nx1 < a.ground && ov1 < R(-1e-4));
+    if (hit) {
+      toi = -(x.y - a.ground) / ov1;
+      f = a.friction * (-ov1);
+      nv1 = 0;
+      nv0 = (ov0 < 0) ? fmin(R(0), ov0 + f) : fmax(R(0), ov0 - f);
+      nv2 = (ov2 < 0) ? fmin(R(0), ov2 + f) : fmax(R(0), ov2 - f);
+    }
+    R gox0 = gx1.x, gox1 = gx1.y, gox2 = gx1.z;
+    R gov0 = toi * gx1.x, gov1 = toi * gx1.y, gov2 = toi * gx1.z;
+    const R dtt = a.dt - toi;
+    const R gnv0 = dtt * gx1.x + gv1.x, gnv1 = dtt * gx1.y + gv1.y, gnv2 = dtt * gx1.z + gv1.z;
+    const R gtoi = gx1.x * ov0 - gx1.x * nv0 + gx1.y * ov1 - gx1.y * nv1 + gx1.z * ov2 - gx1.z * nv2;
+    if (hit) {
+      R gf = 0;
+      if (ov0 < 0) { if (!(R(0) < ov0 + f)) { gov0 += gnv0; gf += gnv0; } }
+      else { if (!(ov0 - f < R(0))) { gov0 += gnv0; gf -= gnv0; } }
+      if (ov2 < 0) { if (!(R(0) < ov2 + f)) { gov2 += gnv2; gf += gnv2; } }
+      else { if (!(ov2 - f < R(0))) { gov2 += gnv2; gf -= gnv2; } }
+      gov1 += -a.friction * gf;
+      gox1 += -gtoi / ov1;
+      gov1 += gtoi * (x.y - a.ground) / (ov1 * ov1);
+    } else {
+      gov0 += gnv0; gov1 += gnv1; gov2 += gnv2;
+    }
+    V4<R> gx0; gx0.x = gox0; gx0.y = gox1; gx0.z = gox2; gx0.w = 0;
+    V4<R> gv0; gv0.x = a.drag_s * gov0; gv0.y = a.drag_s * gov1; gv0.z = a.drag_s * gov2; gv0.w = 0;
+    V4<R> gvi; gvi.x = gov0; gvi.y = gov1; gvi.z = gov2; gvi.w = 0;
+    s.gx[i] = gx0;
+    s.gv[i] = gv0;
+    s.gvinc[i] = gvi;
+  }
+  __syncthreads();
+  // adjoint of apply_spring_force(t)
+  {
+    const size_t o = (size_t)t * a.n_envs + e;
+    const int st_e = steps_of(a, e);
+    const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
+    const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
+    const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
+    spring_adjoint_all<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
+                          act_seed);
+  }
+  __syncthreads();
+  // adjoint of the MLP's output activation
+  {
+    R* dzr = a.rec_dz + a.z_base[L - 1] + (size_t)kslot * a.z_total[L - 1] + ed.z_off[L - 1];
+    for (int q = tid; q < nout; q += nt) {
+      const R dz = s.bufB[q] * act_d<R>(a.act_out, zl[q] + bout[q]);
+      s.dz[q] = dz;
+      dzr[q] = dz;
+    }
+  }
+  __syncthreads();
+}
+
+// Adjoint of substep t from the controller input on: s.bufA holds d loss /
+// d (position columns of the input), s.xs holds x(t).  nn_input / center /
+// loss seeds, then the running-height adjoint (hcarry carries d h across t).
+template <typename R>
+__device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                         const RevSmem<R>& s, int e, int t, R& hcarry) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int N = rb.n_v;
+  const R Br = R(rb.n_env);
+  const R invN = R(1) / R(N);
+  int* redi = reinterpret_cast<int*>(s.red + kRedInt);
+  {
+    R gc[3] = {0, 0, 0};
+    for (int i = tid; i < N; i += nt) {
+      const R g0 = s.bufA[3 * i] / R(0.2), g1 = s.bufA[3 * i + 1] / R(0.2), g2 = s.bufA[3 * i + 2] / R(0.2);
+      R gxi[3] = {g0, g1, g2};
+      gc[0] -= g0; gc[1] -= g1; gc[2] -= g2;
+      if (a.x_full) seed_x_rotation_pose<R>(a, rb, ed, t, e, i, s.xs[i], Br, gxi, gc);
+      V4<R> g = s.gx[i];
+      g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
+      s.gx[i] = g;
+    }
+    block_sum<R, 3>(gc, s.red);
+    if (a.loss_mask & LOSS_VELOCITY) seed_center_velocity<R>(a, t, e, Br, gc);
+    for (int i = tid; i < N; i += nt) {
+      V4<R> g = s.gx[i];
+      g.x += gc[0] * invN; g.y += gc[1] * invN; g.z += gc[2] * invN;
+      s.gx[i] = g;
+    }
+  }
+  // adjoint of compute_height (running max of the lowest point) and upper height
+  if (a.loss_mask & (LOSS_HEIGHT | LOSS_CRAWL)) {
+    const R gh = seed_height<R>(a, t, e, Br) + hcarry;
+    const R gu = seed_upper<R>(a, t, e, Br);
+    hcarry = 0;
+    if (gh != R(0)) {
+      R lo = R(10); int li = -1;
+      for (int i = tid; i < N; i += nt) {
+        const R y = s.xs[i].y;
+        if (!(lo < y)) { lo = y; li = i; }
+      }
+      block_argext<R>(lo, li, true, s.red, redi);
+      R gmin = gh;
+      if (t % a.jump_period != 0) {
+        const R prev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
+        if (lo < prev) { hcarry = gh; gmin = 0; }
+      }
+      if (tid == 0 && li >= 0 && gmin != R(0)) s.gx[li].y += gmin;
+    }
+    if (gu != R(0)) {
+      R hi = R(-10); int hix = -1;
+      for (int i = tid; i < N; i += nt) {
+        const R y = s.xs[i].y;
+        if (!(y < hi)) { hi = y; hix = i; }
+      }
+      block_argext<R>(hi, hix, false, s.red, redi);
+      if (tid == 0 && hix >= 0) s.gx[hix].y += gu;
+    }
+  }
+  __syncthreads();
+}
+
+// Adjoint carry at the start of a reverse range: for the last segment the
+// direct loss terms at x[t_end] (x[steps-1] is written by the last advance but
+// never passed through pre_advance), else the carry left by the later segment.
+template <typename R>
+__device__ __forceinline__ void rev_load_carry(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                               const RevSmem<R>& s, int e, int t_end, bool last_seg,
+                                               R& hcarry) {
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
+  const R Br = R(rb.n_env);
+  hcarry = 0;
+  if (last_seg) {
+    for (int i = tid; i < N; i += nt) {
+      R gxi[3] = {0, 0, 0}, gcd[3] = {0, 0, 0};
+      if (a.x_full) {
+        const V4<R> xi = a.x_full[(size_t)t_end * a.v_total + ed.v_off + i];
+        seed_x_rotation_pose<R>(a, rb, ed, t_end, e, i, xi, Br, gxi, gcd);
+      }
+      V4<R> g; g.x = gxi[0]; g.y = gxi[1]; g.z = gxi[2]; g.w = 0;
+      V4<R> z; z.x = z.y = z.z = z.w = 0;
+      s.gx[i] = g;
+      s.gv[i] = z;
+    }
+  } else {
+    for (int i = tid; i < N; i += nt) { s.gx[i] = a.adj_x[ed.v_off + i]; s.gv[i] = a.adj_v[ed.v_off + i]; }
+    hcarry = a.adj_h[e];
+  }
+  __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ void rev_store_carry(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                                const RevSmem<R>& s, int e, R hcarry) {
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
+  for (int i = tid; i < N; i += nt) {
+    a.adj_x[ed.v_off + i] = s.gx[i];
+    a.adj_v[ed.v_off + i] = s.gv[i];
+  }
+  if (tid == 0) a.adj_h[e] = hcarry;
+  __syncthreads();
+}
+
 template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
 ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
@@ -473,7 +704,6 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
   __shared__ int s_item;
   RevSmem<R> s = carve_rev<R>(smem_raw, a);
   const int tid = threadIdx.x, nt = blockDim.x;
-  int* redi = reinterpret_cast<int*>(s.red + kRedInt);
   for (;;) {
     const int item = next_item(a, &s_item);
     if (item >= a.n_items) break;
@@ -485,122 +715,14 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
     }
     load_descs(a, e, rb, ed);
     const int N = rb.n_v, L = rb.n_layers;
-    const R Br = R(rb.n_env);
-    const R invN = R(1) / R(N);
     R hcarry = 0;
-    if (last_seg) {
-      // x[steps-1] is written by the last advance but never passed through
-      // pre_advance, so only the direct loss terms at t = steps-1 reach it
-      const int tl = t_end;
-      for (int i = tid; i < N; i += nt) {
-        R gxi[3] = {0, 0, 0}, gcd[3] = {0, 0, 0};
-        if (a.x_full) {
-          const V4<R> xi = a.x_full[(size_t)tl * a.v_total + ed.v_off + i];
-          seed_x_rotation_pose<R>(a, rb, ed, tl, e, i, xi, Br, gxi, gcd);
-        }
-        V4<R> g; g.x = gxi[0]; g.y = gxi[1]; g.z = gxi[2]; g.w = 0;
-        V4<R> z; z.x = z.y = z.z = z.w = 0;
-        s.gx[i] = g;
-        s.gv[i] = z;
-      }
-    } else {
-      for (int i = tid; i < N; i += nt) { s.gx[i] = a.adj_x[ed.v_off + i]; s.gv[i] = a.adj_v[ed.v_off + i]; }
-      hcarry = a.adj_h[e];
-    }
-    __syncthreads();
-    const R* wout = a.w + rb.w_off[L - 1];
-    const R* bout = a.bias + rb.b_off[L - 1];
-    const int nout = rb.n_out;
-    (void)wout;
+    rev_load_carry<R>(a, rb, ed, s, e, t_end, last_seg != 0, hcarry);
     CLS_PHASE_START();
     for (int t = t_end - 1; t >= t_begin; --t) {
       const int kk = t - t_begin;
-      {
-        const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
-        const V4<R>* rv = a.rec_v + (size_t)kk * a.v_total + ed.v_off;
-        for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; }
-        const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
-        for (int o = tid; o < nout; o += nt) {
-          s.bufA[o] = act_f<R>(a.act_out, zl[o] + bout[o]);
-          s.bufB[o] = 0;
-        }
-      }
-      __syncthreads();
-      CLS_PHASE(a, 0);
-      // v_inc[t] as recorded by the recompute pass (into gvinc as scratch)
-      {
-        const V4<R>* rvi = a.rec_vinc + (size_t)kk * a.v_total + ed.v_off;
-        for (int i = tid; i < N; i += nt) s.gvinc[i] = rvi[i];
-      }
-      __syncthreads();
-      CLS_PHASE(a, 1);
-      // adjoint of advance_toi(t + 1)
-      for (int i = tid; i < N; i += nt) {
-        const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
-        const V4<R> gx1 = s.gx[i], gv1 = s.gv[i];
-        R ov0 = a.drag_s * v.x + vi.x;
-        R ov1 = a.drag_s * v.y + a.dt * a.gravity + vi.y;
-        R ov2 = a.drag_s * v.z + vi.z;
-        R nv0 = ov0, nv1 = ov1, nv2 = ov2, toi = 0, f = 0;
-        const R nx1 = x.y + a.dt * ov1;
-        const bool hit = (nx1 < a.ground && ov1 < R(-1e-4));
-        if (hit) {
-          toi = -(x.y - a.ground) / ov1;
-          f = a.friction * (-ov1);
-          nv1 = 0;
-          nv0 = (ov0 < 0) ? fmin(R(0), ov0 + f) : fmax(R(0), ov0 - f);
-          nv2 = (ov2 < 0) ? fmin(R(0), ov2 + f) : fmax(R(0), ov2 - f);
-        }
-        R gox0 = gx1.x, gox1 = gx1.y, gox2 = gx1.z;
-        R gov0 = toi * gx1.x, gov1 = toi * gx1.y, gov2 = toi * gx1.z;
-        const R dtt = a.dt - toi;
-        const R gnv0 = dtt * gx1.x + gv1.x, gnv1 = dtt * gx1.y + gv1.y, gnv2 = dtt * gx1.z + gv1.z;
-        const R gtoi = gx1.x * ov0 - gx1.x * nv0 + gx1.y * ov1 - gx1.y * nv1 + gx1.z * ov2 - gx1.z * nv2;
-        if (hit) {
-          R gf = 0;
-          if (ov0 < 0) { if (!(R(0) < ov0 + f)) { gov0 += gnv0; gf += gnv0; } }
-          else { if (!(ov0 - f < R(0))) { gov0 += gnv0; gf -= gnv0; } }
-          if (ov2 < 0) { if (!(R(0) < ov2 + f)) { gov2 += gnv2; gf += gnv2; } }
-          else { if (!(ov2 - f < R(0))) { gov2 += gnv2; gf -= gnv2; } }
-          gov1 += -a.friction * gf;
-          gox1 += -gtoi / ov1;
-          gov1 += gtoi * (x.y - a.ground) / (ov1 * ov1);
-        } else {
-          gov0 += gnv0; gov1 += gnv1; gov2 += gnv2;
-        }
-        V4<R> gx0; gx0.x = gox0; gx0.y = gox1; gx0.z = gox2; gx0.w = 0;
-        V4<R> gv0; gv0.x = a.drag_s * gov0; gv0.y = a.drag_s * gov1; gv0.z = a.drag_s * gov2; gv0.w = 0;
-        V4<R> gvi; gvi.x = gov0; gvi.y = gov1; gvi.z = gov2; gvi.w = 0;
-        s.gx[i] = gx0;
-        s.gv[i] = gv0;
-        s.gvinc[i] = gvi;
-      }
-      __syncthreads();
-      CLS_PHASE(a, 2);
-      // adjoint of apply_spring_force(t)
-      {
-        const size_t o = (size_t)t * a.n_envs + e;
-        const int st_e = steps_of(a, e);
-        const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
-        const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
-        const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
-        spring_adjoint_all<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
-                              act_seed);
-      }
-      __syncthreads();
+      rev_pre<R>(a, rb, ed, s, e, t, kk);
       CLS_PHASE(a, 3);
-      // adjoint of the MLP: output layer first
-      {
-        const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
-        R* dzr = a.rec_dz + a.z_base[L - 1] + (size_t)kk * a.z_total[L - 1] + ed.z_off[L - 1];
-        for (int q = tid; q < nout; q += nt) {
-          const R dz = s.bufB[q] * act_d<R>(a.act_out, zl[q] + bout[q]);
-          s.dz[q] = dz;
-          dzr[q] = dz;
-        }
-      }
-      __syncthreads();
-      CLS_PHASE(a, 4);
+      // hidden layers of the MLP adjoint
       for (int l = L - 1; l >= 1; --l) {
         const int nin = rb.width[l];
         dense_transposed<R>(a.w + rb.w_off[l], rb.pitch[l], rb.width[l + 1], nin, s.dz, s.part,
@@ -615,70 +737,14 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
         }
         __syncthreads();
       }
-      CLS_PHASE(a, 5);
       // first layer: only the position columns carry state dependence
       dense_transposed<R>(a.w + rb.w_off[0], rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
                           reinterpret_cast<V4<R>*>(s.bufA));
       CLS_PHASE(a, 6);
-      // adjoint of nn_input + compute_center + loss seeds at t
-      {
-        R gc[3] = {0, 0, 0};
-        for (int i = tid; i < N; i += nt) {
-          const R g0 = s.bufA[3 * i] / R(0.2), g1 = s.bufA[3 * i + 1] / R(0.2), g2 = s.bufA[3 * i + 2] / R(0.2);
-          R gxi[3] = {g0, g1, g2};
-          gc[0] -= g0; gc[1] -= g1; gc[2] -= g2;
-          if (a.x_full) seed_x_rotation_pose<R>(a, rb, ed, t, e, i, s.xs[i], Br, gxi, gc);
-          V4<R> g = s.gx[i];
-          g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
-          s.gx[i] = g;
-        }
-        block_sum<R, 3>(gc, s.red);
-        if (a.loss_mask & LOSS_VELOCITY) seed_center_velocity<R>(a, t, e, Br, gc);
-        for (int i = tid; i < N; i += nt) {
-          V4<R> g = s.gx[i];
-          g.x += gc[0] * invN; g.y += gc[1] * invN; g.z += gc[2] * invN;
-          s.gx[i] = g;
-        }
-      }
-      CLS_PHASE(a, 7);
-      // adjoint of compute_height (running max of the lowest point) and upper height
-      if (a.loss_mask & (LOSS_HEIGHT | LOSS_CRAWL)) {
-        const R gh = seed_height<R>(a, t, e, Br) + hcarry;
-        const R gu = seed_upper<R>(a, t, e, Br);
-        hcarry = 0;
-        if (gh != R(0)) {
-          R lo = R(10); int li = -1;
-          for (int i = tid; i < N; i += nt) {
-            const R y = s.xs[i].y;
-            if (!(lo < y)) { lo = y; li = i; }
-          }
-          block_argext<R>(lo, li, true, s.red, redi);
-          R gmin = gh;
-          if (t % a.jump_period != 0) {
-            const R prev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
-            if (lo < prev) { hcarry = gh; gmin = 0; }
-          }
-          if (tid == 0 && li >= 0 && gmin != R(0)) s.gx[li].y += gmin;
-        }
-        if (gu != R(0)) {
-          R hi = R(-10); int hix = -1;
-          for (int i = tid; i < N; i += nt) {
-            const R y = s.xs[i].y;
-            if (!(y < hi)) { hi = y; hix = i; }
-          }
-          block_argext<R>(hi, hix, false, s.red, redi);
-          if (tid == 0 && hix >= 0) s.gx[hix].y += gu;
-        }
-      }
-      __syncthreads();
+      rev_post<R>(a, rb, ed, s, e, t, hcarry);
       CLS_PHASE(a, 8);
     }
-    for (int i = tid; i < N; i += nt) {
-      a.adj_x[ed.v_off + i] = s.gx[i];
-      a.adj_v[ed.v_off + i] = s.gv[i];
-    }
-    if (tid == 0) a.adj_h[e] = hcarry;
-    __syncthreads();
+    rev_store_carry<R>(a, rb, ed, s, e, hcarry);
   }
 }
 
@@ -786,6 +852,8 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
   const RobotDesc& rb = a.robots[tl.robot];
   const int l = tl.layer;
   const int M = rb.width[l + 1], Ncol = rb.width[l], pitch = rb.pitch[l];
+  // per-env row strides of the records (rows padded to multiples of 4)
+  const int zp = (M + 3) & ~3, ap = (Ncol + 3) & ~3;
   const int nb = rb.n_env;
   const EnvDesc& e0 = a.envs[rb.env_first];
   if (a.win) {  // served batches: one env per robot, its own window
@@ -811,14 +879,14 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
       if (rho < row_hi) {
         const int k = rho / nb, b = rho - k * nb;
         if (i < M)
-          va = a.rec_dz[a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * M + i];
+          va = a.rec_dz[a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * zp + i];
         const int j = tl.j0 + ii;
         if (j < Ncol) {
           if (l == 0) {
-            vb = a.rec_in[(size_t)k * a.in_total + e0.in_off + (size_t)b * rb.n_c + j];
+            vb = a.rec_in[(size_t)k * a.in_total + e0.in_off + (size_t)b * rb.pitch[0] + j];
           } else {
             const R z = a.rec_z[a.z_base[l - 1] + (size_t)k * a.z_total[l - 1] + e0.z_off[l - 1] +
-                                (size_t)b * Ncol + j];
+                                (size_t)b * ap + j];
             vb = act_f<R>(a.act_hidden, z + biasp[j]);
           }
         }

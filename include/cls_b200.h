@@ -186,9 +186,11 @@ int cls_initialize_train(cls_sim* sim, int32_t iter, int32_t steps, uint64_t see
 /* Per-kernel profile: when enabled, every launch is bracketed by CUDA events
  * on the handle's stream.  cls_profile_read returns, per launch category
  * (0 first-pass forward, 1 segment recompute, 2 reverse, 3 weight-gradient
- * products, 4 loss, 5 optimiser/packing, 6 other), the summed device time in
- * ms and the number of launches; launches are counted even when disabled. */
-#define CLS_PROFILE_KINDS 7
+ * products, 4 loss, 5 optimiser/packing, 6 other, 7 batched controller GEMMs
+ * of the forward passes, 8 batched controller GEMMs of the reverse pass), the
+ * summed device time in ms and the number of launches; launches are counted
+ * even when disabled. */
+#define CLS_PROFILE_KINDS 9
 int cls_profile_enable(cls_sim* sim, int32_t on);
 int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset);
 
@@ -196,6 +198,23 @@ int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset)
  * Adam step) into a CUDA graph and replays it; cls_graph_launch replays. */
 int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam);
 int cls_graph_launch(cls_sim* sim, int32_t iter);
+
+/* Controller path.  The reference evaluates Model.forward per env and
+ * substep (multitask/nn.py:130-146, called from diffphy_trainer.py:246-256);
+ * here the fused segment kernels run it per env (CLS_CONTROLLER_PER_ENV),
+ * while the batched path splits each substep at the controller and runs each
+ * layer as one GEMM over all envs of a robot type (FP32: tensor cores,
+ * tcgen05 with a 3xTF32 split, FP32 accumulate; FP64: SIMT), with the same
+ * results within rounding.  CLS_CONTROLLER_AUTO (the default at creation)
+ * takes the batched path when every robot type has at least 256 envs.  No
+ * reference counterpart: a layout choice of this implementation.  Serving
+ * windows (cls_serve_*) and per-env launches always use the fused kernels. */
+#define CLS_CONTROLLER_AUTO 0
+#define CLS_CONTROLLER_PER_ENV 1
+#define CLS_CONTROLLER_BATCHED 2
+int cls_set_controller_path(cls_sim* sim, int32_t path);
+/* *on = 1 when the batched path is active. */
+int cls_controller_batched(const cls_sim* sim, int32_t* on);
 
 /* ---------------------------------------------------------------------------
  * Serving: one handle as a pool of env slots at different times of their own

@@ -1,0 +1,172 @@
+"""Batched controller path (per-substep step kernels + one GEMM per layer over
+all envs of a robot type; FP32 on the tensor cores with a 3xTF32 split, FP64
+as SIMT tiles) against the reference-generated golden vectors, the FP64
+oracle and the fused per-env path.
+
+Tolerances are the mass-spring suite's: FP64 1e-9 on trajectories and
+losses, 1e-8 on gradients; FP32 rel 1e-5 on trajectories over these
+<= 48-substep rollouts, rel 1e-4 on losses and gradients.
+"""
+import numpy as np
+import pytest
+
+from helpers import (TRAIN_CASES, batch_from_golden, load_golden, max_rel,
+                     oracle_from_golden, rel_err)
+
+pytestmark = pytest.mark.gpu
+
+TOL = {64: dict(traj=1e-9, loss=1e-9, grad=1e-8), 32: dict(traj=1e-5, loss=1e-4, grad=1e-4)}
+
+
+def _batched(g, precision, K, **over):
+    b = batch_from_golden(g, precision=precision, K=K, **over)
+    b.set_controller_path("batched")
+    assert b.controller_batched
+    return b
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("case", TRAIN_CASES)
+def test_batched_forward_matches_golden(case, precision):
+    g = load_golden(case)
+    steps = int(g["steps"])
+    b = _batched(g, precision, K=7)
+    b.forward(steps)
+    terms, env = b.loss()
+    obs = b.observables()
+    tol = TOL[precision]
+    assert max_rel(obs["center"], g["center"]) < tol["traj"]
+    assert max_rel(obs["height"], g["height"]) < tol["traj"]
+    B, N = int(g["B"]), g["objects"].shape[0]
+    gx = g["x"].reshape(g["x"].shape[0], B * N, 3)
+    assert max_rel(b.trajectory()[:steps], gx[:steps]) < tol["traj"]
+    xf, _ = b.final_state()
+    assert max_rel(xf, gx[steps - 1]) < tol["traj"]
+    assert abs(terms["total"] - float(g["loss"])) <= tol["loss"] * abs(float(g["loss"]))
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("case", TRAIN_CASES)
+def test_batched_gradients_match_oracle(case, precision):
+    g = load_golden(case)
+    steps = int(g["steps"])
+    o = oracle_from_golden(g)
+    o.run(steps)
+    b = _batched(g, precision, K=9)
+    loss = b.simulate(steps)
+    tol = TOL[precision]
+    assert abs(loss - o.loss[0]) <= tol["loss"] * abs(o.loss[0])
+    for l in range(2):
+        gW, gb = b.get_grads(0, l)
+        assert rel_err(gW, o.gW[l]) < tol["grad"], (l, rel_err(gW, o.gW[l]))
+        assert rel_err(gb, o.gb[l]) < tol["grad"], (l, rel_err(gb, o.gb[l]))
+    gx0, gv0 = b.state_grads()
+    B, N = int(g["B"]), g["objects"].shape[0]
+    assert rel_err(gx0, o.gx[0].reshape(B * N, 3)) < tol["grad"]
+    assert rel_err(gv0, o.gv[0].reshape(B * N, 3)) < tol["grad"]
+    b.close()
+
+
+def _many_env_batch(precision, n_envs, hidden, K, steps_max, path):
+    import cls_b200
+    from helpers import params_from_golden
+    g = load_golden("quad_ref")
+    robot = cls_b200.Robot(g["objects"], g["springs"], robot_id=int(g["robot_id"]), hidden=hidden,
+                           n_outputs=0)
+    p = params_from_golden(g, precision=precision, K=K, max_steps=steps_max,
+                           loss=["velocity", "height", "rotation"])
+    b = cls_b200.MassSpringBatch([robot], [0] * n_envs, p)
+    b.set_controller_path(path)
+    rng = np.random.default_rng(11)
+    b.set_state(np.tile(g["x0"][0], (n_envs, 1)) + rng.normal(0, 1e-3, (n_envs * g["objects"].shape[0], 3)))
+    b.set_targets(rng.uniform(-0.1, 0.1, (steps_max, n_envs, 3)), rng.choice([-1.0, 0.0, 1.0], (steps_max, n_envs)))
+    for l in range(len(hidden) + 1):
+        rows, cols = b.layer_shape(0, l)
+        b.set_weights(0, l, rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6 / cols), rng.uniform(-0.1, 0.1, rows))
+    return b
+
+
+def _run(b, steps, n_layers):
+    loss = b.simulate(steps)
+    grads = [b.get_grads(0, l) for l in range(n_layers)]
+    x, _ = b.final_state()
+    gx0, _ = b.state_grads()
+    return loss, grads, x, gx0
+
+
+def test_batched_equals_per_env_with_partial_tiles_fp64():
+    """300 envs (tiles of 64 envs: four full and one partial) and hidden
+    widths 70 and 50 (partial output tiles); several checkpoint segments."""
+    hidden, steps = [70, 50], 40
+    ref = _many_env_batch(64, 300, hidden, 9, 48, "per_env")
+    assert not ref.controller_batched
+    r_loss, r_grads, r_x, r_gx = _run(ref, steps, 3)
+    ref.close()
+    b = _many_env_batch(64, 300, hidden, 9, 48, "auto")
+    assert b.controller_batched          # >= 256 envs of one type: automatic
+    loss, grads, x, gx = _run(b, steps, 3)
+    b.close()
+    tol = TOL[64]
+    assert abs(loss - r_loss) <= tol["loss"] * abs(r_loss)
+    assert max_rel(x, r_x) < tol["traj"]
+    for (gW, gb), (rW, rb) in zip(grads, r_grads):
+        assert rel_err(gW, rW) < tol["grad"] and rel_err(gb, rb) < tol["grad"]
+    assert rel_err(gx, r_gx) < tol["grad"]
+
+
+def test_batched_fp32_as_accurate_as_per_env_fp32():
+    """The same 300-env batch with random Xavier weights and contact-heavy
+    targets is ill-conditioned enough that FP32 itself (the fused per-env
+    path, plain FP32 arithmetic) misses the FP64 gradients by ~2.5e-4.  The
+    tensor-core path (3xTF32, FP32 accumulate) must agree with the FP32
+    per-env path to 1e-4 and be no less accurate than it against FP64."""
+    hidden, steps = [70, 50], 40
+    runs = {}
+    for prec, path in ((64, "per_env"), (32, "per_env"), (32, "batched")):
+        b = _many_env_batch(prec, 300, hidden, 9, 48, path)
+        runs[(prec, path)] = _run(b, steps, 3)
+        b.close()
+    r64, p32, b32 = runs[(64, "per_env")], runs[(32, "per_env")], runs[(32, "batched")]
+    assert abs(b32[0] - p32[0]) <= 1e-5 * abs(p32[0])
+    assert max_rel(b32[2], p32[2]) < 1e-5
+    for (gW, gb), (pW, pb), (rW, rb) in zip(b32[1], p32[1], r64[1]):
+        assert rel_err(gW, pW) < 1e-4 and rel_err(gb, pb) < 1e-4
+        assert rel_err(gW, rW) <= 1.25 * rel_err(pW, rW) + 1e-5
+        assert rel_err(gb, rb) <= 1.25 * rel_err(pb, rb) + 1e-5
+    assert rel_err(b32[3], p32[3]) < 1e-4
+    assert rel_err(b32[3], r64[3]) <= 1.25 * rel_err(p32[3], r64[3]) + 1e-5
+
+
+def test_batched_graph_replay_matches_eager():
+    """The forward pass (spring gather, tensor-core GEMMs) is deterministic, so
+    the replayed loss is identical; the reverse pass's shared-memory atomics
+    only change the gradients' rounding."""
+    import torch
+    b = _many_env_batch(32, 260, [64], 10, 40, "batched")
+    e_loss, e_grads, _, _ = _run(b, 30, 2)
+    s = torch.cuda.Stream()
+    b.set_stream(s.cuda_stream)
+    b.graph_capture(30)
+    for _ in range(2):
+        b.graph_launch()
+    b.synchronize()
+    g_loss, _ = b.loss()
+    assert g_loss["total"] == e_loss
+    for l in range(2):
+        gW, gb = b.get_grads(0, l)
+        assert rel_err(gW, e_grads[l][0]) < 1e-5
+        assert rel_err(gb, e_grads[l][1]) < 1e-5
+    b.close()
+
+
+def test_batched_profile_counts_gemm_launches():
+    b = _many_env_batch(32, 256, [64, 64], 10, 30, "batched")
+    b.profile(True)
+    b.simulate(20)
+    ms, n = b.profile_read(reset=True)
+    b.close()
+    # forward: 19 substeps x 3 layers; recompute: 19 x 3; reverse: 19 x 3
+    assert n["ctrl_gemm"] == 2 * 19 * 3
+    assert n["ctrl_gemm_adj"] == 19 * 3
+    assert ms["ctrl_gemm"] > 0 and ms["ctrl_gemm_adj"] > 0
