@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: automatic)")
+    ap.add_argument("--controller", default="auto", choices=["auto", "per_env", "batched"],
+                    help="controller path: batched = one tensor-core GEMM per layer over all envs "
+                         "of a robot type (automatic for types with >= 256 envs)")
     ap.add_argument("--tick-segments", type=int, default=4,
                     help="serve: checkpoint segments a tick advances every request by")
     a = ap.parse_args()
@@ -273,6 +276,8 @@ def run_ours(a):
     import cls_b200
     from cls_b200 import workloads
     b, robots, env_robot, (tv, th) = make_ms_batch(a, a.robots, 1000 * rank)
+    b.set_controller_path(a.controller)
+    batched = b.controller_batched
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     env_substeps = b.n_envs * (a.substeps - 1)
@@ -281,11 +286,18 @@ def run_ours(a):
         b.simulate(a.substeps)
         b.adam_step(it)
 
-    for it in range(a.warmup):
-        iteration(it)
+    # the timed training iteration (forward, loss, backward, Adam) is one CUDA
+    # graph replay; the eager path is measured separately as e2e below
+    iteration(0)
     b.synchronize()
-    b.profile(True)
-    b.profile_read(reset=True)
+    b.graph_capture(a.substeps, with_adam=True)
+
+    def replay(it):
+        b.graph_launch(it)
+
+    for it in range(a.warmup):
+        replay(it)
+    b.synchronize()
     clk = ClockSampler(local)
     if world > 1:
         torch.distributed.barrier()
@@ -294,47 +306,71 @@ def run_ours(a):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for it in range(a.steps):
-        iteration(a.warmup + it)
+        replay(a.warmup + it)
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = ev0.elapsed_time(ev1)
-    prof_ms, prof_n = b.profile_read(reset=True)
-    b.profile(False)
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / a.steps
+    # per-kernel breakdown: one more iteration, outside the timed region, with
+    # CUDA events around every launch (their gaps would inflate the timed loop)
+    b.profile(True)
+    b.profile_read(reset=True)
+    iteration(a.warmup + a.steps)
+    b.synchronize()
+    prof_ms, prof_n = b.profile_read(reset=True)
+    b.profile(False)
     value = world * env_substeps / (ms_per_step / 1e3)
     print("timed: %.1f ms/step, %.3e %s, kernels %s" % (ms_per_step, value, UNIT, prof_ms),
           file=sys.stderr)
 
     # roofline of the dominant kernel (CUDA events around each launch above)
-    alg = workloads.algorithmic_bytes(robots, env_robot)
+    alg = workloads.algorithmic_bytes(robots, env_robot, batched=batched)
     subs_total = a.substeps - 1
-    kinds = {"forward": subs_total, "recompute": subs_total, "reverse": subs_total}
-    top = max(kinds, key=lambda k: prof_ms[k])
-    bytes_region = alg[top] * subs_total * a.steps
-    achieved = bytes_region / (prof_ms[top] / 1e3) / 1e9
+    cands = ["forward", "recompute", "reverse"] + (["ctrl_gemm", "ctrl_gemm_adj"] if batched else [])
+    top = max(cands, key=lambda k: prof_ms[k])
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             peaks = json.load(f)
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+        hbm, bf16, peak_src = float(peaks["hbm_gbs"]), float(peaks["bf16_tflops"]), "measured"
     except (OSError, KeyError, ValueError):
-        peak, peak_src = 6650.0, "fallback"
-    kernel_name = {"forward": "ms_forward_kernel (first pass)", "recompute": "ms_forward_kernel (recompute)",
-                   "reverse": "ms_reverse_kernel"}[top]
-    traffic = None
-    if top in TRAFFIC_RATIO:
-        per_launch = alg[top] * (subs_total if top == "forward" else a.checkpoint)
-        traffic = TRAFFIC_RATIO[top] * per_launch
-    roofline = {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                "traffic": traffic,
-                "share_of_step": prof_ms[top] / max(1e-9, sum(prof_ms.values())),
-                "kernel_ms": prof_ms, "launches": prof_n}
+        hbm, bf16, peak_src = 6650.0, 1590.0, "fallback"
+    share = prof_ms[top] / max(1e-9, sum(prof_ms.values()))
+    if top in ("ctrl_gemm", "ctrl_gemm_adj"):
+        # tensor-core GEMMs: the three TF32 products of the 3xTF32 split, 2 M N K
+        # each; TF32 runs at half the BF16 dense rate
+        fl = workloads.controller_flops(robots, env_robot)
+        passes = 2 if top == "ctrl_gemm" else 1       # first pass + recompute / reverse
+        flops = 3 * fl["forward" if top == "ctrl_gemm" else "adjoint"] * subs_total * passes
+        achieved = flops / (prof_ms[top] / 1e3) / 1e12
+        peak = 0.5 * bf16
+        roofline = {"kernel": "ms_ctrl_gemm_tc_kernel (%s)" % ("forward" if top == "ctrl_gemm" else "adjoint"),
+                    "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": peak_src + " bf16 dense x 0.5 (TF32 rate)",
+                    "note": "achieved counts the 3 TF32 MMA products per FP32 product (3xTF32 split)",
+                    "share_of_step": share, "kernel_ms": prof_ms, "launches": prof_n}
+    else:
+        bytes_region = alg[top] * subs_total
+        achieved = bytes_region / (prof_ms[top] / 1e3) / 1e9
+        if batched:
+            kernel_name = {"forward": "ms_step_fwd_kernel (first pass)",
+                           "recompute": "ms_step_fwd_kernel (recompute)", "reverse": "ms_step_rev_kernel"}[top]
+        else:
+            kernel_name = {"forward": "ms_forward_kernel (first pass)",
+                           "recompute": "ms_forward_kernel (recompute)", "reverse": "ms_reverse_kernel"}[top]
+        traffic = None
+        if top in TRAFFIC_RATIO and not batched:
+            per_launch = alg[top] * (subs_total if top == "forward" else a.checkpoint)
+            traffic = TRAFFIC_RATIO[top] * per_launch
+        roofline = {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": hbm,
+                    "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
+                    "traffic": traffic, "share_of_step": share, "kernel_ms": prof_ms, "launches": prof_n}
 
     # plain form: the same kernels, one robot per launch, on a bounded sample
     plain = None
@@ -413,8 +449,9 @@ def run_ours(a):
                 "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded random lattices, targets and weights)",
-                "config": config_dict(a, world), "clocks": clocks,
-                "gpu_launches": int(sum(prof_n.values())), "roofline": roofline,
+                "config": dict(config_dict(a, world), controller="batched" if batched else "per_env"),
+                "clocks": clocks,
+                "gpu_launches": int(sum(prof_n.values())) * a.steps, "roofline": roofline,
                 "plain": plain, "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(line))
     b.close()

@@ -20,6 +20,8 @@
 // path's layout (rows padded to 4 floats), so the weight-gradient kernel and
 // the checkpoint schedule are shared.
 #pragma once
+#include <type_traits>
+
 #include "ms_segment.cuh"
 #include "umma_gemm.cuh"
 
@@ -72,6 +74,13 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
     R hprev = 0;
     if ((mode & FWD_OBS) && t > 0) hprev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
     fwd_pre<R>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
+    if constexpr (std::is_same<R, float>::value) {
+      // the input row as the first layer's pre-split A operand
+      const umma::SplitTiles st{a.tiles + rb.ta_f[0], umma::TM, (rb.n_c + 31) / 32};
+      const int j = e - rb.env_first;
+      for (int q = 4 * tid; q < rb.n_c; q += 4 * nt)
+        st.store4(j, q, make_float4(s.ain[q], s.ain[q + 1], s.ain[q + 2], s.ain[q + 3]));
+    }
     for (int i = tid; i < N; i += nt) {
       a.live_x[ed.v_off + i] = s.xs[i];
       a.live_v[ed.v_off + i] = s.vs[i];
@@ -110,7 +119,20 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
     __syncthreads();
     rev_post<R>(a, rb, ed, s, e, t_post, hcarry);
   }
-  if (t_pre >= 0) rev_pre<R>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
+  if (t_pre >= 0) {
+    rev_pre<R>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
+    if constexpr (std::is_same<R, float>::value) {
+      // dZ of the output layer as the adjoint GEMM's pre-split A operand
+      const int no = rb.n_out;
+      const umma::SplitTiles st{a.tiles + rb.ta_b[rb.n_layers - 1], umma::TM, (no + 31) / 32};
+      const int j = e - rb.env_first;
+      for (int q = 4 * tid; q < no; q += 4 * nt) {
+        float4 v = make_float4(s.dz[q], q + 1 < no ? s.dz[q + 1] : 0.f, q + 2 < no ? s.dz[q + 2] : 0.f,
+                               q + 3 < no ? s.dz[q + 3] : 0.f);
+        st.store4(j, q, v);
+      }
+    }
+  }
   rev_store_carry<R>(a, rb, ed, s, e, hcarry);
 }
 
@@ -255,33 +277,106 @@ __device__ __forceinline__ BwdOperands<R> bwd_operands(const MsArgs<R>& a, const
 }
 
 // ------------------------------------------------------- tensor-core GEMMs
-constexpr int kDenseTN = 64;  // output columns per tensor-core tile
+// FP32: one 128-env x 64-output tile per CTA, operands streamed as pre-split
+// tiles (umma::tile_gemm_bulk).  The epilogue writes, along rows (16 bytes per
+// thread), the FP32 record the adjoint and the weight-gradient products read
+// and the next GEMM's pre-split A operand:
+//   forward l:  Z_l record; act(Z_l + b_l) as layer l + 1's A (hidden layers)
+//   adjoint l:  dZ_{l-1} = C act'(Z_{l-1} + b_{l-1}) record and as layer l-1's
+//               adjoint A (l > 0); d input positions (l = 0)
+constexpr int kDenseTN = 64;     // output columns per tensor-core tile
+constexpr int kBulkStages = 4;   // 4 x 48 KB stage ring
+
+__device__ __forceinline__ float4 mask4(float4 v, int col, int n) {
+  if (col + 1 > n) v.x = 0.f;
+  if (col + 2 > n) v.y = 0.f;
+  if (col + 3 > n) v.z = 0.f;
+  if (col + 4 > n) v.w = 0.f;
+  return v;
+}
 
 template <int BWD>
-__global__ void __launch_bounds__(umma::kThreads)
+__global__ void __launch_bounds__(umma::kBulkThreads)
 ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
   extern __shared__ __align__(1024) float smem_f[];
-  __shared__ umma::TileShared ts;
+  __shared__ umma::BulkShared bs;
   const DenseJob jb = jobs[blockIdx.x];
-  int m_valid, n_valid, kpad;
-  bool ok;
-  if (BWD) {
-    const BwdOperands<float> op = bwd_operands<float>(a, jb, kslot, m_valid, n_valid, kpad, umma::TM, kDenseTN);
-    ok = umma::tile_gemm<kDenseTN>(
-        smem_f, ts, 0, kpad, m_valid, n_valid,
-        [&](int k, int i) { const V4<float> v = op.load_a(k, i); return make_float4(v.x, v.y, v.z, v.w); },
-        [&](int k, int j) { const V4<float> v = op.load_b(k, j); return make_float4(v.x, v.y, v.z, v.w); },
-        [&](int i, int j, float v) { op.store(i, j, v); });
-  } else {
-    const FwdOperands<float> op = fwd_operands<float>(a, jb, kslot, m_valid, n_valid, kpad, umma::TM, kDenseTN);
-    ok = umma::tile_gemm<kDenseTN>(
-        smem_f, ts, 0, kpad, m_valid, n_valid,
-        [&](int k, int i) { const V4<float> v = op.load_a(k, i); return make_float4(v.x, v.y, v.z, v.w); },
-        [&](int k, int j) { const V4<float> v = op.load_b(k, j); return make_float4(v.x, v.y, v.z, v.w); },
-        [&](int i, int j, float v) { op.store(i, j, v); });
-  }
+  const RobotDesc& rb = a.robots[jb.robot];
+  const EnvDesc& e0 = a.envs[rb.env_first];
+  const int l = jb.layer;
+  const int kin = BWD ? rb.width[l + 1] : rb.width[l];
+  const int nkt = (kin + 31) / 32;
+  const float* ab = a.tiles + (BWD ? rb.ta_b[l] : rb.ta_f[l]) + (size_t)(jb.m0 / umma::TM) * nkt * 64 * umma::TM;
+  const float* bb = a.tiles + (BWD ? rb.tb_b[l] : rb.tb_f[l]) + (size_t)(jb.n0 / kDenseTN) * nkt * 64 * kDenseTN;
+  const int m_valid = min(umma::TM, rb.n_env - jb.m0);
+  const int ncol = BWD ? (l > 0 ? rb.width[l] : 3 * rb.n_v) : rb.width[l + 1];
+  const int n_valid = min(kDenseTN, ncol - jb.n0);
+  const int act = a.act_hidden;
+  const bool ok = umma::tile_gemm_bulk<kDenseTN, kBulkStages>(smem_f, bs, ab, bb, nkt, [&](const float* cs, int ld) {
+    constexpr int C4 = kDenseTN / 4;
+    for (int q = threadIdx.x; q < umma::TM * C4; q += blockDim.x) {
+      const int i = q / C4, j = 4 * (q % C4);
+      if (i >= m_valid || j >= n_valid) continue;
+      const float4 v = *reinterpret_cast<const float4*>(cs + i * ld + j);
+      const int row = jb.m0 + i, col = jb.n0 + j;
+      if (!BWD) {
+        const int w = rb.width[l + 1];
+        float* zr = a.rec_z + a.z_base[l] + (size_t)kslot * a.z_total[l] + e0.z_off[l] + (size_t)row * pad4(w) + col;
+        *reinterpret_cast<float4*>(zr) = v;
+        if (l + 1 < rb.n_layers) {
+          const float4 b = *reinterpret_cast<const float4*>(a.bias + rb.b_off[l] + col);
+          const float4 y = make_float4(act_f<float>(act, v.x + b.x), act_f<float>(act, v.y + b.y),
+                                       act_f<float>(act, v.z + b.z), act_f<float>(act, v.w + b.w));
+          const umma::SplitTiles st{a.tiles + rb.ta_f[l + 1], umma::TM, (w + 31) / 32};
+          st.store4(row, col, mask4(y, col, w));
+        }
+      } else if (l > 0) {
+        const int w = rb.width[l];
+        const size_t o = a.z_base[l - 1] + (size_t)kslot * a.z_total[l - 1] + e0.z_off[l - 1] + (size_t)row * pad4(w) + col;
+        const float4 z = *reinterpret_cast<const float4*>(a.rec_z + o);
+        const float4 b = *reinterpret_cast<const float4*>(a.bias + rb.b_off[l - 1] + col);
+        const float4 dz = mask4(make_float4(v.x * act_d<float>(act, z.x + b.x), v.y * act_d<float>(act, z.y + b.y),
+                                            v.z * act_d<float>(act, z.z + b.z), v.w * act_d<float>(act, z.w + b.w)),
+                                col, w);
+        *reinterpret_cast<float4*>(a.rec_dz + o) = dz;
+        const umma::SplitTiles st{a.tiles + rb.ta_b[l - 1], umma::TM, (w + 31) / 32};
+        st.store4(row, col, dz);
+      } else {
+        float* dp = a.din + (size_t)3 * (e0.v_off + (size_t)row * rb.n_v) + col;
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (j + u < n_valid) dp[u] = vv[u];
+      }
+    }
+  });
   if (!ok && threadIdx.x == 0) atomicOr(a.status, ERR_TIMEOUT);
   if (threadIdx.x < 32) umma::tmem_relinquish();
+}
+
+// pre-split tiles of every layer's W_l (forward B: rows = outputs) and W_l^T
+// (adjoint B: rows = inputs), one thread per weight
+struct SplitSeg {
+  long long w_off, tf_off, tb_off;
+  int rows, cols, pitch;  // W_l: rows = outputs, cols = inputs
+  long long first;        // first weight of this block in the launch
+};
+
+__global__ void __launch_bounds__(256) ms_split_weights_kernel(const float* __restrict__ w, float* tiles,
+                                                               const SplitSeg* segs, int n_segs, long long total) {
+  for (long long q = blockIdx.x * 256ll + threadIdx.x; q < total; q += (long long)gridDim.x * 256) {
+    int lo = 0, hi = n_segs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (segs[mid].first <= q) lo = mid; else hi = mid - 1;
+    }
+    const SplitSeg sg = segs[lo];
+    const long long r = q - sg.first;
+    const int o = (int)(r / sg.cols), i = (int)(r % sg.cols);
+    const float v = w[sg.w_off + (size_t)o * sg.pitch + i];
+    umma::SplitTiles{tiles + sg.tf_off, kDenseTN, (sg.cols + 31) / 32}.store(o, i, v);
+    umma::SplitTiles{tiles + sg.tb_off, kDenseTN, (sg.rows + 31) / 32}.store(i, o, v);
+  }
 }
 
 // ---------------------------------------------------------------- SIMT GEMMs

@@ -39,6 +39,10 @@ struct RobotDesc {
   int b_off[kMaxLayers];             // bias offsets
   long long wt_off[kMaxLayers];      // transposed compact weights (batched controller)
   int wt_pitch[kMaxLayers];          // row pitch of W_l^T: width[l + 1] padded to 4
+  // batched controller, FP32: offsets in `tiles` of the pre-split operand
+  // tiles of layer l's forward GEMM (A: inputs of the type's envs, B: W_l) and
+  // adjoint GEMM (A: dZ_l, B: W_l^T)
+  long long ta_f[kMaxLayers], tb_f[kMaxLayers], ta_b[kMaxLayers], tb_b[kMaxLayers];
   int n_env;                         // envs of this type: B in the loss normalisation
   int env_first;                     // envs are sorted by type
   int rot_idx[4];                    // heading vertices for robot 100
@@ -108,6 +112,7 @@ struct MsArgs {
   // batched controller: state between step launches, d input positions
   // [v_total][3], transposed compact weights
   V4<R>* live_x; V4<R>* live_v; R* din; const R* wt;
+  R* tiles;                          // FP32: pre-split GEMM operand tiles
   // status
   int* status;
   // per-phase clock totals, only written by builds with CLS_PHASE_TIMERS

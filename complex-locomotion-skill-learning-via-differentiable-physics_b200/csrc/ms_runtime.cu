@@ -657,6 +657,7 @@ class SimImpl final : public SimBase {
     a.live_v = d_livev_.p;
     a.din = d_din_.p;
     a.wt = d_wt_.p;
+    a.tiles = d_split_.p;
     return a;
   }
 
@@ -810,6 +811,34 @@ class SimImpl final : public SimBase {
     d_din_.alloc((size_t)3 * V_);
     d_wt_.alloc(std::max<long long>(1, wt_total_));
     CLS_CUDA(cudaMemset(d_wt_.p, 0, sizeof(R) * d_wt_.n));
+    if constexpr (f32) {
+      // pre-split operand tiles of every layer's GEMMs (zero padding stays zero)
+      long long off = 0;
+      ssegs_.clear();
+      split_total_ = 0;
+      for (int r = 0; r < (int)hr_.size(); ++r) {
+        RobotDesc& d = rd_host_[r];
+        const HostRobot& h = hr_[r];
+        if (d.n_env == 0) continue;
+        for (int l = 0; l < h.n_layers; ++l) {
+          const int wi = h.width[l], wo = h.width[l + 1];
+          d.ta_f[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wi);
+          d.ta_b[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wo);
+          d.tb_f[l] = off; off += (long long)umma::split_tiles_floats(wo, kDenseTN, wi);
+          d.tb_b[l] = off; off += (long long)umma::split_tiles_floats(wi, kDenseTN, wo);
+          SplitSeg sg{};
+          sg.w_off = d.w_off[l]; sg.tf_off = d.tb_f[l]; sg.tb_off = d.tb_b[l];
+          sg.rows = wo; sg.cols = wi; sg.pitch = d.pitch[l]; sg.first = split_total_;
+          split_total_ += (long long)wo * wi;
+          ssegs_.push_back(sg);
+        }
+      }
+      d_split_.alloc(std::max<long long>(1, off));
+      CLS_CUDA(cudaMemset(d_split_.p, 0, sizeof(R) * d_split_.n));
+      d_ssegs_.alloc(std::max<size_t>(1, ssegs_.size()));
+      CLS_CUDA(cudaMemcpy(d_ssegs_.p, ssegs_.data(), sizeof(SplitSeg) * ssegs_.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_robots_.p, rd_host_.data(), sizeof(RobotDesc) * rd_host_.size(), cudaMemcpyHostToDevice));
+    }
     // step kernels: one CTA per env, no controller inside
     int nv = 0;
     for (const HostRobot& h : hr_) nv = std::max(nv, h.n_v);
@@ -829,7 +858,7 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaFuncSetAttribute(dense_rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)((size_t)optin - ra.sharedSizeBytes)));
     if constexpr (f32) {
-      const int sm = (int)umma::Shape<kDenseTN>::kSmemBytes;
+      const int sm = (int)umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes;
       CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
       CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     }
@@ -855,9 +884,9 @@ class SimImpl final : public SimBase {
     const DenseJob* jobs = d_jobs_.p + (bwd ? jb_off_[l] : jf_off_[l]);
     timed(bwd ? PK_CGEMM_ADJ : PK_CGEMM, [&] {
       if constexpr (std::is_same<R, float>::value) {
-        const size_t sm = umma::Shape<kDenseTN>::kSmemBytes;
-        if (bwd) ms_ctrl_gemm_tc_kernel<1><<<cnt, umma::kThreads, sm, stream>>>(a, jobs, kslot);
-        else ms_ctrl_gemm_tc_kernel<0><<<cnt, umma::kThreads, sm, stream>>>(a, jobs, kslot);
+        const size_t sm = umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes;
+        if (bwd) ms_ctrl_gemm_tc_kernel<1><<<cnt, umma::kBulkThreads, sm, stream>>>(a, jobs, kslot);
+        else ms_ctrl_gemm_tc_kernel<0><<<cnt, umma::kBulkThreads, sm, stream>>>(a, jobs, kslot);
       } else {
         if (bwd) ms_ctrl_gemm_simt_kernel<R, 1><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
         else ms_ctrl_gemm_simt_kernel<R, 0><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
@@ -1003,10 +1032,20 @@ class SimImpl final : public SimBase {
   // once the batched path has been enabled)
   void transpose_weights() {
     if (!d_wt_.p || n_ttiles_ == 0) return;
-    timed(PK_ADAM, [&] {
-      ms_transpose_weights_kernel<R><<<n_ttiles_, 256, 0, stream>>>(d_w_.p, d_wt_.p, d_tsegs_.p,
-                                                                    (int)tsegs_.size());
-    });
+    if constexpr (std::is_same<R, float>::value) {
+      // FP32: the GEMMs read W_l and W_l^T as pre-split tiles
+      if (split_total_ == 0) return;
+      const int blocks = (int)std::min<long long>(4096, (split_total_ + 255) / 256);
+      timed(PK_ADAM, [&] {
+        ms_split_weights_kernel<<<blocks, 256, 0, stream>>>(d_w_.p, d_split_.p, d_ssegs_.p, (int)ssegs_.size(),
+                                                            split_total_);
+      });
+    } else {
+      timed(PK_ADAM, [&] {
+        ms_transpose_weights_kernel<R><<<n_ttiles_, 256, 0, stream>>>(d_w_.p, d_wt_.p, d_tsegs_.p,
+                                                                      (int)tsegs_.size());
+      });
+    }
   }
 
   void adam(int iter, double* tns) override {
@@ -1551,7 +1590,10 @@ class SimImpl final : public SimBase {
   DevBuf<DenseJob> d_jobs_;
   DevBuf<TransSeg> d_tsegs_;
   DevBuf<V4<R>> d_livex_, d_livev_;
-  DevBuf<R> d_din_, d_wt_;
+  DevBuf<R> d_din_, d_wt_, d_split_;
+  std::vector<SplitSeg> ssegs_;
+  DevBuf<SplitSeg> d_ssegs_;
+  long long split_total_ = 0;
 
  public:
   void phase_read(unsigned long long* out) override {

@@ -97,10 +97,16 @@ def spider_batch(n_envs=4096, steps=1000, K=50, seed=0, precision=32, **over):
     return b, [robot], (tv, th)
 
 
-def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4):
+def _widths(rb):
+    N, S = rb.n_vertices, rb.n_springs
+    return [(-(-3 * N // 4) * 4) + 8 + 2 + 1] + list(rb.hidden) + [rb.n_outputs if rb.n_outputs > 0 else S]
+
+
+def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4, batched=False):
     """Compulsory DRAM bytes per substep of the whole batch, per kernel.
 
-    Per env-substep of robot r (N vertices, S springs, MLP rows x pitch):
+    Fused per-env path, per env-substep of robot r (N vertices, S springs, MLP
+    rows x pitch):
       weights:   sum_l rows_l * pitch_l * 4   (read once per pass; the batch's
                  weights exceed L2, so every pass streams them)
       forward:   weights + trajectory write 16 N (x[t], when kept)
@@ -109,22 +115,52 @@ def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4):
                  (dz) + trajectory reads 32 N (rotation loss at t - rp, t + rp)
     The spring table (32 B per incidence, 2 S per robot) is read from L2 each
     substep and counted once per pass.
+
+    Batched-controller path, step kernels only (the controller's GEMMs are
+    counted in FLOPs by controller_flops), per env-substep:
+      forward:   state read + write 64 N, input row write 4 n_c, output-layer
+                 pre-activations read 4 n_out, trajectory write 16 N
+      recompute: forward without the trajectory + record writes 32 N (x, v)
+                 + 16 N (v_inc)
+      reverse:   record reads 48 N (x, v, v_inc) + 16 N (x of t + 1), adjoint
+                 state read + write 64 N, d input positions 12 N, output-layer
+                 z read + dz write 8 n_out, trajectory reads 32 N
     """
     out = dict(forward=0.0, recompute=0.0, reverse=0.0)
     for r in env_robot:
         rb = robots[r]
         N, S = rb.n_vertices, rb.n_springs
-        widths = [(-(-3 * N // 4) * 4) + 8 + 2 + 1] + list(rb.hidden) + [
-            rb.n_outputs if rb.n_outputs > 0 else S]
+        widths = _widths(rb)
+        traj = 16 * N if keep_trajectory else 0
+        if batched:
+            n_c, n_out = widths[0], widths[-1]
+            out["forward"] += 64 * N + 4 * n_c + 4 * n_out + traj
+            out["recompute"] += 64 * N + 4 * n_c + 4 * n_out + 48 * N
+            out["reverse"] += 64 * N + 64 * N + 12 * N + 8 * n_out + 2 * traj
+            continue
         pitch = [-(-w // 4) * 4 for w in widths]
         wbytes = sum(widths[l + 1] * pitch[l] for l in range(len(widths) - 1)) * dtype_bytes
         rows = sum(widths[1:]) * dtype_bytes
         springs = 2 * S * 32
-        traj = 16 * N if keep_trajectory else 0
         out["forward"] += wbytes + springs + traj
         out["recompute"] += wbytes + springs + 32 * N + widths[0] * dtype_bytes + rows
         out["reverse"] += wbytes + springs + 32 * N + 2 * rows + 2 * traj
     return out
+
+
+def controller_flops(robots, env_robot):
+    """Useful FP32 FLOPs (2 M N K) of the batched controller's GEMMs per
+    substep of the whole batch: forward (every layer, K = the layer's inputs)
+    and adjoint (every layer back to its inputs; the first layer only to the
+    3 N position columns)."""
+    fw = ad = 0.0
+    for r in env_robot:
+        rb = robots[r]
+        w = _widths(rb)
+        for l in range(len(w) - 1):
+            fw += 2.0 * w[l + 1] * w[l]
+            ad += 2.0 * w[l + 1] * (w[l] if l > 0 else 3 * rb.n_vertices)
+    return {"forward": fw, "adjoint": ad}
 
 
 def legged_body(n_grid=64, ppc=2, torso=(24, 8, 14), leg=(5, 10, 5), origin_cells=(18, 4, 25)):
