@@ -36,25 +36,44 @@ struct DenseJob {
 __host__ __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 // ------------------------------------------------------------ step kernels
-// Forward step t of a range [t_first, t_end) (one CTA per env):
+// One CTA per env (G = BlockGroup; WarpGroup with kStepWarps envs per CTA is
+// the alternative the group abstraction allows): the substep halves with the
+// env's state in the group's slice of shared memory (per_group bytes, the
+// fused kernels' carve with the controller buffers sized for the output
+// layer only).
+constexpr int kStepWarps = 4;
+
+template <typename G>
+__device__ __forceinline__ int step_slot() { return G::kWarp ? (threadIdx.x >> 5) : 0; }
+template <typename G>
+__device__ __forceinline__ int step_item() {
+  return G::kWarp ? blockIdx.x * kStepWarps + (threadIdx.x >> 5) : blockIdx.x;
+}
+
+// Forward step t of a range [t_first, t_end):
 //   t > t_first: controller outputs of t-1 from the output layer's record
 //                (slot k_prev), then spring forces and advance of t-1;
 //   t < t_end:   checkpoint / records / observables of x(t), the input row of
-//                t into record slot k_cur (zero padded), state to live_x/v;
+//                t into record slot k_cur (zero padded) and, FP32, into the
+//                first GEMM's pre-split operand; state to live_x/v;
 //   t == t_end:  the range's end (checkpoint, final state).
 // The state comes from checkpoint slot src_slot at t == t_first, else from
 // live_x/v.
-template <typename R, int MAXT>
+template <typename R, typename G, int MAXT>
 __global__ void __launch_bounds__(MAXT)
 ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src_slot, int k_prev,
-                   int k_cur) {
+                   int k_cur, int per_group) {
   extern __shared__ __align__(256) char smem_raw[];
-  __shared__ RobotDesc rb;
-  __shared__ EnvDesc ed;
-  FwdSmem<R> s = carve_fwd<R>(smem_raw, a);
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int e = a.order[blockIdx.x];
-  load_descs(a, e, rb, ed);
+  __shared__ RobotDesc rbs[G::kWarp ? kStepWarps : 1];
+  __shared__ EnvDesc eds[G::kWarp ? kStepWarps : 1];
+  const int w = step_slot<G>(), item = step_item<G>();
+  if (item >= a.n_items) return;  // whole groups only
+  RobotDesc& rb = rbs[w];
+  EnvDesc& ed = eds[w];
+  FwdSmem<R> s = carve_fwd<R>(smem_raw + (size_t)w * per_group, a);
+  const int tid = G::rank(), nt = G::size();
+  const int e = a.order[item];
+  load_descs<R, G>(a, e, rb, ed);
   const int N = rb.n_v, L = rb.n_layers;
   {
     const bool first = (t == t_first);
@@ -62,21 +81,21 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
     const V4<R>* cv = first ? a.ckpt_v + (size_t)src_slot * a.v_total + ed.v_off : a.live_v + ed.v_off;
     for (int i = tid; i < N; i += nt) { s.xs[i] = cx[i]; s.vs[i] = cv[i]; }
   }
-  __syncthreads();
+  G::sync();
   if (t > t_first) {
     const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)k_prev * a.z_total[L - 1] + ed.z_off[L - 1];
     const R* bo = a.bias + rb.b_off[L - 1];
     for (int o = tid; o < rb.n_out; o += nt) s.buf0[o] = act_f<R>(a.act_out, zl[o] + bo[o]);
-    __syncthreads();
-    fwd_post<R>(a, rb, ed, s, t - 1, mode, k_prev, s.buf0);
+    G::sync();
+    fwd_post<R, G>(a, rb, ed, s, t - 1, mode, k_prev, s.buf0);
   }
   if (t < t_end) {
     R hprev = 0;
     if ((mode & FWD_OBS) && t > 0) hprev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
-    fwd_pre<R>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
+    fwd_pre<R, G>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
     if constexpr (std::is_same<R, float>::value) {
       // the input row as the first layer's pre-split A operand
-      const umma::SplitTiles st{a.tiles + rb.ta_f[0], umma::TM, (rb.n_c + 31) / 32};
+      const umma::SplitTiles st{a.tiles + a.dense[ed.robot].ta_f[0], umma::TM, (rb.n_c + 31) / 32};
       const int j = e - rb.env_first;
       for (int q = 4 * tid; q < rb.n_c; q += 4 * nt)
         st.store4(j, q, make_float4(s.ain[q], s.ain[q + 1], s.ain[q + 2], s.ain[q + 3]));
@@ -86,54 +105,59 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
       a.live_v[ed.v_off + i] = s.vs[i];
     }
   } else {
-    fwd_finish<R>(a, rb, ed, s, t_first, t_end, mode);
+    fwd_finish<R, G>(a, rb, ed, s, t_first, t_end, mode);
   }
 }
 
-// Reverse step over a segment [t_begin, t_end) (one CTA per env):
+// Reverse step over a segment [t_begin, t_end):
 //   t_post >= 0: adjoint of substep t_post from its controller input on
 //                (d input positions in din, x(t_post) from the records);
-//   t_pre >= 0:  adjoint of substep t_pre up to dZ of the output layer.
+//   t_pre >= 0:  adjoint of substep t_pre up to dZ of the output layer (and,
+//                FP32, dZ as the adjoint GEMM's pre-split operand).
 // The adjoint state is carried in adj_x/v/h between launches; the first
 // launch of the segment (t_pre = t_end - 1) seeds it (last segment) or takes
 // the carry of the later segment.
-template <typename R, int MAXT>
+template <typename R, typename G, int MAXT>
 __global__ void __launch_bounds__(MAXT)
-ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, int last_seg) {
+ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, int last_seg, int per_group) {
   extern __shared__ __align__(256) char smem_raw[];
-  __shared__ RobotDesc rb;
-  __shared__ EnvDesc ed;
-  RevSmem<R> s = carve_rev<R>(smem_raw, a);
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int e = a.order[blockIdx.x];
-  load_descs(a, e, rb, ed);
+  __shared__ RobotDesc rbs[G::kWarp ? kStepWarps : 1];
+  __shared__ EnvDesc eds[G::kWarp ? kStepWarps : 1];
+  const int w = step_slot<G>(), item = step_item<G>();
+  if (item >= a.n_items) return;
+  RobotDesc& rb = rbs[w];
+  EnvDesc& ed = eds[w];
+  RevSmem<R> s = carve_rev<R>(smem_raw + (size_t)w * per_group, a);
+  const int tid = G::rank(), nt = G::size();
+  const int e = a.order[item];
+  load_descs<R, G>(a, e, rb, ed);
   const int N = rb.n_v;
   R hcarry = 0;
-  rev_load_carry<R>(a, rb, ed, s, e, t_end, t_pre == t_end - 1 && last_seg != 0, hcarry);
+  rev_load_carry<R, G>(a, rb, ed, s, e, t_end, t_pre == t_end - 1 && last_seg != 0, hcarry);
   if (t_post >= 0) {
     const int kk = t_post - t_begin;
     const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
     for (int i = tid; i < N; i += nt) s.xs[i] = rx[i];
     const R* dp = a.din + (size_t)3 * ed.v_off;
     for (int q = tid; q < 3 * N; q += nt) s.bufA[q] = dp[q];
-    __syncthreads();
-    rev_post<R>(a, rb, ed, s, e, t_post, hcarry);
+    G::sync();
+    rev_post<R, G>(a, rb, ed, s, e, t_post, hcarry);
   }
   if (t_pre >= 0) {
-    rev_pre<R>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
+    rev_pre<R, G>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
     if constexpr (std::is_same<R, float>::value) {
       // dZ of the output layer as the adjoint GEMM's pre-split A operand
       const int no = rb.n_out;
-      const umma::SplitTiles st{a.tiles + rb.ta_b[rb.n_layers - 1], umma::TM, (no + 31) / 32};
+      const umma::SplitTiles st{a.tiles + a.dense[ed.robot].ta_b[rb.n_layers - 1], umma::TM, (no + 31) / 32};
       const int j = e - rb.env_first;
       for (int q = 4 * tid; q < no; q += 4 * nt) {
-        float4 v = make_float4(s.dz[q], q + 1 < no ? s.dz[q + 1] : 0.f, q + 2 < no ? s.dz[q + 2] : 0.f,
-                               q + 3 < no ? s.dz[q + 3] : 0.f);
+        const float4 v = make_float4(s.dz[q], q + 1 < no ? s.dz[q + 1] : 0.f, q + 2 < no ? s.dz[q + 2] : 0.f,
+                                     q + 3 < no ? s.dz[q + 3] : 0.f);
         st.store4(j, q, v);
       }
     }
   }
-  rev_store_carry<R>(a, rb, ed, s, e, hcarry);
+  rev_store_carry<R, G>(a, rb, ed, s, e, hcarry);
 }
 
 // ------------------------------------------------------------ GEMM operands
@@ -253,8 +277,8 @@ __device__ __forceinline__ BwdOperands<R> bwd_operands(const MsArgs<R>& a, const
   kpad = pad4(op.kin);
   op.astride = kpad;
   op.arow = a.rec_dz + a.z_base[l] + (size_t)kslot * a.z_total[l] + e0.z_off[l] + (size_t)jb.m0 * kpad;
-  op.wtpitch = rb.wt_pitch[l];
-  op.WT = a.wt + rb.wt_off[l] + (size_t)jb.n0 * op.wtpitch;
+  op.wtpitch = a.dense[jb.robot].wt_pitch[l];
+  op.WT = a.wt + a.dense[jb.robot].wt_off[l] + (size_t)jb.n0 * op.wtpitch;
   int ncol;
   if (l > 0) {
     ncol = rb.width[l];
@@ -302,12 +326,13 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
   __shared__ umma::BulkShared bs;
   const DenseJob jb = jobs[blockIdx.x];
   const RobotDesc& rb = a.robots[jb.robot];
+  const DenseDesc& dd = a.dense[jb.robot];
   const EnvDesc& e0 = a.envs[rb.env_first];
   const int l = jb.layer;
   const int kin = BWD ? rb.width[l + 1] : rb.width[l];
   const int nkt = (kin + 31) / 32;
-  const float* ab = a.tiles + (BWD ? rb.ta_b[l] : rb.ta_f[l]) + (size_t)(jb.m0 / umma::TM) * nkt * 64 * umma::TM;
-  const float* bb = a.tiles + (BWD ? rb.tb_b[l] : rb.tb_f[l]) + (size_t)(jb.n0 / kDenseTN) * nkt * 64 * kDenseTN;
+  const float* ab = a.tiles + (BWD ? dd.ta_b[l] : dd.ta_f[l]) + (size_t)(jb.m0 / umma::TM) * nkt * 64 * umma::TM;
+  const float* bb = a.tiles + (BWD ? dd.tb_b[l] : dd.tb_f[l]) + (size_t)(jb.n0 / kDenseTN) * nkt * 64 * kDenseTN;
   const int m_valid = min(umma::TM, rb.n_env - jb.m0);
   const int ncol = BWD ? (l > 0 ? rb.width[l] : 3 * rb.n_v) : rb.width[l + 1];
   const int n_valid = min(kDenseTN, ncol - jb.n0);
@@ -327,7 +352,7 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
           const float4 b = *reinterpret_cast<const float4*>(a.bias + rb.b_off[l] + col);
           const float4 y = make_float4(act_f<float>(act, v.x + b.x), act_f<float>(act, v.y + b.y),
                                        act_f<float>(act, v.z + b.z), act_f<float>(act, v.w + b.w));
-          const umma::SplitTiles st{a.tiles + rb.ta_f[l + 1], umma::TM, (w + 31) / 32};
+          const umma::SplitTiles st{a.tiles + dd.ta_f[l + 1], umma::TM, (w + 31) / 32};
           st.store4(row, col, mask4(y, col, w));
         }
       } else if (l > 0) {
@@ -339,7 +364,7 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
                                             v.z * act_d<float>(act, z.z + b.z), v.w * act_d<float>(act, z.w + b.w)),
                                 col, w);
         *reinterpret_cast<float4*>(a.rec_dz + o) = dz;
-        const umma::SplitTiles st{a.tiles + rb.ta_b[l - 1], umma::TM, (w + 31) / 32};
+        const umma::SplitTiles st{a.tiles + dd.ta_b[l - 1], umma::TM, (w + 31) / 32};
         st.store4(row, col, dz);
       } else {
         float* dp = a.din + (size_t)3 * (e0.v_off + (size_t)row * rb.n_v) + col;

@@ -37,15 +37,21 @@ struct RobotDesc {
   int pitch[kMaxLayers];             // row pitch (elements, multiple of 4) of layer l
   long long w_off[kMaxLayers];       // compact weight offsets (elements)
   int b_off[kMaxLayers];             // bias offsets
-  long long wt_off[kMaxLayers];      // transposed compact weights (batched controller)
-  int wt_pitch[kMaxLayers];          // row pitch of W_l^T: width[l + 1] padded to 4
-  // batched controller, FP32: offsets in `tiles` of the pre-split operand
-  // tiles of layer l's forward GEMM (A: inputs of the type's envs, B: W_l) and
-  // adjoint GEMM (A: dZ_l, B: W_l^T)
-  long long ta_f[kMaxLayers], tb_f[kMaxLayers], ta_b[kMaxLayers], tb_b[kMaxLayers];
   int n_env;                         // envs of this type: B in the loss normalisation
   int env_first;                     // envs are sorted by type
   int rot_idx[4];                    // heading vertices for robot 100
+};
+
+// Batched-controller offsets of one robot type, kept out of RobotDesc (which
+// the fused kernels hold in shared memory) so that the fused kernels' shared
+// footprint does not grow with them.
+struct DenseDesc {
+  long long wt_off[kMaxLayers];      // transposed compact weights
+  int wt_pitch[kMaxLayers];          // row pitch of W_l^T: width[l + 1] padded to 4
+  // FP32: offsets in `tiles` of the pre-split operand tiles of layer l's
+  // forward GEMM (A: inputs of the type's envs, B: W_l) and adjoint GEMM
+  // (A: dZ_l, B: W_l^T)
+  long long ta_f[kMaxLayers], tb_f[kMaxLayers], ta_b[kMaxLayers], tb_b[kMaxLayers];
 };
 
 struct EnvDesc {
@@ -113,6 +119,7 @@ struct MsArgs {
   // [v_total][3], transposed compact weights
   V4<R>* live_x; V4<R>* live_v; R* din; const R* wt;
   R* tiles;                          // FP32: pre-split GEMM operand tiles
+  const DenseDesc* dense;            // per robot type
   // status
   int* status;
   // per-phase clock totals, only written by builds with CLS_PHASE_TIMERS
@@ -222,6 +229,28 @@ __host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, i
          rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads);
 }
 
+// ------------------------------------------------------------ thread groups
+// The substep bodies run on a thread group that owns one env: the whole CTA
+// in the fused segment kernels (BlockGroup) or one warp in the batched
+// controller's step kernels (WarpGroup, several envs per CTA, no CTA-wide
+// barrier anywhere on that path).
+struct BlockGroup {
+  static constexpr bool kWarp = false;
+  __device__ static int rank() { return threadIdx.x; }
+  __device__ static int size() { return blockDim.x; }
+  __device__ static int warp() { return threadIdx.x >> 5; }
+  __device__ static int warps() { return blockDim.x >> 5; }
+  __device__ static void sync() { __syncthreads(); }
+};
+struct WarpGroup {
+  static constexpr bool kWarp = true;
+  __device__ static int rank() { return threadIdx.x & 31; }
+  __device__ static int size() { return 32; }
+  __device__ static int warp() { return 0; }
+  __device__ static int warps() { return 1; }
+  __device__ static void sync() { __syncwarp(); }
+};
+
 // ------------------------------------------------------------- primitives
 
 // Hooke + dashpot impulse of one spring seen from one of its endpoints
@@ -303,13 +332,13 @@ __device__ __forceinline__ void accumulate_incidence(const MsArgs<R>& a, const I
 // not depend on scheduling (the recompute pass reproduces the first pass bit
 // for bit).  Each half-warp prefetches the first incidence of U vertices
 // before computing, so U records per lane are in flight.
-template <typename R>
+template <typename R, typename G = BlockGroup>
 __device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotDesc& rb, int N,
                                                 const V4<R>* xs, const V4<R>* vs, const R* out,
                                                 V4<R>* vinc, V4<R>* rec) {
   constexpr int U = 4;
   const unsigned long long pol = policy_evict_last();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, wid = G::warp(), nw = G::warps();
   const int l16 = lane & 15, half = lane >> 4;
   const int* ptr = a.inc_ptr + rb.ptr_off;
   const int stride = nw * 2;

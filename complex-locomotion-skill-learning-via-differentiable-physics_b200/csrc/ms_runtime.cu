@@ -16,6 +16,11 @@
 #include "cls_profile.cuh"
 #include "ms_dense.cuh"
 
+// threads of the batched controller's step kernels (one CTA per env)
+#ifndef CLS_STEP_THREADS
+#define CLS_STEP_THREADS 128
+#endif
+
 namespace cls {
 
 static thread_local std::string g_create_error;
@@ -211,6 +216,7 @@ class SimImpl final : public SimBase {
     nmax_ = 0;
     int p0max = 4, dmax = 4, amax = 4, omax = 4;
     m_off_.assign(nr, std::vector<long long>(L_));
+    dd_host_.assign(nr, DenseDesc{});
     for (int r = 0; r < nr; ++r) {
       const HostRobot& h = hr_[r];
       RobotDesc& d = rd[r];
@@ -232,13 +238,14 @@ class SimImpl final : public SimBase {
         boff += round4(h.width[l + 1]);
         m_off_[r][l] = moff;
         moff += (long long)h.width[l + 1] * h.full_cols[l];
-        d.wt_pitch[l] = round4(h.width[l + 1]);
-        d.wt_off[l] = wtoff;
-        wtoff += (long long)d.wt_pitch[l] * h.width[l];
+        DenseDesc& dd = dd_host_[r];
+        dd.wt_pitch[l] = round4(h.width[l + 1]);
+        dd.wt_off[l] = wtoff;
+        wtoff += (long long)dd.wt_pitch[l] * h.width[l];
         wtoff = (wtoff + 7) & ~7LL;
         TransSeg tsg{};
-        tsg.w_off = d.w_off[l]; tsg.wt_off = d.wt_off[l];
-        tsg.rows = h.width[l + 1]; tsg.cols = h.width[l]; tsg.pitch = d.pitch[l]; tsg.wt_pitch = d.wt_pitch[l];
+        tsg.w_off = d.w_off[l]; tsg.wt_off = dd.wt_off[l];
+        tsg.rows = h.width[l + 1]; tsg.cols = h.width[l]; tsg.pitch = d.pitch[l]; tsg.wt_pitch = dd.wt_pitch[l];
         tsg.tile0 = n_ttiles_;
         n_ttiles_ += ((tsg.rows + 31) / 32) * ((tsg.cols + 31) / 32);
         tsegs_.push_back(tsg);
@@ -658,6 +665,7 @@ class SimImpl final : public SimBase {
     a.din = d_din_.p;
     a.wt = d_wt_.p;
     a.tiles = d_split_.p;
+    a.dense = d_dense_.p;
     return a;
   }
 
@@ -817,17 +825,18 @@ class SimImpl final : public SimBase {
       ssegs_.clear();
       split_total_ = 0;
       for (int r = 0; r < (int)hr_.size(); ++r) {
-        RobotDesc& d = rd_host_[r];
+        const RobotDesc& d = rd_host_[r];
+        DenseDesc& dd = dd_host_[r];
         const HostRobot& h = hr_[r];
         if (d.n_env == 0) continue;
         for (int l = 0; l < h.n_layers; ++l) {
           const int wi = h.width[l], wo = h.width[l + 1];
-          d.ta_f[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wi);
-          d.ta_b[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wo);
-          d.tb_f[l] = off; off += (long long)umma::split_tiles_floats(wo, kDenseTN, wi);
-          d.tb_b[l] = off; off += (long long)umma::split_tiles_floats(wi, kDenseTN, wo);
+          dd.ta_f[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wi);
+          dd.ta_b[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wo);
+          dd.tb_f[l] = off; off += (long long)umma::split_tiles_floats(wo, kDenseTN, wi);
+          dd.tb_b[l] = off; off += (long long)umma::split_tiles_floats(wi, kDenseTN, wo);
           SplitSeg sg{};
-          sg.w_off = d.w_off[l]; sg.tf_off = d.tb_f[l]; sg.tb_off = d.tb_b[l];
+          sg.w_off = d.w_off[l]; sg.tf_off = dd.tb_f[l]; sg.tb_off = dd.tb_b[l];
           sg.rows = wo; sg.cols = wi; sg.pitch = d.pitch[l]; sg.first = split_total_;
           split_total_ += (long long)wo * wi;
           ssegs_.push_back(sg);
@@ -837,14 +846,18 @@ class SimImpl final : public SimBase {
       CLS_CUDA(cudaMemset(d_split_.p, 0, sizeof(R) * d_split_.n));
       d_ssegs_.alloc(std::max<size_t>(1, ssegs_.size()));
       CLS_CUDA(cudaMemcpy(d_ssegs_.p, ssegs_.data(), sizeof(SplitSeg) * ssegs_.size(), cudaMemcpyHostToDevice));
-      CLS_CUDA(cudaMemcpy(d_robots_.p, rd_host_.data(), sizeof(RobotDesc) * rd_host_.size(), cudaMemcpyHostToDevice));
     }
-    // step kernels: one CTA per env, no controller inside
-    int nv = 0;
-    for (const HostRobot& h : hr_) nv = std::max(nv, h.n_v);
-    dense_threads_ = nv <= 192 ? 128 : (nv <= 768 ? 256 : 512);
-    dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_dmax_, smem_p0max_);
-    drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, dense_threads_);
+    d_dense_.alloc(std::max<size_t>(1, dd_host_.size()));
+    CLS_CUDA(cudaMemcpy(d_dense_.p, dd_host_.data(), sizeof(DenseDesc) * dd_host_.size(), cudaMemcpyHostToDevice));
+    // step kernels: one CTA of CLS_STEP_THREADS threads per env (64 and 128
+    // measured the same on the 4096-env spider); per CTA the fused kernels'
+    // shared-memory carve with the controller buffers sized for the output
+    // layer only (step_args)
+    dense_threads_ = CLS_STEP_THREADS;
+    dfwd_warp_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_);
+    drev_warp_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_);
+    dfwd_smem_ = dfwd_warp_;
+    drev_smem_ = drev_warp_;
     int dev = 0, optin = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -866,16 +879,20 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaStreamSynchronize(stream));
   }
 
-  using DFwdFn = void (*)(MsArgs<R>, int, int, int, int, int, int, int);
-  using DRevFn = void (*)(MsArgs<R>, int, int, int, int, int);
-  DFwdFn dense_fwd_fn() const {
-    return dense_threads_ <= 128 ? ms_step_fwd_kernel<R, 128>
-                                 : (dense_threads_ <= 256 ? ms_step_fwd_kernel<R, 256> : ms_step_fwd_kernel<R, 512>);
+  using DFwdFn = void (*)(MsArgs<R>, int, int, int, int, int, int, int, int);
+  using DRevFn = void (*)(MsArgs<R>, int, int, int, int, int, int);
+  DFwdFn dense_fwd_fn() const { return ms_step_fwd_kernel<R, BlockGroup, CLS_STEP_THREADS>; }
+  DRevFn dense_rev_fn() const { return ms_step_rev_kernel<R, BlockGroup, CLS_STEP_THREADS>; }
+
+  // launch arguments of the step kernels: the per-warp carve sizes the
+  // controller buffers for the output layer only
+  MsArgs<R> step_args(const MsArgs<R>& a) const {
+    MsArgs<R> b = a;
+    b.smem_dmax = smem_omax_;
+    b.n_items = E_;
+    return b;
   }
-  DRevFn dense_rev_fn() const {
-    return dense_threads_ <= 128 ? ms_step_rev_kernel<R, 128>
-                                 : (dense_threads_ <= 256 ? ms_step_rev_kernel<R, 256> : ms_step_rev_kernel<R, 512>);
-  }
+  int step_grid() const { return E_; }
 
   // one layer's GEMM over all batched envs (record slot kslot)
   void ctrl_gemm(const MsArgs<R>& a, bool bwd, int l, int kslot) {
@@ -904,8 +921,8 @@ class SimImpl final : public SimBase {
       const int k_prev = t > t_first ? (first_pass ? (t - 1) % K_ : t - 1 - t_first) : 0;
       const int k_cur = t < t_end ? (first_pass ? t % K_ : t - t_first) : 0;
       timed(kind, [&] {
-        dense_fwd_fn()<<<E_, dense_threads_, dfwd_smem_, stream>>>(a, t, t_first, t_end, mode, src_slot, k_prev,
-                                                                    k_cur);
+        dense_fwd_fn()<<<step_grid(), dense_threads_, dfwd_smem_, stream>>>(
+            step_args(a), t, t_first, t_end, mode, src_slot, k_prev, k_cur, (int)dfwd_warp_);
       });
       if (t < t_end)
         for (int l = 0; l < L_; ++l) ctrl_gemm(a, false, l, k_cur);
@@ -919,7 +936,8 @@ class SimImpl final : public SimBase {
       const int t_post = (t + 1 < t1) ? t + 1 : -1;
       const int t_pre = (t >= t0) ? t : -1;
       timed(PK_REV, [&] {
-        dense_rev_fn()<<<E_, dense_threads_, drev_smem_, stream>>>(a, t_post, t_pre, t0, t1, last ? 1 : 0);
+        dense_rev_fn()<<<step_grid(), dense_threads_, drev_smem_, stream>>>(step_args(a), t_post, t_pre, t0, t1,
+                                                                             last ? 1 : 0, (int)drev_warp_);
       });
       if (t_pre >= 0)
         for (int l = L_ - 1; l >= 0; --l) ctrl_gemm(a, true, l, t_pre - t0);
@@ -1582,7 +1600,7 @@ class SimImpl final : public SimBase {
   // batched controller path
   bool dense_ = false;
   int dense_threads_ = 128, n_ttiles_ = 0;
-  size_t dfwd_smem_ = 0, drev_smem_ = 0;
+  size_t dfwd_smem_ = 0, drev_smem_ = 0, dfwd_warp_ = 0, drev_warp_ = 0;
   long long wt_total_ = 0;
   std::vector<TransSeg> tsegs_;
   std::vector<DenseJob> jobs_h_;
@@ -1591,6 +1609,8 @@ class SimImpl final : public SimBase {
   DevBuf<TransSeg> d_tsegs_;
   DevBuf<V4<R>> d_livex_, d_livev_;
   DevBuf<R> d_din_, d_wt_, d_split_;
+  std::vector<DenseDesc> dd_host_;
+  DevBuf<DenseDesc> d_dense_;
   std::vector<SplitSeg> ssegs_;
   DevBuf<SplitSeg> d_ssegs_;
   long long split_total_ = 0;
