@@ -27,11 +27,6 @@
 
 namespace cls {
 
-// one output tile of one layer's GEMM: envs [m0, m0 + tile) of robot `robot`
-// (env index within the type), outputs [n0, n0 + tile)
-struct DenseJob {
-  int robot, layer, m0, n0;
-};
 
 __host__ __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
@@ -379,14 +374,9 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
   if (threadIdx.x < 32) umma::tmem_relinquish();
 }
 
+
 // pre-split tiles of every layer's W_l (forward B: rows = outputs) and W_l^T
 // (adjoint B: rows = inputs), one thread per weight
-struct SplitSeg {
-  long long w_off, tf_off, tb_off;
-  int rows, cols, pitch;  // W_l: rows = outputs, cols = inputs
-  long long first;        // first weight of this block in the launch
-};
-
 __global__ void __launch_bounds__(256) ms_split_weights_kernel(const float* __restrict__ w, float* tiles,
                                                                const SplitSeg* segs, int n_segs, long long total) {
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < total; q += (long long)gridDim.x * 256) {
@@ -475,11 +465,6 @@ __global__ void __launch_bounds__(256) ms_ctrl_gemm_simt_kernel(MsArgs<R> a, con
 // ------------------------------------------------------- transposed weights
 // W_l^T of every (robot, layer) block listed in segs: WT[i][o] = W[o][i] for
 // i < cols, o < rows; rows of WT padded to wt_pitch (pad entries stay zero).
-struct TransSeg {
-  long long w_off, wt_off;
-  int rows, cols, pitch, wt_pitch;
-  int tile0;  // first 32 x 32 tile of this block in the launch
-};
 
 template <typename R>
 __global__ void __launch_bounds__(256) ms_transpose_weights_kernel(const R* __restrict__ w, R* __restrict__ wt,

@@ -54,6 +54,26 @@ struct DenseDesc {
   long long ta_f[kMaxLayers], tb_f[kMaxLayers], ta_b[kMaxLayers], tb_b[kMaxLayers];
 };
 
+// one output tile of one layer's GEMM: envs [m0, m0 + tile) of robot `robot`
+// (env index within the type), outputs [n0, n0 + tile)
+struct DenseJob {
+  int robot, layer, m0, n0;
+};
+
+// one (robot, layer) block of the pre-split weight packing
+struct SplitSeg {
+  long long w_off, tf_off, tb_off;
+  int rows, cols, pitch;  // W_l: rows = outputs, cols = inputs
+  long long first;        // first weight of this block in the launch
+};
+
+// one (robot, layer) block of the W_l^T transpose (FP64 batched path)
+struct TransSeg {
+  long long w_off, wt_off;
+  int rows, cols, pitch, wt_pitch;
+  int tile0;  // first 32 x 32 tile of this block in the launch
+};
+
 struct EnvDesc {
   int robot;
   int v_off;                         // vertex offset in packed state arrays

@@ -14,7 +14,8 @@
 
 #include "../../include/cls_b200.h"
 #include "cls_profile.cuh"
-#include "ms_dense.cuh"
+#include "ms_dense_host.h"
+#include "ms_segment.cuh"
 
 // threads of the batched controller's step kernels (one CTA per env)
 #ifndef CLS_STEP_THREADS
@@ -789,7 +790,7 @@ class SimImpl final : public SimBase {
 
   void enable_dense() {
     constexpr bool f32 = std::is_same<R, float>::value;
-    const int tm = f32 ? umma::TM : kSimtTile, tn = f32 ? kDenseTN : kSimtTile;
+    const int tm = DenseLaunch<R>::tile_m(), tn = DenseLaunch<R>::tile_n();
     jobs_h_.clear();
     for (int l = 0; l < L_; ++l) {
       jf_off_[l] = (int)jobs_h_.size();
@@ -831,10 +832,10 @@ class SimImpl final : public SimBase {
         if (d.n_env == 0) continue;
         for (int l = 0; l < h.n_layers; ++l) {
           const int wi = h.width[l], wo = h.width[l + 1];
-          dd.ta_f[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wi);
-          dd.ta_b[l] = off; off += (long long)umma::split_tiles_floats(d.n_env, umma::TM, wo);
-          dd.tb_f[l] = off; off += (long long)umma::split_tiles_floats(wo, kDenseTN, wi);
-          dd.tb_b[l] = off; off += (long long)umma::split_tiles_floats(wi, kDenseTN, wo);
+          dd.ta_f[l] = off; off += DenseLaunch<R>::split_floats(d.n_env, tm, wi);
+          dd.ta_b[l] = off; off += DenseLaunch<R>::split_floats(d.n_env, tm, wo);
+          dd.tb_f[l] = off; off += DenseLaunch<R>::split_floats(wo, tn, wi);
+          dd.tb_b[l] = off; off += DenseLaunch<R>::split_floats(wi, tn, wo);
           SplitSeg sg{};
           sg.w_off = d.w_off[l]; sg.tf_off = dd.tb_f[l]; sg.tb_off = dd.tb_b[l];
           sg.rows = wo; sg.cols = wi; sg.pitch = d.pitch[l]; sg.first = split_total_;
@@ -861,28 +862,13 @@ class SimImpl final : public SimBase {
     int dev = 0, optin = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fa{}, ra{};
-    CLS_CUDA(cudaFuncGetAttributes(&fa, dense_fwd_fn()));
-    CLS_CUDA(cudaFuncGetAttributes(&ra, dense_rev_fn()));
-    CLS_REQUIRE(dfwd_smem_ + fa.sharedSizeBytes <= (size_t)optin && drev_smem_ + ra.sharedSizeBytes <= (size_t)optin,
+    size_t fwd_static = 0, rev_static = 0;
+    CLS_CUDA(DenseLaunch<R>::setup(dense_threads_, &fwd_static, &rev_static, optin));
+    CLS_REQUIRE(dfwd_smem_ + fwd_static <= (size_t)optin && drev_smem_ + rev_static <= (size_t)optin,
                 "robot too large for the batched controller's step kernels");
-    CLS_CUDA(cudaFuncSetAttribute(dense_fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)optin - fa.sharedSizeBytes)));
-    CLS_CUDA(cudaFuncSetAttribute(dense_rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)optin - ra.sharedSizeBytes)));
-    if constexpr (f32) {
-      const int sm = (int)umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes;
-      CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-      CLS_CUDA(cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    }
     transpose_weights();
     CLS_CUDA(cudaStreamSynchronize(stream));
   }
-
-  using DFwdFn = void (*)(MsArgs<R>, int, int, int, int, int, int, int, int);
-  using DRevFn = void (*)(MsArgs<R>, int, int, int, int, int, int);
-  DFwdFn dense_fwd_fn() const { return ms_step_fwd_kernel<R, BlockGroup, CLS_STEP_THREADS>; }
-  DRevFn dense_rev_fn() const { return ms_step_rev_kernel<R, BlockGroup, CLS_STEP_THREADS>; }
 
   // launch arguments of the step kernels: the per-warp carve sizes the
   // controller buffers for the output layer only
@@ -899,16 +885,7 @@ class SimImpl final : public SimBase {
     const int cnt = bwd ? jb_cnt_[l] : jf_cnt_[l];
     if (cnt == 0) return;
     const DenseJob* jobs = d_jobs_.p + (bwd ? jb_off_[l] : jf_off_[l]);
-    timed(bwd ? PK_CGEMM_ADJ : PK_CGEMM, [&] {
-      if constexpr (std::is_same<R, float>::value) {
-        const size_t sm = umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes;
-        if (bwd) ms_ctrl_gemm_tc_kernel<1><<<cnt, umma::kBulkThreads, sm, stream>>>(a, jobs, kslot);
-        else ms_ctrl_gemm_tc_kernel<0><<<cnt, umma::kBulkThreads, sm, stream>>>(a, jobs, kslot);
-      } else {
-        if (bwd) ms_ctrl_gemm_simt_kernel<R, 1><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
-        else ms_ctrl_gemm_simt_kernel<R, 0><<<cnt, 256, 0, stream>>>(a, jobs, kslot);
-      }
-    });
+    timed(bwd ? PK_CGEMM_ADJ : PK_CGEMM, [&] { DenseLaunch<R>::gemm(a, bwd, cnt, jobs, kslot, stream); });
   }
 
   // forward over [t_first, t_end): a step launch per substep boundary and the
@@ -921,8 +898,8 @@ class SimImpl final : public SimBase {
       const int k_prev = t > t_first ? (first_pass ? (t - 1) % K_ : t - 1 - t_first) : 0;
       const int k_cur = t < t_end ? (first_pass ? t % K_ : t - t_first) : 0;
       timed(kind, [&] {
-        dense_fwd_fn()<<<step_grid(), dense_threads_, dfwd_smem_, stream>>>(
-            step_args(a), t, t_first, t_end, mode, src_slot, k_prev, k_cur, (int)dfwd_warp_);
+        DenseLaunch<R>::step_fwd(step_args(a), step_grid(), dense_threads_, dfwd_smem_, stream, t, t_first, t_end, mode,
+                                 src_slot, k_prev, k_cur, (int)dfwd_warp_);
       });
       if (t < t_end)
         for (int l = 0; l < L_; ++l) ctrl_gemm(a, false, l, k_cur);
@@ -936,8 +913,8 @@ class SimImpl final : public SimBase {
       const int t_post = (t + 1 < t1) ? t + 1 : -1;
       const int t_pre = (t >= t0) ? t : -1;
       timed(PK_REV, [&] {
-        dense_rev_fn()<<<step_grid(), dense_threads_, drev_smem_, stream>>>(step_args(a), t_post, t_pre, t0, t1,
-                                                                             last ? 1 : 0, (int)drev_warp_);
+        DenseLaunch<R>::step_rev(step_args(a), step_grid(), dense_threads_, drev_smem_, stream, t_post, t_pre, t0, t1,
+                                 last ? 1 : 0, (int)drev_warp_);
       });
       if (t_pre >= 0)
         for (int l = L_ - 1; l >= 0; --l) ctrl_gemm(a, true, l, t_pre - t0);
@@ -1050,20 +1027,11 @@ class SimImpl final : public SimBase {
   // once the batched path has been enabled)
   void transpose_weights() {
     if (!d_wt_.p || n_ttiles_ == 0) return;
-    if constexpr (std::is_same<R, float>::value) {
-      // FP32: the GEMMs read W_l and W_l^T as pre-split tiles
-      if (split_total_ == 0) return;
-      const int blocks = (int)std::min<long long>(4096, (split_total_ + 255) / 256);
-      timed(PK_ADAM, [&] {
-        ms_split_weights_kernel<<<blocks, 256, 0, stream>>>(d_w_.p, d_split_.p, d_ssegs_.p, (int)ssegs_.size(),
-                                                            split_total_);
-      });
-    } else {
-      timed(PK_ADAM, [&] {
-        ms_transpose_weights_kernel<R><<<n_ttiles_, 256, 0, stream>>>(d_w_.p, d_wt_.p, d_tsegs_.p,
-                                                                      (int)tsegs_.size());
-      });
-    }
+    // FP32: the GEMMs read W_l and W_l^T as pre-split tiles; FP64: W_l^T
+    timed(PK_ADAM, [&] {
+      DenseLaunch<R>::pack_weights(d_w_.p, d_wt_.p, d_split_.p, d_tsegs_.p, (int)tsegs_.size(), n_ttiles_,
+                                   d_ssegs_.p, (int)ssegs_.size(), split_total_, stream);
+    });
   }
 
   void adam(int iter, double* tns) override {
