@@ -40,6 +40,7 @@ cudaError_t DenseLaunch<R>::setup(int threads, size_t* fwd_static, size_t* rev_s
     const int sm = (int)umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes;
     if (e == cudaSuccess) e = cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(ms_ctrl_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(ms_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   }
   return e;
 }
@@ -81,6 +82,18 @@ void DenseLaunch<R>::pack_weights(const R* w, R* wt, R* tiles, const TransSeg* t
   } else {
     if (n_ttiles == 0) return;
     ms_transpose_weights_kernel<R><<<n_ttiles, 256, 0, s>>>(w, wt, tsegs, n_tsegs);
+  }
+}
+
+template <typename R>
+void DenseLaunch<R>::wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int nslots, const WgTrans* trans,
+                           const WgCol* cols, int n_jobs, const WgJob* jobs, R* gw, R* gb, cudaStream_t s) {
+  if constexpr (std::is_same<R, float>::value) {
+    if (n_cols > 0 && nslots > 0)
+      ms_wgrad_transpose_kernel<<<dim3(grid_x, n_cols, nslots), 256, 0, s>>>(a, trans, cols);
+    if (n_jobs > 0)
+      ms_wgrad_tc_kernel<<<n_jobs, umma::kBulkThreads, umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes, s>>>(
+          a, jobs, nslots, gw, gb);
   }
 }
 

@@ -375,6 +375,96 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
 }
 
 
+// --------------------------------------------- weight-gradient products (FP32)
+// dW_l[o][i] = sum over the segment's (slot, env) rows of dZ_l[o] A_l[i] and
+// db_l[o] = sum dZ_l[o]: a contraction over ~K x envs rows, run as the bulk
+// tensor-core tile with M = outputs, N = inputs + 1 (a row of ones turns the
+// bias gradient into the last column) and K = the rows.  First the FP32
+// records are transposed into pre-split K-major tiles: one CTA moves 32 envs
+// x 32 columns of one record slot through shared memory, reading env rows
+// (128 bytes each) and writing each column's 32 K values as one 128-byte
+// line per precision part.
+__global__ void __launch_bounds__(256)
+ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* cols) {
+  __shared__ float tile[32][33];
+  const WgCol wc = cols[blockIdx.y];
+  const WgTrans jb = jobs[wc.job];
+  const RobotDesc& rb = a.robots[jb.robot];
+  const DenseDesc& dd = a.dense[jb.robot];
+  const EnvDesc& e0 = a.envs[rb.env_first];
+  const int kk = blockIdx.z, j0 = blockIdx.x * 32;
+  if (j0 >= dd.nep) return;
+  const int l = jb.layer, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int rows = jb.cols + (jb.kind == 2 ? 0 : 1);
+  const float* src;
+  int stride;
+  if (jb.kind == 0) {
+    stride = rb.pitch[0];
+    src = a.rec_in + (size_t)kk * a.in_total + e0.in_off;
+  } else if (jb.kind == 1) {
+    stride = pad4(rb.width[l]);
+    src = a.rec_z + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + e0.z_off[l - 1];
+  } else {
+    stride = pad4(rb.width[l + 1]);
+    src = a.rec_dz + a.z_base[l] + (size_t)kk * a.z_total[l] + e0.z_off[l];
+  }
+  const float* bias = jb.kind == 1 ? a.bias + rb.b_off[l - 1] : nullptr;
+  for (int r = ty; r < 32; r += 8) {
+    const int j = j0 + r, c = wc.c0 + tx;
+    float v = 0.f;
+    if (j < rb.n_env) {
+      if (c < jb.cols) {
+        v = src[(size_t)j * stride + c];
+        if (bias) v = act_f<float>(a.act_hidden, v + bias[c]);
+      } else if (c == jb.cols && jb.kind != 2) {
+        v = 1.f;
+      }
+    }
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  const umma::SplitTiles st{a.wtiles + (jb.kind == 2 ? dd.tw_d[l] : dd.tw_a[l]), jb.kind == 2 ? umma::TM : kDenseTN,
+                            dd.nkt_w};
+  for (int r = ty; r < 32; r += 8) {
+    const int c = wc.c0 + r;
+    if (c < rows) st.store(c, kk * dd.nep + j0 + tx, tile[tx][r]);
+  }
+}
+
+// one 128-output x 64-input tile of one layer's weight gradient over K split
+// `split` of the segment's nslots x nep rows; atomic adds (several splits
+// and segments add into one gradient)
+__global__ void __launch_bounds__(umma::kBulkThreads)
+ms_wgrad_tc_kernel(MsArgs<float> a, const WgJob* jobs, int nslots, float* gw, float* gb) {
+  extern __shared__ __align__(1024) float smem_f[];
+  __shared__ umma::BulkShared bs;
+  const WgJob jb = jobs[blockIdx.x];
+  const RobotDesc& rb = a.robots[jb.robot];
+  const DenseDesc& dd = a.dense[jb.robot];
+  const int l = jb.layer;
+  const int total = nslots * dd.nep / 32;
+  const int k0 = (int)((long long)total * jb.split / jb.nsplit);
+  const int k1 = (int)((long long)total * (jb.split + 1) / jb.nsplit);
+  const float* ab = a.wtiles + dd.tw_d[l] + ((size_t)(jb.o0 / umma::TM) * dd.nkt_w + k0) * (64 * umma::TM);
+  const float* bb = a.wtiles + dd.tw_a[l] + ((size_t)(jb.i0 / kDenseTN) * dd.nkt_w + k0) * (64 * kDenseTN);
+  const int nout = rb.width[l + 1], nin = rb.width[l], pitch = rb.pitch[l];
+  float* W = gw + rb.w_off[l];
+  float* B = gb + rb.b_off[l];
+  const bool ok = umma::tile_gemm_bulk<kDenseTN, kBulkStages>(
+      smem_f, bs, ab, bb, k1 - k0, [&](const float* cs, int ld) {
+        for (int q = threadIdx.x; q < umma::TM * kDenseTN; q += blockDim.x) {
+          const int i = q / kDenseTN, j = q % kDenseTN;
+          const int o = jb.o0 + i, c = jb.i0 + j;
+          if (o >= nout || c > nin) continue;
+          const float v = cs[i * ld + j];
+          if (c < nin) atomicAdd(W + (size_t)o * pitch + c, v);
+          else atomicAdd(B + o, v);
+        }
+      });
+  if (!ok && threadIdx.x == 0) atomicOr(a.status, ERR_TIMEOUT);
+  if (threadIdx.x < 32) umma::tmem_relinquish();
+}
+
 // pre-split tiles of every layer's W_l (forward B: rows = outputs) and W_l^T
 // (adjoint B: rows = inputs), one thread per weight
 __global__ void __launch_bounds__(256) ms_split_weights_kernel(const float* __restrict__ w, float* tiles,

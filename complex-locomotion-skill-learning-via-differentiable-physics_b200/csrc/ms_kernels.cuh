@@ -52,6 +52,29 @@ struct DenseDesc {
   // forward GEMM (A: inputs of the type's envs, B: W_l) and adjoint GEMM
   // (A: dZ_l, B: W_l^T)
   long long ta_f[kMaxLayers], tb_f[kMaxLayers], ta_b[kMaxLayers], tb_b[kMaxLayers];
+  // FP32 weight-gradient products of a segment, offsets in `wtiles`: dZ_l^T
+  // (rows = outputs, tile 128) and A_l^T plus a row of ones (rows = inputs + 1,
+  // tile 64), K = (record slot, env) with the envs padded to nep (a multiple
+  // of 32) and nkt_w K blocks of 32 allocated
+  long long tw_d[kMaxLayers], tw_a[kMaxLayers];
+  int nep, nkt_w;
+};
+
+// one (robot, layer, operand) source of the per-segment transposes for the
+// weight-gradient products
+struct WgTrans {
+  int robot, layer;
+  int kind;   // 0: inputs (rec_in), 1: act(rec_z of layer - 1 + bias), 2: dZ (rec_dz)
+  int cols;   // valid columns; kinds 0/1 add a row of ones at `cols`
+};
+// column tile c0 .. c0 + 31 of transpose job `job`
+struct WgCol {
+  int job, c0;
+};
+// one output tile (outputs o0 .., inputs i0 ..) of layer l's weight gradient,
+// K split `split` of `nsplit`
+struct WgJob {
+  int robot, layer, o0, i0, split, nsplit;
 };
 
 // one output tile of one layer's GEMM: envs [m0, m0 + tile) of robot `robot`
@@ -139,6 +162,7 @@ struct MsArgs {
   // [v_total][3], transposed compact weights
   V4<R>* live_x; V4<R>* live_v; R* din; const R* wt;
   R* tiles;                          // FP32: pre-split GEMM operand tiles
+  R* wtiles;                         // FP32: weight-gradient operand tiles (one segment)
   const DenseDesc* dense;            // per robot type
   // status
   int* status;

@@ -667,6 +667,7 @@ class SimImpl final : public SimBase {
     a.wt = d_wt_.p;
     a.tiles = d_split_.p;
     a.dense = d_dense_.p;
+    a.wtiles = d_wsplit_.p;
     return a;
   }
 
@@ -845,6 +846,54 @@ class SimImpl final : public SimBase {
       }
       d_split_.alloc(std::max<long long>(1, off));
       CLS_CUDA(cudaMemset(d_split_.p, 0, sizeof(R) * d_split_.n));
+      // weight-gradient operands of one segment (K = record slots x envs
+      // padded to 32) and the per-segment transpose / tile lists
+      long long woff = 0;
+      wg_trans_.clear(); wg_cols_.clear(); wg_jobs_.clear();
+      wg_grid_x_ = 0;
+      int n_tiles = 0;
+      for (int r = 0; r < (int)hr_.size(); ++r) {
+        const RobotDesc& d = rd_host_[r];
+        DenseDesc& dd = dd_host_[r];
+        const HostRobot& h = hr_[r];
+        if (d.n_env == 0) continue;
+        dd.nep = (d.n_env + 31) & ~31;
+        dd.nkt_w = K_ * dd.nep / 32;
+        wg_grid_x_ = std::max(wg_grid_x_, dd.nep / 32);
+        for (int l = 0; l < h.n_layers; ++l) {
+          const int wi = h.width[l], wo = h.width[l + 1];
+          dd.tw_d[l] = woff; woff += DenseLaunch<R>::split_floats(wo, tm, K_ * dd.nep);
+          dd.tw_a[l] = woff; woff += DenseLaunch<R>::split_floats(wi + 1, tn, K_ * dd.nep);
+          const WgTrans ta{r, l, l == 0 ? 0 : 1, wi}, td{r, l, 2, wo};
+          for (const WgTrans& tr : {ta, td}) {
+            const int job = (int)wg_trans_.size();
+            wg_trans_.push_back(tr);
+            const int rows = tr.cols + (tr.kind == 2 ? 0 : 1);
+            for (int c0 = 0; c0 < rows; c0 += 32) wg_cols_.push_back({job, c0});
+          }
+          n_tiles += ((wo + tm - 1) / tm) * ((wi + 1 + tn - 1) / tn);
+        }
+      }
+      // K splits: about two CTAs per SM, at least 8 K blocks each
+      int max_kt = 0;
+      for (const DenseDesc& dd : dd_host_) max_kt = std::max(max_kt, dd.nkt_w);
+      const int nsplit = std::max(1, std::min(std::max(1, max_kt / 8), (2 * n_sm_ + n_tiles - 1) / std::max(1, n_tiles)));
+      for (int r = 0; r < (int)hr_.size(); ++r) {
+        if (rd_host_[r].n_env == 0) continue;
+        const HostRobot& h = hr_[r];
+        for (int l = 0; l < h.n_layers; ++l)
+          for (int o0 = 0; o0 < h.width[l + 1]; o0 += tm)
+            for (int i0 = 0; i0 < h.width[l] + 1; i0 += tn)
+              for (int sp = 0; sp < nsplit; ++sp) wg_jobs_.push_back({r, l, o0, i0, sp, nsplit});
+      }
+      d_wsplit_.alloc(std::max<long long>(1, woff));
+      CLS_CUDA(cudaMemset(d_wsplit_.p, 0, sizeof(R) * d_wsplit_.n));
+      d_wg_trans_.alloc(std::max<size_t>(1, wg_trans_.size()));
+      d_wg_cols_.alloc(std::max<size_t>(1, wg_cols_.size()));
+      d_wg_jobs_.alloc(std::max<size_t>(1, wg_jobs_.size()));
+      CLS_CUDA(cudaMemcpy(d_wg_trans_.p, wg_trans_.data(), sizeof(WgTrans) * wg_trans_.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_wg_cols_.p, wg_cols_.data(), sizeof(WgCol) * wg_cols_.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_wg_jobs_.p, wg_jobs_.data(), sizeof(WgJob) * wg_jobs_.size(), cudaMemcpyHostToDevice));
       d_ssegs_.alloc(std::max<size_t>(1, ssegs_.size()));
       CLS_CUDA(cudaMemcpy(d_ssegs_.p, ssegs_.data(), sizeof(SplitSeg) * ssegs_.size(), cudaMemcpyHostToDevice));
     }
@@ -986,11 +1035,18 @@ class SimImpl final : public SimBase {
           });
         });
       }
-      if (!tiles_host_.empty())
+      if (dense_ && !per_env && !wg_jobs_.empty()) {
+        // FP32 batched path: record transposes + tensor-core tiles
+        timed(PK_WGRAD, [&] {
+          DenseLaunch<R>::wgrad(a, wg_grid_x_, (int)wg_cols_.size(), t1 - t0, d_wg_trans_.p, d_wg_cols_.p,
+                                (int)wg_jobs_.size(), d_wg_jobs_.p, d_gw_.p, d_gb_.p, stream);
+        });
+      } else if (!tiles_host_.empty()) {
         timed(PK_WGRAD, [&] {
           ms_wgrad_kernel<R><<<(int)tiles_host_.size(), 256, 0, stream>>>(a, d_tiles_.p, t1 - t0,
                                                                            d_gw_.p, d_gb_.p);
         });
+      }
     }
     CLS_CUDA(cudaGetLastError());
     bwd_done_ = true;
@@ -1579,6 +1635,15 @@ class SimImpl final : public SimBase {
   DevBuf<R> d_din_, d_wt_, d_split_;
   std::vector<DenseDesc> dd_host_;
   DevBuf<DenseDesc> d_dense_;
+  // FP32 batched path: tensor-core weight-gradient products
+  DevBuf<R> d_wsplit_;
+  std::vector<WgTrans> wg_trans_;
+  std::vector<WgCol> wg_cols_;
+  std::vector<WgJob> wg_jobs_;
+  DevBuf<WgTrans> d_wg_trans_;
+  DevBuf<WgCol> d_wg_cols_;
+  DevBuf<WgJob> d_wg_jobs_;
+  int wg_grid_x_ = 0;
   std::vector<SplitSeg> ssegs_;
   DevBuf<SplitSeg> d_ssegs_;
   long long split_total_ = 0;

@@ -1,23 +1,16 @@
-// umma_gemm.cuh -- one 128 x TN output tile of C(i, j) = sum_k A(k, i) B(k, j)
-// on the 5th-generation tensor cores (tcgen05.mma, kind::tf32) with FP32
-// operands split into TF32 high and low parts ("3xTF32": a_hi b_hi + a_hi b_lo
-// + a_lo b_hi, about FP32 accuracy) and the FP32 accumulator in tensor memory.
-//
-// A CTA of 256 threads stages TK = 32 K-rows of both operands at a time into
-// shared memory in the canonical no-swizzle K-major layout of the MMA: core
-// matrices of 8 rows x 16 bytes, element (row r, k) of a tile with R rows at
-// float offset (k / 4) * 4R + r * 4 + k % 4, so the core matrices of one
-// 8-row group are 128 B apart (stride byte offset) and those of consecutive
-// 4-wide K chunks 16 R bytes apart (leading byte offset).  The operands are
-// converted to the TF32 pair while staging; one thread issues the MMAs and
-// commits them to an mbarrier; the warps then read the accumulator rows
-// (lane i = row i) back with tcgen05.ld.  Descriptor and instruction-
-// descriptor bit layouts follow the PTX ISA's tcgen05 matrix descriptors (as
-// CUTLASS's cute/arch/mma_sm100_desc.hpp encodes them).
+// umma_gemm.cuh -- tcgen05 (5th-generation tensor core) building blocks for
+// FP32-accurate GEMM tiles: C(i, j) = sum_k A(i, k) B(j, k) with FP32 operands
+// split into TF32 high and low parts ("3xTF32": a_lo b_hi + a_hi b_lo +
+// a_hi b_hi, about FP32 accuracy) and the FP32 accumulator in tensor memory.
+// Operands arrive pre-split in global memory in the MMA's 128-byte-swizzled
+// K-major layout (SplitTiles) and are streamed into shared memory with bulk
+// copies completing on mbarriers (tile_gemm_bulk).  Descriptor and
+// instruction-descriptor bit layouts follow the PTX ISA's tcgen05 matrix
+// descriptors (as CUTLASS's cute/arch/mma_sm100_desc.hpp encodes them).
 //
 // Tensor memory: TN columns rounded up to a power of two (>= 32).  Callers
-// keep TN <= 128 and at least TN * 456 bytes of shared memory per CTA, so
-// the CTAs that fit on one SM never ask for more than its 512 columns (an
+// keep TN <= 128 and at least TN * 456 bytes of shared memory per CTA, so the
+// CTAs that fit on one SM never ask for more than its 512 columns (an
 // allocation that cannot be satisfied would wait).
 //
 // Every wait is bounded: on a timeout the tile reports failure and returns
@@ -29,19 +22,8 @@ namespace cls {
 namespace umma {
 
 constexpr int TM = 128;        // output rows per tile (MMA M)
-constexpr int TK = 32;         // K rows staged per round (4 MMA K-steps of 8)
-constexpr int kThreads = 256;  // 8 warps; warp w reads accumulator lanes [32 (w % 4), +32)
+constexpr int TK = 32;         // K values per stage (4 MMA K-steps of 8)
 constexpr unsigned kWaitLimit = 1u << 22;
-
-template <int TN>
-struct Shape {
-  static_assert(TN % 16 == 0 && TN >= 16 && TN <= 128, "MMA N: multiple of 16 in [16, 128]");
-  static constexpr int kCols = TN <= 32 ? 32 : (TN <= 64 ? 64 : 128);  // tensor-memory columns
-  static constexpr int kPartFloats = TK * (TM + TN);                    // one precision part of A and B
-  static constexpr size_t kStageBytes = 2 * 2 * kPartFloats * sizeof(float);  // 2 buffers x (hi, lo)
-  static constexpr size_t kSmemBytes =
-      kStageBytes > (size_t)kCols * 456 ? kStageBytes : (size_t)kCols * 456;
-};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -53,20 +35,11 @@ __device__ __forceinline__ uint32_t tf32_bits(float x) {
   return r;
 }
 
-// shared-memory matrix descriptor: start address, leading / stride byte
-// offsets (16-byte units), descriptor version 1, base offset 0, no swizzle
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
-
-// the same for the 128-byte swizzled K-major layout: rows of 128 bytes, 8-row
-// atoms of 1024 bytes (stride byte offset), leading byte offset unused (1),
-// layout type 2; a K step inside the atom advances the start address
+// shared-memory matrix descriptor of the 128-byte swizzled K-major layout:
+// start address (16-byte units), rows of 128 bytes, 8-row atoms of 1024 bytes
+// (stride byte offset), leading byte offset unused (1), descriptor version 1,
+// base offset 0, layout type 2; a K step inside the atom advances the start
+// address
 __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   uint64_t d = 0;
   d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
@@ -160,13 +133,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
   for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-// Shared state of one tile (static shared memory of the calling kernel).
-struct TileShared {
-  uint64_t mbar[2];  // one per stage buffer
-  uint32_t tmem_base;
-  int timed_out;
-};
-
 __device__ __forceinline__ void split4(const float4& v4, uint4& hi, uint4& lo) {
   const float v[4] = {v4.x, v4.y, v4.z, v4.w};
   uint32_t* h = &hi.x;
@@ -176,176 +142,6 @@ __device__ __forceinline__ void split4(const float4& v4, uint4& hi, uint4& lo) {
     h[u] = tf32_bits(v[u]);
     l[u] = tf32_bits(v[u] - __uint_as_float(h[u]));
   }
-}
-
-// Staging map of one round: unit u = it * kThreads + tid covers 4
-// consecutive K values (chunk c) of one operand row.  The 32 lanes of a warp
-// take rows 8 rg .. 8 rg + 7 (p = lane % 8) and chunks 4 h .. 4 h + 3
-// (q = lane / 8), so a warp reads 64 contiguous bytes of each of 8 rows (whole
-// 32-byte sectors) and each quarter-warp stores 8 consecutive 16-byte core
-// rows to shared memory (no bank conflicts).
-struct Unit {
-  int row, c;
-};
-__device__ __forceinline__ Unit unit_of(int u) {
-  const int p = u & 7, q = (u >> 3) & 3, combo = u >> 5;
-  Unit r;
-  r.row = 8 * (combo >> 1) + p;
-  r.c = 4 * (combo & 1) + q;
-  return r;
-}
-
-// Accumulates C(i, j) = sum_{k in [k_lo, k_hi)} A(k, i) B(k, j) for the tile
-// rows i < TM and columns j < TN, and hands each element with i < m_valid,
-// j < n_valid to store(i, j, value).  load_a(k, i) / load_b(k, j) return the
-// four operands at k .. k + 3 (k a multiple of 4) as a float4 and are called
-// for k < k_hi, i < m_valid, j < n_valid only; k_lo and k_hi are multiples of
-// 4 (callers pad operand rows with zeros to a multiple of 4).
-// `smem`: Shape<TN>::kSmemBytes, 16-byte aligned.  All kThreads threads of the
-// CTA call it.  Two stage buffers in shared memory and two rounds of operands
-// in registers: the global loads of round r + 2 are issued right after the
-// MMAs of round r, so a load has a whole round to arrive.  Returns false on a
-// timeout (nothing is stored then).
-template <int TN, typename LoadA, typename LoadB, typename Store>
-__device__ bool tile_gemm(float* smem, TileShared& ts, int k_lo, int k_hi, int m_valid, int n_valid,
-                          LoadA load_a, LoadB load_b, Store store) {
-  using S = Shape<TN>;
-  constexpr int UA = TM * (TK / 4) / kThreads;                    // A units per thread per round
-  constexpr int UB = (TN * (TK / 4) + kThreads - 1) / kThreads;   // B units per thread per round
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t mbar0 = smem_u32(&ts.mbar[0]);
-  if (warp == 0) tmem_alloc(smem_u32(&ts.tmem_base), S::kCols);
-  if (tid == 0) {
-    mbar_init(mbar0, 1);
-    mbar_init(mbar0 + 8, 1);
-    ts.timed_out = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = ts.tmem_base;
-  constexpr uint32_t idesc = instr_desc_tf32(TM, TN);
-  float4 ra0[UA], rb0[UB], ra1[UA], rb1[UB];
-  auto fetch = [&](int k0, float4 (&ra)[UA], float4 (&rb)[UB]) {
-#pragma unroll
-    for (int it = 0; it < UA; ++it) {
-      const Unit w = unit_of(it * kThreads + tid);
-      const int kb = k0 + 4 * w.c;
-      ra[it] = (kb < k_hi && w.row < m_valid) ? load_a(kb, w.row) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int it = 0; it < UB; ++it) {
-      const int uu = it * kThreads + tid;
-      const Unit w = unit_of(uu);
-      const int kb = k0 + 4 * w.c;
-      rb[it] = (uu < TN * (TK / 4) && kb < k_hi && w.row < n_valid) ? load_b(kb, w.row)
-                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  };
-  // one round: stage the registers into buffer round & 1, issue its MMAs
-  auto body = [&](int round, float4 (&ra)[UA], float4 (&rb)[UB]) -> bool {
-    const int buf = round & 1;
-    float* a_hi = smem + buf * 2 * S::kPartFloats;
-    float* b_hi = a_hi + TK * TM;
-    float* a_lo = a_hi + S::kPartFloats;
-    float* b_lo = a_lo + TK * TM;
-    // the MMAs of round - 2 read this buffer: wait for their commit
-    if (round >= 2 && !mbar_wait(mbar0 + 8 * buf, ((round - 2) >> 1) & 1)) ts.timed_out = 1;
-#pragma unroll
-    for (int it = 0; it < UA; ++it) {
-      const Unit w = unit_of(it * kThreads + tid);
-      uint4 hi, lo;
-      split4(ra[it], hi, lo);
-      *reinterpret_cast<uint4*>(a_hi + w.c * 4 * TM + w.row * 4) = hi;
-      *reinterpret_cast<uint4*>(a_lo + w.c * 4 * TM + w.row * 4) = lo;
-    }
-#pragma unroll
-    for (int it = 0; it < UB; ++it) {
-      const int uu = it * kThreads + tid;
-      if (uu < TN * (TK / 4)) {
-        const Unit w = unit_of(uu);
-        uint4 hi, lo;
-        split4(rb[it], hi, lo);
-        *reinterpret_cast<uint4*>(b_hi + w.c * 4 * TN + w.row * 4) = hi;
-        *reinterpret_cast<uint4*>(b_lo + w.c * 4 * TN + w.row * 4) = lo;
-      }
-    }
-    fence_async_shared();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (ts.timed_out) return false;
-    if (tid == 0) {
-#pragma unroll
-      for (int s = 0; s < TK / 8; ++s) {
-        // K step s covers chunks 2s and 2s + 1 (leading byte offset: one chunk)
-        const uint64_t dah = smem_desc(smem_u32(a_hi + 2 * s * 4 * TM), 16 * TM, 128);
-        const uint64_t dal = smem_desc(smem_u32(a_lo + 2 * s * 4 * TM), 16 * TM, 128);
-        const uint64_t dbh = smem_desc(smem_u32(b_hi + 2 * s * 4 * TN), 16 * TN, 128);
-        const uint64_t dbl = smem_desc(smem_u32(b_lo + 2 * s * 4 * TN), 16 * TN, 128);
-        mma_tf32(tmem, dal, dbh, idesc, (round == 0 && s == 0) ? 0u : 1u);
-        mma_tf32(tmem, dah, dbl, idesc, 1u);
-        mma_tf32(tmem, dah, dbh, idesc, 1u);
-      }
-      mma_commit(mbar0 + 8 * buf);
-    }
-    return true;
-  };
-  int round = 0;
-  bool ok = true;
-  if (k_lo < k_hi) fetch(k_lo, ra0, rb0);
-  if (k_lo + TK < k_hi) fetch(k_lo + TK, ra1, rb1);
-  for (int k0 = k_lo; k0 < k_hi; k0 += 2 * TK) {
-    if (!(ok = body(round++, ra0, rb0))) break;
-    if (k0 + 2 * TK < k_hi) fetch(k0 + 2 * TK, ra0, rb0);
-    if (k0 + TK >= k_hi) break;
-    if (!(ok = body(round++, ra1, rb1))) break;
-    if (k0 + 3 * TK < k_hi) fetch(k0 + 3 * TK, ra1, rb1);
-  }
-  if (ok && round > 0) {
-    // the last commit of each buffer: every MMA of the tile has completed and
-    // no arrive is still on its way to either barrier
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const int uses = (round - b + 1) >> 1;
-      if (uses > 0 && !mbar_wait(mbar0 + 8 * b, (uses - 1) & 1)) ts.timed_out = 1;
-    }
-    tc_fence_after();
-    __syncthreads();
-    ok = !ts.timed_out;
-  }
-  // epilogue: warp w reads accumulator lanes 32 (w % 4) ..; warps w and w + 4
-  // take the two halves of the columns
-  constexpr int kHalves = kThreads / 128;
-  constexpr int kColsPer = TN / kHalves;
-  static_assert(kColsPer % 8 == 0, "epilogue reads 8 columns at a time");
-  const int quad = warp & 3, half = warp >> 2;
-  const int i = quad * 32 + lane;
-  if (ok && round > 0) {
-#pragma unroll 1
-    for (int j0 = half * kColsPer; j0 < (half + 1) * kColsPer; j0 += 8) {
-      float v[8];
-      tmem_ld8(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)j0, v);
-      if (i < m_valid) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          if (j0 + q < n_valid) store(i, j0 + q, v[q]);
-      }
-    }
-  } else if (ok) {
-    // empty K range: the product is zero
-    if (i < m_valid)
-      for (int j = half * kColsPer; j < (half + 1) * kColsPer && j < n_valid; ++j) store(i, j, 0.0f);
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, S::kCols);
-  if (ok && tid == 0) {
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mbar0) : "memory");
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mbar0 + 8) : "memory");
-  }
-  return ok;
 }
 
 // ------------------------------------------------------ pre-split operand tiles
