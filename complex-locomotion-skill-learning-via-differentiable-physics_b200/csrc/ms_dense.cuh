@@ -381,53 +381,68 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
 // tensor-core tile with M = outputs, N = inputs + 1 (a row of ones turns the
 // bias gradient into the last column) and K = the rows.  First the FP32
 // records are transposed into pre-split K-major tiles: one CTA moves 32 envs
-// x 32 columns of one record slot through shared memory, reading env rows
-// (128 bytes each) and writing each column's 32 K values as one 128-byte
+// x 32 columns of kWgSlots record slots through shared memory, reading env
+// rows (128 bytes each) and writing each column's 32 K values as one 128-byte
 // line per precision part.
+constexpr int kWgSlots = 10;  // record slots per transpose CTA
+
 __global__ void __launch_bounds__(256)
-ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* cols) {
+ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* cols, int nslots) {
   __shared__ float tile[32][33];
   const WgCol wc = cols[blockIdx.y];
   const WgTrans jb = jobs[wc.job];
   const RobotDesc& rb = a.robots[jb.robot];
   const DenseDesc& dd = a.dense[jb.robot];
   const EnvDesc& e0 = a.envs[rb.env_first];
-  const int kk = blockIdx.z, j0 = blockIdx.x * 32;
+  const int j0 = blockIdx.x * 32;
   if (j0 >= dd.nep) return;
   const int l = jb.layer, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int rows = jb.cols + (jb.kind == 2 ? 0 : 1);
-  const float* src;
-  int stride;
+  const float* src0;
+  int stride, slot;
   if (jb.kind == 0) {
     stride = rb.pitch[0];
-    src = a.rec_in + (size_t)kk * a.in_total + e0.in_off;
+    slot = a.in_total;
+    src0 = a.rec_in + e0.in_off;
   } else if (jb.kind == 1) {
     stride = pad4(rb.width[l]);
-    src = a.rec_z + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + e0.z_off[l - 1];
+    slot = a.z_total[l - 1];
+    src0 = a.rec_z + a.z_base[l - 1] + e0.z_off[l - 1];
   } else {
     stride = pad4(rb.width[l + 1]);
-    src = a.rec_dz + a.z_base[l] + (size_t)kk * a.z_total[l] + e0.z_off[l];
+    slot = a.z_total[l];
+    src0 = a.rec_dz + a.z_base[l] + e0.z_off[l];
   }
   const float* bias = jb.kind == 1 ? a.bias + rb.b_off[l - 1] : nullptr;
-  for (int r = ty; r < 32; r += 8) {
-    const int j = j0 + r, c = wc.c0 + tx;
-    float v = 0.f;
-    if (j < rb.n_env) {
-      if (c < jb.cols) {
-        v = src[(size_t)j * stride + c];
-        if (bias) v = act_f<float>(a.act_hidden, v + bias[c]);
-      } else if (c == jb.cols && jb.kind != 2) {
-        v = 1.f;
+  float* dst = a.wtiles + (jb.kind == 2 ? dd.tw_d[l] : dd.tw_a[l]);
+  const int c = wc.c0 + tx;
+  const float b = (bias && c < jb.cols) ? bias[c] : 0.f;
+  const int kk1 = min(nslots, (int)(blockIdx.z + 1) * kWgSlots);
+  for (int kk = blockIdx.z * kWgSlots; kk < kk1; ++kk) {
+    const float* src = src0 + (size_t)kk * slot;
+    for (int r = ty; r < 32; r += 8) {
+      const int j = j0 + r;
+      float v = 0.f;
+      if (j < rb.n_env) {
+        if (c < jb.cols) {
+          v = src[(size_t)j * stride + c];
+          if (bias) v = act_f<float>(a.act_hidden, v + b);
+        } else if (c == jb.cols && jb.kind != 2) {
+          v = 1.f;
+        }
       }
+      tile[r][tx] = v;
     }
-    tile[r][tx] = v;
-  }
-  __syncthreads();
-  const umma::SplitTiles st{a.wtiles + (jb.kind == 2 ? dd.tw_d[l] : dd.tw_a[l]), jb.kind == 2 ? umma::TM : kDenseTN,
-                            dd.nkt_w};
-  for (int r = ty; r < 32; r += 8) {
-    const int c = wc.c0 + r;
-    if (c < rows) st.store(c, kk * dd.nep + j0 + tx, tile[tx][r]);
+    __syncthreads();
+    const int k = kk * dd.nep + j0 + tx;
+    for (int r = ty; r < 32; r += 8) {
+      const int cc = wc.c0 + r;
+      if (cc >= rows) continue;
+      // the tile height is a compile-time constant per operand (shifts, not divisions)
+      if (jb.kind == 2) umma::SplitTiles{dst, umma::TM, dd.nkt_w}.store_tr<umma::TM>(cc, k, tile[tx][r]);
+      else umma::SplitTiles{dst, kDenseTN, dd.nkt_w}.store_tr<kDenseTN>(cc, k, tile[tx][r]);
+    }
+    __syncthreads();
   }
 }
 

@@ -26,7 +26,7 @@ struct DenseLaunch {
                        int t_pre, int t_begin, int t_end, int last_seg, int per_group);
   static void gemm(const MsArgs<R>& a, bool adjoint, int n_jobs, const DenseJob* jobs, int kslot, cudaStream_t s);
   // FP32 weight-gradient products of one segment (nslots record slots):
-  // record transposes (grid grid_x x n_cols x nslots) then the tensor-core
+  // record transposes (grid grid_x x n_cols x slot groups) then the tensor-core
   // tiles (n_jobs CTAs), adding into gw / gb
   static void wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int nslots, const WgTrans* trans, const WgCol* cols,
                     int n_jobs, const WgJob* jobs, R* gw, R* gb, cudaStream_t s);

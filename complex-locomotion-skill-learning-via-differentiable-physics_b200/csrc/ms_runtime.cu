@@ -878,14 +878,16 @@ class SimImpl final : public SimBase {
       int max_kt = 0;
       for (const DenseDesc& dd : dd_host_) max_kt = std::max(max_kt, dd.nkt_w);
       const int nsplit = std::max(1, std::min(std::max(1, max_kt / 8), (2 * n_sm_ + n_tiles - 1) / std::max(1, n_tiles)));
-      for (int r = 0; r < (int)hr_.size(); ++r) {
-        if (rd_host_[r].n_env == 0) continue;
-        const HostRobot& h = hr_[r];
-        for (int l = 0; l < h.n_layers; ++l)
-          for (int o0 = 0; o0 < h.width[l + 1]; o0 += tm)
-            for (int i0 = 0; i0 < h.width[l] + 1; i0 += tn)
-              for (int sp = 0; sp < nsplit; ++sp) wg_jobs_.push_back({r, l, o0, i0, sp, nsplit});
-      }
+      // split outermost: the tiles of one K range run together and share
+      // their operand blocks through L2 (a segment's operands exceed it)
+      for (int sp = 0; sp < nsplit; ++sp)
+        for (int r = 0; r < (int)hr_.size(); ++r) {
+          if (rd_host_[r].n_env == 0) continue;
+          const HostRobot& h = hr_[r];
+          for (int l = 0; l < h.n_layers; ++l)
+            for (int o0 = 0; o0 < h.width[l + 1]; o0 += tm)
+              for (int i0 = 0; i0 < h.width[l] + 1; i0 += tn) wg_jobs_.push_back({r, l, o0, i0, sp, nsplit});
+        }
       d_wsplit_.alloc(std::max<long long>(1, woff));
       CLS_CUDA(cudaMemset(d_wsplit_.p, 0, sizeof(R) * d_wsplit_.n));
       d_wg_trans_.alloc(std::max<size_t>(1, wg_trans_.size()));

@@ -173,6 +173,16 @@ struct SplitTiles {
     p[o] = __uint_as_float(h);
     p[o + 32 * tr] = __uint_as_float(tf32_bits(v - __uint_as_float(h)));
   }
+  // the same with the tile height TR (== tr) known at compile time
+  template <int TR>
+  __device__ __forceinline__ void store_tr(int r, int k, float v) const {
+    const int kk = k & 31, rr = r % TR;
+    const size_t o = ((size_t)(r / TR) * nkt + (k >> 5)) * (size_t)(64 * TR) + (size_t)rr * 32 +
+                     (size_t)((((kk >> 2) ^ (rr & 7))) << 2) + (kk & 3);
+    const uint32_t h = tf32_bits(v);
+    p[o] = __uint_as_float(h);
+    p[o + 32 * TR] = __uint_as_float(tf32_bits(v - __uint_as_float(h)));
+  }
   // four consecutive columns k .. k + 3 (k a multiple of 4)
   __device__ __forceinline__ void store4(int r, int k, const float4& v) const {
     const size_t o = index(r, k);
