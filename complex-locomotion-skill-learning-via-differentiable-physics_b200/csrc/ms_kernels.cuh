@@ -29,7 +29,7 @@ struct RobotDesc {
   int n_v, n_s, n_out, n_c;          // vertices, springs, MLP outputs, compact inputs
   int ptr_off;                       // CSR row pointers start (n_v + 1 entries)
   int inc_off;                       // incidence entries start (2 n_s entries)
-  int spr_off;                       // per-spring arrays start (n_s entries)
+  int spr_off;                       // per-spring output map start (n_s entries)
   int robot_id;                      // 100 selects the hard-coded heading vertices
   int pos_pad;                       // first compact column after the position block
   int n_layers;
@@ -135,8 +135,6 @@ struct MsArgs {
   const V4<R>* inc_f;                // {rest length, stiffness, actuation coef, 0}
   const int4* inc_p;                 // FP32 only: packed 16-byte incidence records
   const int* spring_out;             // per spring: MLP output index or -1
-  const int4* spr_i;                 // per spring {a, b, out index, 0}
-  const V4<R>* spr_f;                // per spring {rest length, stiffness, actuation coef, 0}
   const R* w;                        // compact weights
   const R* bias;
   const R* sin_table;                // [T + 1][n_sin], sin(omega (t) dt + 2 pi j / n_sin)

@@ -210,8 +210,6 @@ class SimImpl final : public SimBase {
     std::vector<int4> inc_i, inc_p;
     std::vector<V4<R>> inc_f;
     std::vector<int> spring_out;
-    std::vector<int4> spr_i;
-    std::vector<V4<R>> spr_f;
     long long woff = 0, moff = 0, wtoff = 0;
     int boff = 0;
     nmax_ = 0;
@@ -294,12 +292,6 @@ class SimImpl final : public SimBase {
       inc_ptr.push_back(run);
       for (int s = 0; s < h.n_s; ++s) {
         spring_out.push_back(h.out[s]);
-        int4 si;
-        si.x = h.sa[s]; si.y = h.sb[s]; si.z = h.out[s]; si.w = 0;
-        spr_i.push_back(si);
-        V4<R> sf;
-        sf.x = (R)h.len[s]; sf.y = (R)h.stiff[s]; sf.z = (R)h.coef[s]; sf.w = 0;
-        spr_f.push_back(sf);
       }
       nmax_ = std::max(nmax_, h.n_v);
       p0max = std::max(p0max, round4(h.width[0]));
@@ -446,8 +438,6 @@ class SimImpl final : public SimBase {
     d_inc_f_.alloc(std::max<size_t>(1, inc_f.size()));
     d_inc_p_.alloc(std::max<size_t>(1, inc_p.size()));
     d_spring_out_.alloc(std::max<size_t>(1, spring_out.size()));
-    d_spr_i_.alloc(std::max<size_t>(1, spr_i.size()));
-    d_spr_f_.alloc(std::max<size_t>(1, spr_f.size()));
     d_w_.alloc(woff);
     d_gw_.alloc(woff);
     wt_total_ = wtoff;
@@ -523,8 +513,6 @@ class SimImpl final : public SimBase {
     if (!spring_out.empty()) {
       CLS_CUDA(cudaMemcpy(d_spring_out_.p, spring_out.data(), sizeof(int) * spring_out.size(),
                           cudaMemcpyHostToDevice));
-      CLS_CUDA(cudaMemcpy(d_spr_i_.p, spr_i.data(), sizeof(int4) * spr_i.size(), cudaMemcpyHostToDevice));
-      CLS_CUDA(cudaMemcpy(d_spr_f_.p, spr_f.data(), sizeof(V4<R>) * spr_f.size(), cudaMemcpyHostToDevice));
     }
     if (!tiles_host_.empty())
       CLS_CUDA(cudaMemcpy(d_tiles_.p, tiles_host_.data(), sizeof(GemmTile) * tiles_host_.size(),
@@ -630,8 +618,6 @@ class SimImpl final : public SimBase {
     a.inc_f = d_inc_f_.p;
     a.inc_p = d_inc_p_.p;
     a.spring_out = d_spring_out_.p;
-    a.spr_i = d_spr_i_.p;
-    a.spr_f = d_spr_f_.p;
     a.w = d_w_.p;
     a.bias = d_bias_.p;
     a.sin_table = d_sin_.p;
@@ -1616,8 +1602,8 @@ class SimImpl final : public SimBase {
   DevBuf<RobotDesc> d_robots_;
   DevBuf<EnvDesc> d_envs_;
   DevBuf<int> d_order_, d_queue_, d_inc_ptr_, d_spring_out_, d_status_, d_iter_;
-  DevBuf<int4> d_inc_i_, d_spr_i_, d_inc_p_;
-  DevBuf<V4<R>> d_spr_f_, d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_recvinc_, d_obsc_, d_xfull_,
+  DevBuf<int4> d_inc_i_, d_inc_p_;
+  DevBuf<V4<R>> d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_recvinc_, d_obsc_, d_xfull_,
       d_tv_, d_init_, d_adjx_, d_adjv_;
   DevBuf<R> d_w_, d_gw_, d_bias_, d_gb_, d_bm_, d_bv_, d_wm_, d_wmm_, d_wmv_, d_sin_, d_recin_,
       d_recz_, d_recdz_, d_obsh_, d_obsu_, d_obsr_, d_actfull_, d_th_, d_tc_, d_adjh_;

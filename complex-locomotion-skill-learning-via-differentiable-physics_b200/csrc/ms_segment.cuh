@@ -416,83 +416,99 @@ __device__ __forceinline__ R seed_upper(const MsArgs<R>& a, int t, int e, R Br) 
 }
 
 // -------------------------------------------------------------- spring adjoint
-// Accumulates, for vertex i, the adjoint of every incident spring's impulse:
-// d x_i, d v_i; for a-side entries also d actuation (-> gout).
-// Adjoint of apply_spring_force(t), one thread per spring: recompute the
-// spring's impulse, pull d v_inc of both endpoints, and push d x, d v into both
-// endpoints and d actuation into the spring's controller output with shared-
-// memory atomics (the reference scatters its forward with atomics too, so the
-// order of these sums is not fixed; they only change rounding).  Spring
-// records are fetched four at a time with the evict_last L2 policy.
+// Adjoint of apply_spring_force(t) in gather form: each vertex's half-warp
+// takes its incident springs (the CSR incidence list of the forward gather),
+// recomputes each spring's adjoint and adds the part that falls on its own
+// vertex, so d x and d v need no atomics and sum in a fixed order; the
+// a-side incidence of an actuated spring adds d actuation (shared-memory
+// atomic: outputs may drive several springs).  Twice the spring arithmetic of
+// a spring-parallel adjoint, in exchange for its 12 shared-memory atomics per
+// spring, which bounded that form (the reverse kernels 10-16 % faster).
+template <typename R>
+__device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc<R>& in, int v, const V4<R>* xs,
+                                                   const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
+                                                   R act_seed_scale, R act_lim, bool act_seed, R (&gxs)[3],
+                                                   R (&gvs)[3]) {
+  const int o = in.other;
+  const int ia = in.side == 0 ? v : o, ib = in.side == 0 ? o : v;
+  const V4<R> xa = xs[ia], xb = xs[ib], va = vs[ia], vb = vs[ib];
+  const V4<R> ga = gvinc[ia], gb = gvinc[ib];
+  const R act = in.out >= 0 ? outv[in.out] : R(0);
+  const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
+  const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
+  const R r8 = sqrt_s<R>(n2 + R(1e-8));
+  const R length = r8 + R(1e-4);
+  const R inv_length = rcp_s<R>(length);
+  const R target = in.l0 * (R(1) + in.coef * act);
+  const R sc = a.dt * (length - target) * in.k * inv_length;
+  const R invlen = rsqrt_s<R>(n2);
+  const R inv_r8 = rcp_s<R>(r8);
+  const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
+  const R dv0 = va.x - vb.x, dv1 = va.y - vb.y, dv2 = va.z - vb.z;
+  const R vrel = dv0 * n0 + dv1 * n1 + dv2 * nz;
+  const R gi0 = gb.x - ga.x, gi1 = gb.y - ga.y, gi2 = gb.z - ga.z;
+  const R gsc = gi0 * d0 + gi1 * d1 + gi2 * d2;
+  const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
+  const R cdv = a.dashpot * vrel;
+  const R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
+  R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
+  const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
+  const R gr_r = -ginv * invlen * invlen * invlen;
+  gd0 += gr_r * d0; gd1 += gr_r * d1; gd2 += gr_r * d2;
+  const R glen = gsc * a.dt * in.k * target * inv_length * inv_length;
+  const R glen_r8 = glen * inv_r8;
+  gd0 += glen_r8 * d0; gd1 += glen_r8 * d1; gd2 += glen_r8 * d2;
+  const R h0 = gvrel * n0, h1 = gvrel * n1, h2 = gvrel * nz;
+  if (in.side == 0) {
+    gxs[0] += gd0; gxs[1] += gd1; gxs[2] += gd2;
+    gvs[0] += h0; gvs[1] += h1; gvs[2] += h2;
+    if (in.out >= 0) {
+      R gact = -gsc * a.dt * in.k * inv_length * in.l0 * in.coef;
+      if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
+        if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
+      }
+      atomicAdd(gout + in.out, gact);
+    }
+  } else {
+    gxs[0] -= gd0; gxs[1] -= gd1; gxs[2] -= gd2;
+    gvs[0] -= h0; gvs[1] -= h1; gvs[2] -= h2;
+  }
+}
+
 template <typename R, typename G = BlockGroup>
-__device__ __forceinline__ void spring_adjoint_all(const MsArgs<R>& a, const RobotDesc& rb,
-                                                   const V4<R>* xs, const V4<R>* vs,
-                                                   const V4<R>* gvinc, const R* outv, R* gout,
-                                                   V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
-                                                   bool act_seed) {
+__device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const RobotDesc& rb, const V4<R>* xs,
+                                                      const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
+                                                      V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
+                                                      bool act_seed) {
   const unsigned long long pol = policy_evict_last();
-  const int4* ip = a.spr_i + rb.spr_off;
-  const V4<R>* fp = a.spr_f + rb.spr_off;
-  const int S = rb.n_s, nt = G::size();
-  for (int s0 = G::rank(); s0 < S; s0 += 4 * nt) {
-    int4 iiv[4];
-    V4<R> ffv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = (s0 + u * nt < S) ? s0 + u * nt : s0;
-      iiv[u] = ldg_i4_hint(ip + q, pol);
-      ffv[u] = ldg4_hint<R>(fp + q, pol);
+  const int lane = threadIdx.x & 31, wid = G::warp(), nw = G::warps();
+  const int l16 = lane & 15, half = lane >> 4;
+  const int* ptr = a.inc_ptr + rb.ptr_off;
+  const int N = rb.n_v, stride = nw * 2;
+  // the loop bound is warp-uniform (vb0), so every shuffle below has all 32 lanes
+  for (int vb0 = wid * 2; vb0 < N; vb0 += stride) {
+    const int v = vb0 + half;
+    R gxs[3] = {0, 0, 0}, gvs[3] = {0, 0, 0};
+    if (v < N) {
+      const int beg = ptr[v], end = ptr[v + 1];
+      for (int q = beg + l16; q < end; q += 16)
+        spring_adjoint_one<R>(a, load_inc<R>(a, rb, q, pol), v, xs, vs, gvinc, outv, gout, act_seed_scale, act_lim,
+                              act_seed, gxs, gvs);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (s0 + u * nt >= S) break;
-      const int4 ii = iiv[u];
-      const V4<R> ff = ffv[u];
-      const int ia = ii.x, ib = ii.y;
-      const V4<R> xa = xs[ia], xb = xs[ib], va = vs[ia], vb = vs[ib];
-      const V4<R> ga = gvinc[ia], gb = gvinc[ib];
-      const R act = ii.z >= 0 ? outv[ii.z] : R(0);
-      // forward recompute (solver_mass_spring.py:89-103)
-      const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
-      const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
-      const R r8 = sqrt_s<R>(n2 + R(1e-8));
-      const R length = r8 + R(1e-4);
-      const R inv_length = rcp_s<R>(length);
-      const R target = ff.x * (R(1) + ff.z * act);
-      const R sc = a.dt * (length - target) * ff.y * inv_length;
-      const R invlen = rsqrt_s<R>(n2);
-      const R inv_r8 = rcp_s<R>(r8);
-      const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
-      const R dv0 = va.x - vb.x, dv1 = va.y - vb.y, dv2 = va.z - vb.z;
-      const R vrel = dv0 * n0 + dv1 * n1 + dv2 * nz;
-      // impulse enters v_inc[b] with +, v_inc[a] with -
-      const R gi0 = gb.x - ga.x, gi1 = gb.y - ga.y, gi2 = gb.z - ga.z;
-      const R gsc = gi0 * d0 + gi1 * d1 + gi2 * d2;
-      const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
-      const R cdv = a.dashpot * vrel;
-      const R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
-      R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
-      // invlen = 1 / r, r = |dist|:  d r = -d invlen / r^2, d dist += d r * dist / r
-      const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
-      const R gr_r = -ginv * invlen * invlen * invlen;
-      gd0 += gr_r * d0; gd1 += gr_r * d1; gd2 += gr_r * d2;
-      // sc = dt (length - target) k / length:  d length = d sc dt k target / length^2
-      const R glen = gsc * a.dt * ff.y * target * inv_length * inv_length;
-      const R glen_r8 = glen * inv_r8;
-      gd0 += glen_r8 * d0; gd1 += glen_r8 * d1; gd2 += glen_r8 * d2;
-      atomicAdd(&gx[ia].x, gd0); atomicAdd(&gx[ia].y, gd1); atomicAdd(&gx[ia].z, gd2);
-      atomicAdd(&gx[ib].x, -gd0); atomicAdd(&gx[ib].y, -gd1); atomicAdd(&gx[ib].z, -gd2);
-      const R h0 = gvrel * n0, h1 = gvrel * n1, h2 = gvrel * nz;
-      atomicAdd(&gv[ia].x, h0); atomicAdd(&gv[ia].y, h1); atomicAdd(&gv[ia].z, h2);
-      atomicAdd(&gv[ib].x, -h0); atomicAdd(&gv[ib].y, -h1); atomicAdd(&gv[ib].z, -h2);
-      if (ii.z >= 0) {
-        const R gtarget = -gsc * a.dt * ff.y * inv_length;
-        R gact = gtarget * ff.x * ff.z;
-        if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
-          if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
-        }
-        atomicAdd(gout + ii.z, gact);
+    for (int o = 8; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        gxs[c] += __shfl_xor_sync(0xffffffffu, gxs[c], o);
+        gvs[c] += __shfl_xor_sync(0xffffffffu, gvs[c], o);
       }
+    }
+    if (l16 == 0 && v < N) {
+      V4<R> x = gx[v], w = gv[v];
+      x.x += gxs[0]; x.y += gxs[1]; x.z += gxs[2];
+      w.x += gvs[0]; w.y += gvs[1]; w.z += gvs[2];
+      gx[v] = x;
+      gv[v] = w;
     }
   }
 }
@@ -578,7 +594,7 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
     const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
     const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
-    spring_adjoint_all<R, G>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
+    spring_adjoint_gather<R, G>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
                           act_seed);
   }
   G::sync();

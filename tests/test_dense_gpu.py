@@ -140,8 +140,9 @@ def test_batched_fp32_as_accurate_as_per_env_fp32():
 
 def test_batched_graph_replay_matches_eager():
     """The forward pass (spring gather, tensor-core GEMMs) is deterministic, so
-    the replayed loss is identical; the reverse pass's shared-memory atomics
-    only change the gradients' rounding."""
+    the replayed loss is identical; the atomic adds of the reverse pass
+    (actuation gradients, split-K weight gradients) only change the gradients'
+    rounding."""
     import torch
     b = _many_env_batch(32, 260, [64], 10, 40, "batched")
     e_loss, e_grads, _, _ = _run(b, 30, 2)

@@ -81,7 +81,7 @@ def test_checkpoint_interval_does_not_change_gradients(K):
     gw = b.get_grads(0, 0)[0]
     # the forward kernels are deterministic, so the recompute reproduces the
     # first pass bit for bit; K only regroups the per-segment weight-gradient
-    # sums and the shared-memory atomics of the spring adjoint
+    # sums and the atomic adds of the actuation gradients
     assert rel_err(b.state_grads()[0], gx_ref) < 1e-12
     assert rel_err(gw, gw_ref) < 1e-12
 
@@ -95,7 +95,7 @@ def test_per_env_launch_equals_batched():
     l2 = b.simulate(steps, per_env=True)
     g2 = b.get_grads(0, 0)[0]
     assert l1 == l2          # deterministic forward: identical losses
-    assert rel_err(g2, g1) < 1e-5   # the adjoint's atomics only change rounding
+    assert rel_err(g2, g1) < 1e-5   # atomic adds (actuation, weight gradients) only change rounding
 
 
 def test_eval_rollout_matches_golden():

@@ -3,7 +3,7 @@ mix that folds other requests into the running launches, and both equal the
 plain one-env batch (cls_forward + cls_loss + cls_backward) of the same robot,
 weights and targets.  Losses within rel 1e-6 (the first pass is
 deterministic), weight gradients within rel 1e-5 (the reverse pass adds
-spring adjoints with shared-memory atomics); FP64 at 1e-10."""
+actuation gradients and weight-gradient splits with atomic adds); FP64 at 1e-10."""
 import numpy as np
 import pytest
 
