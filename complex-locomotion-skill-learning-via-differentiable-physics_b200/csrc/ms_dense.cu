@@ -25,8 +25,8 @@ long long DenseLaunch<R>::split_floats(int rows, int tile_rows, int k) {
 template <typename R>
 cudaError_t DenseLaunch<R>::setup(int threads, size_t* fwd_static, size_t* rev_static, int optin) {
   if (threads != CLS_STEP_THREADS) return cudaErrorInvalidValue;
-  auto fwd = ms_step_fwd_kernel<R, BlockGroup, CLS_STEP_THREADS>;
-  auto rev = ms_step_rev_kernel<R, BlockGroup, CLS_STEP_THREADS>;
+  auto fwd = ms_step_fwd_kernel<R, CLS_STEP_THREADS>;
+  auto rev = ms_step_rev_kernel<R, CLS_STEP_THREADS>;
   cudaFuncAttributes fa{}, ra{};
   cudaError_t e = cudaFuncGetAttributes(&fa, fwd);
   if (e == cudaSuccess) e = cudaFuncGetAttributes(&ra, rev);
@@ -47,16 +47,16 @@ cudaError_t DenseLaunch<R>::setup(int threads, size_t* fwd_static, size_t* rev_s
 
 template <typename R>
 void DenseLaunch<R>::step_fwd(const MsArgs<R>& a, int grid, int threads, size_t smem, cudaStream_t s, int t,
-                              int t_first, int t_end, int mode, int src_slot, int k_prev, int k_cur, int per_group) {
-  ms_step_fwd_kernel<R, BlockGroup, CLS_STEP_THREADS><<<grid, threads, smem, s>>>(a, t, t_first, t_end, mode, src_slot,
-                                                                                   k_prev, k_cur, per_group);
+                              int t_first, int t_end, int mode, int src_slot, int k_prev, int k_cur) {
+  ms_step_fwd_kernel<R, CLS_STEP_THREADS><<<grid, threads, smem, s>>>(a, t, t_first, t_end, mode, src_slot,
+                                                                       k_prev, k_cur);
 }
 
 template <typename R>
 void DenseLaunch<R>::step_rev(const MsArgs<R>& a, int grid, int threads, size_t smem, cudaStream_t s, int t_post,
-                              int t_pre, int t_begin, int t_end, int last_seg, int per_group) {
-  ms_step_rev_kernel<R, BlockGroup, CLS_STEP_THREADS><<<grid, threads, smem, s>>>(a, t_post, t_pre, t_begin, t_end,
-                                                                                   last_seg, per_group);
+                              int t_pre, int t_begin, int t_end, int last_seg) {
+  ms_step_rev_kernel<R, CLS_STEP_THREADS><<<grid, threads, smem, s>>>(a, t_post, t_pre, t_begin, t_end,
+                                                                       last_seg);
 }
 
 template <typename R>

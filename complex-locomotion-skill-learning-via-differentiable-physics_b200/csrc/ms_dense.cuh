@@ -31,19 +31,10 @@ namespace cls {
 __host__ __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 // ------------------------------------------------------------ step kernels
-// One CTA per env (G = BlockGroup; WarpGroup with kStepWarps envs per CTA is
-// the alternative the group abstraction allows): the substep halves with the
-// env's state in the group's slice of shared memory (per_group bytes, the
-// fused kernels' carve with the controller buffers sized for the output
-// layer only).
-constexpr int kStepWarps = 4;
-
-template <typename G>
-__device__ __forceinline__ int step_slot() { return G::kWarp ? (threadIdx.x >> 5) : 0; }
-template <typename G>
-__device__ __forceinline__ int step_item() {
-  return G::kWarp ? blockIdx.x * kStepWarps + (threadIdx.x >> 5) : blockIdx.x;
-}
+// One CTA per env; the substep halves with the env's state in the CTA's
+// shared memory (the fused kernels' carve with the controller buffers sized
+// for the output layer only).  One warp per env
+// (several envs per CTA, no CTA barrier) measured slower.
 
 // Forward step t of a range [t_first, t_end):
 //   t > t_first: controller outputs of t-1 from the output layer's record
@@ -54,21 +45,19 @@ __device__ __forceinline__ int step_item() {
 //   t == t_end:  the range's end (checkpoint, final state).
 // The state comes from checkpoint slot src_slot at t == t_first, else from
 // live_x/v.
-template <typename R, typename G, int MAXT>
+template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT)
 ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src_slot, int k_prev,
-                   int k_cur, int per_group) {
+                   int k_cur) {
   extern __shared__ __align__(256) char smem_raw[];
-  __shared__ RobotDesc rbs[G::kWarp ? kStepWarps : 1];
-  __shared__ EnvDesc eds[G::kWarp ? kStepWarps : 1];
-  const int w = step_slot<G>(), item = step_item<G>();
-  if (item >= a.n_items) return;  // whole groups only
-  RobotDesc& rb = rbs[w];
-  EnvDesc& ed = eds[w];
-  FwdSmem<R> s = carve_fwd<R>(smem_raw + (size_t)w * per_group, a);
-  const int tid = G::rank(), nt = G::size();
+  __shared__ RobotDesc rb;
+  __shared__ EnvDesc ed;
+  const int item = blockIdx.x;
+  if (item >= a.n_items) return;
+  FwdSmem<R> s = carve_fwd<R>(smem_raw, a);
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int e = a.order[item];
-  load_descs<R, G>(a, e, rb, ed);
+  load_descs<R>(a, e, rb, ed);
   const int N = rb.n_v, L = rb.n_layers;
   {
     const bool first = (t == t_first);
@@ -76,18 +65,18 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
     const V4<R>* cv = first ? a.ckpt_v + (size_t)src_slot * a.v_total + ed.v_off : a.live_v + ed.v_off;
     for (int i = tid; i < N; i += nt) { s.xs[i] = cx[i]; s.vs[i] = cv[i]; }
   }
-  G::sync();
+  __syncthreads();
   if (t > t_first) {
     const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)k_prev * a.z_total[L - 1] + ed.z_off[L - 1];
     const R* bo = a.bias + rb.b_off[L - 1];
     for (int o = tid; o < rb.n_out; o += nt) s.buf0[o] = act_f<R>(a.act_out, zl[o] + bo[o]);
-    G::sync();
-    fwd_post<R, G>(a, rb, ed, s, t - 1, mode, k_prev, s.buf0);
+    __syncthreads();
+    fwd_post<R>(a, rb, ed, s, t - 1, mode, k_prev, s.buf0);
   }
   if (t < t_end) {
     R hprev = 0;
     if ((mode & FWD_OBS) && t > 0) hprev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
-    fwd_pre<R, G>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
+    fwd_pre<R>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
     if constexpr (std::is_same<R, float>::value) {
       // the input row as the first layer's pre-split A operand
       const umma::SplitTiles st{a.tiles + a.dense[ed.robot].ta_f[0], umma::TM, (rb.n_c + 31) / 32};
@@ -100,7 +89,7 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
       a.live_v[ed.v_off + i] = s.vs[i];
     }
   } else {
-    fwd_finish<R, G>(a, rb, ed, s, t_first, t_end, mode);
+    fwd_finish<R>(a, rb, ed, s, t_first, t_end, mode);
   }
 }
 
@@ -112,34 +101,32 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
 // The adjoint state is carried in adj_x/v/h between launches; the first
 // launch of the segment (t_pre = t_end - 1) seeds it (last segment) or takes
 // the carry of the later segment.
-template <typename R, typename G, int MAXT>
+template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT)
-ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, int last_seg, int per_group) {
+ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, int last_seg) {
   extern __shared__ __align__(256) char smem_raw[];
-  __shared__ RobotDesc rbs[G::kWarp ? kStepWarps : 1];
-  __shared__ EnvDesc eds[G::kWarp ? kStepWarps : 1];
-  const int w = step_slot<G>(), item = step_item<G>();
+  __shared__ RobotDesc rb;
+  __shared__ EnvDesc ed;
+  const int item = blockIdx.x;
   if (item >= a.n_items) return;
-  RobotDesc& rb = rbs[w];
-  EnvDesc& ed = eds[w];
-  RevSmem<R> s = carve_rev<R>(smem_raw + (size_t)w * per_group, a);
-  const int tid = G::rank(), nt = G::size();
+  RevSmem<R> s = carve_rev<R>(smem_raw, a);
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int e = a.order[item];
-  load_descs<R, G>(a, e, rb, ed);
+  load_descs<R>(a, e, rb, ed);
   const int N = rb.n_v;
   R hcarry = 0;
-  rev_load_carry<R, G>(a, rb, ed, s, e, t_end, t_pre == t_end - 1 && last_seg != 0, hcarry);
+  rev_load_carry<R>(a, rb, ed, s, e, t_end, t_pre == t_end - 1 && last_seg != 0, hcarry);
   if (t_post >= 0) {
     const int kk = t_post - t_begin;
     const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
     for (int i = tid; i < N; i += nt) s.xs[i] = rx[i];
     const R* dp = a.din + (size_t)3 * ed.v_off;
     for (int q = tid; q < 3 * N; q += nt) s.bufA[q] = dp[q];
-    G::sync();
-    rev_post<R, G>(a, rb, ed, s, e, t_post, hcarry);
+    __syncthreads();
+    rev_post<R>(a, rb, ed, s, e, t_post, hcarry);
   }
   if (t_pre >= 0) {
-    rev_pre<R, G>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
+    rev_pre<R>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
     if constexpr (std::is_same<R, float>::value) {
       // dZ of the output layer as the adjoint GEMM's pre-split A operand
       const int no = rb.n_out;
@@ -152,7 +139,7 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
       }
     }
   }
-  rev_store_carry<R, G>(a, rb, ed, s, e, hcarry);
+  rev_store_carry<R>(a, rb, ed, s, e, hcarry);
 }
 
 // ------------------------------------------------------------ GEMM operands

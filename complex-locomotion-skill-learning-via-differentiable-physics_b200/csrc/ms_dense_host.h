@@ -21,9 +21,9 @@ struct DenseLaunch {
   // static shared bytes are returned for the capacity check
   static cudaError_t setup(int threads, size_t* fwd_static, size_t* rev_static, int optin);
   static void step_fwd(const MsArgs<R>& a, int grid, int threads, size_t smem, cudaStream_t s, int t, int t_first,
-                       int t_end, int mode, int src_slot, int k_prev, int k_cur, int per_group);
+                       int t_end, int mode, int src_slot, int k_prev, int k_cur);
   static void step_rev(const MsArgs<R>& a, int grid, int threads, size_t smem, cudaStream_t s, int t_post,
-                       int t_pre, int t_begin, int t_end, int last_seg, int per_group);
+                       int t_pre, int t_begin, int t_end, int last_seg);
   static void gemm(const MsArgs<R>& a, bool adjoint, int n_jobs, const DenseJob* jobs, int kslot, cudaStream_t s);
   // FP32 weight-gradient products of one segment (nslots record slots):
   // record transposes (grid grid_x x n_cols x slot groups) then the tensor-core

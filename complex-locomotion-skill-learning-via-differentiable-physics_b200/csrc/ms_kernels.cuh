@@ -271,28 +271,6 @@ __host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, i
          rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads);
 }
 
-// ------------------------------------------------------------ thread groups
-// The substep bodies run on a thread group that owns one env: the whole CTA
-// in the fused segment kernels (BlockGroup) or one warp in the batched
-// controller's step kernels (WarpGroup, several envs per CTA, no CTA-wide
-// barrier anywhere on that path).
-struct BlockGroup {
-  static constexpr bool kWarp = false;
-  __device__ static int rank() { return threadIdx.x; }
-  __device__ static int size() { return blockDim.x; }
-  __device__ static int warp() { return threadIdx.x >> 5; }
-  __device__ static int warps() { return blockDim.x >> 5; }
-  __device__ static void sync() { __syncthreads(); }
-};
-struct WarpGroup {
-  static constexpr bool kWarp = true;
-  __device__ static int rank() { return threadIdx.x & 31; }
-  __device__ static int size() { return 32; }
-  __device__ static int warp() { return 0; }
-  __device__ static int warps() { return 1; }
-  __device__ static void sync() { __syncwarp(); }
-};
-
 // ------------------------------------------------------------- primitives
 
 // Hooke + dashpot impulse of one spring seen from one of its endpoints
@@ -374,13 +352,13 @@ __device__ __forceinline__ void accumulate_incidence(const MsArgs<R>& a, const I
 // not depend on scheduling (the recompute pass reproduces the first pass bit
 // for bit).  Each half-warp prefetches the first incidence of U vertices
 // before computing, so U records per lane are in flight.
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotDesc& rb, int N,
                                                 const V4<R>* xs, const V4<R>* vs, const R* out,
                                                 V4<R>* vinc, V4<R>* rec) {
   constexpr int U = 4;
   const unsigned long long pol = policy_evict_last();
-  const int lane = threadIdx.x & 31, wid = G::warp(), nw = G::warps();
+  const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
   const int l16 = lane & 15, half = lane >> 4;
   const int* ptr = a.inc_ptr + rb.ptr_off;
   const int stride = nw * 2;

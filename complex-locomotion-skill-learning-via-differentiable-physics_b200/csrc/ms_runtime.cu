@@ -892,10 +892,8 @@ class SimImpl final : public SimBase {
     // shared-memory carve with the controller buffers sized for the output
     // layer only (step_args)
     dense_threads_ = CLS_STEP_THREADS;
-    dfwd_warp_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_);
-    drev_warp_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_);
-    dfwd_smem_ = dfwd_warp_;
-    drev_smem_ = drev_warp_;
+    dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_);
+    drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_);
     int dev = 0, optin = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -907,7 +905,7 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaStreamSynchronize(stream));
   }
 
-  // launch arguments of the step kernels: the per-warp carve sizes the
+  // launch arguments of the step kernels: the shared-memory carve sizes the
   // controller buffers for the output layer only
   MsArgs<R> step_args(const MsArgs<R>& a) const {
     MsArgs<R> b = a;
@@ -936,7 +934,7 @@ class SimImpl final : public SimBase {
       const int k_cur = t < t_end ? (first_pass ? t % K_ : t - t_first) : 0;
       timed(kind, [&] {
         DenseLaunch<R>::step_fwd(step_args(a), step_grid(), dense_threads_, dfwd_smem_, stream, t, t_first, t_end, mode,
-                                 src_slot, k_prev, k_cur, (int)dfwd_warp_);
+                                 src_slot, k_prev, k_cur);
       });
       if (t < t_end)
         for (int l = 0; l < L_; ++l) ctrl_gemm(a, false, l, k_cur);
@@ -951,7 +949,7 @@ class SimImpl final : public SimBase {
       const int t_pre = (t >= t0) ? t : -1;
       timed(PK_REV, [&] {
         DenseLaunch<R>::step_rev(step_args(a), step_grid(), dense_threads_, drev_smem_, stream, t_post, t_pre, t0, t1,
-                                 last ? 1 : 0, (int)drev_warp_);
+                                 last ? 1 : 0);
       });
       if (t_pre >= 0)
         for (int l = L_ - 1; l >= 0; --l) ctrl_gemm(a, true, l, t_pre - t0);
@@ -1612,7 +1610,7 @@ class SimImpl final : public SimBase {
   // batched controller path
   bool dense_ = false;
   int dense_threads_ = 128, n_ttiles_ = 0;
-  size_t dfwd_smem_ = 0, drev_smem_ = 0, dfwd_warp_ = 0, drev_warp_ = 0;
+  size_t dfwd_smem_ = 0, drev_smem_ = 0;
   long long wt_total_ = 0;
   std::vector<TransSeg> tsegs_;
   std::vector<DenseJob> jobs_h_;

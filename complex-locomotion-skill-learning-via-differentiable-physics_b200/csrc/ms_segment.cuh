@@ -14,7 +14,7 @@ __device__ __forceinline__ int steps_of(const MsArgs<R>& a, int e) {
 }
 
 // sum of M values over the block, deterministic; red must hold 32*M entries
-template <typename R, int M, typename G = BlockGroup>
+template <typename R, int M>
 __device__ __forceinline__ void block_sum(R (&v)[M], R* red) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -22,7 +22,6 @@ __device__ __forceinline__ void block_sum(R (&v)[M], R* red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[m] += __shfl_xor_sync(0xffffffffu, v[m], o);
   }
-  if constexpr (G::kWarp) return;  // every lane of the warp holds the sum
   __syncthreads();
   if (lane == 0) {
 #pragma unroll
@@ -39,7 +38,7 @@ __device__ __forceinline__ void block_sum(R (&v)[M], R* red) {
 }
 
 // min (or max) of y with the LAST index attaining it, over the block
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void block_argext(R& val, int& idx, bool is_min, R* red, int* redi) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   auto better = [&](R v1, int i1, R v2, int i2) {  // is (v2,i2) preferred over (v1,i1)?
@@ -52,7 +51,6 @@ __device__ __forceinline__ void block_argext(R& val, int& idx, bool is_min, R* r
     int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
     if (better(val, idx, v2, i2)) { val = v2; idx = i2; }
   }
-  if constexpr (G::kWarp) return;  // every lane holds the warp's extremum
   __syncthreads();
   if (lane == 0) { red[wid] = val; redi[wid] = idx; }
   __syncthreads();
@@ -65,17 +63,17 @@ __device__ __forceinline__ void block_argext(R& val, int& idx, bool is_min, R* r
   __syncthreads();
 }
 
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void load_descs(const MsArgs<R>& a, int e, RobotDesc& rb, EnvDesc& ed) {
   // cooperative word copy of the two small descriptors into shared memory
   const int* se = reinterpret_cast<const int*>(a.envs + e);
   int* de = reinterpret_cast<int*>(&ed);
-  for (int q = G::rank(); q < (int)(sizeof(EnvDesc) / 4); q += G::size()) de[q] = se[q];
-  G::sync();
+  for (int q = threadIdx.x; q < (int)(sizeof(EnvDesc) / 4); q += blockDim.x) de[q] = se[q];
+  __syncthreads();
   const int* sr = reinterpret_cast<const int*>(a.robots + ed.robot);
   int* dr = reinterpret_cast<int*>(&rb);
-  for (int q = G::rank(); q < (int)(sizeof(RobotDesc) / 4); q += G::size()) dr[q] = sr[q];
-  G::sync();
+  for (int q = threadIdx.x; q < (int)(sizeof(RobotDesc) / 4); q += blockDim.x) dr[q] = sr[q];
+  __syncthreads();
 }
 
 // goal columns of the compact input: (vx, vz) / max_speed if duplicate_v > 0,
@@ -116,11 +114,11 @@ __device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
 // pitch 0).  The input row is recorded at slot kslot when `rec_in` (FWD_RECORD
 // or the batched path, which also records the zero padding).  hprev: running
 // height of t - 1, updated to t.
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                         const FwdSmem<R>& s, int e, int t, int t_begin, int mode,
                                         int kslot, bool rec_in, bool rec_pad, R& hprev) {
-  const int tid = G::rank(), nt = G::size();
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v;
   const R invN = R(1) / R(N);
   if ((mode & FWD_CKPT) && t > t_begin && (t % a.K) == 0) {
@@ -147,14 +145,14 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
   for (int i = tid; i < N; i += nt) {
     c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
   }
-  block_sum<R, 3, G>(c, s.red);
+  block_sum<R, 3>(c, s.red);
   if (mode & FWD_OBS) {
     // compute_height / upper height (solver_mass_spring.py:158-173)
     R lo = R(10), hi = R(-10);
     for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
     int li = 0, hiidx = 0;
-    block_argext<R, G>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
-    block_argext<R, G>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+    block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+    block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
     // compute_rotation (solver_mass_spring.py:175-192)
     R rot;
     if (rb.robot_id == 100) {
@@ -170,7 +168,7 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
       unsigned char* hd = a.head + ed.v_off;
       if (t == 0) {
         for (int i = tid; i < N; i += nt) hd[i] = (s.xs[i].x < c[0]) ? 1 : 0;
-        G::sync();
+        __syncthreads();
       }
       R hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int i = tid; i < N; i += nt) {
@@ -178,7 +176,7 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
         if (hd[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
         else { hs[4] += p.x; hs[5] += p.y; hs[6] += p.z; hs[7] += R(1); }
       }
-      block_sum<R, 8, G>(hs, s.red);
+      block_sum<R, 8>(hs, s.red);
       const R d0 = -hs[0] * hs[7] + hs[4] * hs[3];
       const R d2 = -hs[2] * hs[7] + hs[6] * hs[3];
       rot = datan2<R>(d2, d0);
@@ -193,9 +191,9 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
       a.obs_rot[o] = rot;
       s.red[0] = h;
     }
-    G::sync();
+    __syncthreads();
     hprev = s.red[0];
-    G::sync();
+    __syncthreads();
   }
   // -- nn_input (taichi_env.py:149-183) in the compact column order
   {
@@ -216,32 +214,32 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
       if (rin && q < nrec) rin[q] = val;
     }
   }
-  G::sync();
+  __syncthreads();
 }
 
 // Substep t after the controller: actuation record, apply_spring_force
 // (gather form) with the controller outputs `out`, advance_toi.
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void fwd_post(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                          const FwdSmem<R>& s, int t, int mode, int kslot, const R* out) {
-  const int tid = G::rank(), nt = G::size();
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v, L = rb.n_layers;
   if ((mode & FWD_OBS) && a.act_full) {
     R* af = a.act_full + (size_t)t * a.z_total[L - 1] + ed.z_off[L - 1];
     for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
   }
-  gather_vinc_all<R, G>(a, rb, N, s.xs, s.vs, out, s.vinc,
+  gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc,
                      (mode & FWD_RECORD) ? a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off : nullptr);
-  G::sync();
+  __syncthreads();
   for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
-  G::sync();
+  __syncthreads();
 }
 
 // State after the last processed step of a range ending at t_end.
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void fwd_finish(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                            const FwdSmem<R>& s, int t_begin, int t_end, int mode) {
-  const int tid = G::rank(), nt = G::size(), N = rb.n_v;
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
   if ((mode & FWD_CKEND) && t_end % a.K == 0 && t_end > t_begin) {
     V4<R>* cx = a.ckpt_x + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
     V4<R>* cv = a.ckpt_v + (size_t)(t_end / a.K) * a.v_total + ed.v_off;
@@ -257,7 +255,7 @@ __device__ __forceinline__ void fwd_finish(const MsArgs<R>& a, const RobotDesc& 
       for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
     }
   }
-  G::sync();
+  __syncthreads();
 }
 
 // Advances every env from t_begin (state in checkpoint slot src_slot) through
@@ -475,13 +473,13 @@ __device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc
   }
 }
 
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const RobotDesc& rb, const V4<R>* xs,
                                                       const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
                                                       V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
                                                       bool act_seed) {
   const unsigned long long pol = policy_evict_last();
-  const int lane = threadIdx.x & 31, wid = G::warp(), nw = G::warps();
+  const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
   const int l16 = lane & 15, half = lane >> 4;
   const int* ptr = a.inc_ptr + rb.ptr_off;
   const int N = rb.n_v, stride = nw * 2;
@@ -520,10 +518,10 @@ __device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const 
 // Adjoint of substep t up to the controller outputs: x(t), v(t) from the
 // records (slot kslot), advance_toi adjoint, spring-force adjoint, then
 // dz of the output layer (recorded, and left in s.dz).
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                         const RevSmem<R>& s, int e, int t, int kslot) {
-  const int tid = G::rank(), nt = G::size();
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v, L = rb.n_layers;
   const R Br = R(rb.n_env);
   const R* bout = a.bias + rb.b_off[L - 1];
@@ -538,13 +536,13 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
       s.bufB[o] = 0;
     }
   }
-  G::sync();
+  __syncthreads();
   // v_inc[t] as recorded by the recompute pass (into gvinc as scratch)
   {
     const V4<R>* rvi = a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off;
     for (int i = tid; i < N; i += nt) s.gvinc[i] = rvi[i];
   }
-  G::sync();
+  __syncthreads();
   // adjoint of advance_toi(t + 1)
   for (int i = tid; i < N; i += nt) {
     const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
@@ -586,7 +584,7 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     s.gv[i] = gv0;
     s.gvinc[i] = gvi;
   }
-  G::sync();
+  __syncthreads();
   // adjoint of apply_spring_force(t)
   {
     const size_t o = (size_t)t * a.n_envs + e;
@@ -594,10 +592,10 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
     const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
     const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
-    spring_adjoint_gather<R, G>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
+    spring_adjoint_gather<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
                           act_seed);
   }
-  G::sync();
+  __syncthreads();
   // adjoint of the MLP's output activation
   {
     R* dzr = a.rec_dz + a.z_base[L - 1] + (size_t)kslot * a.z_total[L - 1] + ed.z_off[L - 1];
@@ -607,16 +605,16 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
       dzr[q] = dz;
     }
   }
-  G::sync();
+  __syncthreads();
 }
 
 // Adjoint of substep t from the controller input on: s.bufA holds d loss /
 // d (position columns of the input), s.xs holds x(t).  nn_input / center /
 // loss seeds, then the running-height adjoint (hcarry carries d h across t).
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                          const RevSmem<R>& s, int e, int t, R& hcarry) {
-  const int tid = G::rank(), nt = G::size();
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v;
   const R Br = R(rb.n_env);
   const R invN = R(1) / R(N);
@@ -632,7 +630,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
       g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
       s.gx[i] = g;
     }
-    block_sum<R, 3, G>(gc, s.red);
+    block_sum<R, 3>(gc, s.red);
     if (a.loss_mask & LOSS_VELOCITY) seed_center_velocity<R>(a, t, e, Br, gc);
     for (int i = tid; i < N; i += nt) {
       V4<R> g = s.gx[i];
@@ -651,7 +649,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
         const R y = s.xs[i].y;
         if (!(lo < y)) { lo = y; li = i; }
       }
-      block_argext<R, G>(lo, li, true, s.red, redi);
+      block_argext<R>(lo, li, true, s.red, redi);
       R gmin = gh;
       if (t % a.jump_period != 0) {
         const R prev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
@@ -665,21 +663,21 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
         const R y = s.xs[i].y;
         if (!(y < hi)) { hi = y; hix = i; }
       }
-      block_argext<R, G>(hi, hix, false, s.red, redi);
+      block_argext<R>(hi, hix, false, s.red, redi);
       if (tid == 0 && hix >= 0) s.gx[hix].y += gu;
     }
   }
-  G::sync();
+  __syncthreads();
 }
 
 // Adjoint carry at the start of a reverse range: for the last segment the
 // direct loss terms at x[t_end] (x[steps-1] is written by the last advance but
 // never passed through pre_advance), else the carry left by the later segment.
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void rev_load_carry(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                                const RevSmem<R>& s, int e, int t_end, bool last_seg,
                                                R& hcarry) {
-  const int tid = G::rank(), nt = G::size(), N = rb.n_v;
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
   const R Br = R(rb.n_env);
   hcarry = 0;
   if (last_seg) {
@@ -698,19 +696,19 @@ __device__ __forceinline__ void rev_load_carry(const MsArgs<R>& a, const RobotDe
     for (int i = tid; i < N; i += nt) { s.gx[i] = a.adj_x[ed.v_off + i]; s.gv[i] = a.adj_v[ed.v_off + i]; }
     hcarry = a.adj_h[e];
   }
-  G::sync();
+  __syncthreads();
 }
 
-template <typename R, typename G = BlockGroup>
+template <typename R>
 __device__ __forceinline__ void rev_store_carry(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                                 const RevSmem<R>& s, int e, R hcarry) {
-  const int tid = G::rank(), nt = G::size(), N = rb.n_v;
+  const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
   for (int i = tid; i < N; i += nt) {
     a.adj_x[ed.v_off + i] = s.gx[i];
     a.adj_v[ed.v_off + i] = s.gv[i];
   }
   if (tid == 0) a.adj_h[e] = hcarry;
-  G::sync();
+  __syncthreads();
 }
 
 template <typename R, int MAXT>
