@@ -449,7 +449,7 @@ def run_ours(a):
                 "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded random lattices, targets and weights)",
-                "config": dict(config_dict(a, world), controller="batched" if batched else "per_env"),
+                "config": config_dict(a, world), "controller_path": "batched" if batched else "per_env",
                 "clocks": clocks,
                 "gpu_launches": int(sum(prof_n.values())) * a.steps, "roofline": roofline,
                 "plain": plain, "e2e": e2e, "cpu_baseline": cpu}
