@@ -65,7 +65,9 @@ def parse():
     ap.add_argument("--robots", "--envs", dest="robots", type=int, default=None,
                     help="robots (uneven) or envs per GPU (default: the configuration's)")
     ap.add_argument("--substeps", type=int, default=None)
-    ap.add_argument("--checkpoint", type=int, default=50)
+    ap.add_argument("--checkpoint", type=int, default=None,
+                    help="substeps per checkpoint segment (default: 50; the spider and quadruped "
+                         "episodes as one segment, whose records the first pass keeps)")
     ap.add_argument("--plain-sample", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -80,6 +82,11 @@ def parse():
         a.robots = DEFAULT_ENVS[a.config]
     if a.substeps is None:
         a.substeps = DEFAULT_SUBSTEPS[a.config]
+    if a.checkpoint is None:
+        # the uneven configuration fixes 50; the spider and quadruped episodes
+        # fit in HBM with every substep's records (tens of GB for the spider),
+        # so they run as one segment and skip the recompute pass
+        a.checkpoint = a.substeps if a.config in ("spider", "quadruped") else 50
     return a
 
 

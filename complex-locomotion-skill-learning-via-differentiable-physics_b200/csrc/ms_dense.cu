@@ -86,12 +86,12 @@ void DenseLaunch<R>::pack_weights(const R* w, R* wt, R* tiles, const TransSeg* t
 }
 
 template <typename R>
-void DenseLaunch<R>::wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int nslots, const WgTrans* trans,
+void DenseLaunch<R>::wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int slot0, int nslots, const WgTrans* trans,
                            const WgCol* cols, int n_jobs, const WgJob* jobs, R* gw, R* gb, cudaStream_t s) {
   if constexpr (std::is_same<R, float>::value) {
     if (n_cols > 0 && nslots > 0)
       ms_wgrad_transpose_kernel<<<dim3(grid_x, n_cols, (nslots + kWgSlots - 1) / kWgSlots), 256, 0, s>>>(
-          a, trans, cols, nslots);
+          a, trans, cols, slot0, nslots);
     if (n_jobs > 0)
       ms_wgrad_tc_kernel<<<n_jobs, umma::kBulkThreads, umma::BulkShape<kDenseTN, kBulkStages>::kSmemBytes, s>>>(
           a, jobs, nslots, gw, gb);

@@ -374,7 +374,7 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
 constexpr int kWgSlots = 10;  // record slots per transpose CTA
 
 __global__ void __launch_bounds__(256)
-ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* cols, int nslots) {
+ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* cols, int slot0, int nslots) {
   __shared__ float tile[32][33];
   const WgCol wc = cols[blockIdx.y];
   const WgTrans jb = jobs[wc.job];
@@ -406,7 +406,7 @@ ms_wgrad_transpose_kernel(MsArgs<float> a, const WgTrans* jobs, const WgCol* col
   const float b = (bias && c < jb.cols) ? bias[c] : 0.f;
   const int kk1 = min(nslots, (int)(blockIdx.z + 1) * kWgSlots);
   for (int kk = blockIdx.z * kWgSlots; kk < kk1; ++kk) {
-    const float* src = src0 + (size_t)kk * slot;
+    const float* src = src0 + (size_t)(slot0 + kk) * slot;
     for (int r = ty; r < 32; r += 8) {
       const int j = j0 + r;
       float v = 0.f;

@@ -25,11 +25,11 @@ struct DenseLaunch {
   static void step_rev(const MsArgs<R>& a, int grid, int threads, size_t smem, cudaStream_t s, int t_post,
                        int t_pre, int t_begin, int t_end, int last_seg);
   static void gemm(const MsArgs<R>& a, bool adjoint, int n_jobs, const DenseJob* jobs, int kslot, cudaStream_t s);
-  // FP32 weight-gradient products of one segment (nslots record slots):
+  // FP32 weight-gradient products of record slots [slot0, slot0 + nslots):
   // record transposes (grid grid_x x n_cols x slot groups) then the tensor-core
   // tiles (n_jobs CTAs), adding into gw / gb
-  static void wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int nslots, const WgTrans* trans, const WgCol* cols,
-                    int n_jobs, const WgJob* jobs, R* gw, R* gb, cudaStream_t s);
+  static void wgrad(const MsArgs<R>& a, int grid_x, int n_cols, int slot0, int nslots, const WgTrans* trans,
+                    const WgCol* cols, int n_jobs, const WgJob* jobs, R* gw, R* gb, cudaStream_t s);
   // FP32: W_l and W_l^T as pre-split tiles; FP64: W_l^T
   static void pack_weights(const R* w, R* wt, R* tiles, const TransSeg* tsegs, int n_tsegs, int n_ttiles,
                            const SplitSeg* ssegs, int n_ssegs, long long split_total, cudaStream_t s);

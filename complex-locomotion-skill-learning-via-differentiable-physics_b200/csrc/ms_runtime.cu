@@ -740,13 +740,16 @@ class SimImpl final : public SimBase {
     const int t_end = eval ? steps + 1 : steps - 1;
     MsArgs<R> a = args(steps);
     qslot_ = 0;
+    // a training episode of one checkpoint segment (steps - 1 <= K): the first
+    // pass records what the segment's recompute would (same kernels, same
+    // values), and the reverse pass starts without a recompute
+    recorded_ = !eval && t_end <= K_;
+    const int mode = FWD_CKPT | FWD_OBS | (recorded_ ? FWD_RECORD : 0);
     if (dense_ && !per_env) {
-      dense_pass(a, 0, t_end, FWD_CKPT | FWD_OBS, 0, true, PK_FWD);
+      dense_pass(a, 0, t_end, mode, 0, true, PK_FWD);
     } else {
       each_launch(per_env, a, qslot_, [&](const MsArgs<R>& b, int grid) {
-        timed(PK_FWD, [&] {
-          fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, FWD_CKPT | FWD_OBS, 0);
-        });
+        timed(PK_FWD, [&] { fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, 0, t_end, mode, 0); });
       });
     }
     CLS_CUDA(cudaGetLastError());
@@ -837,6 +840,7 @@ class SimImpl final : public SimBase {
       long long woff = 0;
       wg_trans_.clear(); wg_cols_.clear(); wg_jobs_.clear();
       wg_grid_x_ = 0;
+      wg_chunk_ = std::min(K_, kWgChunkSlots);
       int n_tiles = 0;
       for (int r = 0; r < (int)hr_.size(); ++r) {
         const RobotDesc& d = rd_host_[r];
@@ -844,12 +848,12 @@ class SimImpl final : public SimBase {
         const HostRobot& h = hr_[r];
         if (d.n_env == 0) continue;
         dd.nep = (d.n_env + 31) & ~31;
-        dd.nkt_w = K_ * dd.nep / 32;
+        dd.nkt_w = wg_chunk_ * dd.nep / 32;
         wg_grid_x_ = std::max(wg_grid_x_, dd.nep / 32);
         for (int l = 0; l < h.n_layers; ++l) {
           const int wi = h.width[l], wo = h.width[l + 1];
-          dd.tw_d[l] = woff; woff += DenseLaunch<R>::split_floats(wo, tm, K_ * dd.nep);
-          dd.tw_a[l] = woff; woff += DenseLaunch<R>::split_floats(wi + 1, tn, K_ * dd.nep);
+          dd.tw_d[l] = woff; woff += DenseLaunch<R>::split_floats(wo, tm, wg_chunk_ * dd.nep);
+          dd.tw_a[l] = woff; woff += DenseLaunch<R>::split_floats(wi + 1, tn, wg_chunk_ * dd.nep);
           const WgTrans ta{r, l, l == 0 ? 0 : 1, wi}, td{r, l, 2, wo};
           for (const WgTrans& tr : {ta, td}) {
             const int job = (int)wg_trans_.size();
@@ -1006,15 +1010,17 @@ class SimImpl final : public SimBase {
     int qslot = qslot_;
     for (int s = n_seg - 1; s >= 0; --s) {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
+      const bool recompute = !(recorded_ && n_seg == 1);
       if (dense_ && !per_env) {
-        dense_pass(a, t0, t1, FWD_RECORD, s, false, PK_RECOMP);
+        if (recompute) dense_pass(a, t0, t1, FWD_RECORD, s, false, PK_RECOMP);
         dense_reverse(a, t0, t1, s == n_seg - 1);
       } else {
-        each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
-          timed(PK_RECOMP, [&] {
-            fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+        if (recompute)
+          each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
+            timed(PK_RECOMP, [&] {
+              fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+            });
           });
-        });
         each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
           timed(PK_REV, [&] {
             rev_fn()<<<grid, threads_, rev_smem_, stream>>>(b, t0, t1, s == n_seg - 1 ? 1 : 0);
@@ -1022,11 +1028,15 @@ class SimImpl final : public SimBase {
         });
       }
       if (dense_ && !per_env && !wg_jobs_.empty()) {
-        // FP32 batched path: record transposes + tensor-core tiles
-        timed(PK_WGRAD, [&] {
-          DenseLaunch<R>::wgrad(a, wg_grid_x_, (int)wg_cols_.size(), t1 - t0, d_wg_trans_.p, d_wg_cols_.p,
-                                (int)wg_jobs_.size(), d_wg_jobs_.p, d_gw_.p, d_gb_.p, stream);
-        });
+        // FP32 batched path: record transposes + tensor-core tiles, in chunks
+        // of at most wg_chunk_ record slots (the operand buffers' size)
+        for (int c0 = 0; c0 < t1 - t0; c0 += wg_chunk_) {
+          const int c1 = std::min(t1 - t0, c0 + wg_chunk_);
+          timed(PK_WGRAD, [&] {
+            DenseLaunch<R>::wgrad(a, wg_grid_x_, (int)wg_cols_.size(), c0, c1 - c0, d_wg_trans_.p, d_wg_cols_.p,
+                                  (int)wg_jobs_.size(), d_wg_jobs_.p, d_gw_.p, d_gb_.p, stream);
+          });
+        }
       } else if (!tiles_host_.empty()) {
         timed(PK_WGRAD, [&] {
           ms_wgrad_kernel<R><<<(int)tiles_host_.size(), 256, 0, stream>>>(a, d_tiles_.p, t1 - t0,
@@ -1629,7 +1639,10 @@ class SimImpl final : public SimBase {
   DevBuf<WgTrans> d_wg_trans_;
   DevBuf<WgCol> d_wg_cols_;
   DevBuf<WgJob> d_wg_jobs_;
-  int wg_grid_x_ = 0;
+  int wg_grid_x_ = 0, wg_chunk_ = 1;
+  // record slots per weight-gradient pass (bounds its operand buffers)
+  static constexpr int kWgChunkSlots = 50;
+  bool recorded_ = false;  // the first pass recorded the only segment
   std::vector<SplitSeg> ssegs_;
   DevBuf<SplitSeg> d_ssegs_;
   long long split_total_ = 0;

@@ -138,6 +138,27 @@ def test_batched_fp32_as_accurate_as_per_env_fp32():
     assert rel_err(b32[3], r64[3]) <= 1.25 * rel_err(p32[3], r64[3]) + 1e-5
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batched_single_segment_equals_segments(precision):
+    """The batched path with the episode as one segment (records from the
+    first pass, no recompute) against the same batch with K = 9."""
+    hidden, steps = [70, 50], 40
+    ref = _many_env_batch(precision, 300, hidden, 9, 48, "batched")
+    r_loss, r_grads, _, r_gx = _run(ref, steps, 3)
+    ref.close()
+    b = _many_env_batch(precision, 300, hidden, 48, 48, "batched")
+    b.profile(True)
+    loss, grads, _, gx = _run(b, steps, 3)
+    _, n = b.profile_read(reset=True)
+    b.close()
+    assert n["recompute"] == 0
+    assert loss == r_loss                 # the same first pass
+    tol = 1e-12 if precision == 64 else 1e-5
+    for (gW, gb), (rW, rb) in zip(grads, r_grads):
+        assert rel_err(gW, rW) < tol and rel_err(gb, rb) < tol
+    assert rel_err(gx, r_gx) < tol
+
+
 def test_batched_graph_replay_matches_eager():
     """The forward pass (spring gather, tensor-core GEMMs) is deterministic, so
     the replayed loss is identical; the atomic adds of the reverse pass

@@ -86,6 +86,30 @@ def test_checkpoint_interval_does_not_change_gradients(K):
     assert rel_err(gw, gw_ref) < 1e-12
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+def test_single_segment_records_in_first_pass(precision):
+    """An episode of one checkpoint segment (steps - 1 <= K) takes its records
+    from the first pass and skips the recompute: the same gradients as a
+    multi-segment schedule (FP64 to rounding of the regrouped weight-gradient
+    sums; FP32 within its atomic-add rounding) and one forward launch fewer
+    per segment."""
+    g = load_golden("quad_ref")
+    steps = int(g["steps"])
+    ref = batch_from_golden(g, precision=precision, K=7)
+    ref.simulate(steps)
+    one = batch_from_golden(g, precision=precision, K=int(g["x"].shape[0]))
+    one.profile(True)
+    one.simulate(steps)
+    _, n = one.profile_read(reset=True)
+    assert n["recompute"] == 0
+    tol = 1e-12 if precision == 64 else 1e-5
+    for l in range(2):
+        assert rel_err(one.get_grads(0, l)[0], ref.get_grads(0, l)[0]) < tol
+    assert rel_err(one.state_grads()[0], ref.state_grads()[0]) < tol
+    ref.close()
+    one.close()
+
+
 def test_per_env_launch_equals_batched():
     g = load_golden("spider_ref")
     steps = int(g["steps"])
