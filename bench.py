@@ -134,14 +134,13 @@ def config_dict(a, n_gpus):
 
 
 # ----------------------------------------------------------- CPU baseline
-def cpu_sample(robots, seed, n_robots, substeps, threads):
+def cpu_sample(robots, seed, n_robots, substeps, threads, min_wall=0.0):
     """Time the FP64 oracle (reference algorithm restated) on a bounded sample:
-    n_robots robots of the workload, `substeps` substeps each, forward + loss +
-    backward, one robot per worker thread."""
+    batches of n_robots robots of the workload (seeded picks), `substeps`
+    substeps each, forward + loss + backward, one robot per worker thread;
+    batches repeat until `min_wall` seconds have passed."""
     from oracle.ms_oracle import MassSpringOracle
     from cls_b200 import workloads
-    rng = np.random.default_rng(seed)
-    pick = rng.choice(len(robots), size=min(n_robots, len(robots)), replace=False)
     T = substeps
 
     def one(r):
@@ -163,13 +162,19 @@ def cpu_sample(robots, seed, n_robots, substeps, threads):
         o.run(T)
         return time.perf_counter() - t0, T - 1
 
-    t0 = time.perf_counter()
+    wall, env_substeps, n_run, batch = 0.0, 0, 0, 0
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        res = list(ex.map(one, pick))
-    wall = time.perf_counter() - t0
-    env_substeps = sum(n for _, n in res)
-    return env_substeps / wall, "%d robots of the workload x %d substeps (forward+loss+backward, FP64)" % (
-        len(pick), T - 1), wall
+        while batch == 0 or wall < min_wall:
+            rng = np.random.default_rng(seed + 7919 * batch)
+            pick = rng.choice(len(robots), size=min(n_robots, len(robots)), replace=False)
+            t0 = time.perf_counter()
+            res = list(ex.map(one, pick))
+            wall += time.perf_counter() - t0
+            env_substeps += sum(n for _, n in res)
+            n_run += len(pick)
+            batch += 1
+    return env_substeps / wall, ("%d robots of the workload (%d batches) x %d substeps "
+                                 "(forward+loss+backward, FP64)" % (n_run, batch, T - 1)), wall
 
 
 def run_reference(a):
@@ -195,8 +200,12 @@ def run_reference(a):
     cores = os.cpu_count() or 1
     vals = []
     sample = ""
+    # warm-up steps run one batch; each timed step is a bounded sample of at
+    # least min(10 s, 150 s / steps) so that the whole run ends within minutes
+    per_step = min(10.0, 150.0 / max(1, a.steps))
     for i in range(a.warmup + a.steps):
-        v, sample, wall = cpu_sample(robots, 100 + i, n_robots=cores * 2, substeps=200, threads=cores)
+        v, sample, wall = cpu_sample(robots, 100 + i, n_robots=cores * 2, substeps=200, threads=cores,
+                                     min_wall=per_step if i >= a.warmup else 0.0)
         if i >= a.warmup:
             vals.append(v)
     value = float(np.mean(vals))
@@ -447,7 +456,7 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = os.cpu_count() or 1
         v, sample, wall = cpu_sample([robots[r] for r in env_robot], 11, n_robots=cores * 2,
-                                     substeps=200, threads=cores)
+                                     substeps=200, threads=cores, min_wall=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": sample + "; wall %.1f s; reference Taichi not installed (no network)" % wall}
 
@@ -468,10 +477,11 @@ def run_ours(a):
 
 
 # ------------------------------------------------------------------- MPM
-def mpm_cpu_sample(a, seed, envs, substeps):
+def mpm_cpu_sample(a, seed, envs, substeps, min_wall=0.0):
     """Time the FP64 MPM oracle (OpenMP over envs, all host cores) on `envs`
     envs of the workload body for `substeps` substeps, forward + loss +
-    backward."""
+    backward, repeated with fresh seeded actuation until `min_wall` seconds
+    have passed."""
     from oracle.mpm_oracle import MPMOracle
     from cls_b200 import workloads
     pos, mus, fib = workloads.legged_body()
@@ -480,21 +490,26 @@ def mpm_cpu_sample(a, seed, envs, substeps):
                   mu=E / (2 * (1 + nu)), la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3,
                   gravity=-10.0, bound=3, material="neo_hookean", fibre=fib, n_muscles=16)
     rng = np.random.default_rng(seed)
-    o.act[...] = rng.uniform(-1, 1, o.act.shape)
     o.loss_w[substeps] = 1.0
     o.target[...] = pos.mean(axis=0) + np.array([0.05, 0.0, 0.0])
-    t0 = time.perf_counter()
-    o.run(substeps)
-    wall = time.perf_counter() - t0
-    return envs * substeps / wall, "%d envs x %d substeps of the workload body (forward+loss+backward, " \
-        "FP64, OpenMP over envs)" % (envs, substeps), wall
+    wall, runs = 0.0, 0
+    while runs == 0 or wall < min_wall:
+        o.act[...] = rng.uniform(-1, 1, o.act.shape)
+        t0 = time.perf_counter()
+        o.run(substeps)
+        wall += time.perf_counter() - t0
+        runs += 1
+    return runs * envs * substeps / wall, "%d envs x %d substeps of the workload body, %d runs " \
+        "(forward+loss+backward, FP64, OpenMP over envs)" % (envs, substeps, runs), wall
 
 
 def run_reference_mpm(a):
     cores = os.cpu_count() or 1
     vals, sample = [], ""
+    per_step = min(10.0, 150.0 / max(1, a.steps))
     for i in range(a.warmup + a.steps):
-        v, sample, _ = mpm_cpu_sample(a, 100 + i, envs=cores, substeps=24)
+        v, sample, _ = mpm_cpu_sample(a, 100 + i, envs=cores, substeps=24,
+                                      min_wall=per_step if i >= a.warmup else 0.0)
         if i >= a.warmup:
             vals.append(v)
     value = float(np.mean(vals))
@@ -616,7 +631,7 @@ def run_mpm(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        v, sample, wall = mpm_cpu_sample(a, 11, envs=cores, substeps=24)
+        v, sample, wall = mpm_cpu_sample(a, 11, envs=cores, substeps=24, min_wall=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": sample + "; wall %.1f s; the reference's MPM is 2D and needs Taichi" % wall}
 
