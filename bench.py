@@ -71,7 +71,10 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: automatic)")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="threads per CTA of the fused kernels (0: autotuned, see --no-autotune)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="mass-spring: skip the launch-shape autotuner (cls_autotune) before warm-up")
     ap.add_argument("--controller", default="auto", choices=["auto", "per_env", "batched"],
                     help="controller path: batched = one tensor-core GEMM per layer over all envs "
                          "of a robot type (automatic for types with >= 256 envs)")
@@ -292,10 +295,25 @@ def run_ours(a):
     import cls_b200
     from cls_b200 import workloads
     b, robots, env_robot, (tv, th) = make_ms_batch(a, a.robots, 1000 * rank)
-    b.set_controller_path(a.controller)
-    batched = b.controller_batched
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
+    # launch shape (and, with --controller auto, the controller path) picked
+    # by timing this workload's own rollouts, before warm-up and outside the
+    # timed region
+    tuned = None
+    if not a.no_autotune and not a.threads:
+        t0 = time.perf_counter()
+        tuned = b.autotune(repeats=1)
+        tuned["seconds"] = time.perf_counter() - t0
+    if a.controller != "auto" or tuned is None:
+        b.set_controller_path(a.controller)
+    batched = b.controller_batched
+    tpb, cps = b.launch_shape
+    launch_shape = {"threads_per_block": tpb, "ctas_per_sm": cps, "autotuned": tuned is not None}
+    if tuned is not None:
+        launch_shape.update(candidates=len(tuned["table"]), tuning_s=round(tuned["seconds"], 2),
+                            table=[[e["controller_path"], e["threads_per_block"], e["ctas_per_sm"],
+                                    round(e["ms"], 3)] for e in tuned["table"]])
     env_substeps = b.n_envs * (a.substeps - 1)
 
     def iteration(it):
@@ -392,6 +410,7 @@ def run_ours(a):
     plain = None
     if rank == 0 and a.plain_sample > 0:
         pb, _, sub, _ = make_ms_batch(a, min(a.plain_sample, a.robots), 7, robots=robots[:a.plain_sample])
+        pb.set_launch_shape(tpb, cps)
         ps = torch.cuda.Stream()
         pb.set_stream(ps.cuda_stream)
         pb.simulate(a.substeps, per_env=True)
@@ -466,6 +485,7 @@ def run_ours(a):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded random lattices, targets and weights)",
                 "config": config_dict(a, world), "controller_path": "batched" if batched else "per_env",
+                "launch_shape": launch_shape,
                 "clocks": clocks,
                 "gpu_launches": int(sum(prof_n.values())) * a.steps, "roofline": roofline,
                 "plain": plain, "e2e": e2e, "cpu_baseline": cpu}

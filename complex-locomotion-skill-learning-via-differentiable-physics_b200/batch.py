@@ -270,6 +270,75 @@ class MassSpringBatch:
         self._c(self.lib.cls_controller_batched(self.h, on.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
         return bool(on[0])
 
+    # ------------------------------------------------------------ launch shape
+    def set_launch_shape(self, threads_per_block, ctas_per_sm=2):
+        """Threads per CTA of the fused segment kernels and the CTAs per SM the
+        persistent grid is sized for (``cls_set_launch_shape``)."""
+        self._c(self.lib.cls_set_launch_shape(self.h, int(threads_per_block), int(ctas_per_sm)))
+
+    @property
+    def launch_shape(self):
+        t, c = np.zeros(1, dtype=np.int32), np.zeros(1, dtype=np.int32)
+        self._c(self.lib.cls_get_launch_shape(self.h, ptr(t, _capi.P_I), ptr(c, _capi.P_I)))
+        return int(t[0]), int(c[0])
+
+    def _tune_key(self, steps):
+        import hashlib
+        import json
+        try:
+            import torch
+            device = torch.cuda.get_device_name(torch.cuda.current_device())
+        except Exception:                                    # no torch: key on the rest
+            device = "cuda"
+        counts = np.bincount(self.env_robot, minlength=len(self.robots))
+        sig = {"device": device, "precision": int(self.params.precision),
+               "K": int(self.params.checkpoint_every), "T": int(self.T), "steps": int(steps),
+               "types": [[r.n_vertices, r.n_springs, list(map(int, r.hidden)), int(r.n_outputs),
+                          int(n)] for r, n in zip(self.robots, counts)]}
+        return hashlib.sha1(json.dumps(sig, sort_keys=True).encode()).hexdigest()
+
+    def autotune(self, steps=0, repeats=2, cache=None):
+        """Time the fused kernels' launch shapes (threads per CTA x CTAs per SM)
+        and, for robot types with many envs, the batched controller path on this
+        batch's own workload, and apply the fastest (``cls_autotune``).  Needs
+        the state, targets and weights set.  ``cache``: path of a JSON file; a
+        workload tuned before (same device, robot shapes, env counts,
+        precision, K, horizon) is applied from it without timing.  Returns
+        ``{"threads_per_block", "ctas_per_sm", "controller_path", "table",
+        "cached"}``."""
+        import json
+        import os
+        key = self._tune_key(steps)
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                hit = json.load(f).get(key)
+            if hit:
+                self.set_controller_path(hit["controller_path"])
+                self.set_launch_shape(hit["threads_per_block"], hit["ctas_per_sm"])
+                return dict(hit, cached=True)
+        cap = 64
+        table = (_capi.LaunchShape * cap)()
+        n = np.zeros(1, dtype=np.int32)
+        self._c(self.lib.cls_autotune(self.h, int(steps), int(repeats), table, cap, ptr(n, _capi.P_I)))
+        names = {v: k for k, v in self.CONTROLLER_PATHS.items()}
+        rows = [{"controller_path": names[e.controller_path], "threads_per_block": e.threads_per_block,
+                 "ctas_per_sm": e.ctas_per_sm, "ms": float(e.ms)} for e in table[:min(int(n[0]), cap)]]
+        t, c = self.launch_shape
+        out = {"threads_per_block": t, "ctas_per_sm": c,
+               "controller_path": "batched" if self.controller_batched else "per_env", "table": rows}
+        if cache:
+            data = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    data = json.load(f)
+            data[key] = out
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            tmp = cache + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(data, f, indent=1)
+            os.replace(tmp, cache)
+        return dict(out, cached=False)
+
     # ----------------------------------------------------------------- outputs
     def observables(self):
         T, E = self.T, self.n_envs

@@ -173,6 +173,10 @@ class SimBase {
   // controller path: 0 auto, 1 per env (fused segment kernels), 2 batched
   virtual void set_controller_path(int path) = 0;
   virtual bool controller_batched() const = 0;
+  // fused kernels' launch shape and the autotuner over it
+  virtual void set_launch_shape(int threads, int ctas) = 0;
+  virtual void launch_shape(int* threads, int* ctas) const = 0;
+  virtual void autotune(int steps, int repeats, std::vector<cls_launch_shape>& table) = 0;
 };
 
 template <typename R>
@@ -389,33 +393,15 @@ class SimImpl final : public SimBase {
     std::stable_sort(order_host_.begin(), order_host_.end(),
                      [&](int a, int b) { return cost(a) > cost(b); });
     // launch shape
-    threads_ = p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads();
-    CLS_REQUIRE(threads_ % 32 == 0 && threads_ >= 64 && threads_ <= 1024,
-                "threads_per_block must be a multiple of 32 in [64, 1024]");
     smem_p0max_ = p0max;
     smem_dmax_ = dmax;
     smem_amax_ = amax;
     smem_omax_ = omax;
     fwd_smem_ = fwd_smem_bytes<R>(nmax_, dmax, p0max);
-    rev_smem_ = rev_smem_bytes<R>(nmax_, amax, omax, dmax, threads_);
-    int dev = 0, optin = 0;
+    int dev = 0;
     CLS_CUDA(cudaGetDevice(&dev));
-    CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     CLS_CUDA(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, dev));
-    // The dynamic shared-memory limit is a per-kernel, process-wide attribute:
-    // raise it once to the device maximum (minus the kernel's static shared
-    // memory) so that handles with different robot sizes never lower it for
-    // one another.
-    cudaFuncAttributes fa{}, ra{};
-    CLS_CUDA(cudaFuncGetAttributes(&fa, fwd_fn()));
-    CLS_CUDA(cudaFuncGetAttributes(&ra, rev_fn()));
-    const size_t fwd_cap = (size_t)optin - fa.sharedSizeBytes;
-    const size_t rev_cap = (size_t)optin - ra.sharedSizeBytes;
-    CLS_REQUIRE(fwd_smem_ <= fwd_cap && rev_smem_ <= rev_cap,
-                "robot too large for one CTA's shared memory (" + std::to_string(rev_smem_) +
-                    " bytes needed, " + std::to_string(rev_cap) + " available)");
-    CLS_CUDA(cudaFuncSetAttribute(fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_cap));
-    CLS_CUDA(cudaFuncSetAttribute(rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_cap));
+    use_threads(p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads());
     // GEMM tiles (per robot, per layer); a robot shared by many envs splits
     // its K = envs x substeps rows over several CTAs (about 2048 rows each)
     for (int r = 0; r < nr; ++r) {
@@ -560,6 +546,141 @@ class SimImpl final : public SimBase {
                            : (threads_ <= 512 ? ms_reverse_kernel<R, 512> : ms_reverse_kernel<R, 1024>);
   }
 
+  // Threads per CTA of the fused kernels: selects the kernel instance, raises
+  // its dynamic shared-memory limit and checks that the largest robot fits and
+  // that at least one CTA can be resident.  The limit is a per-kernel,
+  // process-wide attribute: it is raised to the device maximum (minus the
+  // kernel's static shared memory) so that handles with different robot sizes
+  // never lower it for one another.  On failure the previous shape stays.
+  void use_threads(int threads) {
+    CLS_REQUIRE(threads % 32 == 0 && threads >= 64 && threads <= 1024,
+                "threads_per_block must be a multiple of 32 in [64, 1024]");
+    const int keep = threads_;
+    threads_ = threads;
+    try {
+      const size_t rev = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, threads);
+      int dev = 0, optin = 0;
+      CLS_CUDA(cudaGetDevice(&dev));
+      CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+      cudaFuncAttributes fa{}, ra{};
+      CLS_CUDA(cudaFuncGetAttributes(&fa, fwd_fn()));
+      CLS_CUDA(cudaFuncGetAttributes(&ra, rev_fn()));
+      const size_t fwd_cap = (size_t)optin - fa.sharedSizeBytes;
+      const size_t rev_cap = (size_t)optin - ra.sharedSizeBytes;
+      CLS_REQUIRE(fwd_smem_ <= fwd_cap && rev <= rev_cap,
+                  "robot too large for one CTA's shared memory (" + std::to_string(rev) +
+                      " bytes needed, " + std::to_string(rev_cap) + " available)");
+      CLS_CUDA(cudaFuncSetAttribute(fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_cap));
+      CLS_CUDA(cudaFuncSetAttribute(rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_cap));
+      int nf = 0, nb = 0;
+      CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nf, fwd_fn(), threads, fwd_smem_));
+      CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rev_fn(), threads, rev));
+      CLS_REQUIRE(nf >= 1 && nb >= 1,
+                  "no CTA of " + std::to_string(threads) + " threads can be resident on an SM");
+      rev_smem_ = rev;
+      resident_ = std::min(nf, nb);
+    } catch (...) {
+      threads_ = keep;
+      throw;
+    }
+  }
+
+  void set_launch_shape(int threads, int ctas) override {
+    CLS_REQUIRE(!capturing_, "the launch shape cannot change during graph capture");
+    CLS_REQUIRE(ctas >= 1 && ctas <= 32, "ctas_per_sm must be in [1, 32]");
+    use_threads(threads);
+    ctas_per_sm_ = ctas;
+  }
+  void launch_shape(int* threads, int* ctas) const override {
+    *threads = threads_;
+    *ctas = ctas_per_sm_;
+  }
+
+  // one training rollout (forward, loss, reverse) as the autotuner times it:
+  // one untimed run, then `repeats` runs between CUDA events on the stream
+  float time_rollout(int steps, int repeats) {
+    struct Events {
+      cudaEvent_t a = nullptr, b = nullptr;
+      ~Events() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+      }
+    } ev;
+    CLS_CUDA(cudaEventCreate(&ev.a));
+    CLS_CUDA(cudaEventCreate(&ev.b));
+    auto run = [&] {
+      forward(steps, false, false);
+      loss_device();
+      backward(false);
+    };
+    run();
+    CLS_CUDA(cudaEventRecord(ev.a, stream));
+    for (int i = 0; i < repeats; ++i) run();
+    CLS_CUDA(cudaEventRecord(ev.b, stream));
+    CLS_CUDA(cudaEventSynchronize(ev.b));
+    float ms = 0;
+    CLS_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
+    // a timed-out tensor-core wait fails the tuning; non-finite states (the
+    // caller's data) do not change the timing and stay for the caller's run
+    if (synchronize() == CLS_ERR_CUDA) throw Fail{CLS_ERR_CUDA, err};
+    return ms / repeats;
+  }
+
+  static constexpr int kTuneDenseEnvs = 32;
+  static constexpr int kTuneMaxCtas = 4;
+
+  void autotune(int steps, int repeats, std::vector<cls_launch_shape>& table) override {
+    CLS_REQUIRE(!capturing_ && !prof_.on, "autotune needs profiling off and no graph capture");
+    if (steps <= 0) steps = std::min(T_, std::min(2 * K_ + 1, 101));
+    CLS_REQUIRE(steps >= 2 && steps <= T_, "tuning rollout needs 2 <= steps <= max_steps");
+    repeats = std::max(1, repeats);
+    const int keep_threads = threads_, keep_ctas = ctas_per_sm_;
+    const bool keep_dense = dense_;
+    bool can_dense = true;
+    for (const RobotDesc& d : rd_host_)
+      if (d.n_env > 0 && d.n_env < kTuneDenseEnvs) can_dense = false;
+    table.clear();
+    try {
+      dense_ = false;
+      for (int threads : {128, 256, 512, 1024}) {
+        try {
+          use_threads(threads);
+        } catch (const Fail& f) {
+          if (f.code != CLS_ERR_INVALID) throw;
+          continue;  // the largest robot does not fit this instance
+        }
+        for (int ctas = 1; ctas <= std::min(resident_, kTuneMaxCtas); ++ctas) {
+          ctas_per_sm_ = ctas;
+          table.push_back({CLS_CONTROLLER_PER_ENV, threads, ctas, time_rollout(steps, repeats)});
+        }
+      }
+      CLS_REQUIRE(!table.empty(), "no launch shape fits the largest robot");
+      size_t best = 0;
+      for (size_t i = 1; i < table.size(); ++i)
+        if (table[i].ms < table[best].ms) best = i;
+      // the fused kernels keep their fastest shape (per-env launches and
+      // serving windows use them on either controller path)
+      use_threads(table[best].threads_per_block);
+      ctas_per_sm_ = table[best].ctas_per_sm;
+      if (can_dense) {
+        set_controller_path(CLS_CONTROLLER_BATCHED);
+        table.push_back({CLS_CONTROLLER_BATCHED, threads_, ctas_per_sm_, time_rollout(steps, repeats)});
+        if (table.back().ms >= table[best].ms) set_controller_path(CLS_CONTROLLER_PER_ENV);
+      } else {
+        set_controller_path(CLS_CONTROLLER_PER_ENV);
+      }
+    } catch (...) {
+      try {
+        use_threads(keep_threads);
+      } catch (...) {
+      }
+      ctas_per_sm_ = keep_ctas;
+      dense_ = keep_dense;
+      fwd_done_ = bwd_done_ = false;
+      throw;
+    }
+  }
+
   int auto_threads() const {
     // enough warps for the per-row MLP products and the vertex loops; more
     // threads than that only adds barrier cost
@@ -657,7 +778,7 @@ class SimImpl final : public SimBase {
     return a;
   }
 
-  int grid_for(int items) const { return std::max(1, std::min(items, n_sm_ * 2)); }
+  int grid_for(int items) const { return std::max(1, std::min(items, n_sm_ * ctas_per_sm_)); }
 
   // one batched launch (all envs) or one launch per env
   template <typename F>
@@ -1585,6 +1706,7 @@ class SimImpl final : public SimBase {
   long long z_base_[kMaxLayers] = {0};
   long long rec_z_total_ = 0;
   int smem_p0max_ = 0, smem_dmax_ = 0, smem_amax_ = 0, smem_omax_ = 0, threads_ = 256, n_sm_ = 148, n_ckpt_ = 0;
+  int ctas_per_sm_ = 2, resident_ = 1;
   size_t fwd_smem_ = 0, rev_smem_ = 0, n_queue_ = 0;
   std::vector<int> perm_, user_voff_, env_robot_, order_host_;
   bool identity_perm_ = true;
@@ -1969,6 +2091,30 @@ int cls_controller_batched(const cls_sim* sim, int32_t* on) {
   if (!sim || !sim->impl || !on) return CLS_ERR_INVALID;
   *on = sim->impl->controller_batched() ? 1 : 0;
   return CLS_OK;
+}
+
+int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_per_sm) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_launch_shape(threads_per_block, ctas_per_sm); });
+}
+
+int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm) {
+  if (!sim || !sim->impl || !threads_per_block || !ctas_per_sm) return CLS_ERR_INVALID;
+  int t = 0, c = 0;
+  sim->impl->launch_shape(&t, &c);
+  *threads_per_block = t;
+  *ctas_per_sm = c;
+  return CLS_OK;
+}
+
+int cls_autotune(cls_sim* sim, int32_t steps, int32_t repeats, cls_launch_shape* table,
+                 int32_t max_entries, int32_t* n_entries) {
+  if (max_entries < 0 || (max_entries > 0 && !table)) return CLS_ERR_INVALID;
+  return guarded(sim, [&](cls::SimBase& s) {
+    std::vector<cls_launch_shape> t;
+    s.autotune(steps, repeats, t);
+    for (int i = 0; i < (int)t.size() && i < max_entries; ++i) table[i] = t[i];
+    if (n_entries) *n_entries = (int32_t)t.size();
+  });
 }
 
 }  // extern "C"

@@ -80,3 +80,24 @@ def max_rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def many_env_batch(precision, n_envs, hidden, K, steps_max, path):
+    """n_envs envs of the quadruped golden robot with a custom controller
+    (hidden widths `hidden`, Xavier-uniform weights), seeded perturbed
+    states and targets, on controller path `path`."""
+    import cls_b200
+    g = load_golden("quad_ref")
+    robot = cls_b200.Robot(g["objects"], g["springs"], robot_id=int(g["robot_id"]), hidden=hidden,
+                           n_outputs=0)
+    p = params_from_golden(g, precision=precision, K=K, max_steps=steps_max,
+                           loss=["velocity", "height", "rotation"])
+    b = cls_b200.MassSpringBatch([robot], [0] * n_envs, p)
+    b.set_controller_path(path)
+    rng = np.random.default_rng(11)
+    b.set_state(np.tile(g["x0"][0], (n_envs, 1)) + rng.normal(0, 1e-3, (n_envs * g["objects"].shape[0], 3)))
+    b.set_targets(rng.uniform(-0.1, 0.1, (steps_max, n_envs, 3)), rng.choice([-1.0, 0.0, 1.0], (steps_max, n_envs)))
+    for l in range(len(hidden) + 1):
+        rows, cols = b.layer_shape(0, l)
+        b.set_weights(0, l, rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6 / cols), rng.uniform(-0.1, 0.1, rows))
+    return b

@@ -10,7 +10,7 @@ losses, 1e-8 on gradients; FP32 rel 1e-5 on trajectories over these
 import numpy as np
 import pytest
 
-from helpers import (TRAIN_CASES, batch_from_golden, load_golden, max_rel,
+from helpers import (TRAIN_CASES, batch_from_golden, load_golden, many_env_batch, max_rel,
                      oracle_from_golden, rel_err)
 
 pytestmark = pytest.mark.gpu
@@ -68,25 +68,6 @@ def test_batched_gradients_match_oracle(case, precision):
     b.close()
 
 
-def _many_env_batch(precision, n_envs, hidden, K, steps_max, path):
-    import cls_b200
-    from helpers import params_from_golden
-    g = load_golden("quad_ref")
-    robot = cls_b200.Robot(g["objects"], g["springs"], robot_id=int(g["robot_id"]), hidden=hidden,
-                           n_outputs=0)
-    p = params_from_golden(g, precision=precision, K=K, max_steps=steps_max,
-                           loss=["velocity", "height", "rotation"])
-    b = cls_b200.MassSpringBatch([robot], [0] * n_envs, p)
-    b.set_controller_path(path)
-    rng = np.random.default_rng(11)
-    b.set_state(np.tile(g["x0"][0], (n_envs, 1)) + rng.normal(0, 1e-3, (n_envs * g["objects"].shape[0], 3)))
-    b.set_targets(rng.uniform(-0.1, 0.1, (steps_max, n_envs, 3)), rng.choice([-1.0, 0.0, 1.0], (steps_max, n_envs)))
-    for l in range(len(hidden) + 1):
-        rows, cols = b.layer_shape(0, l)
-        b.set_weights(0, l, rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6 / cols), rng.uniform(-0.1, 0.1, rows))
-    return b
-
-
 def _run(b, steps, n_layers):
     loss = b.simulate(steps)
     grads = [b.get_grads(0, l) for l in range(n_layers)]
@@ -99,11 +80,11 @@ def test_batched_equals_per_env_with_partial_tiles_fp64():
     """300 envs (tiles of 64 envs: four full and one partial) and hidden
     widths 70 and 50 (partial output tiles); several checkpoint segments."""
     hidden, steps = [70, 50], 40
-    ref = _many_env_batch(64, 300, hidden, 9, 48, "per_env")
+    ref = many_env_batch(64, 300, hidden, 9, 48, "per_env")
     assert not ref.controller_batched
     r_loss, r_grads, r_x, r_gx = _run(ref, steps, 3)
     ref.close()
-    b = _many_env_batch(64, 300, hidden, 9, 48, "auto")
+    b = many_env_batch(64, 300, hidden, 9, 48, "auto")
     assert b.controller_batched          # >= 256 envs of one type: automatic
     loss, grads, x, gx = _run(b, steps, 3)
     b.close()
@@ -124,7 +105,7 @@ def test_batched_fp32_as_accurate_as_per_env_fp32():
     hidden, steps = [70, 50], 40
     runs = {}
     for prec, path in ((64, "per_env"), (32, "per_env"), (32, "batched")):
-        b = _many_env_batch(prec, 300, hidden, 9, 48, path)
+        b = many_env_batch(prec, 300, hidden, 9, 48, path)
         runs[(prec, path)] = _run(b, steps, 3)
         b.close()
     r64, p32, b32 = runs[(64, "per_env")], runs[(32, "per_env")], runs[(32, "batched")]
@@ -143,10 +124,10 @@ def test_batched_single_segment_equals_segments(precision):
     """The batched path with the episode as one segment (records from the
     first pass, no recompute) against the same batch with K = 9."""
     hidden, steps = [70, 50], 40
-    ref = _many_env_batch(precision, 300, hidden, 9, 48, "batched")
+    ref = many_env_batch(precision, 300, hidden, 9, 48, "batched")
     r_loss, r_grads, _, r_gx = _run(ref, steps, 3)
     ref.close()
-    b = _many_env_batch(precision, 300, hidden, 48, 48, "batched")
+    b = many_env_batch(precision, 300, hidden, 48, 48, "batched")
     b.profile(True)
     loss, grads, _, gx = _run(b, steps, 3)
     _, n = b.profile_read(reset=True)
@@ -165,7 +146,7 @@ def test_batched_graph_replay_matches_eager():
     (actuation gradients, split-K weight gradients) only change the gradients'
     rounding."""
     import torch
-    b = _many_env_batch(32, 260, [64], 10, 40, "batched")
+    b = many_env_batch(32, 260, [64], 10, 40, "batched")
     e_loss, e_grads, _, _ = _run(b, 30, 2)
     s = torch.cuda.Stream()
     b.set_stream(s.cuda_stream)
@@ -183,7 +164,7 @@ def test_batched_graph_replay_matches_eager():
 
 
 def test_batched_profile_counts_gemm_launches():
-    b = _many_env_batch(32, 256, [64, 64], 10, 30, "batched")
+    b = many_env_batch(32, 256, [64, 64], 10, 30, "batched")
     b.profile(True)
     b.simulate(20)
     ms, n = b.profile_read(reset=True)
