@@ -308,12 +308,13 @@ def run_ours(a):
     if a.controller != "auto" or tuned is None:
         b.set_controller_path(a.controller)
     batched = b.controller_batched
-    tpb, cps = b.launch_shape
-    launch_shape = {"threads_per_block": tpb, "ctas_per_sm": cps, "autotuned": tuned is not None}
+    tpb, cps, wsh = b.launch_shape
+    launch_shape = {"threads_per_block": tpb, "ctas_per_sm": cps, "weights_shared": wsh,
+                    "autotuned": tuned is not None}
     if tuned is not None:
         launch_shape.update(candidates=len(tuned["table"]), tuning_s=round(tuned["seconds"], 2),
                             table=[[e["controller_path"], e["threads_per_block"], e["ctas_per_sm"],
-                                    round(e["ms"], 3)] for e in tuned["table"]])
+                                    e["weights_shared"], round(e["ms"], 3)] for e in tuned["table"]])
     env_substeps = b.n_envs * (a.substeps - 1)
 
     def iteration(it):
@@ -410,7 +411,7 @@ def run_ours(a):
     plain = None
     if rank == 0 and a.plain_sample > 0:
         pb, _, sub, _ = make_ms_batch(a, min(a.plain_sample, a.robots), 7, robots=robots[:a.plain_sample])
-        pb.set_launch_shape(tpb, cps)
+        pb.set_launch_shape(tpb, cps, wsh)
         ps = torch.cuda.Stream()
         pb.set_stream(ps.cuda_stream)
         pb.simulate(a.substeps, per_env=True)

@@ -52,7 +52,7 @@ class SimParams(ctypes.Structure):
 
 class LaunchShape(ctypes.Structure):
     _fields_ = [("controller_path", c_int32), ("threads_per_block", c_int32),
-                ("ctas_per_sm", c_int32), ("ms", ctypes.c_float)]
+                ("ctas_per_sm", c_int32), ("weights_shared", c_int32), ("ms", ctypes.c_float)]
 
 
 class ClsError(RuntimeError):
@@ -97,8 +97,8 @@ _SIGS = {
     "cls_graph_launch": (c_int32, [ctypes.c_void_p, c_int32]),
     "cls_set_controller_path": (c_int32, [ctypes.c_void_p, c_int32]),
     "cls_controller_batched": (c_int32, [ctypes.c_void_p, P_I]),
-    "cls_set_launch_shape": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
-    "cls_get_launch_shape": (c_int32, [ctypes.c_void_p, P_I, P_I]),
+    "cls_set_launch_shape": (c_int32, [ctypes.c_void_p, c_int32, c_int32, c_int32]),
+    "cls_get_launch_shape": (c_int32, [ctypes.c_void_p, P_I, P_I, P_I]),
     "cls_autotune": (c_int32, [ctypes.c_void_p, c_int32, c_int32, ctypes.POINTER(LaunchShape),
                                c_int32, P_I]),
     "cls_serve_reset_env": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D, P_D, P_D, P_D]),

@@ -271,16 +271,21 @@ class MassSpringBatch:
         return bool(on[0])
 
     # ------------------------------------------------------------ launch shape
-    def set_launch_shape(self, threads_per_block, ctas_per_sm=2):
-        """Threads per CTA of the fused segment kernels and the CTAs per SM the
-        persistent grid is sized for (``cls_set_launch_shape``)."""
-        self._c(self.lib.cls_set_launch_shape(self.h, int(threads_per_block), int(ctas_per_sm)))
+    def set_launch_shape(self, threads_per_block, ctas_per_sm=2, weights_shared=-1):
+        """Threads per CTA of the fused segment kernels, the CTAs per SM the
+        persistent grid is sized for, and whether each env's controller is
+        kept in shared memory (1), read from global memory (0) or chosen by
+        fit (-1) (``cls_set_launch_shape``)."""
+        self._c(self.lib.cls_set_launch_shape(self.h, int(threads_per_block), int(ctas_per_sm),
+                                              int(weights_shared)))
 
     @property
     def launch_shape(self):
-        t, c = np.zeros(1, dtype=np.int32), np.zeros(1, dtype=np.int32)
-        self._c(self.lib.cls_get_launch_shape(self.h, ptr(t, _capi.P_I), ptr(c, _capi.P_I)))
-        return int(t[0]), int(c[0])
+        """(threads per CTA, CTAs per SM, controller in shared memory 0/1)."""
+        t, c, w = (np.zeros(1, dtype=np.int32) for _ in range(3))
+        self._c(self.lib.cls_get_launch_shape(self.h, ptr(t, _capi.P_I), ptr(c, _capi.P_I),
+                                              ptr(w, _capi.P_I)))
+        return int(t[0]), int(c[0]), int(w[0])
 
     def _tune_key(self, steps):
         import hashlib
@@ -304,8 +309,8 @@ class MassSpringBatch:
         the state, targets and weights set.  ``cache``: path of a JSON file; a
         workload tuned before (same device, robot shapes, env counts,
         precision, K, horizon) is applied from it without timing.  Returns
-        ``{"threads_per_block", "ctas_per_sm", "controller_path", "table",
-        "cached"}``."""
+        ``{"threads_per_block", "ctas_per_sm", "weights_shared",
+        "controller_path", "table", "cached"}``."""
         import json
         import os
         key = self._tune_key(steps)
@@ -314,7 +319,7 @@ class MassSpringBatch:
                 hit = json.load(f).get(key)
             if hit:
                 self.set_controller_path(hit["controller_path"])
-                self.set_launch_shape(hit["threads_per_block"], hit["ctas_per_sm"])
+                self.set_launch_shape(hit["threads_per_block"], hit["ctas_per_sm"], hit["weights_shared"])
                 return dict(hit, cached=True)
         cap = 64
         table = (_capi.LaunchShape * cap)()
@@ -322,9 +327,10 @@ class MassSpringBatch:
         self._c(self.lib.cls_autotune(self.h, int(steps), int(repeats), table, cap, ptr(n, _capi.P_I)))
         names = {v: k for k, v in self.CONTROLLER_PATHS.items()}
         rows = [{"controller_path": names[e.controller_path], "threads_per_block": e.threads_per_block,
-                 "ctas_per_sm": e.ctas_per_sm, "ms": float(e.ms)} for e in table[:min(int(n[0]), cap)]]
-        t, c = self.launch_shape
-        out = {"threads_per_block": t, "ctas_per_sm": c,
+                 "ctas_per_sm": e.ctas_per_sm, "weights_shared": e.weights_shared, "ms": float(e.ms)}
+                for e in table[:min(int(n[0]), cap)]]
+        t, c, w = self.launch_shape
+        out = {"threads_per_block": t, "ctas_per_sm": c, "weights_shared": w,
                "controller_path": "batched" if self.controller_batched else "per_env", "table": rows}
         if cache:
             data = {}

@@ -120,6 +120,10 @@ struct MsArgs {
   // layer outputs (max of hidden widths and n_out, padded to 4), reverse
   // buffer A (max of outputs and the position block), MLP outputs alone
   int smem_nmax, smem_p0max, smem_dmax, smem_amax, smem_omax;
+  // controller in shared memory for the whole item (fused kernels, robots
+  // small enough): capacities of the weight and bias copies in elements;
+  // 0: weights and biases are read from global memory every substep
+  int w_smem, b_smem;
   R dt, gravity, ground, drag_s, dashpot, friction, max_speed;
   // tables
   const RobotDesc* robots;
@@ -199,6 +203,7 @@ struct FwdSmem {
   R* ain;          // compact input, padded
   R* buf0; R* buf1;
   R* red;          // kRed entries
+  R* w; R* b;      // the env's controller when MsArgs::w_smem > 0, else null
 };
 
 template <typename R>
@@ -213,7 +218,16 @@ __device__ __forceinline__ FwdSmem<R> carve_fwd(char* base, const MsArgs<R>& a) 
   s.buf0 = (R*)take(sizeof(R) * a.smem_dmax);
   s.buf1 = (R*)take(sizeof(R) * a.smem_dmax);
   s.red = (R*)take(sizeof(R) * kRed);
+  s.w = a.w_smem ? (R*)take(sizeof(R) * a.w_smem) : nullptr;
+  s.b = a.w_smem ? (R*)take(sizeof(R) * a.b_smem) : nullptr;
   return s;
+}
+
+// shared memory of the controller copy (weights, then biases)
+template <typename R>
+__host__ __device__ inline size_t ctrl_smem_bytes(long long w_elems, long long b_elems) {
+  auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return w_elems > 0 ? rb(sizeof(R) * (size_t)w_elems) + rb(sizeof(R) * (size_t)b_elems) : 0;
 }
 
 template <typename R>
@@ -235,6 +249,7 @@ struct RevSmem {
   R* dz;           // union region, MLP phase
   V4<R>* part;     // union region, MLP phase: blockDim partials
   R* red;
+  R* w; R* b;      // the env's controller when MsArgs::w_smem > 0, else null
 };
 
 template <typename R>
@@ -261,6 +276,8 @@ __device__ __forceinline__ RevSmem<R> carve_rev(char* base, const MsArgs<R>& a) 
   s.gvinc = (V4<R>*)u;
   s.dz = (R*)u;
   s.part = (V4<R>*)(u + ((sizeof(R) * a.smem_dmax + 255) & ~size_t(255)));
+  s.w = a.w_smem ? (R*)take(sizeof(R) * a.w_smem) : nullptr;
+  s.b = a.w_smem ? (R*)take(sizeof(R) * a.b_smem) : nullptr;
   return s;
 }
 
@@ -425,12 +442,36 @@ __device__ __forceinline__ void advance_vertex(const MsArgs<R>& a, V4<R>& x, V4<
   v.x = nv0; v.y = nv1; v.z = nv2;
 }
 
+// One 4-wide group of controller weights: from the shared-memory copy (SH) or
+// from global memory, not allocated in L1 and evict-first in L2 (pol).
+template <typename R, bool SH>
+__device__ __forceinline__ V4<R> ldw4(const V4<R>* p, unsigned long long pol) {
+  if constexpr (SH) return *p;
+  else return ldg4_hint<R>(p, pol);
+}
+
+// The env's controller -- weights and biases, each contiguous per robot --
+// copied into shared memory (sw, sb) at the start of a work item; the caller
+// synchronises before the first product.
+template <typename R>
+__device__ __forceinline__ void load_controller_smem(const R* __restrict__ w, const R* __restrict__ bias,
+                                                     const RobotDesc& rb, R* sw, R* sb) {
+  const int L = rb.n_layers;
+  const long long w0 = rb.w_off[0];
+  const long long n4 = (rb.w_off[L - 1] + (long long)rb.width[L] * rb.pitch[L - 1] - w0) >> 2;
+  const V4<R>* src = reinterpret_cast<const V4<R>*>(w + w0);
+  V4<R>* dst = reinterpret_cast<V4<R>*>(sw);
+  for (long long i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = ldg4<R>(src + i);
+  const int b0 = rb.b_off[0], nb = rb.b_off[L - 1] + ((rb.width[L] + 3) & ~3) - b0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) sb[i] = bias[b0 + i];
+}
+
 // y = act(W x + b) for one layer.  Each warp owns RB consecutive rows at a
 // time and streams them together (RB independent float4 loads per lane per
 // column step), so short rows -- the 128-wide output layer of a robot with
 // thousands of actuators -- still keep enough loads in flight.
 // Records z (pre-bias sums) when zrec != null.
-template <typename R, int RB>
+template <typename R, int RB, bool SH>
 __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pitch, int nout,
                                                  const R* __restrict__ bias, const R* xin, R* y,
                                                  R* zrec, int act) {
@@ -453,7 +494,7 @@ __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pi
       const V4<R> xv = x4[j];
       V4<R> wv[RB];
 #pragma unroll
-      for (int r = 0; r < RB; ++r) wv[r] = ldg4_hint<R>(w4[r] + j, pol);
+      for (int r = 0; r < RB; ++r) wv[r] = ldw4<R, SH>(w4[r] + j, pol);
 #pragma unroll
       for (int r = 0; r < RB; ++r)
         s[r] += wv[r].x * xv.x + wv[r].y * xv.y + wv[r].z * xv.z + wv[r].w * xv.w;
@@ -475,19 +516,19 @@ __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pi
   }
 }
 
-template <typename R>
+template <typename R, bool SH>
 __device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch, int nout,
                                               const R* __restrict__ bias, const R* xin, R* y,
                                               R* zrec, int act) {
-  if (pitch <= 256) dense_forward_rb<R, 8>(W, pitch, nout, bias, xin, y, zrec, act);
-  else dense_forward_rb<R, 4>(W, pitch, nout, bias, xin, y, zrec, act);
+  if (pitch <= 256) dense_forward_rb<R, 8, SH>(W, pitch, nout, bias, xin, y, zrec, act);
+  else dense_forward_rb<R, 4, SH>(W, pitch, nout, bias, xin, y, zrec, act);
 }
 
 // g_in[j] = sum_i W[i, j] dz[i] for j in [0, ncols) (ncols multiple of 4 or
 // padded), deterministic: fixed row splits, fixed reduction order.
 // Result written to out4[j/4] (V4 groups).  Uses `part` (blockDim entries) as
 // scratch in the narrow-row case.
-template <typename R>
+template <typename R, bool SH>
 __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pitch, int nrows,
                                                  int ncols, const R* dz, V4<R>* part, V4<R>* out4) {
   const int c4 = (ncols + 3) >> 2;
@@ -495,7 +536,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
   const unsigned long long pol = policy_evict_first();
   if (nrows == 1) {
     for (int g = tid; g < c4; g += nt) {
-      const V4<R> wv = ldg4<R>(reinterpret_cast<const V4<R>*>(W) + g);
+      const V4<R> wv = ldw4<R, SH>(reinterpret_cast<const V4<R>*>(W) + g, pol);
       const R d = dz[0];
       V4<R> r; r.x = wv.x * d; r.y = wv.y * d; r.z = wv.z * d; r.w = wv.w * d;
       out4[g] = r;
@@ -522,7 +563,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
         for (int k = 0; k < KMAX; ++k) {
           const int g = base + lt + k * H;
           if (g < c4) {
-            const V4<R> wv = ldg4_hint<R>(row + g, pol);
+            const V4<R> wv = ldw4<R, SH>(row + g, pol);
             acc[k][0] += wv.x * d; acc[k][1] += wv.y * d; acc[k][2] += wv.z * d; acc[k][3] += wv.w * d;
           }
         }
@@ -560,7 +601,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
     R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll 4
     for (int i = r0; i < nrows; i += slices) {
-      const V4<R> wv = ldg4_hint<R>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g, pol);
+      const V4<R> wv = ldw4<R, SH>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g, pol);
       const R d = dz[i];
       s0 += wv.x * d; s1 += wv.y * d; s2 += wv.z * d; s3 += wv.w * d;
     }

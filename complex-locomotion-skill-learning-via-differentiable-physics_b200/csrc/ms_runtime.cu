@@ -174,8 +174,8 @@ class SimBase {
   virtual void set_controller_path(int path) = 0;
   virtual bool controller_batched() const = 0;
   // fused kernels' launch shape and the autotuner over it
-  virtual void set_launch_shape(int threads, int ctas) = 0;
-  virtual void launch_shape(int* threads, int* ctas) const = 0;
+  virtual void set_launch_shape(int threads, int ctas, int wsh) = 0;
+  virtual void launch_shape(int* threads, int* ctas, int* wsh) const = 0;
   virtual void autotune(int steps, int repeats, std::vector<cls_launch_shape>& table) = 0;
 };
 
@@ -252,6 +252,12 @@ class SimImpl final : public SimBase {
         tsg.tile0 = n_ttiles_;
         n_ttiles_ += ((tsg.rows + 31) / 32) * ((tsg.cols + 31) / 32);
         tsegs_.push_back(tsg);
+      }
+      {
+        const int Lr = h.n_layers;
+        wspan_max_ = std::max(wspan_max_, d.w_off[Lr - 1] + (long long)d.pitch[Lr - 1] * h.width[Lr] -
+                                              d.w_off[0]);
+        bspan_max_ = std::max(bspan_max_, (long long)(d.b_off[Lr - 1] + round4(h.width[Lr]) - d.b_off[0]));
       }
       int rid[4] = {45, 46, 34, 36};
       for (int q = 0; q < 4; ++q) d.rot_idx[q] = rid[q];
@@ -397,11 +403,11 @@ class SimImpl final : public SimBase {
     smem_dmax_ = dmax;
     smem_amax_ = amax;
     smem_omax_ = omax;
-    fwd_smem_ = fwd_smem_bytes<R>(nmax_, dmax, p0max);
+    fwd_base_ = fwd_smem_bytes<R>(nmax_, dmax, p0max);
     int dev = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, dev));
-    use_threads(p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads());
+    use_shape(p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads(), -1);
     // GEMM tiles (per robot, per layer); a robot shared by many envs splits
     // its K = envs x substeps rows over several CTAs (about 2048 rows each)
     for (int r = 0; r < nr; ++r) {
@@ -546,19 +552,24 @@ class SimImpl final : public SimBase {
                            : (threads_ <= 512 ? ms_reverse_kernel<R, 512> : ms_reverse_kernel<R, 1024>);
   }
 
-  // Threads per CTA of the fused kernels: selects the kernel instance, raises
-  // its dynamic shared-memory limit and checks that the largest robot fits and
-  // that at least one CTA can be resident.  The limit is a per-kernel,
-  // process-wide attribute: it is raised to the device maximum (minus the
-  // kernel's static shared memory) so that handles with different robot sizes
-  // never lower it for one another.  On failure the previous shape stays.
-  void use_threads(int threads) {
+  // Launch shape of the fused kernels: threads per CTA select the kernel
+  // instance; its dynamic shared-memory limit is raised, the largest robot
+  // must fit and at least one CTA must be resident.  wsh: the controller
+  // (weights, biases) in shared memory for a whole work item -- 1 on (it must
+  // fit), 0 off (read from global memory every substep), -1 on when it fits
+  // without fewer resident CTAs.  The limit is a per-kernel, process-wide
+  // attribute: it is raised to the device maximum (minus the kernel's static
+  // shared memory) so that handles with different robot sizes never lower it
+  // for one another.  On failure the previous shape stays.
+  void use_shape(int threads, int wsh) {
     CLS_REQUIRE(threads % 32 == 0 && threads >= 64 && threads <= 1024,
                 "threads_per_block must be a multiple of 32 in [64, 1024]");
+    CLS_REQUIRE(wsh >= -1 && wsh <= 1, "weights_shared must be -1 (automatic), 0 or 1");
     const int keep = threads_;
     threads_ = threads;
     try {
-      const size_t rev = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, threads);
+      const size_t rev0 = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, threads);
+      const size_t ctrl = ctrl_smem_bytes<R>(wspan_max_, bspan_max_);
       int dev = 0, optin = 0;
       CLS_CUDA(cudaGetDevice(&dev));
       CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -567,33 +578,47 @@ class SimImpl final : public SimBase {
       CLS_CUDA(cudaFuncGetAttributes(&ra, rev_fn()));
       const size_t fwd_cap = (size_t)optin - fa.sharedSizeBytes;
       const size_t rev_cap = (size_t)optin - ra.sharedSizeBytes;
-      CLS_REQUIRE(fwd_smem_ <= fwd_cap && rev <= rev_cap,
-                  "robot too large for one CTA's shared memory (" + std::to_string(rev) +
+      CLS_REQUIRE(fwd_base_ <= fwd_cap && rev0 <= rev_cap,
+                  "robot too large for one CTA's shared memory (" + std::to_string(rev0) +
                       " bytes needed, " + std::to_string(rev_cap) + " available)");
       CLS_CUDA(cudaFuncSetAttribute(fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_cap));
       CLS_CUDA(cudaFuncSetAttribute(rev_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_cap));
-      int nf = 0, nb = 0;
-      CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nf, fwd_fn(), threads, fwd_smem_));
-      CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rev_fn(), threads, rev));
-      CLS_REQUIRE(nf >= 1 && nb >= 1,
+      // CTAs of both kernels resident per SM with the given shared memory
+      auto resident = [&](size_t f, size_t r) {
+        if (f > fwd_cap || r > rev_cap) return 0;
+        int nf = 0, nb = 0;
+        CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nf, fwd_fn(), threads, f));
+        CLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rev_fn(), threads, r));
+        return std::min(nf, nb);
+      };
+      const int r_off = resident(fwd_base_, rev0);
+      CLS_REQUIRE(r_off >= 1,
                   "no CTA of " + std::to_string(threads) + " threads can be resident on an SM");
-      rev_smem_ = rev;
-      resident_ = std::min(nf, nb);
+      const int r_on = resident(fwd_base_ + ctrl, rev0 + ctrl);
+      CLS_REQUIRE(wsh != 1 || r_on >= 1,
+                  "the controller (" + std::to_string(ctrl) + " bytes) does not fit in shared memory "
+                  "beside the kernels' own");
+      const bool on = wsh == 1 || (wsh == -1 && r_on >= 1 && r_on >= r_off);
+      fwd_smem_ = fwd_base_ + (on ? ctrl : 0);
+      rev_smem_ = rev0 + (on ? ctrl : 0);
+      resident_ = on ? r_on : r_off;
+      wsh_on_ = on;
     } catch (...) {
       threads_ = keep;
       throw;
     }
   }
 
-  void set_launch_shape(int threads, int ctas) override {
+  void set_launch_shape(int threads, int ctas, int wsh) override {
     CLS_REQUIRE(!capturing_, "the launch shape cannot change during graph capture");
     CLS_REQUIRE(ctas >= 1 && ctas <= 32, "ctas_per_sm must be in [1, 32]");
-    use_threads(threads);
+    use_shape(threads, wsh);
     ctas_per_sm_ = ctas;
   }
-  void launch_shape(int* threads, int* ctas) const override {
+  void launch_shape(int* threads, int* ctas, int* wsh) const override {
     *threads = threads_;
     *ctas = ctas_per_sm_;
+    *wsh = wsh_on_ ? 1 : 0;
   }
 
   // one training rollout (forward, loss, reverse) as the autotuner times it:
@@ -634,7 +659,7 @@ class SimImpl final : public SimBase {
     if (steps <= 0) steps = std::min(T_, std::min(2 * K_ + 1, 101));
     CLS_REQUIRE(steps >= 2 && steps <= T_, "tuning rollout needs 2 <= steps <= max_steps");
     repeats = std::max(1, repeats);
-    const int keep_threads = threads_, keep_ctas = ctas_per_sm_;
+    const int keep_threads = threads_, keep_ctas = ctas_per_sm_, keep_wsh = wsh_on_ ? 1 : 0;
     const bool keep_dense = dense_;
     bool can_dense = true;
     for (const RobotDesc& d : rd_host_)
@@ -643,15 +668,17 @@ class SimImpl final : public SimBase {
     try {
       dense_ = false;
       for (int threads : {128, 256, 512, 1024}) {
-        try {
-          use_threads(threads);
-        } catch (const Fail& f) {
-          if (f.code != CLS_ERR_INVALID) throw;
-          continue;  // the largest robot does not fit this instance
-        }
-        for (int ctas = 1; ctas <= std::min(resident_, kTuneMaxCtas); ++ctas) {
-          ctas_per_sm_ = ctas;
-          table.push_back({CLS_CONTROLLER_PER_ENV, threads, ctas, time_rollout(steps, repeats)});
+        for (int wsh : {0, 1}) {
+          try {
+            use_shape(threads, wsh);
+          } catch (const Fail& f) {
+            if (f.code != CLS_ERR_INVALID) throw;
+            continue;  // the largest robot (or its controller) does not fit this instance
+          }
+          for (int ctas = 1; ctas <= std::min(resident_, kTuneMaxCtas); ++ctas) {
+            ctas_per_sm_ = ctas;
+            table.push_back({CLS_CONTROLLER_PER_ENV, threads, ctas, wsh, time_rollout(steps, repeats)});
+          }
         }
       }
       CLS_REQUIRE(!table.empty(), "no launch shape fits the largest robot");
@@ -660,18 +687,19 @@ class SimImpl final : public SimBase {
         if (table[i].ms < table[best].ms) best = i;
       // the fused kernels keep their fastest shape (per-env launches and
       // serving windows use them on either controller path)
-      use_threads(table[best].threads_per_block);
+      use_shape(table[best].threads_per_block, table[best].weights_shared);
       ctas_per_sm_ = table[best].ctas_per_sm;
       if (can_dense) {
         set_controller_path(CLS_CONTROLLER_BATCHED);
-        table.push_back({CLS_CONTROLLER_BATCHED, threads_, ctas_per_sm_, time_rollout(steps, repeats)});
+        table.push_back({CLS_CONTROLLER_BATCHED, threads_, ctas_per_sm_, wsh_on_ ? 1 : 0,
+                         time_rollout(steps, repeats)});
         if (table.back().ms >= table[best].ms) set_controller_path(CLS_CONTROLLER_PER_ENV);
       } else {
         set_controller_path(CLS_CONTROLLER_PER_ENV);
       }
     } catch (...) {
       try {
-        use_threads(keep_threads);
+        use_shape(keep_threads, keep_wsh);
       } catch (...) {
       }
       ctas_per_sm_ = keep_ctas;
@@ -723,6 +751,8 @@ class SimImpl final : public SimBase {
     a.smem_dmax = smem_dmax_;
     a.smem_amax = smem_amax_;
     a.smem_omax = smem_omax_;
+    a.w_smem = wsh_on_ ? (int)wspan_max_ : 0;
+    a.b_smem = wsh_on_ ? (int)bspan_max_ : 0;
     a.dt = (R)p_.dt;
     a.gravity = (R)p_.gravity;
     a.ground = (R)p_.ground_height;
@@ -1035,6 +1065,7 @@ class SimImpl final : public SimBase {
   MsArgs<R> step_args(const MsArgs<R>& a) const {
     MsArgs<R> b = a;
     b.smem_dmax = smem_omax_;
+    b.w_smem = b.b_smem = 0;  // the step kernels read the controller from its GEMM tiles
     b.n_items = E_;
     return b;
   }
@@ -1707,6 +1738,11 @@ class SimImpl final : public SimBase {
   long long rec_z_total_ = 0;
   int smem_p0max_ = 0, smem_dmax_ = 0, smem_amax_ = 0, smem_omax_ = 0, threads_ = 256, n_sm_ = 148, n_ckpt_ = 0;
   int ctas_per_sm_ = 2, resident_ = 1;
+  // controller span of the largest robot (elements) and whether the fused
+  // kernels keep it in shared memory; forward shared memory without it
+  long long wspan_max_ = 0, bspan_max_ = 0;
+  bool wsh_on_ = false;
+  size_t fwd_base_ = 0;
   size_t fwd_smem_ = 0, rev_smem_ = 0, n_queue_ = 0;
   std::vector<int> perm_, user_voff_, env_robot_, order_host_;
   bool identity_perm_ = true;
@@ -2093,16 +2129,21 @@ int cls_controller_batched(const cls_sim* sim, int32_t* on) {
   return CLS_OK;
 }
 
-int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_per_sm) {
-  return guarded(sim, [&](cls::SimBase& s) { s.set_launch_shape(threads_per_block, ctas_per_sm); });
+int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_per_sm,
+                         int32_t weights_shared) {
+  return guarded(sim, [&](cls::SimBase& s) {
+    s.set_launch_shape(threads_per_block, ctas_per_sm, weights_shared);
+  });
 }
 
-int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm) {
+int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm,
+                         int32_t* weights_shared) {
   if (!sim || !sim->impl || !threads_per_block || !ctas_per_sm) return CLS_ERR_INVALID;
-  int t = 0, c = 0;
-  sim->impl->launch_shape(&t, &c);
+  int t = 0, c = 0, w = 0;
+  sim->impl->launch_shape(&t, &c, &w);
   *threads_per_block = t;
   *ctas_per_sm = c;
+  if (weights_shared) *weights_shared = w;
   return CLS_OK;
 }
 

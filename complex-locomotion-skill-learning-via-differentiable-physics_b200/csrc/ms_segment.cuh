@@ -285,6 +285,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
       const V4<R>* cv = a.ckpt_v + (size_t)src_slot * a.v_total + ed.v_off;
       for (int i = tid; i < N; i += nt) { s.xs[i] = cx[i]; s.vs[i] = cv[i]; }
     }
+    if (s.w) load_controller_smem<R>(a.w, a.bias, rb, s.w, s.b);
     R hprev = 0;
     if ((mode & FWD_OBS) && t_begin > 0) hprev = a.obs_height[(size_t)(t_begin - 1) * a.n_envs + e];
     __syncthreads();
@@ -301,8 +302,13 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
         const int nout = rb.width[l + 1];
         R* zrec = (mode & FWD_RECORD) ? a.rec_z + a.z_base[l] + (size_t)kk * a.z_total[l] + ed.z_off[l]
                                       : nullptr;
-        dense_forward<R>(a.w + rb.w_off[l], rb.pitch[l], nout, a.bias + rb.b_off[l], in, y, zrec,
-                         l == L - 1 ? a.act_out : a.act_hidden);
+        const int act = l == L - 1 ? a.act_out : a.act_hidden;
+        if (s.w)
+          dense_forward<R, true>(s.w + (rb.w_off[l] - rb.w_off[0]), rb.pitch[l], nout,
+                                 s.b + (rb.b_off[l] - rb.b_off[0]), in, y, zrec, act);
+        else
+          dense_forward<R, false>(a.w + rb.w_off[l], rb.pitch[l], nout, a.bias + rb.b_off[l], in, y,
+                                  zrec, act);
         // zero the padding up to the next layer's pitch
         const int padto = (l + 1 < L) ? rb.pitch[l + 1] : ((nout + 3) & ~3);
         for (int q = nout + tid; q < padto; q += nt) y[q] = 0;
@@ -732,7 +738,9 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
     load_descs(a, e, rb, ed);
     const int N = rb.n_v, L = rb.n_layers;
     R hcarry = 0;
+    if (s.w) load_controller_smem<R>(a.w, a.bias, rb, s.w, s.b);  // read after the syncs below
     rev_load_carry<R>(a, rb, ed, s, e, t_end, last_seg != 0, hcarry);
+    __syncthreads();
     CLS_PHASE_START();
     for (int t = t_end - 1; t >= t_begin; --t) {
       const int kk = t - t_begin;
@@ -741,11 +749,15 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
       // hidden layers of the MLP adjoint
       for (int l = L - 1; l >= 1; --l) {
         const int nin = rb.width[l];
-        dense_transposed<R>(a.w + rb.w_off[l], rb.pitch[l], rb.width[l + 1], nin, s.dz, s.part,
-                            reinterpret_cast<V4<R>*>(s.bufA));
+        if (s.w)
+          dense_transposed<R, true>(s.w + (rb.w_off[l] - rb.w_off[0]), rb.pitch[l], rb.width[l + 1], nin,
+                                    s.dz, s.part, reinterpret_cast<V4<R>*>(s.bufA));
+        else
+          dense_transposed<R, false>(a.w + rb.w_off[l], rb.pitch[l], rb.width[l + 1], nin, s.dz, s.part,
+                                     reinterpret_cast<V4<R>*>(s.bufA));
         const R* zp = a.rec_z + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + ed.z_off[l - 1];
         R* dzr = a.rec_dz + a.z_base[l - 1] + (size_t)kk * a.z_total[l - 1] + ed.z_off[l - 1];
-        const R* bp = a.bias + rb.b_off[l - 1];
+        const R* bp = s.w ? s.b + (rb.b_off[l - 1] - rb.b_off[0]) : a.bias + rb.b_off[l - 1];
         for (int q = tid; q < nin; q += nt) {
           const R dz = s.bufA[q] * act_d<R>(a.act_hidden, zp[q] + bp[q]);
           s.dz[q] = dz;
@@ -754,8 +766,12 @@ ms_reverse_kernel(MsArgs<R> a, int t_begin0, int t_end0, int last_seg0) {
         __syncthreads();
       }
       // first layer: only the position columns carry state dependence
-      dense_transposed<R>(a.w + rb.w_off[0], rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
-                          reinterpret_cast<V4<R>*>(s.bufA));
+      if (s.w)
+        dense_transposed<R, true>(s.w, rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
+                                  reinterpret_cast<V4<R>*>(s.bufA));
+      else
+        dense_transposed<R, false>(a.w + rb.w_off[0], rb.pitch[0], rb.width[1], 3 * N, s.dz, s.part,
+                                   reinterpret_cast<V4<R>*>(s.bufA));
       CLS_PHASE(a, 6);
       rev_post<R>(a, rb, ed, s, e, t, hcarry);
       CLS_PHASE(a, 8);

@@ -218,31 +218,41 @@ int cls_controller_batched(const cls_sim* sim, int32_t* on);
 
 /* Launch shape of the fused segment kernels: threads per CTA (64..1024, a
  * multiple of 32; up to 256, up to 512 and up to 1024 select kernel
- * instances compiled for 255, 128 and 64 registers per thread) and the CTAs per SM that the
- * persistent grid is sized for (grid = min(envs, SMs x ctas_per_sm); CTAs take
- * envs from a work queue, largest first).  Results do not depend on
- * ctas_per_sm, and depend on threads_per_block only through the rounding of
- * block-wide reductions.  No reference counterpart: Taichi chose its own
- * block sizes per kernel (ti.loop_config).  A CUDA graph captured earlier
- * keeps the shape it was captured with.  CLS_ERR_INVALID when a robot's
- * shared memory does not fit the instance or no CTA of that size can be
- * resident. */
-int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_per_sm);
-int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm);
+ * instances compiled for 255, 128 and 64 registers per thread), the CTAs per
+ * SM that the persistent grid is sized for (grid = min(envs, SMs x
+ * ctas_per_sm); CTAs take envs from a work queue, largest first), and where
+ * the kernels read the controller: weights_shared = 1 copies each env's
+ * weights and biases into shared memory once per work item (the robot's
+ * controller must fit beside the kernels' own shared memory), 0 reads them
+ * from global memory every substep, -1 (the default at creation) chooses 1
+ * when it fits without fewer resident CTAs.  Results do not depend on
+ * ctas_per_sm or weights_shared, and depend on threads_per_block only through
+ * the rounding of block-wide reductions.  No reference counterpart: Taichi
+ * chose its own block sizes per kernel (ti.loop_config).  A CUDA graph
+ * captured earlier keeps the shape it was captured with.  CLS_ERR_INVALID
+ * when a robot's shared memory does not fit the instance or no CTA of that
+ * size can be resident.  cls_get_launch_shape reports weights_shared as the
+ * applied 0 or 1 (the pointer may be NULL). */
+int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_per_sm,
+                         int32_t weights_shared);
+int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm,
+                         int32_t* weights_shared);
 
 /* One timed candidate of cls_autotune. */
 typedef struct cls_launch_shape {
   int32_t controller_path;    /* CLS_CONTROLLER_PER_ENV or CLS_CONTROLLER_BATCHED */
   int32_t threads_per_block;  /* fused kernels (per-env path) */
   int32_t ctas_per_sm;
+  int32_t weights_shared;     /* 0 or 1 */
   float ms;                   /* one forward + loss + backward over the tuning horizon */
 } cls_launch_shape;
 
 /* Autotuner: times one training rollout (cls_forward + the loss + cls_backward,
  * CUDA events on the handle's stream, `repeats` runs after one untimed run) of
  * `steps` substeps (<= 0: min(max_steps, 2 K + 1, 101)) for every feasible
- * launch shape -- threads per CTA in {128, 256, 512, 1024} x CTAs per SM from
- * 1 to what can be resident (at most 4) -- and, when every robot type has at
+ * launch shape -- threads per CTA in {128, 256, 512, 1024} x controller in
+ * global or shared memory x CTAs per SM from 1 to what can be resident (at
+ * most 4) -- and, when every robot type has at
  * least 32 envs, for the batched controller path, then applies the fastest.
  * Needs the state, targets and weights set (it runs the caller's workload);
  * leaves the weights unchanged and the rollout, loss and gradient buffers as

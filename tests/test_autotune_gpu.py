@@ -1,8 +1,9 @@
 """Launch shapes of the fused segment kernels and the autotuner over them
 (cls_set_launch_shape / cls_get_launch_shape / cls_autotune).
 
-The shape changes only how envs are spread over CTAs (CTAs per SM: the
-persistent grid's size; results identical) and the CTA size (threads per
+The shape changes how envs are spread over CTAs (CTAs per SM: the persistent
+grid's size) and where the controller is read from (shared or global memory),
+both without changing a bit of the results, and the CTA size (threads per
 CTA: block-wide reductions regroup, results equal within rounding).
 """
 import json
@@ -26,12 +27,45 @@ def test_launch_shape_validation():
     for bad in ((100, 1), (32, 1), (2048, 1), (256, 0), (256, 33)):
         with pytest.raises(cls_b200._capi.ClsError):
             b.set_launch_shape(*bad)
-    b.set_launch_shape(384, 3)
-    assert b.launch_shape == (384, 3)
+    with pytest.raises(cls_b200._capi.ClsError):
+        b.set_launch_shape(256, 1, 2)
+    b.set_launch_shape(384, 3, 0)
+    assert b.launch_shape == (384, 3, 0)
     with pytest.raises(cls_b200._capi.ClsError):
         b.set_launch_shape(100, 1)
-    assert b.launch_shape == (384, 3)      # a refused shape leaves the previous one
+    assert b.launch_shape == (384, 3, 0)   # a refused shape leaves the previous one
+    b.set_launch_shape(256, 1, 1)           # the quadruped's controller fits in shared memory
+    assert b.launch_shape == (256, 1, 1)
     b.close()
+
+
+def test_controller_too_large_for_shared_memory():
+    import cls_b200
+    b = many_env_batch(32, 4, [1024], 10, 20, "per_env")   # 1024 x 176 weights: 720 KB
+    with pytest.raises(cls_b200._capi.ClsError, match="does not fit"):
+        b.set_launch_shape(256, 1, 1)
+    b.set_launch_shape(256, 1, -1)          # automatic: global memory
+    assert b.launch_shape == (256, 1, 0)
+    assert np.isfinite(b.simulate(15))
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_controller_in_shared_memory_is_bit_identical(precision):
+    """Weights and biases copied to shared memory once per work item give the
+    same bits as reading them from global memory every substep."""
+    b = many_env_batch(precision, 40, [32, 16], 9, 48, "per_env")   # FP64 controller ~80 KB
+    runs = []
+    for wsh in (0, 1):
+        b.set_launch_shape(256, 2, wsh)
+        loss = b.simulate(40)
+        x, _ = b.final_state()
+        runs.append((loss, _grads(b, 3), b.state_grads()[0], x))
+    b.close()
+    (l0, g0, s0, x0), (l1, g1, s1, x1) = runs
+    assert l0 == l1 and np.array_equal(x0, x1) and np.array_equal(s0, s1)
+    for (gW, gb), (rW, rb) in zip(g1, g0):
+        assert np.array_equal(gW, rW) and np.array_equal(gb, rb)
 
 
 @pytest.mark.parametrize("precision", [64, 32])
@@ -85,7 +119,8 @@ def test_autotune_applies_fastest_and_keeps_weights(tmp_path):
     assert per_env and all(e["ms"] > 0 for e in per_env)
     assert {e["threads_per_block"] for e in per_env} <= {128, 256, 512, 1024}
     best = min(per_env, key=lambda e: e["ms"])
-    assert b.launch_shape == (best["threads_per_block"], best["ctas_per_sm"])
+    shape = (best["threads_per_block"], best["ctas_per_sm"], best["weights_shared"])
+    assert b.launch_shape == shape
     assert res["controller_path"] == "per_env"          # one env per type: no batched candidate
     assert all(e["controller_path"] == "per_env" for e in res["table"])
     for (W, bias), (W1, b1) in zip(W0, [b.get_weights(r, l) for r in range(len(robots)) for l in range(3)]):
@@ -99,7 +134,7 @@ def test_autotune_applies_fastest_and_keeps_weights(tmp_path):
     b.set_launch_shape(64, 1)
     hit = b.autotune(repeats=1, cache=cache)
     assert hit["cached"]
-    assert b.launch_shape == (best["threads_per_block"], best["ctas_per_sm"])
+    assert b.launch_shape == shape
     with open(cache) as f:
         assert len(json.load(f)) == 1
     b.close()
