@@ -76,6 +76,7 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
   if (t < t_end) {
     R hprev = 0;
     if ((mode & FWD_OBS) && t > 0) hprev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
+    load_head_smem<R>(a, rb, ed, s, t, mode);
     fwd_pre<R>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
     if constexpr (std::is_same<R, float>::value) {
       // the input row as the first layer's pre-split A operand

@@ -194,15 +194,21 @@ struct MsArgs {
 #endif
 
 // ------------------------------------------------------------ shared memory
-// reduction scratch: 8 values x 32 warps, then 32 ints for arg-reductions
+// reduction scratch: 8 values x 32 warps, then 32 ints for arg-reductions;
+// the forward pass's fused observable reduction (11 sums and two extrema with
+// their indices per warp) takes kRedFwd.  The reverse pass keeps kRed: its
+// shared memory sits just under the 196 KB carveout step for the largest
+// benchmark robot, where 768 more bytes leave it 32 KB less L1.
 constexpr int kRed = 320;
+constexpr int kRedFwd = 512;
 constexpr int kRedInt = 256;
 template <typename R>
 struct FwdSmem {
   V4<R>* xs; V4<R>* vs; V4<R>* vinc;
   R* ain;          // compact input, padded
   R* buf0; R* buf1;
-  R* red;          // kRed entries
+  R* red;          // kRedFwd entries
+  unsigned char* head;  // per-vertex heading side (rotation of robots other than 100)
   R* w; R* b;      // the env's controller when MsArgs::w_smem > 0, else null
 };
 
@@ -217,7 +223,8 @@ __device__ __forceinline__ FwdSmem<R> carve_fwd(char* base, const MsArgs<R>& a) 
   s.ain = (R*)take(sizeof(R) * a.smem_p0max);
   s.buf0 = (R*)take(sizeof(R) * a.smem_dmax);
   s.buf1 = (R*)take(sizeof(R) * a.smem_dmax);
-  s.red = (R*)take(sizeof(R) * kRed);
+  s.red = (R*)take(sizeof(R) * kRedFwd);
+  s.head = (unsigned char*)take(a.smem_nmax);
   s.w = a.w_smem ? (R*)take(sizeof(R) * a.w_smem) : nullptr;
   s.b = a.w_smem ? (R*)take(sizeof(R) * a.b_smem) : nullptr;
   return s;
@@ -234,7 +241,7 @@ template <typename R>
 __host__ __device__ inline size_t fwd_smem_bytes(int nmax, int dmax, int p0max) {
   auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
   return 3 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * p0max) + 2 * rb(sizeof(R) * dmax) +
-         rb(sizeof(R) * kRed);
+         rb(sizeof(R) * kRedFwd) + rb(nmax);
 }
 
 // Reverse-pass shared memory.  gvinc (v_inc, then its adjoint) is live only

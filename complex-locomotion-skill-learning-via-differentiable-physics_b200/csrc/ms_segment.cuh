@@ -78,6 +78,66 @@ __device__ __forceinline__ void load_descs(const MsArgs<R>& a, int e, RobotDesc&
 
 // goal columns of the compact input: (vx, vz) / max_speed if duplicate_v > 0,
 // target height if duplicate_h > 0, crawl target if duplicate_c > 0
+// The observables' reductions of one substep in one pass: sums v[0..10]
+// (centre, then the heading sides' coordinate sums and counts) in block_sum's
+// order, and the min / max of the height with block_argext's order -- the same
+// bits as block_sum<R, 3> + 2 x block_argext + block_sum<R, 8>, with two
+// barriers instead of ten.  red: kRedFwd entries (sums at [m * 32 + warp], the
+// extrema at [352 + warp] and [384 + warp], their indices as ints from 416).
+template <typename R>
+__device__ __forceinline__ void block_obs(R (&v)[11], R& lo, int& li, R& hi, int& hidx, R* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int* redi = reinterpret_cast<int*>(red + 416);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[m] += __shfl_xor_sync(0xffffffffu, v[m], o);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const R l2 = __shfl_xor_sync(0xffffffffu, lo, o);
+    const int li2 = __shfl_xor_sync(0xffffffffu, li, o);
+    if ((l2 < lo) || (l2 == lo && li2 > li)) { lo = l2; li = li2; }
+    const R h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+    const int hi2 = __shfl_xor_sync(0xffffffffu, hidx, o);
+    if ((h2 > hi) || (h2 == hi && hi2 > hidx)) { hi = h2; hidx = hi2; }
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) red[m * 32 + wid] = v[m];
+    red[352 + wid] = lo;
+    red[384 + wid] = hi;
+    redi[wid] = li;
+    redi[32 + wid] = hidx;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    R sm = 0;
+    for (int w = 0; w < nw; ++w) sm += red[m * 32 + w];
+    v[m] = sm;
+  }
+  lo = red[352]; li = redi[0];
+  hi = red[384]; hidx = redi[32];
+  for (int w = 1; w < nw; ++w) {
+    const R l2 = red[352 + w], h2 = red[384 + w];
+    const int li2 = redi[w], hi2 = redi[32 + w];
+    if ((l2 < lo) || (l2 == lo && li2 > li)) { lo = l2; li = li2; }
+    if ((h2 > hi) || (h2 == hi && hi2 > hidx)) { hi = h2; hidx = hi2; }
+  }
+}
+
+// Heading sides of the env's vertices (set at t = 0 by the first pass) into
+// shared memory, for a range that starts after t = 0; the vertex-to-thread
+// mapping is the one fwd_pre reads them with.
+template <typename R>
+__device__ __forceinline__ void load_head_smem(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
+                                               const FwdSmem<R>& s, int t, int mode) {
+  if (!(mode & FWD_OBS) || t == 0 || rb.robot_id == 100) return;
+  for (int i = threadIdx.x; i < rb.n_v; i += blockDim.x) s.head[i] = a.head[ed.v_off + i];
+}
+
 template <typename R>
 __device__ __forceinline__ R goal_value(const MsArgs<R>& a, int g, size_t o) {
   if (a.dup_v > 0) {
@@ -140,22 +200,39 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
     V4<R>* xf = a.x_full + (size_t)t * a.v_total + ed.v_off;
     for (int i = tid; i < N; i += nt) xf[i] = s.xs[i];
   }
-  // -- compute_center (solver_mass_spring.py:150-156): sum of x / n
+  // the goal and sine columns of the input do not depend on the state: their
+  // loads are issued here and stored after the reductions
+  const int p0 = rb.pos_pad, nc = rb.n_c;
+  const int qpre = p0 + tid;
+  R pre = 0;
+  if (qpre < nc)
+    pre = (qpre < p0 + a.n_sin) ? a.sin_table[(size_t)t * a.n_sin + (qpre - p0)]
+                                : goal_value<R>(a, qpre - p0 - a.n_sin, (size_t)t * a.n_envs + e);
   R c[3] = {0, 0, 0};
-  for (int i = tid; i < N; i += nt) {
-    c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
-  }
-  block_sum<R, 3>(c, s.red);
-  if (mode & FWD_OBS) {
-    // compute_height / upper height (solver_mass_spring.py:158-173)
+  if ((mode & FWD_OBS) && (rb.robot_id == 100 || t > 0)) {
+    // compute_center / compute_height / upper height / compute_rotation
+    // (solver_mass_spring.py:150-192) in one reduction (heading sides fixed)
+    const bool heading = rb.robot_id != 100;
+    R v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     R lo = R(10), hi = R(-10);
-    for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
     int li = 0, hiidx = 0;
-    block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
-    block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
-    // compute_rotation (solver_mass_spring.py:175-192)
+    for (int i = tid; i < N; i += nt) {
+      const V4<R> p = s.xs[i];
+      v[0] += p.x * invN; v[1] += p.y * invN; v[2] += p.z * invN;
+      lo = fmin(lo, p.y); hi = fmax(hi, p.y);
+      if (heading) {
+        if (s.head[i]) { v[3] += p.x; v[4] += p.y; v[5] += p.z; v[6] += R(1); }
+        else { v[7] += p.x; v[8] += p.y; v[9] += p.z; v[10] += R(1); }
+      }
+    }
+    block_obs<R>(v, lo, li, hi, hiidx, s.red);
+    c[0] = v[0]; c[1] = v[1]; c[2] = v[2];
     R rot;
-    if (rb.robot_id == 100) {
+    if (heading) {
+      const R d0 = -v[3] * v[10] + v[7] * v[6];
+      const R d2 = -v[5] * v[10] + v[9] * v[6];
+      rot = datan2<R>(d2, d0);
+    } else {
       R d0 = 0, d2 = 0;
       if (tid == 0) {
         const V4<R> p = s.xs[rb.rot_idx[0]], q = s.xs[rb.rot_idx[1]];
@@ -164,43 +241,67 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
         d2 = p.z + q.z - u.z - w.z;
       }
       rot = datan2<R>(d2, d0);
-    } else {
+    }
+    // every thread holds the same lo and hprev: no broadcast
+    const R h = (t % a.jump_period == 0) ? lo : fmax(hprev, lo);
+    if (tid == 0) {
+      const size_t o = (size_t)t * a.n_envs + e;
+      V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
+      a.obs_center[o] = cc;
+      a.obs_height[o] = h;
+      a.obs_upper[o] = hi;
+      a.obs_rot[o] = rot;
+    }
+    hprev = h;
+  } else {
+    // -- compute_center (solver_mass_spring.py:150-156): sum of x / n
+    for (int i = tid; i < N; i += nt) {
+      c[0] += s.xs[i].x * invN; c[1] += s.xs[i].y * invN; c[2] += s.xs[i].z * invN;
+    }
+    block_sum<R, 3>(c, s.red);
+    if (mode & FWD_OBS) {
+      // t = 0, heading sides from the centre: compute_height / upper height
+      // (solver_mass_spring.py:158-173), compute_rotation (:175-192)
+      R lo = R(10), hi = R(-10);
+      for (int i = tid; i < N; i += nt) { lo = fmin(lo, s.xs[i].y); hi = fmax(hi, s.xs[i].y); }
+      int li = 0, hiidx = 0;
+      block_argext<R>(lo, li, true, s.red, reinterpret_cast<int*>(s.red + kRedInt));
+      block_argext<R>(hi, hiidx, false, s.red, reinterpret_cast<int*>(s.red + kRedInt));
       unsigned char* hd = a.head + ed.v_off;
-      if (t == 0) {
-        for (int i = tid; i < N; i += nt) hd[i] = (s.xs[i].x < c[0]) ? 1 : 0;
-        __syncthreads();
+      for (int i = tid; i < N; i += nt) {
+        const unsigned char f = (s.xs[i].x < c[0]) ? 1 : 0;
+        hd[i] = f;
+        s.head[i] = f;
       }
       R hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int i = tid; i < N; i += nt) {
         const V4<R> p = s.xs[i];
-        if (hd[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
+        if (s.head[i]) { hs[0] += p.x; hs[1] += p.y; hs[2] += p.z; hs[3] += R(1); }
         else { hs[4] += p.x; hs[5] += p.y; hs[6] += p.z; hs[7] += R(1); }
       }
       block_sum<R, 8>(hs, s.red);
       const R d0 = -hs[0] * hs[7] + hs[4] * hs[3];
       const R d2 = -hs[2] * hs[7] + hs[6] * hs[3];
-      rot = datan2<R>(d2, d0);
-    }
-    if (tid == 0) {
-      const size_t o = (size_t)t * a.n_envs + e;
-      V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
-      a.obs_center[o] = cc;
+      const R rot = datan2<R>(d2, d0);
       const R h = (t % a.jump_period == 0) ? lo : fmax(hprev, lo);
-      a.obs_height[o] = h;
-      a.obs_upper[o] = hi;
-      a.obs_rot[o] = rot;
-      s.red[0] = h;
+      if (tid == 0) {
+        const size_t o = (size_t)t * a.n_envs + e;
+        V4<R> cc; cc.x = c[0]; cc.y = c[1]; cc.z = c[2]; cc.w = 0;
+        a.obs_center[o] = cc;
+        a.obs_height[o] = h;
+        a.obs_upper[o] = hi;
+        a.obs_rot[o] = rot;
+      }
+      hprev = h;
     }
-    __syncthreads();
-    hprev = s.red[0];
-    __syncthreads();
   }
   // -- nn_input (taichi_env.py:149-183) in the compact column order
   {
-    const int p0 = rb.pos_pad, nc = rb.n_c, pitch0 = rb.pitch[0];
+    const int pitch0 = rb.pitch[0];
     const int nrec = rec_pad ? pitch0 : nc;
     R* rin = rec_in ? a.rec_in + (size_t)kslot * a.in_total + ed.in_off : nullptr;
     for (int q = tid; q < pitch0; q += nt) {
+      if (q >= p0 && q < nc && q - p0 < nt) continue;  // loaded ahead (pre)
       R val = 0;
       if (q < 3 * N) {
         const int i = q / 3, d = q - 3 * (q / 3);
@@ -212,6 +313,10 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
       }
       s.ain[q] = val;
       if (rin && q < nrec) rin[q] = val;
+    }
+    if (qpre < nc) {
+      s.ain[qpre] = pre;
+      if (rin && qpre < nrec) rin[qpre] = pre;
     }
   }
   __syncthreads();
@@ -286,6 +391,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
       for (int i = tid; i < N; i += nt) { s.xs[i] = cx[i]; s.vs[i] = cv[i]; }
     }
     if (s.w) load_controller_smem<R>(a.w, a.bias, rb, s.w, s.b);
+    load_head_smem<R>(a, rb, ed, s, t_begin, mode);
     R hprev = 0;
     if ((mode & FWD_OBS) && t_begin > 0) hprev = a.obs_height[(size_t)(t_begin - 1) * a.n_envs + e];
     __syncthreads();
