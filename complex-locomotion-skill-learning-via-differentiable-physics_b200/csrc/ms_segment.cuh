@@ -436,22 +436,42 @@ __device__ __forceinline__ V4<R> obs_c(const MsArgs<R>& a, int t, int e) {
 }
 
 // d loss / d center[t] from the velocity loss (taichi_env.py:185-211)
+// Its observables and targets are loaded first (load_center_velocity, before
+// the block reduction of the centre adjoint, so the loads overlap it) and
+// applied after (apply_center_velocity, the same expressions in the same order).
 template <typename R>
-__device__ __forceinline__ void seed_center_velocity(const MsArgs<R>& a, int t, int e, R Br, R g[3]) {
+struct CenterVelocitySeed {
+  bool on1, on2;
+  R sc;
+  V4<R> c1a, c0a, tva, c1b, c0b, tvb;
+};
+template <typename R>
+__device__ __forceinline__ CenterVelocitySeed<R> load_center_velocity(const MsArgs<R>& a, int t, int e, R Br) {
   const int rp = a.run_period, tp = a.turn_period, st = steps_of(a, e);
-  const R sc = R(2) * R(100) / R(st) / Br;
-  if (t >= rp && t % tp > rp && t <= st && t < a.T) {
-    const V4<R> c1 = obs_c(a, t, e), c0 = obs_c(a, t - rp, e);
-    const V4<R> tv = a.tv[(size_t)(t - rp) * a.n_envs + e];
-    g[0] += (c1.x - c0.x - tv.x) * sc;
-    g[2] += (c1.z - c0.z - tv.z) * sc;
+  CenterVelocitySeed<R> q;
+  q.sc = R(2) * R(100) / R(st) / Br;
+  q.on1 = (a.loss_mask & LOSS_VELOCITY) && t >= rp && t % tp > rp && t <= st && t < a.T;
+  if (q.on1) {
+    q.c1a = obs_c(a, t, e); q.c0a = obs_c(a, t - rp, e);
+    q.tva = a.tv[(size_t)(t - rp) * a.n_envs + e];
   }
   const int u = t + rp;
-  if (u <= st && u < a.T && u % tp > rp) {
-    const V4<R> c1 = obs_c(a, u, e), c0 = obs_c(a, t, e);
-    const V4<R> tv = a.tv[(size_t)t * a.n_envs + e];
-    g[0] -= (c1.x - c0.x - tv.x) * sc;
-    g[2] -= (c1.z - c0.z - tv.z) * sc;
+  q.on2 = (a.loss_mask & LOSS_VELOCITY) && u <= st && u < a.T && u % tp > rp;
+  if (q.on2) {
+    q.c1b = obs_c(a, u, e); q.c0b = obs_c(a, t, e);
+    q.tvb = a.tv[(size_t)t * a.n_envs + e];
+  }
+  return q;
+}
+template <typename R>
+__device__ __forceinline__ void apply_center_velocity(const CenterVelocitySeed<R>& q, R g[3]) {
+  if (q.on1) {
+    g[0] += (q.c1a.x - q.c0a.x - q.tva.x) * q.sc;
+    g[2] += (q.c1a.z - q.c0a.z - q.tva.z) * q.sc;
+  }
+  if (q.on2) {
+    g[0] -= (q.c1b.x - q.c0b.x - q.tvb.x) * q.sc;
+    g[2] -= (q.c1b.z - q.c0b.z - q.tvb.z) * q.sc;
   }
 }
 
@@ -642,17 +662,13 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
   {
     const V4<R>* rx = a.rec_x + (size_t)kslot * a.v_total + ed.v_off;
     const V4<R>* rv = a.rec_v + (size_t)kslot * a.v_total + ed.v_off;
-    for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; }
+    // with v_inc[t] as recorded by the forward pass (into gvinc as scratch)
+    const V4<R>* rvi = a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off;
+    for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; s.gvinc[i] = rvi[i]; }
     for (int o = tid; o < nout; o += nt) {
       s.bufA[o] = act_f<R>(a.act_out, zl[o] + bout[o]);
       s.bufB[o] = 0;
     }
-  }
-  __syncthreads();
-  // v_inc[t] as recorded by the recompute pass (into gvinc as scratch)
-  {
-    const V4<R>* rvi = a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off;
-    for (int i = tid; i < N; i += nt) s.gvinc[i] = rvi[i];
   }
   __syncthreads();
   // adjoint of advance_toi(t + 1)
@@ -732,6 +748,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
   const R invN = R(1) / R(N);
   int* redi = reinterpret_cast<int*>(s.red + kRedInt);
   {
+    const CenterVelocitySeed<R> vseed = load_center_velocity<R>(a, t, e, Br);
     R gc[3] = {0, 0, 0};
     for (int i = tid; i < N; i += nt) {
       const R g0 = s.bufA[3 * i] / R(0.2), g1 = s.bufA[3 * i + 1] / R(0.2), g2 = s.bufA[3 * i + 2] / R(0.2);
@@ -743,7 +760,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
       s.gx[i] = g;
     }
     block_sum<R, 3>(gc, s.red);
-    if (a.loss_mask & LOSS_VELOCITY) seed_center_velocity<R>(a, t, e, Br, gc);
+    apply_center_velocity<R>(vseed, gc);
     for (int i = tid; i < N; i += nt) {
       V4<R> g = s.gx[i];
       g.x += gc[0] * invN; g.y += gc[1] * invN; g.z += gc[2] * invN;
