@@ -193,6 +193,13 @@ int cls_initialize_train(cls_sim* sim, int32_t iter, int32_t steps, uint64_t see
 #define CLS_PROFILE_KINDS 9
 int cls_profile_enable(cls_sim* sim, int32_t on);
 int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset);
+/* Per-phase clock totals of the fused kernels, out[32] (clock64 cycles summed
+ * over CTAs; forward: 10 observables and controller input, 13 controller,
+ * 16 springs and advance; reverse: 3 advance and spring adjoints up to the
+ * output layer's dz, 6 controller adjoint, 8 input / centre / height
+ * adjoints).  Written only by a library built with -DCLS_PHASE_TIMERS; zeros
+ * otherwise.  No reference counterpart. */
+int cls_phase_read(cls_sim* sim, unsigned long long* out);
 
 /* Captures one training iteration (forward + loss + backward, optionally the
  * Adam step) into a CUDA graph and replays it; cls_graph_launch replays. */
