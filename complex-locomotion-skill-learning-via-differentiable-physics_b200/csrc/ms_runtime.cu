@@ -1809,6 +1809,7 @@ class SimImpl final : public SimBase {
   void phase_read(unsigned long long* out) override {
     CLS_CUDA(cudaStreamSynchronize(stream));
     if (d_phase_.p) CLS_CUDA(cudaMemcpy(out, d_phase_.p, sizeof(unsigned long long) * 32, cudaMemcpyDeviceToHost));
+    else std::memset(out, 0, sizeof(unsigned long long) * 32);
   }
 
  private:
@@ -2104,12 +2105,11 @@ int cls_profile_read(cls_sim* sim, double* ms, int64_t* launches, int32_t reset)
   });
 }
 
-#ifdef CLS_PHASE_TIMERS
-// profiling builds only: per-phase clock totals (32 slots)
+// per-phase clock totals (32 slots); zeros unless built with CLS_PHASE_TIMERS
 int cls_phase_read(cls_sim* sim, unsigned long long* out) {
+  if (!out) return CLS_ERR_INVALID;
   return guarded(sim, [&](cls::SimBase& s) { s.phase_read(out); });
 }
-#endif
 
 int cls_graph_capture(cls_sim* sim, int32_t steps, int32_t with_adam) {
   return guarded(sim, [&](cls::SimBase& s) { s.graph_capture(steps, with_adam != 0); });
