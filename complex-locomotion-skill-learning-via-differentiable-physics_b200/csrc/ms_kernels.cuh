@@ -139,6 +139,9 @@ struct MsArgs {
   const V4<R>* inc_f;                // {rest length, stiffness, actuation coef, 0}
   const int4* inc_p;                 // FP32 only: packed 16-byte incidence records
   const int* spring_out;             // per spring: MLP output index or -1
+  const int4* spr_ab;                // per spring {a, b, MLP output or -1, 0} (spr_off)
+  const V4<R>* spr_p;                // per spring {rest length, stiffness, actuation coef, 0}
+  int imp_cap;                       // springs of the shared impulse table (0: none)
   const R* w;                        // compact weights
   const R* bias;
   const R* sin_table;                // [T + 1][n_sin], sin(omega (t) dt + 2 pi j / n_sin)
@@ -209,6 +212,7 @@ struct FwdSmem {
   R* buf0; R* buf1;
   R* red;          // kRedFwd entries
   unsigned char* head;  // per-vertex heading side (rotation of robots other than 100)
+  V4<R>* imp;      // per-spring impulses when MsArgs::imp_cap > 0, else null
   R* w; R* b;      // the env's controller when MsArgs::w_smem > 0, else null
 };
 
@@ -225,6 +229,7 @@ __device__ __forceinline__ FwdSmem<R> carve_fwd(char* base, const MsArgs<R>& a) 
   s.buf1 = (R*)take(sizeof(R) * a.smem_dmax);
   s.red = (R*)take(sizeof(R) * kRedFwd);
   s.head = (unsigned char*)take(a.smem_nmax);
+  s.imp = a.imp_cap ? (V4<R>*)take(sizeof(V4<R>) * a.imp_cap) : nullptr;
   s.w = a.w_smem ? (R*)take(sizeof(R) * a.w_smem) : nullptr;
   s.b = a.w_smem ? (R*)take(sizeof(R) * a.b_smem) : nullptr;
   return s;
@@ -238,10 +243,10 @@ __host__ __device__ inline size_t ctrl_smem_bytes(long long w_elems, long long b
 }
 
 template <typename R>
-__host__ __device__ inline size_t fwd_smem_bytes(int nmax, int dmax, int p0max) {
+__host__ __device__ inline size_t fwd_smem_bytes(int nmax, int dmax, int p0max, size_t imp_cap) {
   auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
   return 3 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * p0max) + 2 * rb(sizeof(R) * dmax) +
-         rb(sizeof(R) * kRedFwd) + rb(nmax);
+         rb(sizeof(R) * kRedFwd) + rb(nmax) + (imp_cap ? rb(sizeof(V4<R>) * imp_cap) : 0);
 }
 
 // Reverse-pass shared memory.  gvinc (v_inc, then its adjoint) is live only
@@ -411,6 +416,75 @@ __device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotD
         if (q < end[k]) accumulate_incidence<R>(a, first[k], xi, vi, xs, vs, out, s0, s1, s2);
         for (q += 16; q < end[k]; q += 16)
           accumulate_incidence<R>(a, load_inc<R>(a, rb, q, pol), xi, vi, xs, vs, out, s0, s1, s2);
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+      if (l16 == 0 && v < N) {
+        V4<R> r; r.x = s0; r.y = s1; r.z = s2; r.w = 0;
+        vinc[v] = r;
+        if (rec) rec[v] = r;
+      }
+    }
+  }
+}
+
+// The same v_inc with each spring's impulse computed once: phase A evaluates
+// every spring (spring-parallel, a -> b order as both of its incidences do) into
+// imp[], phase B is gather_vinc_all's half-warp gather with the impulses read
+// from imp[] instead of recomputed, in the same lanes and the same order.  For
+// robots whose impulse table fits in shared memory (MsArgs::imp_cap).
+template <typename R>
+__device__ __forceinline__ void gather_vinc_table(const MsArgs<R>& a, const RobotDesc& rb, int N,
+                                                  const V4<R>* xs, const V4<R>* vs, const R* out,
+                                                  V4<R>* imp, V4<R>* vinc, V4<R>* rec) {
+  constexpr int U = 4;
+  const unsigned long long pol = policy_evict_last();
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int sp = tid; sp < rb.n_s; sp += nt) {
+    const int4 ab = ldg_i4_hint(a.spr_ab + rb.spr_off + sp, pol);
+    const V4<R> f = ldg4_hint<R>(a.spr_p + rb.spr_off + sp, pol);
+    const R act = ab.z >= 0 ? out[ab.z] : R(0);
+    R im[3];
+    spring_impulse<R>(xs[ab.x], xs[ab.y], vs[ab.x], vs[ab.y], f.x, f.y, f.z, act, a.dt, a.dashpot, im);
+    V4<R> r; r.x = im[0]; r.y = im[1]; r.z = im[2]; r.w = 0;
+    imp[sp] = r;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
+  const int l16 = lane & 15, half = lane >> 4;
+  const int* ptr = a.inc_ptr + rb.ptr_off;
+  const int stride = nw * 2;
+  for (int vb0 = wid * 2; vb0 < N; vb0 += stride * U) {
+    const int vb = vb0 + half;
+    int beg[U], end[U];
+    int4 first[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int v = vb + k * stride;
+      beg[k] = 0;
+      end[k] = 0;
+      if (v < N) { beg[k] = ptr[v]; end[k] = ptr[v + 1]; }
+      const int q = beg[k] + l16;
+      first[k] = make_int4(0, 0, 0, 0);
+      if (q < end[k]) first[k] = ldg_i4_hint(a.inc_i + rb.inc_off + q, pol);
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int v = vb + k * stride;
+      R s0 = 0, s1 = 0, s2 = 0;
+      if (v < N) {
+        int q = beg[k] + l16;
+        for (int4 in = first[k]; q < end[k];) {
+          const V4<R> im = imp[in.z];
+          if (in.y == 0) { s0 -= im.x; s1 -= im.y; s2 -= im.z; }
+          else { s0 += im.x; s1 += im.y; s2 += im.z; }
+          q += 16;
+          if (q < end[k]) in = ldg_i4_hint(a.inc_i + rb.inc_off + q, pol);
+        }
       }
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) {

@@ -214,6 +214,9 @@ class SimImpl final : public SimBase {
     std::vector<int4> inc_i, inc_p;
     std::vector<V4<R>> inc_f;
     std::vector<int> spring_out;
+    std::vector<int4> spr_ab;  // per spring {a, b, MLP output or -1, 0}
+    std::vector<V4<R>> spr_p;  // per spring {rest length, stiffness, actuation coef, 0}
+    int smax = 0;
     long long woff = 0, moff = 0, wtoff = 0;
     int boff = 0;
     nmax_ = 0;
@@ -302,7 +305,15 @@ class SimImpl final : public SimBase {
       inc_ptr.push_back(run);
       for (int s = 0; s < h.n_s; ++s) {
         spring_out.push_back(h.out[s]);
+        spr_ab.push_back(make_int4(h.sa[s], h.sb[s], h.out[s], 0));
+        V4<R> f;
+        f.x = (R)h.len[s];  // the incidence records' values, bit for bit
+        f.y = (R)h.stiff[s];
+        f.z = (R)h.coef[s];
+        f.w = 0;
+        spr_p.push_back(f);
       }
+      smax = std::max(smax, h.n_s);
       nmax_ = std::max(nmax_, h.n_v);
       p0max = std::max(p0max, round4(h.width[0]));
       omax = std::max(omax, round4(h.n_out));
@@ -403,7 +414,10 @@ class SimImpl final : public SimBase {
     smem_dmax_ = dmax;
     smem_amax_ = amax;
     smem_omax_ = omax;
-    fwd_base_ = fwd_smem_bytes<R>(nmax_, dmax, p0max);
+    // spring impulses computed once per spring into shared memory when the
+    // largest robot's table is small (the forward gathers then read them)
+    imp_cap_ = (size_t)smax * sizeof(V4<R>) <= kImpSmemMax ? smax : 0;
+    fwd_base_ = fwd_smem_bytes<R>(nmax_, dmax, p0max, imp_cap_);
     int dev = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, dev));
@@ -430,6 +444,8 @@ class SimImpl final : public SimBase {
     d_inc_f_.alloc(std::max<size_t>(1, inc_f.size()));
     d_inc_p_.alloc(std::max<size_t>(1, inc_p.size()));
     d_spring_out_.alloc(std::max<size_t>(1, spring_out.size()));
+    d_spr_ab_.alloc(std::max<size_t>(1, spr_ab.size()));
+    d_spr_p_.alloc(std::max<size_t>(1, spr_p.size()));
     d_w_.alloc(woff);
     d_gw_.alloc(woff);
     wt_total_ = wtoff;
@@ -501,6 +517,10 @@ class SimImpl final : public SimBase {
       CLS_CUDA(cudaMemcpy(d_inc_i_.p, inc_i.data(), sizeof(int4) * inc_i.size(), cudaMemcpyHostToDevice));
       CLS_CUDA(cudaMemcpy(d_inc_f_.p, inc_f.data(), sizeof(V4<R>) * inc_f.size(), cudaMemcpyHostToDevice));
       CLS_CUDA(cudaMemcpy(d_inc_p_.p, inc_p.data(), sizeof(int4) * inc_p.size(), cudaMemcpyHostToDevice));
+    }
+    if (!spr_ab.empty()) {
+      CLS_CUDA(cudaMemcpy(d_spr_ab_.p, spr_ab.data(), sizeof(int4) * spr_ab.size(), cudaMemcpyHostToDevice));
+      CLS_CUDA(cudaMemcpy(d_spr_p_.p, spr_p.data(), sizeof(V4<R>) * spr_p.size(), cudaMemcpyHostToDevice));
     }
     if (!spring_out.empty()) {
       CLS_CUDA(cudaMemcpy(d_spring_out_.p, spring_out.data(), sizeof(int) * spring_out.size(),
@@ -769,6 +789,9 @@ class SimImpl final : public SimBase {
     a.inc_f = d_inc_f_.p;
     a.inc_p = d_inc_p_.p;
     a.spring_out = d_spring_out_.p;
+    a.spr_ab = d_spr_ab_.p;
+    a.spr_p = d_spr_p_.p;
+    a.imp_cap = (int)imp_cap_;
     a.w = d_w_.p;
     a.bias = d_bias_.p;
     a.sin_table = d_sin_.p;
@@ -1047,7 +1070,7 @@ class SimImpl final : public SimBase {
     // shared-memory carve with the controller buffers sized for the output
     // layer only (step_args)
     dense_threads_ = CLS_STEP_THREADS;
-    dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_);
+    dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_, imp_cap_);
     drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_);
     int dev = 0, optin = 0;
     CLS_CUDA(cudaGetDevice(&dev));
@@ -1768,7 +1791,10 @@ class SimImpl final : public SimBase {
   DevBuf<RobotDesc> d_robots_;
   DevBuf<EnvDesc> d_envs_;
   DevBuf<int> d_order_, d_queue_, d_inc_ptr_, d_spring_out_, d_status_, d_iter_;
-  DevBuf<int4> d_inc_i_, d_inc_p_;
+  DevBuf<int4> d_inc_i_, d_inc_p_, d_spr_ab_;
+  DevBuf<V4<R>> d_spr_p_;
+  size_t imp_cap_ = 0;
+  static constexpr size_t kImpSmemMax = 48 * 1024;
   DevBuf<V4<R>> d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_recvinc_, d_obsc_, d_xfull_,
       d_tv_, d_init_, d_adjx_, d_adjv_;
   DevBuf<R> d_w_, d_gw_, d_bias_, d_gb_, d_bm_, d_bv_, d_wm_, d_wmm_, d_wmv_, d_sin_, d_recin_,

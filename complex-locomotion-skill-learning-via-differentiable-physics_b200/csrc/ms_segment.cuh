@@ -333,8 +333,11 @@ __device__ __forceinline__ void fwd_post(const MsArgs<R>& a, const RobotDesc& rb
     R* af = a.act_full + (size_t)t * a.z_total[L - 1] + ed.z_off[L - 1];
     for (int o = tid; o < rb.n_out; o += nt) af[o] = out[o];
   }
-  gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc,
-                     (mode & FWD_RECORD) ? a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off : nullptr);
+  V4<R>* rec = (mode & FWD_RECORD) ? a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off : nullptr;
+  if (s.imp)
+    gather_vinc_table<R>(a, rb, N, s.xs, s.vs, out, s.imp, s.vinc, rec);
+  else
+    gather_vinc_all<R>(a, rb, N, s.xs, s.vs, out, s.vinc, rec);
   __syncthreads();
   for (int i = tid; i < N; i += nt) advance_vertex<R>(a, s.xs[i], s.vs[i], s.vinc[i]);
   __syncthreads();
