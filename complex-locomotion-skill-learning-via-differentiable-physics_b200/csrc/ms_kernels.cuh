@@ -142,6 +142,8 @@ struct MsArgs {
   const int4* spr_ab;                // per spring {a, b, MLP output or -1, 0} (spr_off)
   const V4<R>* spr_p;                // per spring {rest length, stiffness, actuation coef, 0}
   int imp_cap;                       // springs of the shared impulse table (0: none)
+  int adj_cap;                       // springs of the shared adjoint table (0: none; the
+                                     // batched step kernels keep their occupancy instead)
   const R* w;                        // compact weights
   const R* bias;
   const R* sin_table;                // [T + 1][n_sin], sin(omega (t) dt + 2 pi j / n_sin)
@@ -261,6 +263,7 @@ struct RevSmem {
   R* dz;           // union region, MLP phase
   V4<R>* part;     // union region, MLP phase: blockDim partials
   R* red;
+  V4<R>* adj;      // per-spring adjoint terms (2 per spring) when MsArgs::adj_cap > 0
   R* w; R* b;      // the env's controller when MsArgs::w_smem > 0, else null
 };
 
@@ -288,16 +291,19 @@ __device__ __forceinline__ RevSmem<R> carve_rev(char* base, const MsArgs<R>& a) 
   s.gvinc = (V4<R>*)u;
   s.dz = (R*)u;
   s.part = (V4<R>*)(u + ((sizeof(R) * a.smem_dmax + 255) & ~size_t(255)));
+  s.adj = a.adj_cap ? (V4<R>*)take(2 * sizeof(V4<R>) * a.adj_cap) : nullptr;
   s.w = a.w_smem ? (R*)take(sizeof(R) * a.w_smem) : nullptr;
   s.b = a.w_smem ? (R*)take(sizeof(R) * a.b_smem) : nullptr;
   return s;
 }
 
 template <typename R>
-__host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, int dmax, int threads) {
+__host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, int dmax, int threads,
+                                                size_t adj_cap) {
   auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
   return 4 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * amax) + rb(sizeof(R) * omax) +
-         rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads);
+         rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads) +
+         (adj_cap ? rb(2 * sizeof(V4<R>) * adj_cap) : 0);
 }
 
 // ------------------------------------------------------------- primitives

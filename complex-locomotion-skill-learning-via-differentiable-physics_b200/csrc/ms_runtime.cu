@@ -588,7 +588,7 @@ class SimImpl final : public SimBase {
     const int keep = threads_;
     threads_ = threads;
     try {
-      const size_t rev0 = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, threads);
+      const size_t rev0 = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_dmax_, threads, imp_cap_);
       const size_t ctrl = ctrl_smem_bytes<R>(wspan_max_, bspan_max_);
       int dev = 0, optin = 0;
       CLS_CUDA(cudaGetDevice(&dev));
@@ -792,6 +792,7 @@ class SimImpl final : public SimBase {
     a.spr_ab = d_spr_ab_.p;
     a.spr_p = d_spr_p_.p;
     a.imp_cap = (int)imp_cap_;
+    a.adj_cap = (int)imp_cap_;
     a.w = d_w_.p;
     a.bias = d_bias_.p;
     a.sin_table = d_sin_.p;
@@ -1071,7 +1072,7 @@ class SimImpl final : public SimBase {
     // layer only (step_args)
     dense_threads_ = CLS_STEP_THREADS;
     dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_, imp_cap_);
-    drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_);
+    drev_smem_ = rev_smem_bytes<R>(nmax_, smem_amax_, smem_omax_, smem_omax_, dense_threads_, 0);
     int dev = 0, optin = 0;
     CLS_CUDA(cudaGetDevice(&dev));
     CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1089,6 +1090,7 @@ class SimImpl final : public SimBase {
     MsArgs<R> b = a;
     b.smem_dmax = smem_omax_;
     b.w_smem = b.b_smem = 0;  // the step kernels read the controller from its GEMM tiles
+    b.adj_cap = 0;            // and keep their residency: the spring adjoint gathers directly
     b.n_items = E_;
     return b;
   }

@@ -557,23 +557,24 @@ __device__ __forceinline__ R seed_upper(const MsArgs<R>& a, int t, int e, R Br) 
 // atomic: outputs may drive several springs).  Twice the spring arithmetic of
 // a spring-parallel adjoint, in exchange for its 12 shared-memory atomics per
 // spring, which bounded that form (the reverse kernels 10-16 % faster).
+// Adjoint terms of one spring's impulse (evaluated in a -> b order): gd =
+// d loss / d x_a (x_b takes -gd), h = d loss / d v_a (v_b takes -h), and the
+// actuation gradient's factor gact_f (d act = gact_f * coef * l0 * ...).
 template <typename R>
-__device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc<R>& in, int v, const V4<R>* xs,
-                                                   const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
-                                                   R act_seed_scale, R act_lim, bool act_seed, R (&gxs)[3],
-                                                   R (&gvs)[3]) {
-  const int o = in.other;
-  const int ia = in.side == 0 ? v : o, ib = in.side == 0 ? o : v;
-  const V4<R> xa = xs[ia], xb = xs[ib], va = vs[ia], vb = vs[ib];
-  const V4<R> ga = gvinc[ia], gb = gvinc[ib];
-  const R act = in.out >= 0 ? outv[in.out] : R(0);
+struct SpringAdj {
+  R gd0, gd1, gd2, h0, h1, h2, gact;
+};
+template <typename R>
+__device__ __forceinline__ SpringAdj<R> spring_adjoint_terms(const MsArgs<R>& a, const V4<R>& xa, const V4<R>& xb,
+                                                             const V4<R>& va, const V4<R>& vb, const V4<R>& ga,
+                                                             const V4<R>& gb, R act, R l0, R k, R coef) {
   const R d0 = xa.x - xb.x, d1 = xa.y - xb.y, d2 = xa.z - xb.z;
   const R n2 = d0 * d0 + d1 * d1 + d2 * d2;
   const R r8 = sqrt_s<R>(n2 + R(1e-8));
   const R length = r8 + R(1e-4);
   const R inv_length = rcp_s<R>(length);
-  const R target = in.l0 * (R(1) + in.coef * act);
-  const R sc = a.dt * (length - target) * in.k * inv_length;
+  const R target = l0 * (R(1) + coef * act);
+  const R sc = a.dt * (length - target) * k * inv_length;
   const R invlen = rsqrt_s<R>(n2);
   const R inv_r8 = rcp_s<R>(r8);
   const R n0 = d0 * invlen, n1 = d1 * invlen, nz = d2 * invlen;
@@ -584,27 +585,109 @@ __device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc
   const R gvrel = a.dashpot * (gi0 * n0 + gi1 * n1 + gi2 * nz);
   const R cdv = a.dashpot * vrel;
   const R gn0 = cdv * gi0 + gvrel * dv0, gn1 = cdv * gi1 + gvrel * dv1, gn2 = cdv * gi2 + gvrel * dv2;
-  R gd0 = sc * gi0 + invlen * gn0, gd1 = sc * gi1 + invlen * gn1, gd2 = sc * gi2 + invlen * gn2;
+  SpringAdj<R> r;
+  r.gd0 = sc * gi0 + invlen * gn0; r.gd1 = sc * gi1 + invlen * gn1; r.gd2 = sc * gi2 + invlen * gn2;
   const R ginv = gn0 * d0 + gn1 * d1 + gn2 * d2;
   const R gr_r = -ginv * invlen * invlen * invlen;
-  gd0 += gr_r * d0; gd1 += gr_r * d1; gd2 += gr_r * d2;
-  const R glen = gsc * a.dt * in.k * target * inv_length * inv_length;
+  r.gd0 += gr_r * d0; r.gd1 += gr_r * d1; r.gd2 += gr_r * d2;
+  const R glen = gsc * a.dt * k * target * inv_length * inv_length;
   const R glen_r8 = glen * inv_r8;
-  gd0 += glen_r8 * d0; gd1 += glen_r8 * d1; gd2 += glen_r8 * d2;
-  const R h0 = gvrel * n0, h1 = gvrel * n1, h2 = gvrel * nz;
+  r.gd0 += glen_r8 * d0; r.gd1 += glen_r8 * d1; r.gd2 += glen_r8 * d2;
+  r.h0 = gvrel * n0; r.h1 = gvrel * n1; r.h2 = gvrel * nz;
+  r.gact = -gsc * a.dt * k * inv_length * l0 * coef;
+  return r;
+}
+
+// d act of the spring's output, with the actuation loss's seed
+// (taichi_env.py:276-285, per spring)
+template <typename R>
+__device__ __forceinline__ R spring_gact(R gact, R act, R act_seed_scale, R act_lim, bool act_seed) {
+  if (act_seed) {
+    if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
+  }
+  return gact;
+}
+
+template <typename R>
+__device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc<R>& in, int v, const V4<R>* xs,
+                                                   const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
+                                                   R act_seed_scale, R act_lim, bool act_seed, R (&gxs)[3],
+                                                   R (&gvs)[3]) {
+  const int o = in.other;
+  const int ia = in.side == 0 ? v : o, ib = in.side == 0 ? o : v;
+  const R act = in.out >= 0 ? outv[in.out] : R(0);
+  const SpringAdj<R> t = spring_adjoint_terms<R>(a, xs[ia], xs[ib], vs[ia], vs[ib], gvinc[ia], gvinc[ib], act,
+                                                 in.l0, in.k, in.coef);
   if (in.side == 0) {
-    gxs[0] += gd0; gxs[1] += gd1; gxs[2] += gd2;
-    gvs[0] += h0; gvs[1] += h1; gvs[2] += h2;
-    if (in.out >= 0) {
-      R gact = -gsc * a.dt * in.k * inv_length * in.l0 * in.coef;
-      if (act_seed) {  // actuation loss (taichi_env.py:276-285), per spring
-        if (R(0) < dabs<R>(act) - act_lim) gact += ((act > 0) - (act < 0)) * act_seed_scale;
-      }
-      atomicAdd(gout + in.out, gact);
-    }
+    gxs[0] += t.gd0; gxs[1] += t.gd1; gxs[2] += t.gd2;
+    gvs[0] += t.h0; gvs[1] += t.h1; gvs[2] += t.h2;
+    if (in.out >= 0) atomicAdd(gout + in.out, spring_gact<R>(t.gact, act, act_seed_scale, act_lim, act_seed));
   } else {
-    gxs[0] -= gd0; gxs[1] -= gd1; gxs[2] -= gd2;
-    gvs[0] -= h0; gvs[1] -= h1; gvs[2] -= h2;
+    gxs[0] -= t.gd0; gxs[1] -= t.gd1; gxs[2] -= t.gd2;
+    gvs[0] -= t.h0; gvs[1] -= t.h1; gvs[2] -= t.h2;
+  }
+}
+
+// The same with each spring's adjoint evaluated once: phase A (spring-
+// parallel) stores gd and h per spring in adj[2 s], adj[2 s + 1] and adds the
+// actuation gradient, phase B is spring_adjoint_gather's half-warp gather over
+// the table (same lanes, same order).  For robots whose table fits in shared
+// memory, in the fused reverse kernel (MsArgs::adj_cap).
+template <typename R>
+__device__ __forceinline__ void spring_adjoint_table(const MsArgs<R>& a, const RobotDesc& rb, const V4<R>* xs,
+                                                     const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
+                                                     V4<R>* adj, V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
+                                                     bool act_seed) {
+  const unsigned long long pol = policy_evict_last();
+  for (int sp = threadIdx.x; sp < rb.n_s; sp += blockDim.x) {
+    const int4 ab = ldg_i4_hint(a.spr_ab + rb.spr_off + sp, pol);
+    const V4<R> f = ldg4_hint<R>(a.spr_p + rb.spr_off + sp, pol);
+    const R act = ab.z >= 0 ? outv[ab.z] : R(0);
+    const SpringAdj<R> t = spring_adjoint_terms<R>(a, xs[ab.x], xs[ab.y], vs[ab.x], vs[ab.y], gvinc[ab.x],
+                                                   gvinc[ab.y], act, f.x, f.y, f.z);
+    V4<R> g; g.x = t.gd0; g.y = t.gd1; g.z = t.gd2; g.w = 0;
+    V4<R> h; h.x = t.h0; h.y = t.h1; h.z = t.h2; h.w = 0;
+    adj[2 * sp] = g;
+    adj[2 * sp + 1] = h;
+    if (ab.z >= 0) atomicAdd(gout + ab.z, spring_gact<R>(t.gact, act, act_seed_scale, act_lim, act_seed));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
+  const int l16 = lane & 15, half = lane >> 4;
+  const int* ptr = a.inc_ptr + rb.ptr_off;
+  const int N = rb.n_v, stride = nw * 2;
+  for (int vb0 = wid * 2; vb0 < N; vb0 += stride) {
+    const int v = vb0 + half;
+    R gxs[3] = {0, 0, 0}, gvs[3] = {0, 0, 0};
+    if (v < N) {
+      const int beg = ptr[v], end = ptr[v + 1];
+      for (int q = beg + l16; q < end; q += 16) {
+        const int4 in = ldg_i4_hint(a.inc_i + rb.inc_off + q, pol);
+        const V4<R> g = adj[2 * in.z], h = adj[2 * in.z + 1];
+        if (in.y == 0) {
+          gxs[0] += g.x; gxs[1] += g.y; gxs[2] += g.z;
+          gvs[0] += h.x; gvs[1] += h.y; gvs[2] += h.z;
+        } else {
+          gxs[0] -= g.x; gxs[1] -= g.y; gxs[2] -= g.z;
+          gvs[0] -= h.x; gvs[1] -= h.y; gvs[2] -= h.z;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        gxs[c] += __shfl_xor_sync(0xffffffffu, gxs[c], o);
+        gvs[c] += __shfl_xor_sync(0xffffffffu, gvs[c], o);
+      }
+    }
+    if (l16 == 0 && v < N) {
+      V4<R> x = gx[v], w = gv[v];
+      x.x += gxs[0]; x.y += gxs[1]; x.z += gxs[2];
+      w.x += gvs[0]; w.y += gvs[1]; w.z += gvs[2];
+      gx[v] = x;
+      gv[v] = w;
+    }
   }
 }
 
@@ -723,8 +806,12 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     const bool act_seed = (a.loss_mask & LOSS_ACTUATION) && t < st_e && a.th[o] < R(0.1 + 1e-4);
     const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
     const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
-    spring_adjoint_gather<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
-                          act_seed);
+    if (s.adj)
+      spring_adjoint_table<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.adj, s.gx, s.gv, act_scale, lim,
+                              act_seed);
+    else
+      spring_adjoint_gather<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
+                               act_seed);
   }
   __syncthreads();
   // adjoint of the MLP's output activation
