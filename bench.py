@@ -19,7 +19,15 @@ workload; the reference itself needs Taichi, which is not installed.
 lattice, 1000 substeps, MLP 1x64), ``spider`` (4096 envs of the spider lattice,
 1000 substeps, MLP 2x256) or ``mpm`` (3D MLS-MPM legged body of 29,504
 particles on a 64^3 grid, 8 envs, 1000 substeps of dt 1e-4, neo-Hookean with
-16 fibre-actuated muscle groups, forward + checkpointed adjoint).
+16 fibre-actuated muscle groups, forward + checkpointed adjoint).  The
+quadruped and spider episodes run as one checkpoint segment by default (their
+records fit in HBM; ``--checkpoint`` sets K).
+
+Before warm-up the mass-spring configurations run the launch-shape autotuner
+(``cls_autotune``: threads per CTA, CTAs per SM, controller in shared memory,
+and the batched controller path for types with many envs) on their own
+workload; the chosen shape and the timed candidates are reported as
+``launch_shape`` (``--no-autotune`` or ``--threads N`` skip it).
 """
 import argparse
 import json
