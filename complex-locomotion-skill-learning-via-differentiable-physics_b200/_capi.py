@@ -98,6 +98,8 @@ _SIGS = {
     "cls_set_controller_path": (c_int32, [ctypes.c_void_p, c_int32]),
     "cls_controller_batched": (c_int32, [ctypes.c_void_p, P_I]),
     "cls_phase_read": (c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "cls_set_spring_tables": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_spring_tables": (c_int32, [ctypes.c_void_p, P_I]),
     "cls_set_launch_shape": (c_int32, [ctypes.c_void_p, c_int32, c_int32, c_int32]),
     "cls_get_launch_shape": (c_int32, [ctypes.c_void_p, P_I, P_I, P_I]),
     "cls_autotune": (c_int32, [ctypes.c_void_p, c_int32, c_int32, ctypes.POINTER(LaunchShape),

@@ -287,6 +287,17 @@ class MassSpringBatch:
                                               ptr(w, _capi.P_I)))
         return int(t[0]), int(c[0]), int(w[0])
 
+    def set_spring_tables(self, mode=-1):
+        """Per-spring tables in shared memory: -1 when they fit (default), 0
+        off (direct gathers from both endpoints), 1 on (``cls_set_spring_tables``)."""
+        self._c(self.lib.cls_set_spring_tables(self.h, int(mode)))
+
+    @property
+    def spring_tables(self):
+        on = np.zeros(1, dtype=np.int32)
+        self._c(self.lib.cls_spring_tables(self.h, ptr(on, _capi.P_I)))
+        return bool(on[0])
+
     def _tune_key(self, steps):
         import hashlib
         import json

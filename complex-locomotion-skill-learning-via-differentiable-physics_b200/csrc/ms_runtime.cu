@@ -177,6 +177,8 @@ class SimBase {
   virtual void set_launch_shape(int threads, int ctas, int wsh) = 0;
   virtual void launch_shape(int* threads, int* ctas, int* wsh) const = 0;
   virtual void autotune(int steps, int repeats, std::vector<cls_launch_shape>& table) = 0;
+  virtual void set_spring_tables(int mode) = 0;
+  virtual bool spring_tables() const = 0;
 };
 
 template <typename R>
@@ -416,6 +418,7 @@ class SimImpl final : public SimBase {
     smem_omax_ = omax;
     // spring impulses computed once per spring into shared memory when the
     // largest robot's table is small (the forward gathers then read them)
+    smax_ = smax;
     imp_cap_ = (size_t)smax * sizeof(V4<R>) <= kImpSmemMax ? smax : 0;
     fwd_base_ = fwd_smem_bytes<R>(nmax_, dmax, p0max, imp_cap_);
     int dev = 0;
@@ -628,6 +631,44 @@ class SimImpl final : public SimBase {
       throw;
     }
   }
+
+  // Per-spring tables in shared memory (forward impulses, reverse adjoint
+  // terms): -1 when the largest robot's impulse table fits kImpSmemMax (the
+  // default), 0 never (direct gathers), 1 on (it must fit).  Recomputes the
+  // fused and step kernels' shared memory with the launch shape.
+  void set_spring_tables(int mode) override {
+    CLS_REQUIRE(!capturing_, "the spring tables cannot change during graph capture");
+    CLS_REQUIRE(mode >= -1 && mode <= 1, "spring_tables must be -1 (automatic), 0 or 1");
+    const size_t fit = (size_t)smax_ * sizeof(V4<R>) <= kImpSmemMax ? (size_t)smax_ : 0;
+    CLS_REQUIRE(mode != 1 || fit, "the spring tables do not fit in shared memory");
+    const size_t keep = imp_cap_;
+    auto apply = [&](size_t cap) {
+      imp_cap_ = cap;
+      fwd_base_ = fwd_smem_bytes<R>(nmax_, smem_dmax_, smem_p0max_, imp_cap_);
+      use_shape(threads_, wsh_on_ ? 1 : 0);
+      if (d_wt_.p) {  // the batched step kernels carve with the same table
+        dfwd_smem_ = fwd_smem_bytes<R>(nmax_, smem_omax_, smem_p0max_, imp_cap_);
+        int dev = 0, optin = 0;
+        CLS_CUDA(cudaGetDevice(&dev));
+        CLS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        size_t fwd_static = 0, rev_static = 0;
+        CLS_CUDA(DenseLaunch<R>::setup(dense_threads_, &fwd_static, &rev_static, optin));
+        CLS_REQUIRE(dfwd_smem_ + fwd_static <= (size_t)optin,
+                    "robot too large for the batched controller's step kernels");
+      }
+    };
+    try {
+      apply(mode == 0 ? 0 : fit);
+    } catch (...) {
+      try {
+        apply(keep);
+      } catch (...) {
+      }
+      throw;
+    }
+    fwd_done_ = bwd_done_ = false;
+  }
+  bool spring_tables() const override { return imp_cap_ > 0; }
 
   void set_launch_shape(int threads, int ctas, int wsh) override {
     CLS_REQUIRE(!capturing_, "the launch shape cannot change during graph capture");
@@ -1796,6 +1837,7 @@ class SimImpl final : public SimBase {
   DevBuf<int4> d_inc_i_, d_inc_p_, d_spr_ab_;
   DevBuf<V4<R>> d_spr_p_;
   size_t imp_cap_ = 0;
+  int smax_ = 0;
   static constexpr size_t kImpSmemMax = 48 * 1024;
   DevBuf<V4<R>> d_inc_f_, d_ckx_, d_ckv_, d_finx_, d_finv_, d_recx_, d_recv_, d_recvinc_, d_obsc_, d_xfull_,
       d_tv_, d_init_, d_adjx_, d_adjv_;
@@ -2172,6 +2214,16 @@ int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t
   *threads_per_block = t;
   *ctas_per_sm = c;
   if (weights_shared) *weights_shared = w;
+  return CLS_OK;
+}
+
+int cls_set_spring_tables(cls_sim* sim, int32_t mode) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_spring_tables(mode); });
+}
+
+int cls_spring_tables(const cls_sim* sim, int32_t* on) {
+  if (!sim || !sim->impl || !on) return CLS_ERR_INVALID;
+  *on = sim->impl->spring_tables() ? 1 : 0;
   return CLS_OK;
 }
 

@@ -245,6 +245,17 @@ int cls_set_launch_shape(cls_sim* sim, int32_t threads_per_block, int32_t ctas_p
 int cls_get_launch_shape(const cls_sim* sim, int32_t* threads_per_block, int32_t* ctas_per_sm,
                          int32_t* weights_shared);
 
+/* Per-spring tables of the fused and step kernels: each spring's impulse
+ * (forward) and adjoint terms (fused reverse) evaluated once into shared
+ * memory and gathered per vertex, instead of evaluated from both of its
+ * endpoints.  mode -1 (the default at creation): on when the largest robot's
+ * table fits (<= 3072 springs in FP32); 0 off; 1 on (CLS_ERR_INVALID when it
+ * does not fit).  The same results (each spring is evaluated in the same
+ * argument order either way and gathered in the same order).  No reference
+ * counterpart. */
+int cls_set_spring_tables(cls_sim* sim, int32_t mode);
+int cls_spring_tables(const cls_sim* sim, int32_t* on);
+
 /* One timed candidate of cls_autotune. */
 typedef struct cls_launch_shape {
   int32_t controller_path;    /* CLS_CONTROLLER_PER_ENV or CLS_CONTROLLER_BATCHED */

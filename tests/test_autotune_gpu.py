@@ -39,6 +39,27 @@ def test_launch_shape_validation():
     b.close()
 
 
+def test_spring_tables_switch():
+    import cls_b200
+    g = load_golden("quad_ref")
+    b = batch_from_golden(g, precision=32, K=7)
+    assert b.spring_tables                  # 272 springs: the tables fit
+    with pytest.raises(cls_b200._capi.ClsError):
+        b.set_spring_tables(2)
+    b.set_spring_tables(0)
+    assert not b.spring_tables
+    b.set_spring_tables(-1)
+    assert b.spring_tables
+    b.close()
+    from cls_b200 import workloads
+    big, _, _ = workloads.uneven_batch(n_robots=2, steps=20, K=10, seed=5, vmin=1800, vmax=2000)
+    assert not big.spring_tables            # > 3072 springs: direct gathers
+    with pytest.raises(cls_b200._capi.ClsError, match="do not fit"):
+        big.set_spring_tables(1)
+    assert np.isfinite(big.simulate(20))
+    big.close()
+
+
 def test_controller_too_large_for_shared_memory():
     import cls_b200
     b = many_env_batch(32, 4, [1024], 10, 20, "per_env")   # 1024 x 176 weights: 720 KB

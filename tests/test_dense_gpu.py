@@ -140,6 +140,26 @@ def test_batched_single_segment_equals_segments(precision):
     assert rel_err(gx, r_gx) < tol
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batched_direct_spring_gathers_equal_tables(precision):
+    """The batched path's step kernels with the spring impulse table and with
+    the direct gathers."""
+    hidden, steps = [70, 50], 40
+    runs = []
+    for mode in (1, 0):
+        b = many_env_batch(precision, 300, hidden, 9, 48, "batched")
+        b.set_spring_tables(mode)
+        runs.append(_run(b, steps, 3))
+        b.close()
+    same = 1e-12 if precision == 64 else 1e-5
+    (l1, g1, x1, s1), (l0, g0, x0, s0) = runs
+    assert abs(l1 - l0) <= same * abs(l0)
+    assert max_rel(x1, x0) < same
+    for (gW, gb), (rW, rb) in zip(g1, g0):
+        assert rel_err(gW, rW) < same and rel_err(gb, rb) < same
+    assert rel_err(s1, s0) < same
+
+
 def test_batched_graph_replay_matches_eager():
     """The forward pass (spring gather, tensor-core GEMMs) is deterministic, so
     the replayed loss is identical; the atomic adds of the reverse pass

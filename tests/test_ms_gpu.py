@@ -152,6 +152,42 @@ def test_graph_replay_matches_eager():
     np.testing.assert_allclose(g_graph, g_eager, rtol=1e-6, atol=1e-9)
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("case", TRAIN_CASES)
+def test_direct_spring_gathers_match_oracle_and_tables(case, precision):
+    """The direct gathers -- each spring evaluated from both endpoints, the
+    path of robots whose spring tables do not fit in shared memory (the
+    uneven benchmark's) -- against the oracle, and against the table path."""
+    g = load_golden(case)
+    steps = int(g["steps"])
+    o = oracle_from_golden(g)
+    o.run(steps)
+    runs = {}
+    for mode in (0, 1):
+        b = batch_from_golden(g, precision=precision, K=7)
+        b.set_spring_tables(mode)
+        assert b.spring_tables == bool(mode)
+        loss = b.simulate(steps)
+        runs[mode] = (loss, [b.get_grads(0, l) for l in range(2)], b.state_grads()[0],
+                      b.trajectory()[:steps])
+        b.close()
+    tol = TOL[precision]
+    loss0, grads0, gx0, traj0 = runs[0]
+    assert abs(loss0 - o.loss[0]) <= tol["loss"] * abs(o.loss[0])
+    for l in range(2):
+        assert rel_err(grads0[l][0], o.gW[l]) < tol["grad"]
+        assert rel_err(grads0[l][1], o.gb[l]) < tol["grad"]
+    B, N = int(g["B"]), g["objects"].shape[0]
+    assert rel_err(gx0, o.gx[0].reshape(B * N, 3)) < tol["grad"]
+    same = 1e-12 if precision == 64 else 1e-6   # the same arithmetic either way
+    loss1, grads1, gx1, traj1 = runs[1]
+    assert abs(loss1 - loss0) <= same * abs(loss0)
+    assert max_rel(traj1, traj0) < same
+    for (gW, gb), (rW, rb) in zip(grads1, grads0):
+        assert rel_err(gW, rW) < same and rel_err(gb, rb) < same
+    assert rel_err(gx1, gx0) < same
+
+
 def test_adam_step_matches_oracle():
     g = load_golden("x_all_losses")
     steps = int(g["steps"])
