@@ -51,3 +51,22 @@ def test_invalid_arguments_rejected_before_any_device_work():
     bad = cls_b200.Robot(np.zeros((2, 3)), np.array([[0, 5, 0.1, 1e4, 0.0]]), hidden=[4])
     with pytest.raises(cls_b200._capi.ClsError, match="endpoint"):
         cls_b200.MassSpringBatch([bad], [0])
+
+
+def test_shape_and_table_entry_points_reject_null_handles():
+    """Launch-shape, autotuner, spring-table and phase-clock calls return
+    CLS_ERR_INVALID for a NULL handle or output pointer (no device work)."""
+    import ctypes
+    import cls_b200
+    lib = cls_b200._capi.load()
+    inv = -1  # CLS_ERR_INVALID
+    i32 = ctypes.c_int32()
+    table = (cls_b200._capi.LaunchShape * 4)()
+    clocks = (ctypes.c_uint64 * 32)()
+    assert lib.cls_set_launch_shape(None, 256, 1, -1) == inv
+    assert lib.cls_get_launch_shape(None, ctypes.byref(i32), ctypes.byref(i32), None) == inv
+    assert lib.cls_autotune(None, 0, 1, table, 4, ctypes.byref(i32)) == inv
+    assert lib.cls_autotune(None, 0, 1, None, 4, ctypes.byref(i32)) == inv   # table missing
+    assert lib.cls_set_spring_tables(None, 0) == inv
+    assert lib.cls_spring_tables(None, ctypes.byref(i32)) == inv
+    assert lib.cls_phase_read(None, clocks) == inv
