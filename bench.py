@@ -106,6 +106,28 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest of every rank's x (a time: the job takes as long as its
+    slowest rank); x itself when there is one rank.  Every rank calls it at the
+    same point."""
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world, device="cuda"):
+    """The sum of every rank's x (work done); x itself when there is one rank."""
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item())
+
+
 def config_dict(a, n_gpus):
     par = "env-sharded replicas x%d (no data-path collective)" % n_gpus
     if a.config == "uneven":
@@ -353,11 +375,7 @@ def run_ours(a):
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     ms_per_step = ms / a.steps
     # per-kernel breakdown: one more iteration, outside the timed region, with
     # CUDA events around every launch (their gaps would inflate the timed loop)
@@ -469,10 +487,7 @@ def run_ours(a):
             cls_b200._capi.check(lib.cls_adam_step(h, it, None), h)
             cls_b200._capi.check(lib.cls_synchronize(h), h)
         e2e_s = (time.perf_counter() - t0) / a.e2e_steps
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, world)
         h2d = (x0.numel() + v0.numel() + tvh.numel() + thh.numel()) * 8
         d2h = (loss_terms.numel() + b.n_envs * 8) * 8
         e2e = {"value": world * env_substeps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -597,11 +612,7 @@ def run_mpm(a):
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     ms_per_step = ms / a.steps
     value = world * env_substeps / (ms_per_step / 1e3)
     print("timed: %.1f ms/step, %.3e %s, kernels %s" % (ms_per_step, value, UNIT, prof_ms),
@@ -647,10 +658,7 @@ def run_mpm(a):
             b._c(lib.cls_mpm_backward(h))
             b._c(lib.cls_mpm_get_grads(h, pd(gact), None, None, None, None))
         e2e_s = (time.perf_counter() - t0) / a.e2e_steps
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, world)
         e2e = {"value": world * env_substeps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int((x0.numel() + v0.numel() + act.numel()) * 8),
                "d2h_bytes_per_step": int(gact.numel() * 8 + 8),
@@ -784,12 +792,8 @@ def run_serve(a):
             launches[k] = launches.get(k, 0) + n[k]
     wall = st["wall_s"]
     substeps = st["env_substeps_per_s"] * wall
-    if world > 1:
-        t = torch.tensor([wall, substeps], device="cuda", dtype=torch.float64)
-        w = t.clone()
-        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-        wall, substeps = float(w[0].item()), float(t[1].item())
+    wall = max_over_ranks(wall, world)
+    substeps = sum_over_ranks(substeps, world)
     value = substeps / wall
     # roofline of the first-pass kernel: algorithmic bytes of the served
     # forward substeps over its device time
