@@ -20,9 +20,21 @@
 //     the GPU race with each other and give wrong results; serialise them;
 //   * each call clears the part it uses before the first substep, so nothing
 //     left from an earlier call leaks into the result;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture on that device.
+//   * a __device__ array's address belongs to a CUDA context, so the first
+//     call in each context (the runtime's primary context of a device, or a
+//     context the caller created and made current with the driver API) looks
+//     up the array's device address (cudaGetSymbolAddress) with that context
+//     current and keeps it keyed by the context's unique id (cuCtxGetId: ids
+//     are never reused, so a context created after cudaDeviceReset or
+//     cuCtxDestroy gets a fresh lookup); make that first call before any
+//     stream capture in that context;
+//   * spring endpoints must lie in [0, n_vertices); a spring whose endpoint
+//     does not is skipped (it exerts no force), so a bad table never reads or
+//     writes outside the env's rows;
+//   * a CUDA error already pending when the call starts (from the caller's
+//     earlier work) is left in place and reported as CLS_ERR_CUDA without
+//     launching anything.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -34,14 +46,80 @@
 namespace {
 
 constexpr long long kScratchFloats = 1LL << 21;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;
 
 // v_inc scratch ([env][vertex][3]); in host code this name is only a handle
 // for cudaGetSymbolAddress, never a usable address
 static __device__ __align__(256) float g_vinc_scratch[kScratchFloats];
 
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+// the scratch's address per CUDA context, keyed by the context's unique id
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  void* addr;
+};
+ScratchEntry g_scratch[kMaxContexts] = {};
+int g_scratch_used = 0, g_scratch_next = 0;
 std::mutex g_scratch_mutex;
+
+// driver entry points, resolved through the runtime so that the library does
+// not link libcuda (it must load on machines without a driver)
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+bool resolve_driver_calls() {
+  if (g_ctx_get_current && g_ctx_get_id) return true;
+  void* f0 = nullptr;
+  void* f1 = nullptr;
+  cudaDriverEntryPointQueryResult q0, q1;
+  if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+      q0 != cudaDriverEntryPointSuccess || !f0)
+    return false;
+  if (cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+      q1 != cudaDriverEntryPointSuccess || !f1)
+    return false;
+  g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+  g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+  return true;
+}
+
+// id of the current context (0 when none is current)
+unsigned long long current_ctx_id() {
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// The scratch's device address in the current context; on the first call in a
+// context, cudaGetSymbolAddress (which also makes the device's primary context
+// current when no context is) resolves it with that context current.
+cudaError_t scratch_address(float** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!resolve_driver_calls()) return cudaErrorNotSupported;
+  unsigned long long id = current_ctx_id();
+  if (id) {
+    for (int i = 0; i < g_scratch_used; ++i)
+      if (g_scratch[i].ctx_id == id) {
+        *out = static_cast<float*>(g_scratch[i].addr);
+        return cudaSuccess;
+      }
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_vinc_scratch);
+  if (e != cudaSuccess) return e;
+  if (!p) return cudaErrorInvalidSymbol;
+  if (!id) id = current_ctx_id();   // the lookup made the primary context current
+  if (id) {
+    int slot = g_scratch_used < kMaxContexts ? g_scratch_used++ : g_scratch_next;
+    if (g_scratch_used == kMaxContexts) g_scratch_next = (slot + 1) % kMaxContexts;
+    g_scratch[slot] = ScratchEntry{id, p};
+  }
+  *out = static_cast<float*>(p);
+  return cudaSuccess;
+}
 
 void set_message(const cls_noalloc_advance* a, const char* msg) {
   if (a && a->error_message && a->error_capacity > 0)
@@ -62,6 +140,7 @@ __global__ void na_spring(cls_noalloc_advance a, float* __restrict__ vinc) {
        q += (long long)gridDim.x * blockDim.x) {
     const int e = (int)(q / a.n_springs), s = (int)(q % a.n_springs);
     const int ia = a.spring_a[s], ib = a.spring_b[s];
+    if (ia < 0 || ia >= a.n_vertices || ib < 0 || ib >= a.n_vertices) continue;
     const float* xe = a.x + (size_t)e * a.n_vertices * 3;
     const float* ve = a.v + (size_t)e * a.n_vertices * 3;
     cls::V4<float> xa, xb, va, vb;
@@ -132,24 +211,22 @@ extern "C" int cls_ms_advance_noalloc(const cls_noalloc_advance* a, void* stream
     set_message(a, msg);
     return CLS_ERR_INVALID;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-    set_message(a, "cls_ms_advance_noalloc: no usable current device");
+  // an error left by the caller's earlier work stays pending for the caller
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof(msg),
+             "cls_ms_advance_noalloc: a CUDA error from earlier work is pending (%s); nothing "
+             "launched",
+             cudaGetErrorName(pending));
+    set_message(a, msg);
     return CLS_ERR_CUDA;
   }
   float* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_vinc_scratch);
-      if (e != cudaSuccess || !p) {
-        set_message(a, cudaGetErrorString(e));
-        return CLS_ERR_CUDA;
-      }
-      g_scratch_addr[dev] = p;
-    }
-    scratch = static_cast<float*>(g_scratch_addr[dev]);
+  const cudaError_t se = scratch_address(&scratch);
+  if (se != cudaSuccess) {
+    set_message(a, cudaGetErrorString(se));
+    return CLS_ERR_CUDA;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float drag_s = (float)exp(-(double)a->dt * (double)a->drag_damping);
