@@ -47,7 +47,8 @@ class SimParams(ctypes.Structure):
                 ("precision", c_int32), ("checkpoint_every", c_int32),
                 ("max_speed", c_double), ("max_height", c_double),
                 ("adam_b1", c_double), ("adam_b2", c_double),
-                ("learning_rate", c_double), ("threads_per_block", c_int32)]
+                ("learning_rate", c_double), ("threads_per_block", c_int32),
+                ("keep_trajectory", c_int32)]
 
 
 class LaunchShape(ctypes.Structure):
@@ -85,6 +86,11 @@ _SIGS = {
     "cls_clear_adam": (c_int32, [ctypes.c_void_p]),
     "cls_get_observables": (c_int32, [ctypes.c_void_p, P_D, P_D, P_D, P_D]),
     "cls_get_trajectory": (c_int32, [ctypes.c_void_p, P_D]),
+    "cls_get_targets": (c_int32, [ctypes.c_void_p, P_D, P_D, P_D]),
+    "cls_set_loss_mask": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_set_loss_envs": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
+    "cls_grad_buffers": (c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
+                                   ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64), P_I]),
     "cls_get_final_state": (c_int32, [ctypes.c_void_p, P_D, P_D]),
     "cls_get_state_grads": (c_int32, [ctypes.c_void_p, P_D, P_D]),
     "cls_synchronize": (c_int32, [ctypes.c_void_p]),

@@ -178,6 +178,17 @@ class MassSpringBatch:
         self._c(self.lib.cls_loss(self.h, ptr(terms), ptr(env)))
         return dict(zip(_capi.LOSS_SLOTS, terms.tolist())), env
 
+    def set_loss(self, names):
+        """Losses of the following rollouts, by name or CLS_LOSS_* mask
+        (``cls_set_loss_mask``); the loss set passed to get_loss."""
+        mask = names if isinstance(names, int) else sum(_capi.LOSS_BITS[n] for n in set(names))
+        self._c(self.lib.cls_set_loss_mask(self.h, int(mask)))
+
+    def set_loss_envs(self, robot, n_envs):
+        """The env count robot type `robot`'s losses are divided by (default:
+        this batch's count of the type; ``cls_set_loss_envs``)."""
+        self._c(self.lib.cls_set_loss_envs(self.h, int(robot), int(n_envs)))
+
     def backward(self):
         self._c(self.lib.cls_backward(self.h))
 
@@ -362,6 +373,14 @@ class MassSpringBatch:
         c, h, u, r = np.zeros((T, E, 3)), np.zeros((T, E)), np.zeros((T, E)), np.zeros((T, E))
         self._c(self.lib.cls_get_observables(self.h, ptr(c), ptr(h), ptr(u), ptr(r)))
         return dict(center=c, height=h, upper_height=u, rotation=r)
+
+    def targets(self):
+        """(target_v [T][E][3], target_h [T][E], target_c [T][E]) as the
+        device holds them (after set_targets or initialize_train)."""
+        T, E = self.T, self.n_envs
+        tv, th, tc = np.zeros((T, E, 3)), np.zeros((T, E)), np.zeros((T, E))
+        self._c(self.lib.cls_get_targets(self.h, ptr(tv), ptr(th), ptr(tc)))
+        return tv, th, tc
 
     def trajectory(self):
         x = np.zeros((self.T, self.n_vertices_total, 3))

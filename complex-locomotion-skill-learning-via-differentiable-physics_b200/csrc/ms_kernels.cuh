@@ -37,7 +37,9 @@ struct RobotDesc {
   int pitch[kMaxLayers];             // row pitch (elements, multiple of 4) of layer l
   long long w_off[kMaxLayers];       // compact weight offsets (elements)
   int b_off[kMaxLayers];             // bias offsets
-  int n_env;                         // envs of this type: B in the loss normalisation
+  int n_env;                         // envs of this type in this handle
+  int loss_envs;                     // B in the loss normalisation (n_env unless a rank holds
+                                     // one shard of a controller's envs: cls_set_loss_envs)
   int env_first;                     // envs are sorted by type
   int rot_idx[4];                    // heading vertices for robot 100
 };

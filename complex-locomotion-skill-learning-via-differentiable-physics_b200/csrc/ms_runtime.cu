@@ -151,6 +151,10 @@ class SimBase {
   virtual void clear_adam() = 0;
   virtual void observables(double* c, double* h, double* u, double* rot) = 0;
   virtual void trajectory(double* x) = 0;
+  virtual void targets(double* tv, double* th, double* tc) = 0;
+  virtual void set_loss_mask(int mask) = 0;
+  virtual void set_loss_envs(int r, int n) = 0;
+  virtual void grad_buffers(void** w, long long* nw, void** b, long long* nb, int* elem) = 0;
   virtual void final_state(double* x, double* v) = 0;
   virtual void state_grads(double* gx, double* gv) = 0;
   virtual int synchronize() = 0;
@@ -379,6 +383,7 @@ class SimImpl final : public SimBase {
     }
     for (int r = 0; r < nr; ++r) {
       rd[r].n_env = count[r];
+      rd[r].loss_envs = count[r];
       rd[r].env_first = first[r] < 0 ? 0 : first[r];
     }
     user_voff_.assign(E, 0);
@@ -475,7 +480,7 @@ class SimImpl final : public SimBase {
     d_obsh_.alloc((size_t)T_ * E);
     d_obsu_.alloc((size_t)T_ * E);
     d_obsr_.alloc((size_t)T_ * E);
-    keep_x_ = (p_.loss_mask & (LOSS_ROTATION | LOSS_POSE)) != 0;
+    keep_x_ = (p_.loss_mask & (LOSS_ROTATION | LOSS_POSE)) != 0 || p_.keep_trajectory != 0;
     if (keep_x_) d_xfull_.alloc((size_t)T_ * V_);
     if (p_.loss_mask & LOSS_ACTUATION) d_actfull_.alloc((size_t)T_ * z_total_[L_ - 1]);
     d_tv_.alloc((size_t)T_ * E);
@@ -1203,7 +1208,7 @@ class SimImpl final : public SimBase {
     if (env) {
       for (int ie = 0; ie < E_; ++ie) {
         const int ue = perm_[ie];
-        const double B = rd_host_[ed_host_[ie].robot].n_env;
+        const double B = rd_host_[ed_host_[ie].robot].loss_envs;
         double tot = 0;
         for (int l = 0; l < LS_COUNT; ++l) {
           const double v = raw[(size_t)ie * 8 + l] * B;
@@ -1511,8 +1516,70 @@ class SimImpl final : public SimBase {
     fetch_scalar(d_obsr_.p, rot);
   }
 
+  void grad_buffers(void** w, long long* nw, void** b, long long* nb, int* elem) override {
+    *w = d_gw_.p;
+    *nw = (long long)d_gw_.n;
+    *b = d_gb_.p;
+    *nb = (long long)d_gb_.n;
+    *elem = (int)sizeof(R);
+  }
+
+  void set_loss_envs(int r, int n) override {
+    CLS_REQUIRE(r >= 0 && r < (int)rd_host_.size(), "robot index out of range");
+    CLS_REQUIRE(n >= rd_host_[r].n_env && n > 0,
+                "the loss env count must be at least the handle's env count of the type");
+    CLS_REQUIRE(!capturing_, "the loss normalisation cannot change during graph capture");
+    if (rd_host_[r].loss_envs == n) return;
+    rd_host_[r].loss_envs = n;
+    CLS_CUDA(cudaMemcpyAsync(d_robots_.p + r, &rd_host_[r], sizeof(RobotDesc), cudaMemcpyHostToDevice,
+                             stream));
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    fwd_done_ = false;
+    bwd_done_ = false;
+  }
+
+  void set_loss_mask(int mask) override {
+    CLS_REQUIRE((mask & ~(LOSS_VELOCITY | LOSS_HEIGHT | LOSS_POSE | LOSS_ACTUATION | LOSS_ROTATION |
+                          LOSS_CRAWL)) == 0,
+                "unknown loss bits");
+    CLS_REQUIRE(!(mask & (LOSS_ROTATION | LOSS_POSE)) || d_xfull_.p != nullptr,
+                "rotation and pose losses need the trajectory: create the handle with one of them or "
+                "with keep_trajectory");
+    CLS_REQUIRE(!(mask & LOSS_ACTUATION) || d_actfull_.p != nullptr,
+                "the actuation loss needs its record: create the handle with it");
+    CLS_REQUIRE(!capturing_, "the loss set cannot change during graph capture");
+    if (mask == p_.loss_mask) return;
+    p_.loss_mask = mask;
+    fwd_done_ = false;
+    bwd_done_ = false;
+  }
+
+  void targets(double* tv, double* th, double* tc) override {
+    const long long n = (long long)T_ * E_;
+    auto fetch_scalar = [&](const R* src, double* dst) {
+      if (!dst) return;
+      ms_to_double_kernel<R><<<blocks_for(n), 256, 0, stream>>>(src, d_stage_.p, n);
+      std::vector<double> tmp(n);
+      CLS_CUDA(cudaMemcpyAsync(tmp.data(), d_stage_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      for (int t = 0; t < T_; ++t)
+        for (int ie = 0; ie < E_; ++ie) dst[(size_t)t * E_ + perm_[ie]] = tmp[(size_t)t * E_ + ie];
+    };
+    if (tv) {
+      ms_v4_to_xyz_kernel<R><<<blocks_for(n), 256, 0, stream>>>(d_tv_.p, d_stage_.p, n);
+      std::vector<double> tmp(n * 3);
+      CLS_CUDA(cudaMemcpyAsync(tmp.data(), d_stage_.p, sizeof(double) * n * 3, cudaMemcpyDeviceToHost, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+      for (int t = 0; t < T_; ++t)
+        for (int ie = 0; ie < E_; ++ie)
+          std::memcpy(tv + ((size_t)t * E_ + perm_[ie]) * 3, &tmp[((size_t)t * E_ + ie) * 3], sizeof(double) * 3);
+    }
+    fetch_scalar(d_th_.p, th);
+    fetch_scalar(d_tc_.p, tc);
+  }
+
   void trajectory(double* x) override {
-    CLS_REQUIRE(d_xfull_.p != nullptr, "trajectory is only kept with a rotation or pose loss");
+    CLS_REQUIRE(d_xfull_.p != nullptr, "trajectory is only kept with a rotation or pose loss or keep_trajectory");
     for (int t = 0; t < T_; ++t) get_vstate(d_xfull_.p + (size_t)t * V_, x + (size_t)t * V_ * 3);
   }
 
@@ -1944,6 +2011,7 @@ void cls_default_params(cls_sim_params* p) {
   p->adam_b2 = 0.9;
   p->learning_rate = 3e-4;
   p->threads_per_block = 0;
+  p->keep_trajectory = 0;
 }
 
 int cls_create(const cls_robot_desc* robots, int32_t n_robots, const int32_t* env_robot,
@@ -2133,6 +2201,31 @@ int cls_clear_adam(cls_sim* sim) {
 
 int cls_get_observables(cls_sim* sim, double* center, double* height, double* upper, double* rot) {
   return guarded(sim, [&](cls::SimBase& s) { s.observables(center, height, upper, rot); });
+}
+
+int cls_grad_buffers(cls_sim* sim, void** weight_grads, int64_t* n_weight, void** bias_grads,
+                     int64_t* n_bias, int32_t* elem_bytes) {
+  if (!weight_grads || !n_weight || !bias_grads || !n_bias || !elem_bytes) return CLS_ERR_INVALID;
+  return guarded(sim, [&](cls::SimBase& s) {
+    long long nw = 0, nb = 0;
+    int e = 0;
+    s.grad_buffers(weight_grads, &nw, bias_grads, &nb, &e);
+    *n_weight = nw;
+    *n_bias = nb;
+    *elem_bytes = e;
+  });
+}
+
+int cls_set_loss_envs(cls_sim* sim, int32_t robot, int32_t n_envs) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_loss_envs(robot, n_envs); });
+}
+
+int cls_set_loss_mask(cls_sim* sim, int32_t mask) {
+  return guarded(sim, [&](cls::SimBase& s) { s.set_loss_mask(mask); });
+}
+
+int cls_get_targets(cls_sim* sim, double* tv, double* th, double* tc) {
+  return guarded(sim, [&](cls::SimBase& s) { s.targets(tv, th, tc); });
 }
 
 int cls_get_trajectory(cls_sim* sim, double* x) {

@@ -741,7 +741,7 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
                                         const RevSmem<R>& s, int e, int t, int kslot) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v, L = rb.n_layers;
-  const R Br = R(rb.n_env);
+  const R Br = R(rb.loss_envs);
   const R* bout = a.bias + rb.b_off[L - 1];
   const int nout = rb.n_out;
   const R* zl = a.rec_z + a.z_base[L - 1] + (size_t)kslot * a.z_total[L - 1] + ed.z_off[L - 1];
@@ -834,7 +834,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
                                          const RevSmem<R>& s, int e, int t, R& hcarry) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v;
-  const R Br = R(rb.n_env);
+  const R Br = R(rb.loss_envs);
   const R invN = R(1) / R(N);
   int* redi = reinterpret_cast<int*>(s.red + kRedInt);
   {
@@ -897,7 +897,7 @@ __device__ __forceinline__ void rev_load_carry(const MsArgs<R>& a, const RobotDe
                                                const RevSmem<R>& s, int e, int t_end, bool last_seg,
                                                R& hcarry) {
   const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
-  const R Br = R(rb.n_env);
+  const R Br = R(rb.loss_envs);
   hcarry = 0;
   if (last_seg) {
     for (int i = tid; i < N; i += nt) {
@@ -1005,7 +1005,7 @@ __global__ void ms_loss_kernel(MsArgs<R> a, double* out, const int* envs) {
   const EnvDesc ed = a.envs[e];
   const RobotDesc& rb = a.robots[ed.robot];
   const int N = rb.n_v, st = steps_of(a, e), rp = a.run_period, tp = a.turn_period, jp = a.jump_period;
-  const double Br = rb.n_env;
+  const double Br = rb.loss_envs;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   acc[7] = 0.0;
   const int tmax = (st < a.T - 1) ? st : a.T - 1;

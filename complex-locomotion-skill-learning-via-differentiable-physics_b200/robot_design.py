@@ -85,6 +85,9 @@ class CubeLattice:
             self.faces.append((quad[0], quad[1], quad[2]))
             self.faces.append((quad[3], quad[0], quad[2]))
 
+    def faces_array(self):
+        return np.asarray(self.faces, dtype=np.int64).reshape(-1, 3)
+
     def arrays(self):
         return (np.asarray(self.objects, dtype=np.float64).reshape(-1, 3),
                 np.asarray(self.springs, dtype=np.float64).reshape(-1, 5))
@@ -142,12 +145,28 @@ def _robot_d(L, act, skeleton):   # spider, id 103 (:470-505)
                  (25, 26), (36, 9), (21, 24), (10, 11)}
     for a, b in list(motor_set) + _SPIDER_EXTRA:
         L.spring(a, b, act if motor(a, b) else 0.0)
+    # mesh faces: every triangle of skeleton links, vertices ascending
+    linked = set()
+    for a, b in data["links"]:
+        linked.add((a, b))
+        linked.add((b, a))
+    n = len(L.objects)
+    nbr = [sorted(b for b in range(n) if (a, b) in linked) for a in range(n)]
+    for a in range(n):
+        for b in nbr[a]:
+            if b <= a:
+                continue
+            for c in nbr[b]:
+                if c > b and (a, c) in linked:
+                    L.faces.append((a, b, c))
 
 
-def reference_robot(robot_id, spring_stiffness, spring_actuation, skeleton=None):
-    """objects, springs of one of the reference's five 3D robots (ids 100-104).
-    The spider (103) reads its node/link table from ``skeleton`` (the
-    reference's cfg3d/skeleton.json)."""
+def reference_robot(robot_id, spring_stiffness, spring_actuation, skeleton=None, faces=False):
+    """objects, springs of one of the reference's five 3D robots (ids 100-104)
+    and, with ``faces=True``, also its triangle list [(a, b, c)] for mesh
+    export (two triangles per cube face, robot_design.py:419-427; the spider's
+    skeleton triangles, :500-504).  The spider (103) reads its node/link table
+    from ``skeleton`` (the reference's cfg3d/skeleton.json)."""
     L = CubeLattice(spring_stiffness, spring_actuation)
     if robot_id == 100:
         _robot_a(L, spring_actuation)
@@ -163,6 +182,8 @@ def reference_robot(robot_id, spring_stiffness, spring_actuation, skeleton=None)
         _robot_e(L, spring_actuation)
     else:
         raise ValueError("invalid robot id %r" % (robot_id,))
+    if faces:
+        return L.arrays() + (np.asarray(L.faces, dtype=np.int64).reshape(-1, 3),)
     return L.arrays()
 
 

@@ -58,10 +58,12 @@ def load_config(src, overrides=None, skeleton=None, seed=None):
     robot = cfg["robot"]
     if robot.get("simulator", "mass_spring") != "mass_spring" or int(robot.get("dim", 3)) != 3:
         raise NotImplementedError("the trainer drives 3D mass-spring robots (MPM: cls_b200.mpm)")
-    objects, springs = robot_design.reference_robot(int(robot["robot_id"]), float(robot["spring_stiffness"]),
-                                                    float(robot["spring_actuation"]), skeleton=skeleton)
+    objects, springs, faces = robot_design.reference_robot(
+        int(robot["robot_id"]), float(robot["spring_stiffness"]), float(robot["spring_actuation"]),
+        skeleton=skeleton, faces=True)
     robot["objects"] = objects
     robot["springs"] = springs
+    robot["faces"] = faces
     robot["n_objects"] = int(len(objects))
     robot["n_springs"] = int(len(springs))
     pr, sim, nn = cfg["process"], cfg["simulator"], cfg["nn"]
@@ -84,7 +86,7 @@ def load_config(src, overrides=None, skeleton=None, seed=None):
     return cfg
 
 
-def sim_params(cfg, precision=32, checkpoint_every=50, max_steps=None):
+def sim_params(cfg, precision=32, checkpoint_every=50, max_steps=None, keep_trajectory=False):
     """Batch parameters of a loaded config (the solver's constants:
     solver_mass_spring.py:58-148, taichi_env.py:149-183, nn.py:173-191)."""
     pr, sim, nn = cfg["process"], cfg["simulator"], cfg["nn"]
@@ -99,7 +101,27 @@ def sim_params(cfg, precision=32, checkpoint_every=50, max_steps=None):
         duplicate_c=int(nn["duplicate_c"]), activation_hidden="sin", activation_output="sin",
         loss=list(cfg["train"]["task"]), precision=precision, checkpoint_every=checkpoint_every,
         max_speed=float(pr["max_speed"]), max_height=float(pr["max_height"]), adam_b1=float(nn["adam_b1"]),
-        adam_b2=float(nn["adam_b2"]), learning_rate=float(nn["learning_rate"]))
+        adam_b2=float(nn["adam_b2"]), learning_rate=float(nn["learning_rate"]),
+        keep_trajectory=1 if keep_trajectory else 0)
+
+
+def write_obj_frames(x, faces, folder, stride=10):
+    """Headless mesh export of one env's trajectory (the evaluation
+    visualiser's 3D branch, diffphy_trainer.py:334-347): every `stride`-th
+    state of x [T][N][3] becomes ``{i:06d}.obj`` (i = index of the written
+    frame) with ``v x y z`` lines (6 decimals) and 1-based ``f a b c``
+    triangles.  Returns the paths written."""
+    os.makedirs(folder, exist_ok=True)
+    frames = np.asarray(x, np.float64)[::stride]
+    face_lines = "".join("f %d %d %d\n" % (a + 1, b + 1, c + 1) for a, b, c in np.asarray(faces).reshape(-1, 3))
+    paths = []
+    for i, xt in enumerate(frames):
+        path = os.path.join(folder, "%06d.obj" % i)
+        with open(path, "w") as f:
+            f.write("".join("v %.6f %.6f %.6f\n" % (p[0], p[1], p[2]) for p in xt))
+            f.write(face_lines)
+        paths.append(path)
+    return paths
 
 
 def script_targets(T, steps, max_speed):
@@ -140,7 +162,7 @@ class DiffPhyTrainer:
     change_iter = 5000
 
     def __init__(self, config, batch_size=None, precision=32, checkpoint_every=50, evaluate=False,
-                 weights_seed=0, log_path=None, stream=None):
+                 weights_seed=0, log_path=None, stream=None, keep_trajectory=False):
         self.config = config if isinstance(config, dict) and "objects" in config.get("robot", {}) \
             else load_config(config)
         cfg = self.config
@@ -156,7 +178,9 @@ class DiffPhyTrainer:
                            robot_id=int(robot["robot_id"]), hidden=[int(nn["n_hidden"])])
         # the reference steps max_steps + 1 states in evaluation (t in [0, steps])
         T = self.max_steps + 2 if evaluate else self.max_steps
-        self.params = sim_params(cfg, precision, checkpoint_every, max_steps=T)
+        self.faces = np.asarray(robot.get("faces", np.zeros((0, 3), np.int64)), np.int64).reshape(-1, 3)
+        self.params = sim_params(cfg, precision, checkpoint_every, max_steps=T,
+                                 keep_trajectory=keep_trajectory)
         self.batch = MassSpringBatch([self.robot], [0] * self.batch_size, self.params)
         if stream is not None:
             self.batch.set_stream(stream)
@@ -273,16 +297,26 @@ class DiffPhyTrainer:
                 log.close()
         return self.losses_list
 
-    def evaluate(self, load_path=None, steps=None, max_speed=None):
+    def evaluate(self, load_path=None, steps=None, max_speed=None, mesh_dir=None, mesh_stride=10):
         """Evaluation rollout (diffphy_trainer.py:304-435, one weights file):
         loads `load_path` (a reference pickle) when given and returns the loss
-        terms of the scripted episode."""
+        terms of the scripted episode.  With `mesh_dir`, env k's trajectory is
+        written as OBJ frames under ``mesh_dir/k`` (export_meshes)."""
         if load_path is not None:
             self.load_weights(load_path)
         self.reset_state()
         steps = self.batch.T - 2 if steps is None else steps
         self.simulate(steps, train=False, max_speed=self.max_speed if max_speed is None else max_speed)
+        if mesh_dir is not None:
+            for k in range(self.batch_size):
+                self.export_meshes(os.path.join(mesh_dir, str(k)), env=k, stride=mesh_stride)
         return dict(self.loss_dict)
+
+    def export_meshes(self, folder, env=0, stride=10):
+        """OBJ frames of env `env`'s last rollout (write_obj_frames); needs the
+        trajectory kept (keep_trajectory=True, or a rotation / pose loss)."""
+        x = self.batch.trajectory()[:, self.batch.env_slice(env)]
+        return write_obj_frames(x, self.faces, folder, stride)
 
     # ------------------------------------------------------------ weights
     def weights(self):

@@ -87,6 +87,8 @@ typedef struct {
   double max_speed, max_height; /* process.max_speed / max_height */
   double adam_b1, adam_b2, learning_rate;
   int32_t threads_per_block;    /* 0: choose automatically */
+  int32_t keep_trajectory;      /* 1: keep x[t] for every t (cls_get_trajectory, mesh export)
+                                   even when no rotation or pose loss needs it; 0: only then */
 } cls_sim_params;
 
 /* Fills *p with the reference's defaults for cfg3d/sim_quad.json. */
@@ -126,6 +128,11 @@ int cls_set_state(cls_sim* sim, const double* x0, const double* v0);
 int cls_set_targets(cls_sim* sim, const double* target_v, const double* target_h,
                     const double* target_c);
 
+/* The targets as the device holds them (same layouts as cls_set_targets;
+ * any pointer may be NULL): the fields TaichiEnv.initialize_train writes
+ * (multitask/taichi_env.py:385-447), read back after cls_initialize_train. */
+int cls_get_targets(cls_sim* sim, double* target_v, double* target_h, double* target_c);
+
 /* Reference-layout weights W [rows][cols], b [rows] of one layer; layer 0 is
  * weights1/bias1 (multitask/nn.py:31-43).  Replaces Model.load_weights. */
 int cls_set_weights(cls_sim* sim, int32_t robot, int32_t layer, const double* W, const double* b);
@@ -144,6 +151,14 @@ int cls_forward_eval(cls_sim* sim, int32_t steps);
  * crawl; loss_env [8][n_envs] the per-env losses (loss_batch fields, scaled by
  * B as the reference does); either may be NULL. */
 int cls_loss(cls_sim* sim, double* loss_terms, double* loss_env);
+/* Selects the losses of the following rollouts (CLS_LOSS_* bits): the
+ * loss_enable set that DiffPhyTrainer passes to TaichiEnv.get_loss
+ * (multitask/taichi_env.py:304-317).  Rotation and pose need the trajectory
+ * (created with one of them or keep_trajectory), actuation its record
+ * (created with it); CLS_ERR_INVALID otherwise.  A CUDA graph captured
+ * earlier keeps the set it was captured with.  The next cls_backward needs a
+ * new cls_forward. */
+int cls_set_loss_mask(cls_sim* sim, int32_t mask);
 /* Reverse pass (ti.ad.Tape exit, diffphy_trainer.py:246): recompute each
  * segment from its checkpoint and run the hand-written adjoints. */
 int cls_backward(cls_sim* sim);
@@ -155,6 +170,26 @@ int cls_simulate_per_env(cls_sim* sim, int32_t steps, double* loss);
  * 184-191) with bias correction for iteration `iter`; *tns receives the
  * squared gradient norm (Model.get_TNS, :173-182) if non-NULL. */
 int cls_adam_step(cls_sim* sim, int32_t iter, double* tns);
+/* Device buffers of the weight and bias gradients of every robot type (in
+ * the library's packed layout, elem_bytes = 4 or 8 by precision), which
+ * cls_backward writes and cls_adam_step reads; valid until cls_destroy.
+ * Ranks holding identically created handles (the same robot types, each
+ * with a share of one controller's envs) all-reduce them in place between
+ * cls_backward and cls_adam_step to train one shared controller
+ * data-parallel, each having set the total env count with
+ * cls_set_loss_envs.  No reference counterpart: the reference trains one
+ * batch on one device. */
+int cls_grad_buffers(cls_sim* sim, void** weight_grads, int64_t* n_weight, void** bias_grads,
+                     int64_t* n_bias, int32_t* elem_bytes);
+/* The env count B that robot type `robot`'s loss terms are divided by
+ * (multitask/taichi_env.py:185-293 divide by the batch size); default: the
+ * handle's own env count of the type.  A rank holding one shard of a
+ * controller's envs sets the total over all ranks, so that its loss and
+ * gradients are its shard's share of the whole batch's and the all-reduced
+ * sum is the whole batch's.  n_envs must be at least the handle's count.
+ * The next cls_backward needs a new cls_forward; a CUDA graph captured
+ * earlier keeps the value it was captured with.  No reference counterpart. */
+int cls_set_loss_envs(cls_sim* sim, int32_t robot, int32_t n_envs);
 /* zero the Adam moments (Model.clear_adam, multitask/nn.py:111-114) */
 int cls_clear_adam(cls_sim* sim);
 
@@ -163,7 +198,8 @@ int cls_clear_adam(cls_sim* sim);
 int cls_get_observables(cls_sim* sim, double* center, double* height, double* upper_height,
                         double* rotation);
 /* Positions x[t] for all t ([T][n_vertices_total][3]); only available when a
- * rotation or pose loss is enabled (the trajectory is then kept). */
+ * rotation or pose loss is enabled or params.keep_trajectory is set (the
+ * trajectory is then kept). */
 int cls_get_trajectory(cls_sim* sim, double* x);
 /* State after the last processed substep ([n_vertices_total][3]). */
 int cls_get_final_state(cls_sim* sim, double* x, double* v);
@@ -409,14 +445,18 @@ int cls_mpm_profile_read(cls_mpm* sim, double* ms, int64_t* launches, int32_t re
  * library holds until exit.  Larger problems are rejected with
  * CLS_ERR_INVALID and a message.  All calls share that array: calls that
  * overlap on the GPU race and must be serialised by the caller.  Each call
- * clears the part it uses first.  The first call on a device resolves the
- * array's device address with that device current; make it before any stream
- * capture on that device.
+ * clears the part it uses first.  The array's device address belongs to a CUDA
+ * context: the first call in each context (a device's primary context, or one
+ * the caller created with the driver API and made current) resolves it with
+ * that context current; make that first call before any stream capture in that
+ * context.  Spring endpoints must lie in [0, n_vertices); springs whose
+ * endpoints do not are skipped.  A CUDA error already pending when the call
+ * starts is left pending and reported as CLS_ERR_CUDA, with nothing launched.
  * --------------------------------------------------------------------------- */
 typedef struct {
   int32_t n_envs, n_vertices, n_springs, n_substeps;
-  const int32_t* spring_a;      /* [n_springs] first endpoint */
-  const int32_t* spring_b;      /* [n_springs] second endpoint */
+  const int32_t* spring_a;      /* [n_springs] first endpoint, in [0, n_vertices) */
+  const int32_t* spring_b;      /* [n_springs] second endpoint, in [0, n_vertices) */
   const float* rest_length;     /* [n_springs] */
   const float* stiffness;       /* [n_springs] as applied (after any scaling) */
   const float* actuation_coef;  /* [n_springs] */

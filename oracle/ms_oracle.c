@@ -24,7 +24,10 @@
  *   - the MLP output may feed every spring (reference: n_output = n_springs,
  *     multitask/diffphy_trainer.py:178-185) or only actuated springs (out_index);
  *   - friction coefficient is a parameter (reference hard-codes 0.4,
- *     multitask/solver_mass_spring.py:136).
+ *     multitask/solver_mass_spring.py:136);
+ *   - the env count B that the loss terms are divided by may be set apart
+ *     from the batch's own (loss_envs), for a batch that is one shard of a
+ *     larger batch.
  *
  * Precision: double throughout, as the reference (multitask/utils.py:12).
  * Parallelism: OpenMP over environments (independent in every kernel).
@@ -58,6 +61,7 @@ typedef struct {
   int run_period, turn_period, jump_period, robot_id;
   int loss_mask;
   int n_threads;                   /* 0: OpenMP default */
+  int loss_envs;                   /* B of the loss normalisation; 0: the batch's B (reference) */
   double dt, gravity, ground, drag, dashpot, friction, spring_omega;
   double max_speed, max_height;
   /* robot */
@@ -308,6 +312,7 @@ int orc_ms_forward_eval(const orc_ms* p, int steps) { return forward_impl(p, ste
  * loops) are skipped. */
 int orc_ms_loss(const orc_ms* p, int steps) {
   const int B = p->B, rp = p->run_period, tp = p->turn_period, jp = p->jump_period;
+  const double LB = p->loss_envs > 0 ? p->loss_envs : B;
   memset(p->loss, 0, sizeof(double) * L_COUNT);
   memset(p->loss_batch, 0, sizeof(double) * L_COUNT * B);
   double cmh = p->current_max_height ? p->current_max_height[0] : 0.0;
@@ -319,9 +324,9 @@ int orc_ms_loss(const orc_ms* p, int steps) {
           const double* c0 = p->center + IC3(p, t - rp, k);
           const double* tv = p->tv + IC3(p, t - rp, k);
           double ex = c1[0] - c0[0] - tv[0], ez = c1[2] - c0[2] - tv[2];
-          double lx = ex * ex / B / steps * 100, lz = ez * ez / B / steps * 100;
+          double lx = ex * ex / LB / steps * 100, lz = ez * ez / LB / steps * 100;
           p->loss[L_VEL] += lx + lz;
-          p->loss_batch[L_VEL * B + k] += (lx + lz) * B;
+          p->loss_batch[L_VEL * B + k] += (lx + lz) * LB;
         }
       }
     }
@@ -329,9 +334,9 @@ int orc_ms_loss(const orc_ms* p, int steps) {
       for (int t = 1; t <= steps && t < p->T; ++t) {
         if (t % jp == jp - 1 && p->th[IB(p, t, k)] > 0.1 + 1e-6) {
           double e = p->height[IB(p, t, k)] - p->th[IB(p, t, k)];
-          double lh = e * e / B / (steps / jp) * 100;
+          double lh = e * e / LB / (steps / jp) * 100;
           p->loss[L_HEIGHT] += lh;
-          p->loss_batch[L_HEIGHT * B + k] += lh * B;
+          p->loss_batch[L_HEIGHT * B + k] += lh * LB;
           if (p->height[IB(p, t, k)] > cmh) cmh = p->height[IB(p, t, k)];
         }
       }
@@ -345,9 +350,9 @@ int orc_ms_loss(const orc_ms* p, int steps) {
               double e = p->x[IX3(p, t, k, i) + d] - p->init_obj[i * 3 + d];
               d2 += e * e;
             }
-            double lp = d2 / B / (steps / jp);
+            double lp = d2 / LB / (steps / jp);
             p->loss[L_POSE] += lp;
-            p->loss_batch[L_POSE * B + k] += lp * B;
+            p->loss_batch[L_POSE * B + k] += lp * LB;
           }
         }
       }
@@ -357,9 +362,9 @@ int orc_ms_loss(const orc_ms* p, int steps) {
         if (p->th[IB(p, t, k)] < 0.1 + 1e-4) {
           double lim = pow(fabs(p->tv[IC3(p, t, k)]) / 0.08, 0.5);
           for (int i = 0; i < p->S; ++i) {
-            double la = fmax(fabs(p->act[IS(p, t, k, i)]) - lim, 0.0) / p->S / B / steps * 10;
+            double la = fmax(fabs(p->act[IS(p, t, k, i)]) - lim, 0.0) / p->S / LB / steps * 10;
             p->loss[L_ACT] += la;
-            p->loss_batch[L_ACT * B + k] += la * B;
+            p->loss_batch[L_ACT * B + k] += la * LB;
           }
         }
       }
@@ -383,7 +388,7 @@ int orc_ms_loss(const orc_ms* p, int steps) {
             for (int d = 0; d < 3; ++d) n2 += (t0[d] - t2[d]) * (t0[d] - t2[d]);
             double lr = n2 / steps / 40;
             p->loss[L_ROT] += lr;
-            p->loss_batch[L_ROT * B + k] += lr * B;
+            p->loss_batch[L_ROT * B + k] += lr * LB;
           }
         }
       }
@@ -392,9 +397,9 @@ int orc_ms_loss(const orc_ms* p, int steps) {
       for (int t = 1; t <= steps && t < p->T; ++t) {
         if (p->tc[IB(p, t, k)] > 1 - 1e-4) {
           double e = fmax(p->upper[IB(p, t, k)] - 0.1, 0.0);
-          double lc = e * e / B / steps * 5.;
+          double lc = e * e / LB / steps * 5.;
           p->loss[L_CRAWL] += lc;
-          p->loss_batch[L_CRAWL * B + k] += lc * B;
+          p->loss_batch[L_CRAWL * B + k] += lc * LB;
         }
       }
     }
@@ -411,7 +416,8 @@ int orc_ms_loss(const orc_ms* p, int steps) {
 
 /* adjoint of the loss kernels with loss.grad = 1 (Tape seeding) */
 static void a_loss(const orc_ms* p, int steps, int k) {
-  const int B = p->B, rp = p->run_period, tp = p->turn_period, jp = p->jump_period;
+  const int rp = p->run_period, tp = p->turn_period, jp = p->jump_period;
+  const double B = p->loss_envs > 0 ? p->loss_envs : p->B;
   if (p->loss_mask & ORC_LOSS_VELOCITY) {
     for (int t = rp; t <= steps && t < p->T; ++t) {
       if (t % tp > rp) {

@@ -36,7 +36,7 @@ class _OrcMS(ctypes.Structure):
         ("act_hidden", ctypes.c_int), ("act_out", ctypes.c_int),
         ("run_period", ctypes.c_int), ("turn_period", ctypes.c_int),
         ("jump_period", ctypes.c_int), ("robot_id", ctypes.c_int),
-        ("loss_mask", ctypes.c_int), ("n_threads", ctypes.c_int),
+        ("loss_mask", ctypes.c_int), ("n_threads", ctypes.c_int), ("loss_envs", ctypes.c_int),
         ("dt", ctypes.c_double), ("gravity", ctypes.c_double), ("ground", ctypes.c_double),
         ("drag", ctypes.c_double), ("dashpot", ctypes.c_double), ("friction", ctypes.c_double),
         ("spring_omega", ctypes.c_double), ("max_speed", ctypes.c_double),
@@ -102,7 +102,7 @@ class MassSpringOracle:
                  run_period, turn_period, jump_period, robot_id=-1, friction=0.4,
                  act_hidden="sin", act_out="sin", out_index=None, n_out=None,
                  loss=("velocity", "rotation"), max_speed=0.1, max_height=0.1,
-                 stiffness_div=10.0, n_threads=0, initial_objects=None):
+                 stiffness_div=10.0, n_threads=0, initial_objects=None, loss_envs=0):
         objects = np.asarray(objects, dtype=np.float64).reshape(-1, 3)
         springs = np.asarray(springs, dtype=np.float64).reshape(-1, 5)
         N, S = objects.shape[0], springs.shape[0]
@@ -156,6 +156,7 @@ class MassSpringOracle:
         s.robot_id = robot_id
         s.loss_mask = sum(LOSS_BITS[n] for n in loss)
         s.n_threads = n_threads
+        s.loss_envs = loss_envs
         s.dt, s.gravity, s.ground, s.drag, s.dashpot = dt, gravity, ground, drag, dashpot
         s.friction, s.spring_omega = friction, spring_omega
         s.max_speed, s.max_height = max_speed, max_height

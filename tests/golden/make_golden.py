@@ -174,6 +174,89 @@ def robot_geometry(ref_root):
         out["faces_%d" % rid] = np.array(faces, dtype=np.int64)
         out["stiffness_%d" % rid] = np.float64(builder.spring_stiffness)
         out["actuation_%d" % rid] = np.float64(builder.spring_actuation)
+    # the spider's node / link table (cfg3d/skeleton.json), so that the tests
+    # can rebuild robot 103 without the reference tree
+    with open("cfg3d/skeleton.json") as f:
+        sk = json.load(f)
+    keys = list(sk["nodes"])
+    out["skeleton_node_keys"] = np.array(keys)
+    out["skeleton_nodes"] = np.array([sk["nodes"][k] for k in keys], dtype=np.float64)
+    out["skeleton_links"] = np.array(sk["links"], dtype=np.int64)
+    return out
+
+
+def _jsonable(v):
+    if isinstance(v, (set, frozenset)):
+        return sorted(v)
+    if isinstance(v, (list, tuple)):
+        return [_jsonable(x) for x in v]
+    if isinstance(v, dict):
+        return {k: _jsonable(x) for k, x in v.items()}
+    if isinstance(v, np.generic):
+        return v.item()
+    return v
+
+
+def simulate_trace(ti_shim):
+    """The calls that the reference's own DiffPhyTrainer.simulate
+    (multitask/diffphy_trainer.py:219-268) makes on its env, solver and model,
+    recorded by running that method unchanged on recording stand-ins, for the
+    golden cases quad_ref (training rollout) and snake_eval (evaluation
+    rollout).  Entries are [object, method, args, kwargs]; ``tape`` marks the
+    ti.ad.Tape context.  The drop-in objects replay this trace on the GPU."""
+    from multitask.diffphy_trainer import DiffPhyTrainer
+    calls = []
+
+    class Scalar:
+        def __init__(self, name):
+            self.name = name
+
+        def __setitem__(self, key, value):
+            calls.append([self.name, "__setitem__", [key, _jsonable(value)], {}])
+
+    class Obj:
+        def __init__(self, name, **attrs):
+            self._name = name
+            self.__dict__.update(attrs)
+
+        def __getattr__(self, attr):
+            if attr.startswith("__"):
+                raise AttributeError(attr)
+            return lambda *a, **k: calls.append([self._name, attr, _jsonable(list(a)), _jsonable(k)])
+
+    class Tape:
+        def __init__(self, loss):
+            calls.append(["tape", "__enter__", [loss.name], {}])
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            calls.append(["tape", "__exit__", [], {}])
+            return False
+
+    losses = [Scalar("env.losses[%d]" % i) for i in range(7)]
+    env = Obj("env", solver=Obj("solver"), loss=Scalar("env.loss"), losses=losses, dim=3)
+    out = {}
+    saved = ti_shim.ad.Tape
+    ti_shim.ad.Tape = Tape
+    try:
+        for name in ("quad_ref", "snake_eval"):
+            spec = CASES[name]
+            path = "cfg3d/{}.json".format(spec["cfg"])
+            with open(path) as f:
+                raw = json.load(f)
+            deep_update(raw, copy.deepcopy(spec["over"]))
+            pr = raw["process"]
+            fake = types.SimpleNamespace(taichi_env=env, nn=Obj("nn"),
+                                         control_length=raw["robot"]["control_length"])
+            del calls[:]
+            DiffPhyTrainer.simulate(fake, spec["steps"], iter=0, train=spec["train"],
+                                    max_height=pr["max_height"], max_speed=pr["max_speed"],
+                                    loss_enable=spec["loss"])
+            out[name] = dict(steps=spec["steps"], train=spec["train"], calls=list(calls))
+    finally:
+        ti_shim.ad.Tape = saved
     return out
 
 
@@ -223,10 +306,17 @@ def run_mpm_case(steps=24, B=2, seed=21):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("CLS_REFERENCE_ROOT"),
+                    help="root of the reference checkout (default: $CLS_REFERENCE_ROOT)")
     ap.add_argument("--cases", nargs="*", default=sorted(CASES))
+    ap.add_argument("--only-robots", action="store_true",
+                    help="regenerate robots.npz only")
+    ap.add_argument("--only-trace", action="store_true",
+                    help="regenerate simulate_trace.json only")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("--reference (or CLS_REFERENCE_ROOT) is required")
     ti_shim = install_shims()
     ref_root = os.path.abspath(a.reference)
     sys.path.insert(0, ref_root)
@@ -234,12 +324,22 @@ def main():
     out_dir = os.path.abspath(a.out)
     os.chdir(ref_root)  # the reference opens cfg3d/*.json relative to its root
     try:
+        if a.only_robots:
+            geo = robot_geometry(ref_root)
+            np.savez_compressed(os.path.join(out_dir, "robots.npz"), **geo)
+            return
+        if a.only_trace:
+            with open(os.path.join(out_dir, "simulate_trace.json"), "w") as f:
+                json.dump(simulate_trace(ti_shim), f, indent=0)
+            return
         mpm = run_mpm_case()
         np.savez_compressed(os.path.join(out_dir, "mpm2d_ref.npz"), **mpm)
         print("mpm2d_ref x", mpm["x"].shape)
         geo = robot_geometry(ref_root)
         np.savez_compressed(os.path.join(out_dir, "robots.npz"), **geo)
         print("robots", sorted(k for k in geo if k.startswith("objects")))
+        with open(os.path.join(out_dir, "simulate_trace.json"), "w") as f:
+            json.dump(simulate_trace(ti_shim), f, indent=0)
         for name in a.cases:
             data = run_case(name, CASES[name], ref_root, ti_shim)
             np.savez_compressed(os.path.join(out_dir, name + ".npz"), **data)

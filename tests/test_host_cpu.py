@@ -1,5 +1,6 @@
 """Host logic without a GPU: robot builders against the reference builder's
 output, synthetic workload shapes, config schema handling."""
+import json
 import os
 
 import numpy as np
@@ -7,32 +8,41 @@ import pytest
 
 from helpers import GOLDEN
 
-REF_SKELETON = "/root/reference/cfg3d/skeleton.json"
-
 
 def _geo():
     g = np.load(os.path.join(GOLDEN, "robots.npz"))
     return {k: g[k] for k in g.files}
 
 
+def skeleton_file(g, tmp_path):
+    """The spider's node / link table (the reference's cfg3d/skeleton.json,
+    kept in robots.npz by make_golden.py) written back as a JSON file."""
+    path = os.path.join(str(tmp_path), "skeleton.json")
+    nodes = {str(k): [float(c) for c in xyz] for k, xyz in zip(g["skeleton_node_keys"], g["skeleton_nodes"])}
+    with open(path, "w") as f:
+        json.dump({"nodes": nodes, "links": g["skeleton_links"].tolist()}, f)
+    return path
+
+
 @pytest.mark.parametrize("rid", [100, 101, 102, 104])
 def test_cube_robots_match_reference_builder(rid):
     from cls_b200 import robot_design
     g = _geo()
-    obj, spr = robot_design.reference_robot(rid, float(g["stiffness_%d" % rid]),
-                                            float(g["actuation_%d" % rid]))
+    obj, spr, faces = robot_design.reference_robot(rid, float(g["stiffness_%d" % rid]),
+                                                   float(g["actuation_%d" % rid]), faces=True)
     np.testing.assert_array_equal(obj, g["objects_%d" % rid])
     np.testing.assert_array_equal(spr, g["springs_%d" % rid])
+    np.testing.assert_array_equal(faces, g["faces_%d" % rid])
 
 
-@pytest.mark.skipif(not os.path.exists(REF_SKELETON), reason="reference skeleton.json not present")
-def test_spider_matches_reference_builder():
+def test_spider_matches_reference_builder(tmp_path):
     from cls_b200 import robot_design
     g = _geo()
-    obj, spr = robot_design.reference_robot(103, float(g["stiffness_103"]),
-                                            float(g["actuation_103"]), skeleton=REF_SKELETON)
+    obj, spr, faces = robot_design.reference_robot(103, float(g["stiffness_103"]), float(g["actuation_103"]),
+                                                   skeleton=skeleton_file(g, tmp_path), faces=True)
     np.testing.assert_array_equal(obj, g["objects_103"])
     np.testing.assert_array_equal(spr, g["springs_103"])
+    np.testing.assert_array_equal(faces, g["faces_103"])
 
 
 def test_reference_robot_counts():

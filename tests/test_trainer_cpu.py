@@ -79,3 +79,26 @@ def test_reference_pickle_layout_roundtrip():
         assert np.array_equal(W, W2) and np.array_equal(b, b2)
     with pytest.raises(ValueError):
         to_reference_list(layers + layers)
+
+
+def test_obj_frames_format(tmp_path):
+    """write_obj_frames: every stride-th state, 6-decimal vertex lines, then
+    1-based triangles (the evaluation visualiser's mesh files)."""
+    from cls_b200.trainer import write_obj_frames
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-1, 1, (25, 4, 3))
+    faces = np.array([[0, 1, 2], [3, 0, 2]])
+    paths = write_obj_frames(x, faces, str(tmp_path / "mesh"), stride=10)
+    assert [p.rsplit("/", 1)[1] for p in paths] == ["000000.obj", "000001.obj", "000002.obj"]
+    lines = open(paths[1]).read().splitlines()
+    assert lines[:4] == ["v %.6f %.6f %.6f" % tuple(p) for p in x[10]]
+    assert lines[4:] == ["f 1 2 3", "f 4 1 3"]
+
+
+def test_load_config_keeps_the_builder_faces():
+    from cls_b200.trainer import load_config
+    g = load_golden("quad_ref")
+    cfg = load_config(golden_config(g), seed=0)
+    faces = np.asarray(cfg["robot"]["faces"])
+    geo = np.load(__import__("os").path.join(__import__("helpers").GOLDEN, "robots.npz"))
+    np.testing.assert_array_equal(faces, geo["faces_%d" % int(g["robot_id"])])

@@ -92,3 +92,28 @@ def test_train_writes_reference_pickles_and_evaluates(tmp_path):
         assert np.isfinite(terms["total"])
     finally:
         ev.close()
+
+
+def test_evaluate_exports_obj_frames_of_the_rollout(tmp_path):
+    """evaluate(mesh_dir=...) writes every 10th state of each env's scripted
+    rollout as OBJ frames; the vertices are the rollout's own trajectory."""
+    from cls_b200.trainer import DiffPhyTrainer, load_config
+    g = load_golden("quad_ref")
+    cfg = load_config(golden_config(g), seed=1)
+    ev = DiffPhyTrainer(cfg, precision=64, checkpoint_every=8, batch_size=2, evaluate=True,
+                        keep_trajectory=True)
+    try:
+        ev.set_weights([(g["W1"], g["b1"]), (g["W2"], g["b2"])])
+        ev.evaluate(steps=45, mesh_dir=str(tmp_path / "video"))
+        traj = ev.batch.trajectory()
+        for k in range(2):
+            files = sorted(os.listdir(tmp_path / "video" / str(k)))
+            assert len(files) == len(traj[::10])
+            xk = traj[:, ev.batch.env_slice(k)]
+            lines = open(tmp_path / "video" / str(k) / files[3]).read().splitlines()
+            v = np.array([[float(c) for c in ln.split()[1:]] for ln in lines if ln.startswith("v ")])
+            np.testing.assert_allclose(v, xk[30], atol=5e-7)
+            f = [ln for ln in lines if ln.startswith("f ")]
+            assert len(f) == len(ev.faces)
+    finally:
+        ev.close()
