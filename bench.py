@@ -139,9 +139,12 @@ def config_dict(a, n_gpus):
                 "parallelism": par,
                 "l2": "inputs larger than L2 (controller weights ~0.8 GB per GPU)"}
     if a.config in ("quadruped", "spider"):
-        shape = ("quadruped lattice (54 vertices, 323 springs, 40 actuated), MLP 1x64 tanh"
-                 if a.config == "quadruped" else
-                 "spider lattice (136 vertices, 732 springs, 96 actuated), MLP 2x256 tanh")
+        from cls_b200 import robot_design
+        obj, spr = (robot_design.quadruped_lattice() if a.config == "quadruped" else
+                    robot_design.spider_lattice())
+        shape = "%s lattice (%d vertices, %d springs, %d actuated), MLP %s tanh" % (
+            a.config, obj.shape[0], spr.shape[0], int((spr[:, 4] > 0).sum()),
+            "1x64" if a.config == "quadruped" else "2x256")
         return {"workload": "%d envs of the %s x %d substeps, checkpoint every %d, "
                             "velocity+rotation loss, Adam" % (a.robots, shape, a.substeps, a.checkpoint),
                 "envs_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,

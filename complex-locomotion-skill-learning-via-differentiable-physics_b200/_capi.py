@@ -16,7 +16,7 @@ MAX_HIDDEN = 4
 
 CLS_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
-          -4: "non-finite state", -5: "call out of order"}
+          -4: "non-finite state", -5: "call out of order", -6: "bounded wait timed out"}
 
 ACT = {"sin": 0, "tanh": 1}
 LOSS_BITS = {"velocity": 1, "height": 2, "pose": 4, "actuation": 8,
@@ -57,7 +57,11 @@ class LaunchShape(ctypes.Structure):
 
 
 class ClsError(RuntimeError):
-    pass
+    """A failed C-ABI call; ``code`` is the CLS_ERR_* value."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 _lib = None
@@ -89,6 +93,7 @@ _SIGS = {
     "cls_get_targets": (c_int32, [ctypes.c_void_p, P_D, P_D, P_D]),
     "cls_set_loss_mask": (c_int32, [ctypes.c_void_p, c_int32]),
     "cls_set_loss_envs": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
+    "cls_debug_gemm_starve": (c_int32, [ctypes.c_void_p, c_int32, ctypes.c_uint32]),
     "cls_grad_buffers": (c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64), P_I]),
     "cls_get_final_state": (c_int32, [ctypes.c_void_p, P_D, P_D]),
@@ -148,7 +153,7 @@ def check(rc, handle=None):
         lib = load()
         msg = lib.cls_last_error(handle)
         msg = msg.decode() if msg else ""
-        raise ClsError("%s (%d): %s" % (ERRORS.get(rc, "error"), rc, msg))
+        raise ClsError("%s (%d): %s" % (ERRORS.get(rc, "error"), rc, msg), rc)
 
 
 def ptr(a, kind=P_D):

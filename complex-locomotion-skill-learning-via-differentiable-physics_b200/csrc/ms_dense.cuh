@@ -357,7 +357,7 @@ ms_ctrl_gemm_tc_kernel(MsArgs<float> a, const DenseJob* jobs, int kslot) {
           if (j + u < n_valid) dp[u] = vv[u];
       }
     }
-  });
+  }, umma::WaitPolicy{a.gemm_wait_limit, a.gemm_starve});
   if (!ok && threadIdx.x == 0) atomicOr(a.status, ERR_TIMEOUT);
   if (threadIdx.x < 32) umma::tmem_relinquish();
 }
@@ -463,7 +463,7 @@ ms_wgrad_tc_kernel(MsArgs<float> a, const WgJob* jobs, int nslots, float* gw, fl
           if (c < nin) atomicAdd(W + (size_t)o * pitch + c, v);
           else atomicAdd(B + o, v);
         }
-      });
+      }, umma::WaitPolicy{a.gemm_wait_limit, a.gemm_starve});
   if (!ok && threadIdx.x == 0) atomicOr(a.status, ERR_TIMEOUT);
   if (threadIdx.x < 32) umma::tmem_relinquish();
 }

@@ -175,6 +175,10 @@ struct MsArgs {
   const DenseDesc* dense;            // per robot type
   // status
   int* status;
+  // tensor-core tiles: poll limit of their waits (0: default) and the
+  // bounded-wait self-test (cls_debug_gemm_starve)
+  unsigned gemm_wait_limit;
+  int gemm_starve;
   // per-phase clock totals, only written by builds with CLS_PHASE_TIMERS
   unsigned long long* phase;
 };

@@ -154,6 +154,7 @@ class SimBase {
   virtual void targets(double* tv, double* th, double* tc) = 0;
   virtual void set_loss_mask(int mask) = 0;
   virtual void set_loss_envs(int r, int n) = 0;
+  virtual void debug_gemm_starve(int starve, unsigned wait_limit) = 0;
   virtual void grad_buffers(void** w, long long* nw, void** b, long long* nb, int* elem) = 0;
   virtual void final_state(double* x, double* v) = 0;
   virtual void state_grads(double* gx, double* gv) = 0;
@@ -867,6 +868,8 @@ class SimImpl final : public SimBase {
     a.adj_v = d_adjv_.p;
     a.adj_h = d_adjh_.p;
     a.status = d_status_.p;
+    a.gemm_wait_limit = gemm_wait_limit_;
+    a.gemm_starve = gemm_starve_;
     a.phase = d_phase_.p;
     a.live_x = d_livex_.p;
     a.live_v = d_livev_.p;
@@ -1524,6 +1527,12 @@ class SimImpl final : public SimBase {
     *elem = (int)sizeof(R);
   }
 
+  void debug_gemm_starve(int starve, unsigned wait_limit) override {
+    CLS_REQUIRE(!capturing_, "not during graph capture");
+    gemm_starve_ = starve ? 1 : 0;
+    gemm_wait_limit_ = wait_limit;
+  }
+
   void set_loss_envs(int r, int n) override {
     CLS_REQUIRE(r >= 0 && r < (int)rd_host_.size(), "robot index out of range");
     CLS_REQUIRE(n >= rd_host_[r].n_env && n > 0,
@@ -1804,13 +1813,18 @@ class SimImpl final : public SimBase {
     CLS_CUDA(cudaMemcpy(&st, d_status_.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (st) {
       CLS_CUDA(cudaMemset(d_status_.p, 0, sizeof(int)));
+      // a timeout first: the results after it are invalid anyway
+      if (st & ERR_TIMEOUT) {
+        err = (st & ERR_NONFINITE)
+                  ? "a tensor-core GEMM tile's bounded wait for its operands or MMAs ran out (the tile "
+                    "freed its tensor memory and skipped its epilogue); non-finite state was seen too"
+                  : "a tensor-core GEMM tile's bounded wait for its operands or MMAs ran out; the tile "
+                    "freed its tensor memory and skipped its epilogue";
+        return CLS_ERR_TIMEOUT;
+      }
       if (st & ERR_NONFINITE) {
         err = "non-finite state detected";
         return CLS_ERR_NONFINITE;
-      }
-      if (st & ERR_TIMEOUT) {
-        err = "a tensor-core GEMM's wait for its MMAs timed out";
-        return CLS_ERR_CUDA;
       }
     }
     return CLS_OK;
@@ -1893,6 +1907,8 @@ class SimImpl final : public SimBase {
   std::vector<std::vector<long long>> m_off_;
   bool keep_x_ = false, fwd_done_ = false, bwd_done_ = false, eval_ = false, per_env_ = false;
   bool graph_adam_ = false, capturing_ = false;
+  unsigned gemm_wait_limit_ = 0;
+  int gemm_starve_ = 0;
   Profiler prof_;
   int steps_ = 0, qslot_ = 0, iter_host_ = 0;
   double max_height_ = 0;
@@ -2214,6 +2230,10 @@ int cls_grad_buffers(cls_sim* sim, void** weight_grads, int64_t* n_weight, void*
     *n_bias = nb;
     *elem_bytes = e;
   });
+}
+
+int cls_debug_gemm_starve(cls_sim* sim, int32_t starve, uint32_t wait_limit) {
+  return guarded(sim, [&](cls::SimBase& s) { s.debug_gemm_starve(starve, wait_limit); });
 }
 
 int cls_set_loss_envs(cls_sim* sim, int32_t robot, int32_t n_envs) {

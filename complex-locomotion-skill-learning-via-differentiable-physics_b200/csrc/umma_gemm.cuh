@@ -92,12 +92,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
   return ok != 0;
 }
 
-// bounded wait for the phase; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (unsigned it = 0; it < kWaitLimit; ++it)
+// bounded wait for the phase (at most `limit` polls); false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, unsigned limit = kWaitLimit) {
+  for (unsigned it = 0; it < limit; ++it)
     if (mbar_try_wait(mbar, phase)) return true;
   return false;
 }
+
+// Wait policy of a tile: the poll limit of every wait (0: kWaitLimit) and the
+// self-test mode `starve`, in which the producer issues no bulk copies and
+// the MMA issuer no MMAs, so the issuer's first wait for operands runs out
+// with nothing in flight and the tile takes its timeout path (status bit,
+// tensor memory freed, no epilogue).
+struct WaitPolicy {
+  unsigned limit;
+  int starve;
+};
 
 __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -241,8 +251,9 @@ struct BulkShared {
 // kBulkThreads threads.  Returns false on a timeout (epi is not called then).
 template <int TN, int S, typename Epi>
 __device__ bool tile_gemm_bulk(float* smem, BulkShared& bs, const float* a_blocks, const float* b_blocks,
-                               int nkt, Epi epi) {
+                               int nkt, Epi epi, WaitPolicy wp = WaitPolicy{0u, 0}) {
   using Sh = BulkShape<TN, S>;
+  const unsigned lim = wp.limit ? wp.limit : kWaitLimit;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t full0 = smem_u32(&bs.full[0]), empty0 = smem_u32(&bs.empty[0]), done = smem_u32(&bs.done);
   const uint32_t ring = smem_u32(smem);
@@ -261,11 +272,11 @@ __device__ bool tile_gemm_bulk(float* smem, BulkShared& bs, const float* a_block
   tc_fence_after();
   const uint32_t tmem = bs.tmem_base;
   constexpr uint32_t idesc = instr_desc_tf32(TM, TN);
-  if (tid == 0) {
+  if (tid == 0 && !wp.starve) {
     // producer: two bulk copies per stage
     for (int kt = 0; kt < nkt; ++kt) {
       const int s = kt % S;
-      if (kt >= S && !mbar_wait(empty0 + 8 * s, ((kt / S) - 1) & 1)) { bs.timed_out = 1; break; }
+      if (kt >= S && !mbar_wait(empty0 + 8 * s, ((kt / S) - 1) & 1, lim)) { bs.timed_out = 1; break; }
       const uint32_t st = ring + (uint32_t)s * Sh::kStageBytes;
       mbar_arrive_expect_tx(full0 + 8 * s, Sh::kStageBytes);
       bulk_g2s(st, a_blocks + (size_t)kt * (2 * TK * TM), Sh::kABytes, full0 + 8 * s);
@@ -275,7 +286,7 @@ __device__ bool tile_gemm_bulk(float* smem, BulkShared& bs, const float* a_block
     // MMA issuer
     for (int kt = 0; kt < nkt; ++kt) {
       const int s = kt % S;
-      if (!mbar_wait(full0 + 8 * s, (kt / S) & 1)) { bs.timed_out = 1; break; }
+      if (!mbar_wait(full0 + 8 * s, (kt / S) & 1, lim)) { bs.timed_out = 1; break; }
       tc_fence_after();
       const uint32_t a_hi = ring + (uint32_t)s * Sh::kStageBytes, a_lo = a_hi + TK * TM * 4;
       const uint32_t b_hi = a_hi + Sh::kABytes, b_lo = b_hi + TK * TN * 4;
@@ -295,7 +306,7 @@ __device__ bool tile_gemm_bulk(float* smem, BulkShared& bs, const float* a_block
     mma_commit(done);
   }
   __syncwarp();
-  if (nkt > 0 && !mbar_wait(done, 0)) bs.timed_out = 1;
+  if (nkt > 0 && !mbar_wait(done, 0, lim)) bs.timed_out = 1;
   tc_fence_after();
   __syncthreads();
   const bool ok = !bs.timed_out;  // the same for every thread after the barrier

@@ -44,10 +44,11 @@ _CORNER_ORDER = "abcdefgh"
 class CubeLattice:
     """Incremental cube-lattice builder with the reference's numbering rules."""
 
-    def __init__(self, stiffness, actuation, spacing=SPACING, origin=ORIGIN):
+    def __init__(self, stiffness, actuation, spacing=SPACING, origin=ORIGIN, spacing_y=None):
         self.stiffness = float(stiffness)
         self.actuation = float(actuation)
         self.spacing = spacing
+        self.spacing_y = spacing if spacing_y is None else spacing_y   # boxes of the refined lattices
         self.origin = origin
         self.objects = []
         self.springs = []
@@ -59,7 +60,7 @@ class CubeLattice:
         key = (i, j, k)
         if key not in self._point_id:
             self._point_id[key] = len(self.objects)
-            self.objects.append((i * self.spacing + self.origin, j * self.spacing + self.origin,
+            self.objects.append((i * self.spacing + self.origin, j * self.spacing_y + self.origin,
                                  k * self.spacing + self.origin))
         return self._point_id[key]
 
@@ -188,40 +189,52 @@ def reference_robot(robot_id, spring_stiffness, spring_actuation, skeleton=None,
 
 
 # ------------------------------------------------------ synthetic robots
-def quadruped_lattice(stiffness=3e4, actuation=0.25, n_actuated=40):
-    """Torso of 4 x 2 x 1 cubes on four 1 x 1 x 2 legs at its corners.  The
+def quadruped_lattice(stiffness=3e4, actuation=0.25, n_actuated=40, refine=2):
+    """Torso of 4 x 2 x 1 cubes on four 1 x 1 x 2 legs at its corners.
+    ``refine`` splits every cube into that many boxes along the height
+    (``refine=2``: 93 vertices, 608 springs, the robot size of the plain
+    quadruped configuration; ``refine=1``: 54 vertices, 323 springs).  The
     reference's per-cube actuation pattern marks the leg springs; the first
     ``n_actuated`` of them (in creation order) keep their coefficient."""
-    L = CubeLattice(stiffness, actuation)
+    r = int(refine)
+    L = CubeLattice(stiffness, actuation, spacing_y=SPACING / r)
     for (i, k) in ((0, 0), (3, 0), (0, 1), (3, 1)):
-        for j in range(2):
+        for j in range(2 * r):
             L.cube(i, j, k, actuation=actuation)
     for i in range(4):
         for k in range(2):
-            L.cube(i, 2, k, actuation=0.0)
+            for j in range(2 * r, 3 * r):
+                L.cube(i, j, k, actuation=0.0)
     objects, springs = L.arrays()
     act = np.nonzero(springs[:, 4] > 0)[0]
     springs[act[n_actuated:], 4] = 0.0
     return objects, springs
 
 
-def spider_lattice(stiffness=3e4, actuation=0.2):
-    """A 3 x 3 x 1 torso (lattice layer y = 3) with eight 1 x 1 x 3 legs: vertical
+def spider_lattice(stiffness=3e4, actuation=0.2, refine=2):
+    """A 3 x 3 x 1 torso (cube layer 3) with eight 1 x 1 x 3 legs: vertical
     columns of three cubes beside it, one cell apart from each other, whose
-    top cubes sit in the torso layer.  The 4 vertical edges of every leg cube
-    are actuated (8 legs x 3 cubes x 4 = 96 actuators)."""
-    L = CubeLattice(stiffness, 0.0)
+    top cubes sit in the torso layer.  ``refine`` splits every cube into that
+    many boxes along the height (``refine=2``: 236 vertices, 1378 springs,
+    the robot size of the large-batch spider configuration; ``refine=1``:
+    136 vertices, 732 springs).  Four vertical edges of one box per leg cube
+    (the lowest box of each) are actuated: 8 legs x 3 cubes x 4 = 96
+    actuators."""
+    r = int(refine)
+    L = CubeLattice(stiffness, 0.0, spacing_y=SPACING / r)
     legs = [(-1, -1), (-1, 1), (-1, 3), (1, -1), (1, 3), (3, -1), (3, 1), (3, 3)]
     vertical = {("a", "b"), ("c", "d"), ("e", "f"), ("g", "h")}
     for (i, k) in legs:
-        for j in range(1, 4):
+        for j in range(r, 4 * r):
             ids = {c: L.point(i + _CORNER[c][0], j + _CORNER[c][1], k + _CORNER[c][2])
                    for c in _CORNER_ORDER}
+            act = actuation if (j - r) % r == 0 else 0.0
             for p, q, _ in _SQUARE:
-                L.spring(ids[p], ids[q], actuation if (p, q) in vertical else 0.0)
+                L.spring(ids[p], ids[q], act if (p, q) in vertical else 0.0)
     for i in range(3):
         for k in range(3):
-            L.cube(i, 3, k, actuation=0.0)
+            for j in range(3 * r, 4 * r):
+                L.cube(i, j, k, actuation=0.0)
     objects, springs = L.arrays()
     objects[:, 1] -= SPACING  # legs stand on the lattice origin height
     return objects, springs

@@ -34,6 +34,7 @@ extern "C" {
 #define CLS_ERR_OOM (-3)       /* device allocation failed */
 #define CLS_ERR_NONFINITE (-4) /* NaN/Inf detected in the simulated state */
 #define CLS_ERR_STATE (-5)     /* call out of order (e.g. backward before forward) */
+#define CLS_ERR_TIMEOUT (-6)   /* a kernel's bounded wait ran out (reported by cls_synchronize) */
 
 #define CLS_ACT_SIN 0
 #define CLS_ACT_TANH 1
@@ -207,8 +208,19 @@ int cls_get_final_state(cls_sim* sim, double* x, double* v);
 int cls_get_state_grads(cls_sim* sim, double* gx0, double* gv0);
 
 /* Waits for the handle's stream; returns CLS_ERR_NONFINITE if a kernel saw
- * NaN/Inf state since the last check. */
+ * NaN/Inf state, CLS_ERR_TIMEOUT if a tensor-core tile's bounded wait ran out,
+ * since the last check (then clears the status). */
 int cls_synchronize(cls_sim* sim);
+
+/* Self-test of the tensor-core tiles' bounded waits (batched controller path
+ * and weight-gradient tiles): with starve = 1 every tile issues no bulk
+ * copies and no MMAs, so its wait for operands runs out after wait_limit
+ * polls (0: the built-in limit) with nothing in flight; the tile then frees
+ * its tensor memory, skips its epilogue and sets the status that
+ * cls_synchronize reports as CLS_ERR_TIMEOUT.  Results are invalid while
+ * starved; starve = 0 restores normal operation.  No reference
+ * counterpart. */
+int cls_debug_gemm_starve(cls_sim* sim, int32_t starve, uint32_t wait_limit);
 
 /* Model.weights_init (multitask/nn.py:59-67) on the device:
  * W = (u * 2 - 1) * sqrt(6 / fan_in) with u from a counter-based generator

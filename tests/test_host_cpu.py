@@ -55,11 +55,19 @@ def test_reference_robot_counts():
 
 def test_synthetic_lattices():
     from cls_b200 import robot_design
+    # the configurations' robot sizes: quadruped ~90 vertices with 40
+    # actuated springs, spider ~250 vertices / ~1400 springs / 96 actuators
     obj, spr = robot_design.quadruped_lattice()
-    assert (spr[:, 4] > 0).sum() == 40
-    assert obj.shape[0] >= 50
+    assert (obj.shape[0], spr.shape[0], int((spr[:, 4] > 0).sum())) == (93, 608, 40)
     obj, spr = robot_design.spider_lattice()
-    assert (spr[:, 4] > 0).sum() == 96
+    assert (obj.shape[0], spr.shape[0], int((spr[:, 4] > 0).sum())) == (236, 1378, 96)
+    obj, spr = robot_design.spider_lattice(refine=1)
+    assert (obj.shape[0], spr.shape[0], int((spr[:, 4] > 0).sum())) == (136, 732, 96)
+    for build in (robot_design.quadruped_lattice, robot_design.spider_lattice):
+        obj, spr = build()
+        a, b = spr[:, 0].astype(int), spr[:, 1].astype(int)
+        np.testing.assert_allclose(spr[:, 2], np.linalg.norm(obj[a] - obj[b], axis=1), rtol=1e-12)
+        assert abs(obj[:, 1].min() - 0.1) < 1e-12
     rng = np.random.default_rng(0)
     for n in (50, 300, 2000):
         obj, spr = robot_design.random_lattice(rng, n)

@@ -102,3 +102,34 @@ def test_load_config_keeps_the_builder_faces():
     faces = np.asarray(cfg["robot"]["faces"])
     geo = np.load(__import__("os").path.join(__import__("helpers").GOLDEN, "robots.npz"))
     np.testing.assert_array_equal(faces, geo["faces_%d" % int(g["robot_id"])])
+
+
+def test_malformed_configs_are_rejected_on_the_host(tmp_path):
+    """A cfg3d file that is not JSON, lacks a required key, names an unknown
+    robot or an unknown loss, or asks for the MPM simulator of the trainer,
+    fails in load_config / the trainer's constructor with an exception, before
+    any device work."""
+    import json
+    from cls_b200.trainer import load_config
+    g = load_golden("quad_ref")
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"robot": {"robot_id": 100,')
+    with pytest.raises(json.JSONDecodeError):
+        load_config(str(bad))
+    cfg = golden_config(g)
+    del cfg["nn"]["n_sin_waves"]
+    with pytest.raises(KeyError):
+        load_config(cfg)
+    cfg = golden_config(g)
+    cfg["robot"]["robot_id"] = 117
+    with pytest.raises(ValueError, match="invalid robot id"):
+        load_config(cfg)
+    cfg = golden_config(g)
+    cfg["robot"]["simulator"] = "mpm"
+    with pytest.raises(NotImplementedError):
+        load_config(cfg)
+    from cls_b200.dropin import TaichiEnvCUDA
+    cfg = load_config(golden_config(g), seed=0)
+    cfg["train"]["task"] = ["velocity", "flying"]
+    with pytest.raises(ValueError, match="unknown loss"):
+        TaichiEnvCUDA(cfg, batch=object())
