@@ -94,6 +94,8 @@ _SIGS = {
     "cls_set_loss_mask": (c_int32, [ctypes.c_void_p, c_int32]),
     "cls_set_loss_envs": (c_int32, [ctypes.c_void_p, c_int32, c_int32]),
     "cls_debug_gemm_starve": (c_int32, [ctypes.c_void_p, c_int32, ctypes.c_uint32]),
+    "cls_env_step": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D, P_D]),
+    "cls_serve_set_targets": (c_int32, [ctypes.c_void_p, c_int32, c_int32, P_D, P_D, P_D]),
     "cls_grad_buffers": (c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64), P_I]),
     "cls_get_final_state": (c_int32, [ctypes.c_void_p, P_D, P_D]),

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libcls_b200.so")
-SOURCES = ["ms_runtime.cu", "ms_dense.cu", "mpm_runtime.cu", "noalloc.cu"]
+SOURCES = ["ms_runtime.cu", "ms_dense.cu", "ms_env.cu", "mpm_runtime.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 OBJ_DIR = os.path.join(HERE, "_build")

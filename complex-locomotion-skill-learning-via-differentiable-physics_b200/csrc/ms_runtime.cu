@@ -15,6 +15,7 @@
 #include "../../include/cls_b200.h"
 #include "cls_profile.cuh"
 #include "ms_dense_host.h"
+#include "ms_env_host.h"
 #include "ms_segment.cuh"
 
 // threads of the batched controller's step kernels (one CTA per env)
@@ -155,6 +156,8 @@ class SimBase {
   virtual void set_loss_mask(int mask) = 0;
   virtual void set_loss_envs(int r, int n) = 0;
   virtual void debug_gemm_starve(int starve, unsigned wait_limit) = 0;
+  virtual void env_step(int t, const double* outputs, double* obs, double* aux) = 0;
+  virtual void env_set_targets(int ue, int t_from, const double* tv, const double* th, const double* tc) = 0;
   virtual void grad_buffers(void** w, long long* nw, void** b, long long* nb, int* elem) = 0;
   virtual void final_state(double* x, double* v) = 0;
   virtual void state_grads(double* gx, double* gv) = 0;
@@ -1527,6 +1530,81 @@ class SimImpl final : public SimBase {
     *elem = (int)sizeof(R);
   }
 
+  // One substep of every env with outputs from the caller (external policy),
+  // or (outputs == null, t == 0) the observation of the state set by
+  // set_state.  outputs [E][omax] and obs [E][imax] in user env order, aux
+  // [E][4] (centre, height of t).
+  void env_step(int t, const double* outputs, double* obs, double* aux) override {
+    CLS_REQUIRE(!capturing_, "not during graph capture");
+    CLS_REQUIRE(t >= 0 && t < T_, "t out of range");
+    CLS_REQUIRE(outputs != nullptr || t == 0, "without outputs only t = 0 (the initial observation)");
+    CLS_REQUIRE(outputs == nullptr || t >= 1, "a step produces t >= 1");
+    int omax = 1, imax = 1;
+    for (const HostRobot& h : hr_) {
+      omax = std::max(omax, h.width[h.n_layers]);
+      imax = std::max(imax, h.full_cols[0]);
+    }
+    if (!d_livex_.p) { d_livex_.alloc(V_); d_livev_.alloc(V_); }
+    if (d_envout_.n < (size_t)E_ * omax) d_envout_.alloc((size_t)E_ * omax);
+    if (d_envobs_.n < (size_t)E_ * imax) d_envobs_.alloc((size_t)E_ * imax);
+    if (d_envaux_.n < (size_t)E_ * 4) d_envaux_.alloc((size_t)E_ * 4);
+    if (outputs) {
+      std::vector<R> o((size_t)E_ * omax, R(0));
+      for (int ie = 0; ie < E_; ++ie) {
+        const int ue = perm_[ie], no = hr_[ed_host_[ie].robot].width[hr_[ed_host_[ie].robot].n_layers];
+        for (int q = 0; q < no; ++q) o[(size_t)ie * omax + q] = (R)outputs[(size_t)ue * omax + q];
+      }
+      CLS_CUDA(cudaMemcpyAsync(d_envout_.p, o.data(), sizeof(R) * o.size(), cudaMemcpyHostToDevice, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    MsArgs<R> a = args(T_);
+    a.w_smem = 0;
+    a.b_smem = 0;
+    a.live_x = d_livex_.p;
+    a.live_v = d_livev_.p;
+    const size_t smem = fwd_smem_bytes<R>(nmax_, smem_dmax_, smem_p0max_, imp_cap_);
+    CLS_CUDA(EnvLaunch<R>::step(a, smem, stream, t, outputs ? 0 : 1, outputs ? d_envout_.p : nullptr, omax,
+                                d_envobs_.p, imax, d_envaux_.p));
+    std::vector<R> ob((size_t)E_ * imax), ax((size_t)E_ * 4);
+    CLS_CUDA(cudaMemcpyAsync(ob.data(), d_envobs_.p, sizeof(R) * ob.size(), cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaMemcpyAsync(ax.data(), d_envaux_.p, sizeof(R) * ax.size(), cudaMemcpyDeviceToHost, stream));
+    CLS_CUDA(cudaStreamSynchronize(stream));
+    for (int ie = 0; ie < E_; ++ie) {
+      const int ue = perm_[ie];
+      if (obs)
+        for (int q = 0; q < imax; ++q) obs[(size_t)ue * imax + q] = (double)ob[(size_t)ie * imax + q];
+      if (aux)
+        for (int q = 0; q < 4; ++q) aux[(size_t)ue * 4 + q] = (double)ax[(size_t)ie * 4 + q];
+    }
+    fwd_done_ = bwd_done_ = false;
+  }
+
+  // targets of one env for t in [t_from, T), other times and envs untouched
+  void env_set_targets(int ue, int t_from, const double* tv, const double* th, const double* tc) override {
+    const int ie = ienv(ue);
+    CLS_REQUIRE(t_from >= 0 && t_from < T_, "t_from out of range");
+    const int n = T_ - t_from;
+    if (tv) {
+      std::vector<V4<R>> v(n);
+      for (int t = 0; t < n; ++t) {
+        v[t].x = (R)tv[3 * t]; v[t].y = (R)tv[3 * t + 1]; v[t].z = (R)tv[3 * t + 2]; v[t].w = 0;
+      }
+      CLS_CUDA(cudaMemcpy2DAsync(d_tv_.p + (size_t)t_from * E_ + ie, sizeof(V4<R>) * E_, v.data(), sizeof(V4<R>),
+                                 sizeof(V4<R>), n, cudaMemcpyHostToDevice, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+    const double* src[2] = {th, tc};
+    R* dst[2] = {d_th_.p, d_tc_.p};
+    for (int q = 0; q < 2; ++q) {
+      if (!src[q]) continue;
+      std::vector<R> v(n);
+      for (int t = 0; t < n; ++t) v[t] = (R)src[q][t];
+      CLS_CUDA(cudaMemcpy2DAsync(dst[q] + (size_t)t_from * E_ + ie, sizeof(R) * E_, v.data(), sizeof(R), sizeof(R),
+                                 n, cudaMemcpyHostToDevice, stream));
+      CLS_CUDA(cudaStreamSynchronize(stream));
+    }
+  }
+
   void debug_gemm_starve(int starve, unsigned wait_limit) override {
     CLS_REQUIRE(!capturing_, "not during graph capture");
     gemm_starve_ = starve ? 1 : 0;
@@ -1939,6 +2017,7 @@ class SimImpl final : public SimBase {
   DevBuf<DenseJob> d_jobs_;
   DevBuf<TransSeg> d_tsegs_;
   DevBuf<V4<R>> d_livex_, d_livev_;
+  DevBuf<R> d_envout_, d_envobs_, d_envaux_;
   DevBuf<R> d_din_, d_wt_, d_split_;
   std::vector<DenseDesc> dd_host_;
   DevBuf<DenseDesc> d_dense_;
@@ -2230,6 +2309,15 @@ int cls_grad_buffers(cls_sim* sim, void** weight_grads, int64_t* n_weight, void*
     *n_bias = nb;
     *elem_bytes = e;
   });
+}
+
+int cls_env_step(cls_sim* sim, int32_t t, const double* outputs, double* observation, double* center_height) {
+  return guarded(sim, [&](cls::SimBase& s) { s.env_step(t, outputs, observation, center_height); });
+}
+
+int cls_serve_set_targets(cls_sim* sim, int32_t env, int32_t t_from, const double* tv, const double* th,
+                          const double* tc) {
+  return guarded(sim, [&](cls::SimBase& s) { s.env_set_targets(env, t_from, tv, th, tc); });
 }
 
 int cls_debug_gemm_starve(cls_sim* sim, int32_t starve, uint32_t wait_limit) {

@@ -359,6 +359,28 @@ int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* loss_env);
 /* State at the end of the env's last forward window, [n_v][3] each. */
 int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v);
 
+/* Targets of one env for t in [t_from, max_steps) (rows tv [T - t_from][3],
+ * th, tc [T - t_from]; NULL leaves that field), other times and envs
+ * untouched: an interactive client changing its goal while its episode runs
+ * (TaichiEnv.initialize_interactive, multitask/taichi_env.py:333-338, as
+ * interactive_3d.py:13-28 calls it on key presses). */
+int cls_serve_set_targets(cls_sim* sim, int32_t env, int32_t t_from, const double* tv, const double* th,
+                          const double* tc);
+
+/* One substep of every env with controller outputs chosen by the caller (an
+ * external policy in place of the embedded controller): MassSpringEnv.step
+ * (multitask/mass_spring_env.py:55-93) -- pass_actuation, apply_spring_force
+ * and advance_toi of substep t - 1, then compute_center, compute_height and
+ * nn_input of t.  outputs: [n_envs][omax] (omax = the largest robot's output
+ * count; a robot without an output map has one output per spring, as the
+ * reference's actuation field); NULL with t = 0 observes the state set by
+ * cls_set_state (MassSpringEnv.reset, :207-224).  observation: [n_envs][imax]
+ * rows in the reference's input layout (imax = the largest n_input_states);
+ * center_height: [n_envs][4] = centre and height of t.  The state stays on
+ * the device between calls; the observables of t are kept as a rollout's
+ * (cls_get_observables).  No reference counterpart as a C function. */
+int cls_env_step(cls_sim* sim, int32_t t, const double* outputs, double* observation, double* center_height);
+
 /* ---------------------------------------------------------------------------
  * Differentiable MLS-MPM (multitask/solver_mpm.py).  The reference's solver is
  * 2D (fixed-corotated, actuation along y) and unreachable from its env

@@ -135,3 +135,24 @@ def test_model_shape_and_pickle_layout(tmp_path):
         from cls_b200.dropin import ModelCUDA
         ModelCUDA(env.config, 10, env.batch_size, env.n_input_states + 1, env.n_springs, None,
                   env.actuation, env.n_hidden)
+
+
+def test_gym_actions_map_to_controller_outputs():
+    """MassSpringEnvCUDA turns the actions of the actuated springs into the
+    controller-output rows of cls_env_step: one shared row (the reference
+    passes action[i] to every env, mass_spring_env.py:56-58) or one per env."""
+    from cls_b200.clients import MassSpringEnvCUDA
+    env = MassSpringEnvCUDA.__new__(MassSpringEnvCUDA)
+    env.batch_size = 2
+    env.act_spring = np.array([1, 3])
+    env.n_outputs = 5
+    env.spring_output = np.arange(5)
+    out = env._outputs([0.5, -0.25])
+    np.testing.assert_array_equal(out, [[0, 0.5, 0, -0.25, 0]] * 2)
+    out = env._outputs([[1, 2], [3, 4]])
+    np.testing.assert_array_equal(out, [[0, 1, 0, 2, 0], [0, 3, 0, 4, 0]])
+    env.spring_output = np.array([-1, 0, -1, 1, -1])      # outputs for actuated springs only
+    env.n_outputs = 2
+    np.testing.assert_array_equal(env._outputs([7, 8]), [[7, 8], [7, 8]])
+    with pytest.raises(ValueError):
+        env._outputs([1, 2, 3])
