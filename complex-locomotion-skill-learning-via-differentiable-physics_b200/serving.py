@@ -25,6 +25,15 @@ CUDA stream) that ticks at its own pace, so a small robot's requests are not
 held to a large robot's substep time, and the pools' work overlaps on the
 device.
 
+MPM rollouts (``MpmType`` kinds: a particle body driven by seeded muscle
+actuations towards a centre target) are served by pools of their own: each
+slot is a one-env MLS-MPM handle (``cls_mpm_*``) on its own CUDA stream, and a
+request's whole rollout (forward, and the checkpointed reverse pass for
+gradient queries) is enqueued when it is admitted, so the MPM slots' work
+overlaps with each other and with the mass-spring pools' ticks; the MPM
+solver has no per-env windows, so its requests are not folded into shared
+launches.
+
 The scheduling is separate from the GPU backend (``SlotBackend``): the tests
 drive the scheduler with a fake backend on the CPU.
 """
@@ -104,6 +113,168 @@ def footprint_bytes(robot, steps, grad, K, dtype_bytes=4):
     w = params * dtype_bytes * (3 if grad else 1)
     rec = K * (48 * n + 8 * sum(widths[1:]) + 4 * widths[0]) if grad else 0
     return int(ckpt + traj + w + rec)
+
+
+@dataclass
+class MpmType:
+    """A registered MPM body type: particle positions [P][dim], muscle id
+    per particle (-1 passive), fibre directions, and MPMBatch keyword
+    arguments of the solver (material, n_grid, dt, mu, la, ...)."""
+    positions: np.ndarray
+    muscle: np.ndarray
+    fibre: Optional[np.ndarray] = None
+    n_muscles: int = 16
+    solver: dict = field(default_factory=dict)
+    target_offset: Sequence[float] = (0.05, 0.0, 0.0)
+
+
+def mpm_request_inputs(seed, T, steps, n_muscles, dt, dim=3):
+    """Actuation [T][n_muscles] of an MPM request: sinusoids of 2-6 Hz with
+    random phases drawn from its seed (the MPM benchmark's muscle drive);
+    zero after the request's horizon."""
+    rng = np.random.default_rng(seed)
+    freq = rng.uniform(2.0, 6.0, size=n_muscles)
+    phase = rng.uniform(0, 2 * np.pi, size=n_muscles)
+    t = np.arange(T)[:, None] * dt
+    act = np.sin(2 * np.pi * freq[None, :] * t + phase[None, :])
+    act[steps:] = 0.0
+    return act
+
+
+def mpm_footprint_bytes(mt, T, K, dtype_bytes=4):
+    """HBM bytes of one MPM slot: particle checkpoints (x, v, C, F) every K
+    steps over T, one segment's records, the actuation and centre tracks, and
+    the grid (n_grid^dim nodes of 16 bytes, twice for the adjoint)."""
+    P, D = mt.positions.shape
+    n_grid = int(mt.solver.get("n_grid", 64))
+    per_p = (2 * D + 2 * D * D) * dtype_bytes
+    return int(P * per_p * (T // K + 2) + P * per_p * K + 2 * 16 * n_grid ** D
+               + T * (mt.n_muscles + 2 * D) * dtype_bytes)
+
+
+class MpmSlotBackend:
+    """One-env MPM handles (one per slot) of one MPM type, each on its own
+    CUDA stream (torch.cuda.Stream, or the default stream when streams is
+    False)."""
+
+    def __init__(self, mt: MpmType, n_slots, T, K, streams=True):
+        from .mpm import MPMBatch
+        self.mt = mt
+        self.T, self.K = int(T), int(K)
+        dim = mt.positions.shape[1]
+        self.dim = dim
+        self.batches, self.streams, self.events = [], [], []
+        for _ in range(n_slots):
+            b = MPMBatch(mt.positions, mt.muscle, 1, dim=dim, fibre=mt.fibre, n_muscles=mt.n_muscles,
+                         max_steps=self.T, checkpoint_every=self.K, **mt.solver)
+            st = None
+            if streams:
+                import torch
+                st = torch.cuda.Stream()
+                b.set_stream(st.cuda_stream)
+            self.batches.append(b)
+            self.streams.append(st)
+            self.events.append(None)
+        self.c0 = mt.positions.mean(axis=0)
+        self.dt = float(self.batches[0].params.dt)
+
+    def start(self, slot, req):
+        """Enqueues the request's rollout (forward; reverse for gradient
+        queries) on the slot's stream."""
+        b = self.batches[slot]
+        D = self.dim
+        x0 = self.mt.positions if req.x0 is None else req.x0
+        b.set_state(np.asarray(x0, np.float64)[None])
+        b.set_actuation(mpm_request_inputs(req.seed, self.T, req.steps, self.mt.n_muscles, self.dt)[:, None, :])
+        w = np.zeros(self.T + 1)
+        w[req.steps] = 1.0
+        target = np.broadcast_to(self.c0 + np.asarray(self.mt.target_offset[:D]), (self.T + 1, 1, D)).copy()
+        b.set_loss(w, target)
+        b.forward(req.steps)
+        if req.grad:
+            b.backward()
+        if self.streams[slot] is not None:
+            import torch
+            ev = torch.cuda.Event()
+            ev.record(self.streams[slot])
+            self.events[slot] = ev
+
+    def done(self, slot):
+        ev = self.events[slot]
+        return ev is None or ev.query()
+
+    def result(self, slot, req):
+        """(loss, final positions [P][dim], gradients or None) of the slot's
+        finished request; gradients: d loss / d actuation [steps][muscles]
+        and d loss / d x0."""
+        b = self.batches[slot]
+        loss = b.loss()
+        x = b.final_state()[0][0]
+        grads = None
+        if req.grad:
+            g = b.grads()
+            grads = {"act": g["act"][:req.steps, 0], "x0": g["x0"][0]}
+        self.events[slot] = None
+        return loss, x, grads
+
+    def close(self):
+        for b in self.batches:
+            b.close()
+
+
+class MpmPool:
+    """The slots of one MPM type.  A slot runs one request's whole rollout;
+    admitted requests start at once, finished ones are collected as their
+    streams complete."""
+
+    def __init__(self, kind, n_slots, backend):
+        self.kind = kind
+        self.slots = [_Slot(kind) for _ in range(n_slots)]
+        self.backend = backend
+        self.plan = None              # not None while a slot is running
+
+    def free_slot(self, kind):
+        if kind != self.kind:
+            return -1
+        for i, s in enumerate(self.slots):
+            if s.phase == "free":
+                return i
+        return -1
+
+    def busy(self):
+        return any(s.phase != "free" for s in self.slots)
+
+    def launch(self):
+        started = False
+        for i, s in enumerate(self.slots):
+            if s.phase == "fwd":
+                self.backend.start(i, s.req)
+                s.phase = "run"
+                started = True
+        if self.busy():
+            self.plan = True
+        return started
+
+    def ready(self):
+        return any(s.phase == "run" and self.backend.done(i) for i, s in enumerate(self.slots))
+
+    def complete(self, server):
+        """Collects the finished slots; when none has finished yet, waits for
+        the first running one (so a synchronous tick always progresses)."""
+        running = [i for i, s in enumerate(self.slots) if s.phase == "run"]
+        fin = [i for i in running if self.backend.done(i)]
+        if not fin and running:
+            fin = running[:1]
+        out = []
+        for i in fin:
+            s = self.slots[i]
+            loss, x, grads = self.backend.result(i, s.req)
+            server.substeps_done += int(s.req.steps)
+            s.loss, s.fx = loss, x
+            s.terms = {"total": loss}
+            out.append(server._finish(self, i, grads))
+        self.plan = True if self.busy() else None
+        return out
 
 
 class SlotBackend:
@@ -308,9 +479,10 @@ class Pool:
 class Server:
     """Continuous-batching request loop over resident env slots.
 
-    types:         {name: RobotType}
-    slots:         {name: number of slots of that type}; each type is a pool
-                   (one batch on its own CUDA stream) that ticks at its own pace
+    types:         {name: RobotType or MpmType}
+    slots:         {name: number of slots of that type}; each mass-spring type
+                   is a pool (one batch on its own CUDA stream) that ticks at
+                   its own pace, each MPM type a pool of one-env handles
     params:        ``batch.default_params`` of the served batches (max_steps
                    is the longest episode, checkpoint_every the segment length)
     hbm_budget:    bytes of request footprints admitted at once (None: no
@@ -319,7 +491,8 @@ class Server:
     """
 
     def __init__(self, types: Dict[str, RobotType], slots: Dict[str, int], params, hbm_budget=None,
-                 backend_factory=None, streams=True, clock=time.perf_counter, tick_segments=1):
+                 backend_factory=None, streams=True, clock=time.perf_counter, tick_segments=1,
+                 mpm_backend_factory=None):
         self.types = types
         self.K = int(params.checkpoint_every)
         self.rounds = max(1, int(tick_segments))
@@ -337,6 +510,11 @@ class Server:
         self._streams = []
         for name, n in slots.items():
             slot_types = [name] * n
+            if isinstance(types[name], MpmType):
+                mb = (mpm_backend_factory(types[name], n, self.T, self.K) if mpm_backend_factory is not None
+                      else MpmSlotBackend(types[name], n, self.T, self.K, streams))
+                self.pools.append(MpmPool(name, n, mb))
+                continue
             if backend_factory is not None:
                 backend = backend_factory(slot_types, types, params)
             else:
@@ -367,7 +545,10 @@ class Server:
         return req.rid
 
     def footprint(self, req):
-        return footprint_bytes(self.types[req.kind].robot, req.steps, req.grad, self.K)
+        t = self.types[req.kind]
+        if isinstance(t, MpmType):
+            return mpm_footprint_bytes(t, self.T, self.K)
+        return footprint_bytes(t.robot, req.steps, req.grad, self.K)
 
     def _admit(self, pools):
         """FIFO admission into idle pools: a request waits for a free slot of
@@ -384,9 +565,10 @@ class Server:
                 if i < 0:
                     continue
                 s = pool.slots[i]
-                if pool.backend.loaded[i] != req.kind:
-                    pool.backend.load_weights(i, req.kind, self.types[req.kind].weights)
-                pool.backend.reset(i, req, self.types[req.kind].robot)
+                if isinstance(pool, Pool):
+                    if pool.backend.loaded[i] != req.kind:
+                        pool.backend.load_weights(i, req.kind, self.types[req.kind].weights)
+                    pool.backend.reset(i, req, self.types[req.kind].robot)
                 s.req, s.phase, s.pos, s.seg = req, "fwd", 0, 0
                 s.admitted, s.bytes = self.now(), fp
                 self.used_bytes += fp
@@ -445,6 +627,15 @@ class Server:
                 k += 1
             progressed = False
             for pool in self.pools:
+                if isinstance(pool, MpmPool):
+                    # whole-rollout slots: collect what finished, refill free slots
+                    if pool.ready():
+                        self.results.extend(pool.complete(self))
+                        progressed = True
+                    self._admit([pool])
+                    if pool.launch():
+                        progressed = True
+                    continue
                 if pool.plan is not None:
                     if not pool.ready():
                         continue

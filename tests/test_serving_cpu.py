@@ -180,3 +180,51 @@ def test_open_loop_run_serves_every_request_with_independent_pools():
     # the pools ticked independently: both launched
     for p in srv.pools:
         assert any(c[0] == "forward" for c in p.backend.calls)
+
+
+class FakeMpmBackend:
+    """Whole-rollout MPM slots: a request finishes `lag` done() polls after it
+    starts; its loss is a function of the request."""
+
+    def __init__(self, mt, n, T, K, lag=2):
+        self.started = []
+        self.polls = [0] * n
+        self.lag = lag
+
+    def start(self, slot, req):
+        self.started.append((slot, req.rid))
+        self.polls[slot] = 0
+
+    def done(self, slot):
+        self.polls[slot] += 1
+        return self.polls[slot] > self.lag
+
+    def result(self, slot, req):
+        return float(req.seed), np.zeros((2, 3)), ({"act": req.rid} if req.grad else None)
+
+    def close(self):
+        pass
+
+
+def test_mpm_requests_are_served_by_whole_rollout_slots():
+    """MPM requests take a free slot of their type at once (no ticks), run
+    while other slots start and finish, and mix with mass-spring pools."""
+    from cls_b200.serving import MpmType
+    obj, spr = robot_design.quadruped_lattice()
+    types = {"quad": RobotType(Robot.actuated_outputs(obj, spr, hidden=[8])),
+             "blob": MpmType(np.zeros((4, 3)), np.zeros(4, dtype=np.int32), n_muscles=1)}
+    params = SimpleNamespace(checkpoint_every=10, max_steps=100, turn_period=50)
+    srv = Server(types, {"quad": 1, "blob": 2}, params, backend_factory=FakeBackend, streams=False,
+                 mpm_backend_factory=FakeMpmBackend)
+    reqs = [Request("blob", 50, grad=True, seed=3), Request("blob", 60, seed=4), Request("blob", 70, seed=5),
+            Request("quad", 30, seed=6)]
+    for r in reqs:
+        srv.submit(r)
+    res = {r.rid: r for r in srv.drain()}
+    assert sorted(res) == [0, 1, 2, 3]
+    mpm_pool = [p for p in srv.pools if getattr(p, "kind", None) == "blob"][0]
+    # two slots: the third request waited for a slot, then reused one
+    assert [rid for _, rid in mpm_pool.backend.started] == [0, 1, 2]
+    assert res[0].loss == 3.0 and res[0].grads == {"act": 0}
+    assert res[1].grads is None and res[2].loss == 5.0
+    assert srv.used_bytes == 0

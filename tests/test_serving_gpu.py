@@ -115,3 +115,64 @@ def test_open_loop_run_reports_latency():
     assert len(res) == len(reqs) and st["requests"] == len(reqs)
     assert 0 < st["p50_ms"] <= st["p99_ms"]
     assert all(np.isfinite(r.loss) for r in res)
+
+
+def _mpm_type():
+    from cls_b200 import workloads
+    from cls_b200.serving import MpmType
+    pos, mus, fib = workloads.legged_body(n_grid=32, ppc=2, torso=(12, 4, 7), leg=(3, 5, 3),
+                                          origin_cells=(9, 4, 12))
+    E, nu = 1e4, 0.3
+    solver = dict(n_grid=32, bound=3, material="neo_hookean", precision=32, dt=1e-4, gravity=-10.0,
+                  p_vol=1.0, mu=E / (2 * (1 + nu)), la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3,
+                  mass=1.0)
+    return MpmType(pos, mus, fib, n_muscles=16, solver=solver)
+
+
+def _mpm_plain(mt, T, K, req):
+    from cls_b200.mpm import MPMBatch
+    from cls_b200.serving import mpm_request_inputs
+    b = MPMBatch(mt.positions, mt.muscle, 1, dim=3, fibre=mt.fibre, n_muscles=mt.n_muscles, max_steps=T,
+                 checkpoint_every=K, **mt.solver)
+    try:
+        b.set_state(mt.positions[None])
+        b.set_actuation(mpm_request_inputs(req.seed, T, req.steps, 16, 1e-4)[:, None, :])
+        w = np.zeros(T + 1)
+        w[req.steps] = 1.0
+        c0 = mt.positions.mean(axis=0)
+        b.set_loss(w, np.broadcast_to(c0 + np.array([0.05, 0, 0]), (T + 1, 1, 3)).copy())
+        loss = b.run(req.steps)
+        return loss, b.final_state()[0][0], b.grads()["act"][:req.steps, 0]
+    finally:
+        b.close()
+
+
+def test_mpm_requests_same_alone_in_mix_and_as_plain_batch():
+    """MPM rollout requests (configs[2]-style bodies) served in whole-rollout
+    slots beside mass-spring pools: each result equals its alone run and a
+    plain one-env MPMBatch (FP32: loss and positions rel 1e-5, actuation
+    gradients rel 1e-4; the P2G reductions are atomic)."""
+    import copy
+    from cls_b200.serving import Request
+    types = _types(32)
+    types["blob"] = _mpm_type()
+    T, K = 160, 40
+    params = _params(T, 32)
+    params.checkpoint_every = K
+    reqs = [Request("blob", 120, grad=True, seed=21), Request("quad", 150, grad=False, seed=22),
+            Request("blob", 80, grad=False, seed=23), Request("blob", 100, grad=True, seed=24),
+            Request("lat120", 90, grad=True, seed=25)]
+    mix = _serve(types, params, reqs, {"quad": 1, "lat120": 1, "blob": 2}, stagger=True)
+    mt = types["blob"]
+    for req, got in zip(reqs, mix):
+        if req.kind != "blob":
+            continue
+        alone = _serve(types, params, [copy.copy(req)], {"blob": 1}, stagger=False)[0]
+        ref_loss, ref_x, ref_g = _mpm_plain(mt, T, K, req)
+        for r in (got, alone):
+            assert r.loss == pytest.approx(ref_loss, rel=1e-5)
+            assert rel_err(r.final_x, ref_x) < 1e-5
+            if req.grad:
+                assert rel_err(r.grads["act"], ref_g) < 1e-4
+            else:
+                assert r.grads is None
