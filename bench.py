@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad-error", action="store_true",
+                    help="skip the FP32-vs-FP64 gradient error block")
     ap.add_argument("--threads", type=int, default=0,
                     help="threads per CTA of the fused kernels (0: autotuned, see --no-autotune)")
     ap.add_argument("--no-autotune", action="store_true",
@@ -130,6 +132,9 @@ def sum_over_ranks(x, world, device="cuda"):
 
 def config_dict(a, n_gpus):
     par = "env-sharded replicas x%d (no data-path collective)" % n_gpus
+    if a.config in ("quadruped", "spider") and n_gpus > 1:
+        par = ("dp%d: env shards of one shared controller, one NCCL all-reduce of the weight "
+               "gradients per iteration" % n_gpus)
     if a.config == "uneven":
         return {"workload": "batched uneven mass-spring: %d random lattices (50-2000 vertices, "
                             "log-uniform; 30%% springs actuated) x %d substeps, checkpoint every %d, "
@@ -312,9 +317,63 @@ def make_ms_batch(a, n, seed, robots=None):
                                                threads_per_block=a.threads)
         return b, robots, list(range(len(robots))), tt
     build = workloads.quadruped_batch if a.config == "quadruped" else workloads.spider_batch
-    b, robots, tt = build(n_envs=n, steps=a.substeps, K=a.checkpoint, seed=seed,
+    # every rank's shard holds the same controller (weights seeded alike);
+    # targets come from the rank's own seed
+    b, robots, tt = build(n_envs=n, steps=a.substeps, K=a.checkpoint, seed=seed, weights_seed=2,
                           threads_per_block=a.threads)
     return b, robots, [0] * n, tt
+
+
+def grad_error_block(a, robots, env_robot):
+    """The FP32 result against an FP64 build of the same kernels on the same
+    inputs (state, targets, FP32-representable weights): relative 2-norm
+    errors of the loss, of every robot's weight and bias gradients (worst
+    layer and robot) and of d loss / d x0 (worst env), on bounded subsets of
+    the workload; the configuration's gradient bar is rel 1e-4."""
+    from cls_b200 import workloads
+    from cls_b200.batch import MassSpringBatch, default_params
+    if a.config == "uneven":
+        n = min(16, len(robots))
+        cases = [("first %d robots x 200 substeps" % n, robots[:n], list(range(n)), 200),
+                 ("robot 0 (%d vertices) x %d substeps" % (robots[0].n_vertices, a.substeps), robots[:1], [0],
+                  a.substeps)]
+    else:
+        n = min(16, len(env_robot))
+        cases = [("%d envs x %d substeps" % (n, a.substeps), robots, [0] * n, a.substeps)]
+
+    def rel(x, y):
+        x, y = np.asarray(x, np.float64).ravel(), np.asarray(y, np.float64).ravel()
+        d = np.linalg.norm(y)
+        return float(np.linalg.norm(x - y) / (d if d > 0 else 1.0))
+
+    out = []
+    for desc, rb, er, steps in cases:
+        runs = {}
+        for prec in (32, 64):
+            K = min(a.checkpoint, steps)
+            b = MassSpringBatch(rb, er, default_params(**workloads._params(steps, K, precision=prec)))
+            rng = np.random.default_rng(5)
+            tv, th = workloads.targets(rng, steps, len(er))
+            b.set_targets(tv, th)
+            for r, robot in enumerate(rb):
+                for l in range(len(robot.hidden) + 1):
+                    rows, cols = b.layer_shape(r, l)
+                    W = (rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6 / cols)).astype(np.float32)
+                    b.set_weights(r, l, W.astype(np.float64), np.zeros(rows))
+            loss = b.simulate(steps)
+            grads = [b.get_grads(r, l) for r, robot in enumerate(rb) for l in range(len(robot.hidden) + 1)]
+            gx0 = b.state_grads()[0]
+            runs[prec] = (loss, grads, gx0, [b.env_slice(e) for e in range(len(er))])
+            b.close()
+        (l32, g32, x32, sl), (l64, g64, x64, _) = runs[32], runs[64]
+        gw = max(rel(a32[0], a64[0]) for a32, a64 in zip(g32, g64))
+        gb = max(rel(a32[1], a64[1]) for a32, a64 in zip(g32, g64))
+        gx = max(rel(x32[s_], x64[s_]) for s_ in sl)
+        out.append({"sample": desc, "loss_rel": abs(l32 - l64) / abs(l64), "grad_W_rel": gw, "grad_b_rel": gb,
+                    "grad_x0_rel": gx})
+    worst = max(max(c["loss_rel"], c["grad_W_rel"], c["grad_b_rel"]) for c in out)
+    return {"against": "FP64 build of the same kernels", "bar": 1e-4, "cases": out,
+            "worst_rel": worst, "meets_bar": bool(worst <= 1e-4)}
 
 
 def run_ours(a):
@@ -330,6 +389,13 @@ def run_ours(a):
     b, robots, env_robot, (tv, th) = make_ms_batch(a, a.robots, 1000 * rank)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
+    # one controller shared by the envs of every rank (quadruped, spider):
+    # each rank's losses are its shard's share of the whole batch's, and the
+    # weight gradients are summed over ranks before every Adam step
+    shared = world > 1 and a.config in ("quadruped", "spider")
+    if shared:
+        from cls_b200 import sharding
+        sharding.shard_loss_envs(b, [world * a.robots])
     # launch shape (and, with --controller auto, the controller path) picked
     # by timing this workload's own rollouts, before warm-up and outside the
     # timed region
@@ -350,18 +416,28 @@ def run_ours(a):
                                     e["weights_shared"], round(e["ms"], 3)] for e in tuned["table"]])
     env_substeps = b.n_envs * (a.substeps - 1)
 
+    def reduce_grads():
+        if shared:
+            sharding.allreduce_shared_grads(b, stream=stream)
+
     def iteration(it):
         b.simulate(a.substeps)
+        reduce_grads()
         b.adam_step(it)
 
-    # the timed training iteration (forward, loss, backward, Adam) is one CUDA
-    # graph replay; the eager path is measured separately as e2e below
+    # the timed training iteration (forward, loss, backward, [gradient
+    # all-reduce,] Adam) is one CUDA graph replay (the replay, the all-reduce
+    # and an eager Adam step when the controller is shared); the eager path is
+    # measured as e2e below
     iteration(0)
     b.synchronize()
-    b.graph_capture(a.substeps, with_adam=True)
+    b.graph_capture(a.substeps, with_adam=not shared)
 
     def replay(it):
         b.graph_launch(it)
+        if shared:
+            reduce_grads()
+            cls_b200._capi.check(b.lib.cls_adam_step(b.h, it, None), b.h)
 
     for it in range(a.warmup):
         replay(it)
@@ -487,6 +563,7 @@ def run_ours(a):
             cls_b200._capi.check(lib.cls_forward(h, a.substeps), h)
             cls_b200._capi.check(lib.cls_loss(h, pd(loss_terms), pd(env_loss)), h)
             cls_b200._capi.check(lib.cls_backward(h), h)
+            reduce_grads()
             cls_b200._capi.check(lib.cls_adam_step(h, it, None), h)
             cls_b200._capi.check(lib.cls_synchronize(h), h)
         e2e_s = (time.perf_counter() - t0) / a.e2e_steps
@@ -497,6 +574,12 @@ def run_ours(a):
                "d2h_bytes_per_step": int(d2h),
                "path": "cls_set_state/cls_set_targets (pinned host) -> cls_forward -> cls_loss "
                        "(D2H) -> cls_backward -> cls_adam_step -> cls_synchronize"}
+
+    grad_err = None
+    if rank == 0 and not a.no_grad_error:
+        t0 = time.perf_counter()
+        grad_err = grad_error_block(a, robots, env_robot)
+        grad_err["seconds"] = round(time.perf_counter() - t0, 2)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -515,7 +598,7 @@ def run_ours(a):
                 "launch_shape": launch_shape,
                 "clocks": clocks,
                 "gpu_launches": int(sum(prof_n.values())) * a.steps, "roofline": roofline,
-                "plain": plain, "e2e": e2e, "cpu_baseline": cpu}
+                "plain": plain, "e2e": e2e, "cpu_baseline": cpu, "grad_rel_err": grad_err}
         print(json.dumps(line))
     b.close()
     if world > 1:

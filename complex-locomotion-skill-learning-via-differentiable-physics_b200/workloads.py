@@ -73,7 +73,7 @@ def uneven_batch(n_robots=512, steps=2000, K=50, seed=0, precision=32, hidden=(1
     return b, robots, (tv, th)
 
 
-def quadruped_batch(n_envs=32, steps=1000, K=50, seed=0, precision=32, **over):
+def quadruped_batch(n_envs=32, steps=1000, K=50, seed=0, precision=32, weights_seed=None, **over):
     obj, spr = robot_design.quadruped_lattice()
     robot = Robot.actuated_outputs(obj, spr, hidden=[64])
     p = default_params(**_params(steps, K, precision=precision, **over))
@@ -81,11 +81,11 @@ def quadruped_batch(n_envs=32, steps=1000, K=50, seed=0, precision=32, **over):
     rng = np.random.default_rng(seed + 1)
     tv, th = targets(rng, steps, n_envs)
     b.set_targets(tv, th)
-    b.weights_init(seed + 2)
+    b.weights_init(seed + 2 if weights_seed is None else weights_seed)
     return b, [robot], (tv, th)
 
 
-def spider_batch(n_envs=4096, steps=1000, K=50, seed=0, precision=32, **over):
+def spider_batch(n_envs=4096, steps=1000, K=50, seed=0, precision=32, weights_seed=None, **over):
     obj, spr = robot_design.spider_lattice()
     robot = Robot.actuated_outputs(obj, spr, hidden=[256, 256])
     p = default_params(**_params(steps, K, precision=precision, **over))
@@ -93,7 +93,7 @@ def spider_batch(n_envs=4096, steps=1000, K=50, seed=0, precision=32, **over):
     rng = np.random.default_rng(seed + 1)
     tv, th = targets(rng, steps, n_envs)
     b.set_targets(tv, th)
-    b.weights_init(seed + 2)
+    b.weights_init(seed + 2 if weights_seed is None else weights_seed)
     return b, [robot], (tv, th)
 
 
