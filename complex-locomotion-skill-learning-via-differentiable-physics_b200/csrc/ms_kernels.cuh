@@ -393,11 +393,14 @@ __device__ __forceinline__ void accumulate_incidence(const MsArgs<R>& a, const I
 // not depend on scheduling (the recompute pass reproduces the first pass bit
 // for bit).  Each half-warp prefetches the first incidence of U vertices
 // before computing, so U records per lane are in flight.
+#ifndef CLS_GATHER_U
+#define CLS_GATHER_U 4
+#endif
 template <typename R>
 __device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotDesc& rb, int N,
                                                 const V4<R>* xs, const V4<R>* vs, const R* out,
                                                 V4<R>* vinc, V4<R>* rec) {
-  constexpr int U = 4;
+  constexpr int U = CLS_GATHER_U;
   const unsigned long long pol = policy_evict_last();
   const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
   const int l16 = lane & 15, half = lane >> 4;
@@ -559,6 +562,10 @@ __device__ __forceinline__ void load_controller_smem(const R* __restrict__ w, co
   for (int i = threadIdx.x; i < nb; i += blockDim.x) sb[i] = bias[b0 + i];
 }
 
+#ifndef CLS_GEMV_UNROLL
+#define CLS_GEMV_UNROLL 2
+#endif
+constexpr int kGemvUnroll = CLS_GEMV_UNROLL;
 // y = act(W x + b) for one layer.  Each warp owns RB consecutive rows at a
 // time and streams them together (RB independent float4 loads per lane per
 // column step), so short rows -- the 128-wide output layer of a robot with
@@ -582,7 +589,7 @@ __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pi
     R s[RB];
 #pragma unroll
     for (int r = 0; r < RB; ++r) s[r] = 0;
-#pragma unroll 2
+#pragma unroll kGemvUnroll
     for (int j = lane; j < n4; j += 32) {
       const V4<R> xv = x4[j];
       V4<R> wv[RB];
@@ -609,14 +616,28 @@ __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pi
   }
 }
 
+// rows per warp of the controller's products: RB_NARROW for rows of at most
+// 256 inputs, RB_WIDE above.  Measured on the 512-robot uneven batch (151
+// substeps, first pass + recompute + reverse): RB_WIDE 4 -> 8 took the
+// forward launches 25.3 -> 24.3 ms; unrolling the column loop 4 instead of 2
+// changed nothing
+#ifndef CLS_GEMV_RB_NARROW
+#define CLS_GEMV_RB_NARROW 8
+#endif
+#ifndef CLS_GEMV_RB_WIDE
+#define CLS_GEMV_RB_WIDE 8
+#endif
 template <typename R, bool SH>
 __device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch, int nout,
                                               const R* __restrict__ bias, const R* xin, R* y,
                                               R* zrec, int act) {
-  if (pitch <= 256) dense_forward_rb<R, 8, SH>(W, pitch, nout, bias, xin, y, zrec, act);
-  else dense_forward_rb<R, 4, SH>(W, pitch, nout, bias, xin, y, zrec, act);
+  if (pitch <= 256) dense_forward_rb<R, CLS_GEMV_RB_NARROW, SH>(W, pitch, nout, bias, xin, y, zrec, act);
+  else dense_forward_rb<R, CLS_GEMV_RB_WIDE, SH>(W, pitch, nout, bias, xin, y, zrec, act);
 }
 
+#ifndef CLS_TRANS_KMAX
+#define CLS_TRANS_KMAX 4
+#endif
 // g_in[j] = sum_i W[i, j] dz[i] for j in [0, ncols) (ncols multiple of 4 or
 // padded), deterministic: fixed row splits, fixed reduction order.
 // Result written to out4[j/4] (V4 groups).  Uses `part` (blockDim entries) as
@@ -641,7 +662,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
     // Wide rows (the first layer of a large robot): two half-blocks split the
     // rows; each thread keeps up to KMAX column-group partials in registers,
     // the first half stores, the second half adds (fixed order).
-    constexpr int KMAX = 4;
+    constexpr int KMAX = CLS_TRANS_KMAX;
     const int H = nt >> 1, h = tid >= H ? 1 : 0, lt = tid - h * H;
     const int rmid = nrows >> 1, r0 = h ? rmid : 0, r1 = h ? nrows : rmid;
     for (int base = 0; base < c4; base += H * KMAX) {

@@ -311,8 +311,21 @@ class TaichiEnvCUDA:
     # --------------------------------------------------------------- targets
     def inject_targets(self, target_v, target_h, target_c=None):
         """Targets used instead of the next initialize_train draw (parity
-        tests inject the reference's draws; ti.random is time-seeded)."""
-        self._injected = (target_v, target_h, target_c)
+        tests inject the reference's draws; ti.random is time-seeded).
+        Arrays of max_steps rows (the reference's fields) are zero-padded to
+        the batch's trajectory length."""
+        T = self.batch.T
+
+        def pad(a, tail):
+            if a is None:
+                return None
+            a = np.asarray(a, np.float64)
+            out = np.zeros((T,) + tail)
+            out[:min(T, a.shape[0])] = a[:T]
+            return out
+
+        B = self.batch_size
+        self._injected = (pad(target_v, (B, 3)), pad(target_h, (B,)), pad(target_c, (B,)))
 
     def initialize_train(self, iter, steps, max_velocity, max_height):
         if self._injected is not None:
