@@ -333,10 +333,15 @@ def grad_error_block(a, robots, env_robot):
     from cls_b200 import workloads
     from cls_b200.batch import MassSpringBatch, default_params
     if a.config == "uneven":
-        n = min(16, len(robots))
-        cases = [("first %d robots x 200 substeps" % n, robots[:n], list(range(n)), 200),
-                 ("robot 0 (%d vertices) x %d substeps" % (robots[0].n_vertices, a.substeps), robots[:1], [0],
-                  a.substeps)]
+        # the FP64 build's state of one robot must fit one CTA's shared
+        # memory: robots of up to 900 vertices
+        fit = [r for r in robots if r.n_vertices <= 900]
+        sub = fit[:16]
+        med = float(np.median([r.n_vertices for r in robots]))
+        one = min(fit, key=lambda r: abs(r.n_vertices - med))
+        cases = [("first %d robots of <= 900 vertices x 200 substeps" % len(sub), sub, list(range(len(sub))), 200),
+                 ("the %d-vertex robot (workload median %d) x %d substeps" % (one.n_vertices, med, a.substeps),
+                  [one], [0], a.substeps)]
     else:
         n = min(16, len(env_robot))
         cases = [("%d envs x %d substeps" % (n, a.substeps), robots, [0] * n, a.substeps)]

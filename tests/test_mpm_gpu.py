@@ -131,3 +131,33 @@ def test_mpm_checkpoint_interval_and_graph_replay():
     torch.cuda.synchronize()
     assert b.loss() == pytest.approx(L0, rel=1e-12)
     assert rel_err(b.grads()["act"], ga0) < 1e-10
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_mpm3d_legged_body_64_grid_50_substeps_matches_oracle(precision):
+    """The benchmark configuration (64^3 grid, ~29.5k particles, 16 fibre
+    muscle groups, neo-Hookean, dt 1e-4) over 50 substeps, K = 10, against
+    the FP64 oracle whose adjoint the finite-difference test pins on the same
+    body (tests/test_mpm_oracle.py)."""
+    from cls_b200.mpm import MPMBatch
+    from test_mpm_oracle import legged64_oracle
+    steps = 50
+    o, pos, mus, fib = legged64_oracle(steps)
+    L = o.run(steps)
+    E, nu = 1e4, 0.3
+    b = MPMBatch(pos, mus, 1, dim=3, fibre=fib, n_muscles=16, max_steps=steps, n_grid=64, bound=3,
+                 material="neo_hookean", precision=precision, checkpoint_every=10, dt=1e-4, gravity=-10.0,
+                 p_vol=1.0, mu=E / (2 * (1 + nu)), la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3,
+                 mass=1.0)
+    b.set_state(pos[None])
+    b.set_actuation(o.act)
+    b.set_loss(o.loss_w, o.target, (mus >= 0) * 1.0 + 0.1)
+    Lg = b.run(steps)
+    tf, tg = TOL[precision]
+    assert abs(Lg - L) <= max(tf * 10, 1e-7) * abs(L)
+    x, _, _, _ = b.final_state()
+    assert max_rel(x, o.x[steps]) < tf * 10
+    gr = b.grads()
+    for name, ref in (("act", o.gact), ("x0", o.gx0), ("v0", o.gv0), ("F0", o.gF0)):
+        assert rel_err(gr[name], ref) < tg, name
+    b.close()

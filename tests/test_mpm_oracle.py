@@ -101,3 +101,54 @@ def test_mpm3d_neo_hookean_fibre_gradients_match_finite_differences():
     o.run(steps)
     _fd(o, steps, {"act": (o.act, o.gact, 0), "x0": (o.x, o.gx0, 1), "v0": (o.v, o.gv0, 1),
                    "F0": (o.F, o.gF0, 1)}, rng, n=4)
+
+
+def legged64_oracle(steps=50, seed=0):
+    """The 3D MPM benchmark's body and solver: the voxelised legged body on a
+    64^3 grid (dx = 1/64, ~29.5k particles), neo-Hookean E = 1e4, nu = 0.3,
+    fibre actuation of 16 muscle groups, dt = 1e-4, sticky walls; one env,
+    seeded actuation in [-1, 1]; loss: the muscle-weighted centre at the last
+    step towards a point 0.05 ahead."""
+    from cls_b200 import workloads
+    pos, mus, fib = workloads.legged_body()
+    E, nu = 1e4, 0.3
+    o = MPMOracle(pos, mus, 1, steps, dim=3, n_grid=64, dt=1e-4, p_vol=1.0, mu=E / (2 * (1 + nu)),
+                  la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3, gravity=-10.0, bound=3,
+                  material="neo_hookean", fibre=fib, n_muscles=16)
+    rng = np.random.default_rng(seed)
+    o.act[...] = rng.uniform(-1, 1, o.act.shape)
+    o.loss_pw[...] = (mus >= 0) * 1.0 + 0.1
+    o.loss_w[steps] = 1.0
+    o.target[...] = pos.mean(axis=0) + np.array([0.05, 0.0, 0.0])
+    return o, pos, mus, fib
+
+
+def test_mpm3d_legged_body_64_grid_50_substeps_matches_finite_differences():
+    """The benchmark body over 50 substeps: the hand-written adjoint against
+    FP64 central differences on the actuation and initial-position entries
+    with the largest gradients (and one random entry of each), at the FD
+    tests' rel 2e-4 (truncation of the quadratic B-spline weights)."""
+    steps = 50
+    o, pos, mus, fib = legged64_oracle(steps)
+    L0 = o.run(steps)
+    rng = np.random.default_rng(3)
+    checks = []
+    for arr, g, h in ((o.act, o.gact, 1e-4), (o.x, o.gx0, 1e-6)):
+        ga = g.reshape(-1)
+        picks = list(np.argsort(-np.abs(ga))[:2]) + [int(rng.integers(ga.size))]
+        for flat in picks:
+            idx = np.unravel_index(flat, g.shape)
+            full = idx if arr is o.act else (0,) + idx
+            checks.append((arr, full, float(g[idx]), h))
+    for arr, full, an, h in checks:
+        old = arr[full]
+        arr[full] = old + h
+        o.forward(steps)
+        lp = o.compute_loss(steps)
+        arr[full] = old - h
+        o.forward(steps)
+        lm = o.compute_loss(steps)
+        arr[full] = old
+        fd = (lp - lm) / (2 * h)
+        atol = 50 * 1e-16 * abs(L0) / h
+        assert abs(fd - an) <= 2e-4 * max(abs(fd), abs(an)) + atol, (full, fd, an)
