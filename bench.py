@@ -61,6 +61,7 @@ SERVE_SECONDS_PER_STEP = 2.0  # seconds of arrivals per bench step
 # algorithmic bytes by it.
 TRAFFIC_RATIO = {"reverse": 8.620194e9 / 10.330433e9, "recompute": 8.787660e9 / 10.441533e9}
 UNIT = "env-substeps/s"
+SERVE_MPM_SLOTS = 4     # whole-rollout MPM slots of the serving workload (one-env handles)
 
 
 def parse():
@@ -157,11 +158,13 @@ def config_dict(a, n_gpus):
                 "l2": "trajectory and checkpoints written every iteration exceed L2"}
     if a.config == "serve":
         return {"workload": "serving: Poisson rollout requests at %.0f/s over %.0f s; robot mix quadruped "
-                            "25%% (MLP 1x64), spider 25%% (MLP 2x256), random lattices of 100/300/800/1500 "
-                            "vertices 50%% (MLP 2x128); episodes U{100..2000} substeps; 80%% forward-only "
-                            "evaluation, 20%% forward+adjoint gradient queries; %d slots per robot type, "
-                            "ticks of %d substeps" % (SERVE_RATE, a.steps * SERVE_SECONDS_PER_STEP,
-                                                        a.robots, a.checkpoint * a.tick_segments),
+                            "25%% (MLP 1x64), spider 20%% (MLP 2x256), random lattices of 100/300/800/1500 "
+                            "vertices 50%% (MLP 2x128), 3D MPM legged body 5%% (64^3 grid, dt 1e-4, %d "
+                            "whole-rollout slots); episodes U{100..2000} substeps; 80%% forward-only "
+                            "evaluation, 20%% forward+adjoint gradient queries; %d slots per mass-spring "
+                            "type, ticks of %d substeps" % (SERVE_RATE, a.steps * SERVE_SECONDS_PER_STEP,
+                                                             SERVE_MPM_SLOTS, a.robots,
+                                                             a.checkpoint * a.tick_segments),
                 "slots_per_type": a.robots, "rate_per_s": SERVE_RATE,
                 "arrival_seconds": a.steps * SERVE_SECONDS_PER_STEP, "checkpoint_every": a.checkpoint,
                 "parallelism": "independent servers x%d (no data-path collective)" % n_gpus,
@@ -786,6 +789,8 @@ def serve_oracle_sample(types, reqs, threads, cap=200):
     from oracle.ms_oracle import MassSpringOracle
     from cls_b200.serving import request_targets
 
+    reqs = [r for r in reqs if hasattr(types[r.kind], "robot")]   # mass-spring requests
+
     def one(req):
         rb = types[req.kind].robot
         T = min(req.steps, cap)
@@ -815,8 +820,8 @@ def serve_oracle_sample(types, reqs, threads, cap=200):
         res = list(ex.map(one, reqs))
     wall = time.perf_counter() - t0
     n = sum(k for _, k in res)
-    return n / wall, "%d requests of the serving mix, episodes capped at %d substeps (FP64; forward + " \
-        "loss, + reverse pass for gradient queries)" % (len(reqs), cap), wall
+    return n / wall, "%d mass-spring requests of the serving mix, episodes capped at %d substeps (FP64; " \
+        "forward + loss, + reverse pass for gradient queries)" % (len(reqs), cap), wall
 
 
 def run_reference_serve(a):
@@ -856,13 +861,15 @@ def run_serve(a):
     from cls_b200.serving import Server, poisson_requests
     types, kinds, probs = workloads.serving_types()
     params = default_params(**workloads._params(a.substeps, a.checkpoint))
-    srv = Server(types, {k: a.robots for k in kinds}, params, tick_segments=a.tick_segments)
+    srv = Server(types, {k: (SERVE_MPM_SLOTS if k.startswith("mpm") else a.robots) for k in kinds}, params,
+                 tick_segments=a.tick_segments)
     # warm-up: a short burst of requests (kernels loaded, slots exercised)
     warm = poisson_requests(np.random.default_rng(77 + rank), SERVE_RATE, 0.5 * a.warmup, kinds, probs,
                             steps_hi=400)
     srv.run(warm)
     srv.results, srv.substeps_done, srv.ticks = [], 0, 0
-    for p in srv.pools:
+    ms_pools = [p for p in srv.pools if hasattr(p.backend, "batch")]
+    for p in ms_pools:
         p.backend.batch.profile(True)
         p.backend.batch.profile_read(reset=True)
     reqs = poisson_requests(np.random.default_rng(1000 * rank + 1), SERVE_RATE,
@@ -876,7 +883,7 @@ def run_serve(a):
     torch.cuda.synchronize()
     clocks = clk.stop()
     kern_ms, launches = {}, {}
-    for p in srv.pools:
+    for p in ms_pools:
         ms, n = p.backend.batch.profile_read(reset=True)
         for k in ms:
             kern_ms[k] = kern_ms.get(k, 0.0) + ms[k]
@@ -890,6 +897,8 @@ def run_serve(a):
     # forward substeps over its device time
     fwd_bytes = 0.0
     for r in res:
+        if not hasattr(types[r.kind], "robot"):
+            continue
         per = workloads.algorithmic_bytes([types[r.kind].robot], [0])["forward"]
         fwd_bytes += per * (r.steps - 1)
     try:
@@ -906,9 +915,20 @@ def run_serve(a):
                 "traffic": None, "basis": "algorithmic first-pass bytes of the served requests / wall time",
                 "kernel_ms_overlapping_streams": kern_ms, "launches": launches}
     n_req = max(1, len(res))
-    h2d = sum(types[r.kind].robot.n_vertices * 24 + params.max_steps * 40 for r in res) / n_req
-    d2h = sum(types[r.kind].robot.n_vertices * 24 + 64 * a.robots * len(types) +
-              (sum(W.size + b.size for W, b in r.grads) * 8 if r.grads else 0) for r in res) / n_req
+
+    def io_bytes(r):
+        t = types[r.kind]
+        if hasattr(t, "robot"):
+            n = t.robot.n_vertices
+            return (n * 24 + params.max_steps * 40,
+                    n * 24 + 64 * a.robots * len(types) +
+                    (sum(W.size + b.size for W, b in r.grads) * 8 if r.grads else 0))
+        P, M = t.positions.shape[0], t.n_muscles      # MPM: state, actuation, loss in; state, grads out
+        return (P * 24 + params.max_steps * (M + 4) * 8,
+                P * 24 + (r.steps * M * 8 + P * 24 if r.grads else 0))
+
+    h2d = sum(io_bytes(r)[0] for r in res) / n_req
+    d2h = sum(io_bytes(r)[1] for r in res) / n_req
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -922,7 +942,9 @@ def run_serve(a):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded Poisson arrivals, robots, targets and controllers)",
                 "config": config_dict(a, world), "clocks": clocks,
-                "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"]},
+                "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"],
+                               "queue": st["queue_ms"], "service": st["service_ms"],
+                               "per_kind": st["per_kind_ms"]},
                 "requests": st["requests"], "ticks": st["ticks"],
                 "gpu_launches": int(sum(launches.values())), "roofline": roofline,
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(h2d * len(res) / a.steps),

@@ -655,10 +655,24 @@ class Server:
         return self.results, self.stats()
 
     def stats(self):
+        """Latency percentiles over the finished requests, split into the wait
+        for admission (arrival -> admitted) and the service time (admitted ->
+        done), overall and per robot type."""
+        def pct(v):
+            v = np.asarray(v) if len(v) else np.zeros(1)
+            return {"p50": float(np.percentile(v, 50) * 1e3), "p99": float(np.percentile(v, 99) * 1e3)}
+
         lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
         wall = max(self.now(), 1e-9)
+        per_kind = {}
+        for k in sorted({r.kind for r in self.results}):
+            rs = [r for r in self.results if r.kind == k]
+            per_kind[k] = dict(pct([r.latency for r in rs]), n=len(rs))
         return {"requests": len(self.results), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+                "queue_ms": pct([r.admitted - r.arrival for r in self.results]),
+                "service_ms": pct([r.done - r.admitted for r in self.results]),
+                "per_kind_ms": per_kind,
                 "env_substeps_per_s": self.substeps_done / wall, "ticks": self.ticks,
                 "wall_s": wall}
 

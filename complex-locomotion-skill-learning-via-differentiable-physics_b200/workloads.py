@@ -270,12 +270,26 @@ def mpm_algorithmic_bytes(pos, n_envs, n_grid=64, dtype_bytes=4):
     return {k: v * s * n_envs for k, v in per_env.items()}
 
 
-def serving_types(seed=0, lattice_sizes=(100, 300, 800, 1500)):
+def mpm_serving_type(n_grid=64):
+    """The 3D MPM configuration's body and solver as a served type: the
+    legged body, neo-Hookean E = 1e4, nu = 0.3, 16 fibre muscle groups,
+    dt = 1e-4, FP32."""
+    from .serving import MpmType
+    pos, mus, fib = legged_body(n_grid=n_grid)
+    E, nu = 1e4, 0.3
+    solver = dict(n_grid=n_grid, bound=3, material="neo_hookean", precision=32, dt=1e-4, gravity=-10.0,
+                  p_vol=1.0, mu=E / (2 * (1 + nu)), la=E * nu / ((1 + nu) * (1 - 2 * nu)), act_strength=1e3,
+                  mass=1.0)
+    return MpmType(pos, mus, fib, n_muscles=16, solver=solver)
+
+
+def serving_types(seed=0, lattice_sizes=(100, 300, 800, 1500), mpm=True):
     """Robot types of the serving workload (the training configurations'
     robots): the quadruped lattice (MLP 1x64), the spider lattice (MLP
-    2x256) and random lattices of the uneven batch (MLP 2x128), with the
-    request mix: quadruped 25 %, spider 25 %, lattices 50 % (equal shares).
-    Controllers are drawn per type by the server."""
+    2x256), random lattices of the uneven batch (MLP 2x128) and, with
+    ``mpm``, the MPM legged body, with the request mix: quadruped 25 %,
+    spider 20 %, MPM body 5 %, lattices 50 % (equal shares); without MPM the
+    spider takes its 5 %.  Controllers are drawn per type by the server."""
     from .serving import RobotType
     types = {}
     obj, spr = robot_design.quadruped_lattice()
@@ -286,6 +300,8 @@ def serving_types(seed=0, lattice_sizes=(100, 300, 800, 1500)):
     for n in lattice_sizes:
         o, s = robot_design.random_lattice(rng, n)
         types["lattice%d" % n] = RobotType(Robot.actuated_outputs(o, s, hidden=[128, 128]))
+    if mpm:
+        types["mpm_legged"] = mpm_serving_type()
     kinds = list(types)
-    p = [0.25, 0.25] + [0.5 / len(lattice_sizes)] * len(lattice_sizes)
+    p = [0.25, 0.20 if mpm else 0.25] + [0.5 / len(lattice_sizes)] * len(lattice_sizes) + ([0.05] if mpm else [])
     return types, kinds, p
