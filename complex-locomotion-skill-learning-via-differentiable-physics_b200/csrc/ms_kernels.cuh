@@ -638,6 +638,17 @@ __device__ __forceinline__ void dense_forward(const R* __restrict__ W, int pitch
 #ifndef CLS_TRANS_KMAX
 #define CLS_TRANS_KMAX 4
 #endif
+#ifndef CLS_TRANS_WIDE_UNROLL
+#define CLS_TRANS_WIDE_UNROLL 2
+#endif
+// row loops of the transposed products: wide rows (layer 0) unrolled 2,
+// narrow rows 8 (512-robot uneven batch, 151 substeps, reverse launches:
+// narrow 2 / 4 / 8 = 35.8 / 30.7 / 28.7 ms; wide 4 instead of 2: 30.6 ms)
+#ifndef CLS_TRANS_NARROW_UNROLL
+#define CLS_TRANS_NARROW_UNROLL 8
+#endif
+constexpr int kTransWideUnroll = CLS_TRANS_WIDE_UNROLL;
+constexpr int kTransNarrowUnroll = CLS_TRANS_NARROW_UNROLL;
 // g_in[j] = sum_i W[i, j] dz[i] for j in [0, ncols) (ncols multiple of 4 or
 // padded), deterministic: fixed row splits, fixed reduction order.
 // Result written to out4[j/4] (V4 groups).  Uses `part` (blockDim entries) as
@@ -669,7 +680,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
       R acc[KMAX][4];
 #pragma unroll
       for (int k = 0; k < KMAX; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0;
-#pragma unroll 2
+#pragma unroll kTransWideUnroll
       for (int i = r0; i < r1; ++i) {
         const R d = dz[i];
         const V4<R>* row = reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch);
@@ -713,7 +724,7 @@ __device__ __forceinline__ void dense_transposed(const R* __restrict__ W, int pi
   if (tid < used) {
     const int g = tid % c4, r0 = tid / c4;
     R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-#pragma unroll 4
+#pragma unroll kTransNarrowUnroll
     for (int i = r0; i < nrows; i += slices) {
       const V4<R> wv = ldw4<R, SH>(reinterpret_cast<const V4<R>*>(W + (size_t)i * pitch) + g, pol);
       const R d = dz[i];
