@@ -727,6 +727,22 @@ def run_mpm(a):
                 "kernel_ms": prof_ms, "launches": prof_n,
                 "per_kernel_frac": {k: alg[k] * prof_n[k] / (prof_ms[k] / 1e3) / 1e9 / peak
                                     for k in kinds}}
+    # the particle kernels' working set (~33 MB of grid, ~24 MB of particles
+    # for 8 envs) is L2-resident: their scatter roofline is the measured rate
+    # of the 16-byte vector reductions they issue (27 per particle and step:
+    # P2G in the forward kernels, G2P^T's velocity adjoint in the reverse)
+    from cls_b200 import mpm as mpm_mod
+    n_nodes = b.E * (64 // 4) ** 3 * 64
+    red_peak = mpm_mod.reduction_peak(n_nodes)
+    reds = b.E * pos.shape[0] * 27
+    scatter = {}
+    for k in ("particle", "particle_recompute", "particle_adj"):
+        if prof_n.get(k, 0) > 0:
+            rate = reds * prof_n[k] / (prof_ms[k] / 1e3)
+            scatter[k] = {"achieved": rate, "frac": rate / red_peak}
+    roofline["scatter"] = {"bound": "l2 vector reductions", "unit": "reductions/s", "peak": red_peak,
+                           "peak_source": "measured in this run (cls_mpm_reduction_peak, %d nodes)" % n_nodes,
+                           "per_kernel": scatter}
 
     # end to end through the C ABI with host buffers: initial state and
     # actuation in, loss and actuation gradient out, every iteration

@@ -757,6 +757,56 @@ int cls_mpm_graph_launch(cls_mpm* s) {
 int cls_mpm_profile_enable(cls_mpm* s, int32_t on) {
   return mguard(s, [&](cls::mpm::MpmBase& b) { b.profile_enable(on != 0); });
 }
+// Calibration of the scatter roofline: 16-byte vector reductions
+// (red.global.add.v4.f32, the P2G / G2P^T scatter instruction) from every
+// thread into a buffer of n_nodes 16-byte nodes, each warp's 32 lanes on 32
+// distinct nodes of a pseudo-random 1 KB block walk -- the pattern of the
+// particle kernels' scatters, where a warp's lanes hold particles of distinct
+// cells and successive stencil offsets move to neighbouring nodes.
+namespace {
+__global__ void mpm_red_peak_kernel(cls::V4<float>* __restrict__ nodes, long long n_nodes, int per_thread) {
+  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  const unsigned long long warp = tid >> 5, lane = tid & 31;
+  const long long nblk = n_nodes / 64;
+  unsigned long long h = warp * 0x9E3779B97F4A7C15ULL + 1;
+  for (int k = 0; k < per_thread; ++k) {
+    if ((k & 7) == 0) h = h * 6364136223846793005ULL + 1442695040888963407ULL;
+    const long long blk = (long long)((h >> 20) % (unsigned long long)nblk);
+    const long long node = blk * 64 + (long long)((lane * 2 + (k & 7)) & 63);
+    cls::mpm::red4<float>(nodes + node, 1.f, 1.f, 1.f, 1.f);
+  }
+}
+}  // namespace
+
+int cls_mpm_reduction_peak(int64_t n_nodes, int64_t n_ops, double* ops_per_s) {
+  if (!ops_per_s || n_nodes < 64 || n_ops < 1) return CLS_ERR_INVALID;
+  cls::V4<float>* buf = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = CLS_OK;
+  const int per_thread = 64, threads = 256;
+  const long long n_threads = (n_ops + per_thread - 1) / per_thread;
+  const int blocks = (int)std::min<long long>((n_threads + threads - 1) / threads, 1LL << 30);
+  if (cudaMalloc(&buf, sizeof(cls::V4<float>) * (size_t)n_nodes) != cudaSuccess) return CLS_ERR_OOM;
+  float ms = 0.f;
+  if (cudaMemset(buf, 0, sizeof(cls::V4<float>) * (size_t)n_nodes) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = CLS_ERR_CUDA;
+  } else {
+    mpm_red_peak_kernel<<<blocks, threads>>>(buf, n_nodes, per_thread);  // warm-up
+    cudaEventRecord(e0);
+    mpm_red_peak_kernel<<<blocks, threads>>>(buf, n_nodes, per_thread);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+        cudaGetLastError() != cudaSuccess)
+      rc = CLS_ERR_CUDA;
+  }
+  if (rc == CLS_OK) *ops_per_s = (double)blocks * threads * per_thread / (ms * 1e-3);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  return rc;
+}
+
 int cls_mpm_profile_read(cls_mpm* s, double* ms, int64_t* launches, int32_t reset) {
   return mguard(s, [&](cls::mpm::MpmBase& b) {
     b.profile_read(ms, reinterpret_cast<long long*>(launches), reset != 0);

@@ -47,6 +47,7 @@ _SIGS = {
     "cls_mpm_graph_launch": (_i32, [ctypes.c_void_p]),
     "cls_mpm_profile_enable": (_i32, [ctypes.c_void_p, _i32]),
     "cls_mpm_profile_read": (_i32, [ctypes.c_void_p, P_D, ctypes.POINTER(ctypes.c_int64), _i32]),
+    "cls_mpm_reduction_peak": (_i32, [ctypes.c_int64, ctypes.c_int64, P_D]),
 }
 
 # categories of cls_mpm_profile_read
@@ -62,6 +63,16 @@ def _lib():
             fn.argtypes = args
         lib._mpm_bound = True
     return lib
+
+
+def reduction_peak(n_nodes, n_ops=1 << 27):
+    """Measured rate (operations/s) of 16-byte vector reductions into an
+    n_nodes-node buffer (cls_mpm_reduction_peak)."""
+    out = ctypes.c_double()
+    rc = _lib().cls_mpm_reduction_peak(int(n_nodes), int(n_ops), ctypes.byref(out))
+    if rc != 0:
+        raise _capi.ClsError("cls_mpm_reduction_peak failed (%d)" % rc, rc)
+    return out.value
 
 
 def default_params(**over):

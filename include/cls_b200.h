@@ -459,6 +459,14 @@ int cls_mpm_graph_launch(cls_mpm* sim);
  * recompute, 2 grid update, 3 particle adjoint (P2G^T of step f fused with
  * G2P^T of step f-1), 4 grid adjoint, 5 other (centre and actuation-gradient
  * reductions, list resets).  ms / launches have CLS_MPM_PROFILE_KINDS entries. */
+/* Measured throughput (operations/s, *ops_per_s) of the particle kernels'
+ * scatter instruction -- 16-byte vector reductions into an n_nodes x 16-byte
+ * buffer (pass the kernels' grid size: an L2-resident grid measures the L2
+ * reduction rate), each warp's lanes on distinct nodes of one 1 KB block --
+ * over about n_ops reductions; the denominator of the MPM scatter roofline.
+ * Allocates its own buffer on the current device.  No reference
+ * counterpart. */
+int cls_mpm_reduction_peak(int64_t n_nodes, int64_t n_ops, double* ops_per_s);
 #define CLS_MPM_PROFILE_KINDS 6
 int cls_mpm_profile_enable(cls_mpm* sim, int32_t on);
 int cls_mpm_profile_read(cls_mpm* sim, double* ms, int64_t* launches, int32_t reset);
