@@ -620,9 +620,10 @@ __device__ __forceinline__ void dense_forward_rb(const R* __restrict__ W, int pi
 // 256 inputs, RB_WIDE above.  Measured on the 512-robot uneven batch (151
 // substeps, first pass + recompute + reverse): RB_WIDE 4 -> 8 took the
 // forward launches 25.3 -> 24.3 ms; unrolling the column loop 4 instead of 2
-// changed nothing; RB_NARROW 8 -> 16: 24.29 -> 24.23 ms
+// changed nothing; RB_NARROW 16 measured within noise of 8 and spills in the
+// 512-thread instance, so 8 stays
 #ifndef CLS_GEMV_RB_NARROW
-#define CLS_GEMV_RB_NARROW 16
+#define CLS_GEMV_RB_NARROW 8
 #endif
 #ifndef CLS_GEMV_RB_WIDE
 #define CLS_GEMV_RB_WIDE 8
