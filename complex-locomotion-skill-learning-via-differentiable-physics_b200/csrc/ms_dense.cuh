@@ -59,6 +59,7 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
   const int e = a.order[item];
   load_descs<R>(a, e, rb, ed);
   const int N = rb.n_v, L = rb.n_layers;
+  CLS_PHASE_START();
   {
     const bool first = (t == t_first);
     const V4<R>* cx = first ? a.ckpt_x + (size_t)src_slot * a.v_total + ed.v_off : a.live_x + ed.v_off;
@@ -71,13 +72,16 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
     const R* bo = a.bias + rb.b_off[L - 1];
     for (int o = tid; o < rb.n_out; o += nt) s.buf0[o] = act_f<R>(a.act_out, zl[o] + bo[o]);
     __syncthreads();
+    CLS_PHASE(a, 20);
     fwd_post<R>(a, rb, ed, s, t - 1, mode, k_prev, s.buf0);
+    CLS_PHASE(a, 21);
   }
   if (t < t_end) {
     R hprev = 0;
     if ((mode & FWD_OBS) && t > 0) hprev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
     load_head_smem<R>(a, rb, ed, s, t, mode);
     fwd_pre<R>(a, rb, ed, s, e, t, t_first, mode, k_cur, true, true, hprev);
+    CLS_PHASE(a, 22);
     if constexpr (std::is_same<R, float>::value) {
       // the input row as the first layer's pre-split A operand
       const umma::SplitTiles st{a.tiles + a.dense[ed.robot].ta_f[0], umma::TM, (rb.n_c + 31) / 32};
@@ -85,10 +89,12 @@ ms_step_fwd_kernel(MsArgs<R> a, int t, int t_first, int t_end, int mode, int src
       for (int q = 4 * tid; q < rb.n_c; q += 4 * nt)
         st.store4(j, q, make_float4(s.ain[q], s.ain[q + 1], s.ain[q + 2], s.ain[q + 3]));
     }
+    CLS_PHASE(a, 23);
     for (int i = tid; i < N; i += nt) {
       a.live_x[ed.v_off + i] = s.xs[i];
       a.live_v[ed.v_off + i] = s.vs[i];
     }
+    CLS_PHASE(a, 24);
   } else {
     fwd_finish<R>(a, rb, ed, s, t_first, t_end, mode);
   }
@@ -116,7 +122,9 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
   load_descs<R>(a, e, rb, ed);
   const int N = rb.n_v;
   R hcarry = 0;
+  CLS_PHASE_START();
   rev_load_carry<R>(a, rb, ed, s, e, t_end, t_pre == t_end - 1 && last_seg != 0, hcarry);
+  CLS_PHASE(a, 25);
   if (t_post >= 0) {
     const int kk = t_post - t_begin;
     const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
@@ -125,9 +133,11 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
     for (int q = tid; q < 3 * N; q += nt) s.bufA[q] = dp[q];
     __syncthreads();
     rev_post<R>(a, rb, ed, s, e, t_post, hcarry);
+    CLS_PHASE(a, 26);
   }
   if (t_pre >= 0) {
     rev_pre<R>(a, rb, ed, s, e, t_pre, t_pre - t_begin);
+    CLS_PHASE(a, 27);
     if constexpr (std::is_same<R, float>::value) {
       // dZ of the output layer as the adjoint GEMM's pre-split A operand
       const int no = rb.n_out;
@@ -139,8 +149,10 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
         st.store4(j, q, v);
       }
     }
+    CLS_PHASE(a, 28);
   }
   rev_store_carry<R>(a, rb, ed, s, e, hcarry);
+  CLS_PHASE(a, 29);
 }
 
 // ------------------------------------------------------------ GEMM operands

@@ -452,6 +452,12 @@ __device__ __forceinline__ void gather_vinc_all(const MsArgs<R>& a, const RobotD
 // imp[], phase B is gather_vinc_all's half-warp gather with the impulses read
 // from imp[] instead of recomputed, in the same lanes and the same order.  For
 // robots whose impulse table fits in shared memory (MsArgs::imp_cap).
+// spring-parallel table phase: the next spring's records in flight while one
+// is evaluated (spider step kernel, 4096 envs: forward 11.65 -> 11.41 ms per
+// 61 substeps)
+#ifndef CLS_TABLE_PREFETCH
+#define CLS_TABLE_PREFETCH 1
+#endif
 template <typename R>
 __device__ __forceinline__ void gather_vinc_table(const MsArgs<R>& a, const RobotDesc& rb, int N,
                                                   const V4<R>* xs, const V4<R>* vs, const R* out,
@@ -459,6 +465,33 @@ __device__ __forceinline__ void gather_vinc_table(const MsArgs<R>& a, const Robo
   constexpr int U = 4;
   const unsigned long long pol = policy_evict_last();
   const int tid = threadIdx.x, nt = blockDim.x;
+#if CLS_TABLE_PREFETCH
+  // the next spring's records are loaded before this one is evaluated, so
+  // one pair of L2 loads per thread is always in flight (same arithmetic)
+  int4 ab = make_int4(0, 0, -1, 0);
+  V4<R> f;
+  f.x = f.y = f.z = f.w = R(0);
+  if (tid < rb.n_s) {
+    ab = ldg_i4_hint(a.spr_ab + rb.spr_off + tid, pol);
+    f = ldg4_hint<R>(a.spr_p + rb.spr_off + tid, pol);
+  }
+  for (int sp = tid; sp < rb.n_s; sp += nt) {
+    const int nx = sp + nt;
+    int4 ab_n = ab;
+    V4<R> f_n = f;
+    if (nx < rb.n_s) {
+      ab_n = ldg_i4_hint(a.spr_ab + rb.spr_off + nx, pol);
+      f_n = ldg4_hint<R>(a.spr_p + rb.spr_off + nx, pol);
+    }
+    const R act = ab.z >= 0 ? out[ab.z] : R(0);
+    R im[3];
+    spring_impulse<R>(xs[ab.x], xs[ab.y], vs[ab.x], vs[ab.y], f.x, f.y, f.z, act, a.dt, a.dashpot, im);
+    V4<R> r; r.x = im[0]; r.y = im[1]; r.z = im[2]; r.w = 0;
+    imp[sp] = r;
+    ab = ab_n;
+    f = f_n;
+  }
+#else
   for (int sp = tid; sp < rb.n_s; sp += nt) {
     const int4 ab = ldg_i4_hint(a.spr_ab + rb.spr_off + sp, pol);
     const V4<R> f = ldg4_hint<R>(a.spr_p + rb.spr_off + sp, pol);
@@ -468,6 +501,7 @@ __device__ __forceinline__ void gather_vinc_table(const MsArgs<R>& a, const Robo
     V4<R> r; r.x = im[0]; r.y = im[1]; r.z = im[2]; r.w = 0;
     imp[sp] = r;
   }
+#endif
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
   const int l16 = lane & 15, half = lane >> 4;
