@@ -143,6 +143,8 @@ class MassSpringEnvCUDA:
         return self.get_state(self.t)
 
     def step(self, action):
+        if self._obs is None:
+            raise RuntimeError("reset() first: the state on the device is set by reset")
         if self.t + 1 >= self.max_steps:
             raise RuntimeError("the rollout is over (t = %d); reset()" % self.t)
         outputs = np.ascontiguousarray(self._outputs(action))

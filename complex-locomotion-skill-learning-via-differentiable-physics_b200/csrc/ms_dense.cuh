@@ -303,8 +303,14 @@ __device__ __forceinline__ BwdOperands<R> bwd_operands(const MsArgs<R>& a, const
 //   forward l:  Z_l record; act(Z_l + b_l) as layer l + 1's A (hidden layers)
 //   adjoint l:  dZ_{l-1} = C act'(Z_{l-1} + b_{l-1}) record and as layer l-1's
 //               adjoint A (l > 0); d input positions (l = 0)
-constexpr int kDenseTN = 64;     // output columns per tensor-core tile
-constexpr int kBulkStages = 4;   // 4 x 48 KB stage ring
+#ifndef CLS_DENSE_TN
+#define CLS_DENSE_TN 64
+#endif
+#ifndef CLS_BULK_STAGES
+#define CLS_BULK_STAGES 4
+#endif
+constexpr int kDenseTN = CLS_DENSE_TN;        // output columns per tensor-core tile
+constexpr int kBulkStages = CLS_BULK_STAGES;  // stages of the bulk-copy ring (4 x 48 KB at TN = 64)
 
 __device__ __forceinline__ float4 mask4(float4 v, int col, int n) {
   if (col + 1 > n) v.x = 0.f;

@@ -189,7 +189,8 @@ int cls_grad_buffers(cls_sim* sim, void** weight_grads, int64_t* n_weight, void*
  * gradients are its shard's share of the whole batch's and the all-reduced
  * sum is the whole batch's.  n_envs must be at least the handle's count.
  * The next cls_backward needs a new cls_forward; a CUDA graph captured
- * earlier keeps the value it was captured with.  No reference counterpart. */
+ * earlier reads the new value when it is replayed (the robot table lives in
+ * device memory).  No reference counterpart. */
 int cls_set_loss_envs(cls_sim* sim, int32_t robot, int32_t n_envs);
 /* zero the Adam moments (Model.clear_adam, multitask/nn.py:111-114) */
 int cls_clear_adam(cls_sim* sim);
