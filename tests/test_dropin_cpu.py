@@ -78,7 +78,9 @@ def test_injected_targets_replace_the_draw():
     env.inject_targets(g["target_v"], g["target_h"], g["target_c"])
     replay_simulate_trace(load_simulate_trace("quad_ref")["calls"], env, nn, Tape)
     assert [c[0] for c in fake.calls][:1] == ["set_targets"]
-    np.testing.assert_array_equal(fake.tv, g["target_v"])
+    T = g["target_v"].shape[0]
+    np.testing.assert_array_equal(fake.tv[:T], g["target_v"])     # padded to the batch's length
+    assert np.all(fake.tv[T:] == 0.0)
 
 
 def test_evaluation_trace_runs_the_evaluation_rollout():
