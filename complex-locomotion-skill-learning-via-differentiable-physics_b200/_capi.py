@@ -56,6 +56,12 @@ class LaunchShape(ctypes.Structure):
                 ("ctas_per_sm", c_int32), ("weights_shared", c_int32), ("ms", ctypes.c_float)]
 
 
+class Request(ctypes.Structure):
+    """cls_request: one rollout request for cls_admit."""
+    _fields_ = [("id", ctypes.c_uint64), ("robot", c_int32), ("steps", c_int32), ("grad", c_int32),
+                ("x0", P_D), ("target_v", P_D), ("target_h", P_D), ("target_c", P_D)]
+
+
 class ClsError(RuntimeError):
     """A failed C-ABI call; ``code`` is the CLS_ERR_* value."""
 
@@ -122,6 +128,11 @@ _SIGS = {
     "cls_serve_backward": (c_int32, [ctypes.c_void_p, P_I, P_I]),
     "cls_serve_loss": (c_int32, [ctypes.c_void_p, P_I, P_D]),
     "cls_serve_env_state": (c_int32, [ctypes.c_void_p, c_int32, P_D, P_D]),
+    "cls_serve_tick": (c_int32, [ctypes.c_void_p, c_int32]),
+    "cls_admit": (c_int32, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.c_int64, P_I]),
+    "cls_poll": (c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), c_int32, P_I, P_I]),
+    "cls_serve_result": (c_int32, [ctypes.c_void_p, ctypes.c_uint64, P_I, P_D, P_D]),
+    "cls_serve_release": (c_int32, [ctypes.c_void_p, ctypes.c_uint64]),
 }
 
 

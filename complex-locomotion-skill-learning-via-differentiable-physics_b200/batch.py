@@ -234,6 +234,45 @@ class MassSpringBatch:
         self._c(self.lib.cls_serve_env_state(self.h, env, ptr(x), ptr(v)))
         return x, v
 
+    # the library's own admission / poll loop over the envs as slots
+    def serve_tick(self, tick_segments):
+        self._c(self.lib.cls_serve_tick(self.h, int(tick_segments)))
+
+    def admit(self, rid, robot, steps, grad=False, x0=None, target_v=None, target_h=None, target_c=None,
+              budget=-1):
+        """Admit request `rid` on a free slot of slot `robot`'s robot class;
+        returns the slot, or -1 (no free slot, or its footprint does not fit
+        `budget` bytes)."""
+        slot = ctypes.c_int32(-1)
+        n = self.robots[self.env_robot[robot]].n_vertices
+        keep = [None if x0 is None else self._f64(x0, (n, 3)),
+                None if target_v is None else self._f64(target_v, (self.T, 3)),
+                None if target_h is None else self._f64(target_h, (self.T,)),
+                None if target_c is None else self._f64(target_c, (self.T,))]
+        req = _capi.Request(int(rid), int(robot), int(steps), 1 if grad else 0, *[ptr(a) for a in keep])
+        self._c(self.lib.cls_admit(self.h, ctypes.byref(req), int(budget), ctypes.byref(slot)))
+        return slot.value
+
+    def poll(self, capacity=64):
+        """Complete the tick in flight and issue the next; returns (ids of
+        finished requests, slots still running)."""
+        ids = (ctypes.c_uint64 * max(1, capacity))()
+        n_done, n_active = ctypes.c_int32(), ctypes.c_int32()
+        self._c(self.lib.cls_poll(self.h, ids, int(capacity), ctypes.byref(n_done), ctypes.byref(n_active)))
+        return [int(ids[k]) for k in range(n_done.value)], n_active.value
+
+    def serve_result(self, rid):
+        """(slot, loss terms [8], final positions [n_v][3]) of a finished request."""
+        slot = ctypes.c_int32()
+        self._c(self.lib.cls_serve_result(self.h, int(rid), ctypes.byref(slot), None, None))
+        n = self.robots[self.env_robot[slot.value]].n_vertices
+        terms, x = np.zeros(8), np.zeros((n, 3))
+        self._c(self.lib.cls_serve_result(self.h, int(rid), ctypes.byref(slot), ptr(terms), ptr(x)))
+        return slot.value, terms, x
+
+    def serve_release(self, rid):
+        self._c(self.lib.cls_serve_release(self.h, int(rid)))
+
     def adam_step(self, it):
         tns = ctypes.c_double()
         self._c(self.lib.cls_adam_step(self.h, it, ctypes.byref(tns)))

@@ -16,6 +16,7 @@
 #include "cls_profile.cuh"
 #include "ms_dense_host.h"
 #include "ms_env_host.h"
+#include "ms_sched.h"
 #include "ms_segment.cuh"
 
 // threads of the batched controller's step kernels (one CTA per env)
@@ -178,6 +179,14 @@ class SimBase {
   virtual void serve_backward(const int* win, const int* steps) = 0;
   virtual void serve_loss(const int* steps, double* env) = 0;
   virtual void serve_env_state(int ue, double* x, double* v) = 0;
+  // what the slot scheduler needs of env ue: its robot class (envs whose
+  // robot entries have the same geometry and controller shape share one),
+  // vertex count, rest pose and the footprint of a request on it
+  virtual int env_class(int ue) const = 0;
+  virtual int env_vertices(int ue) const = 0;
+  virtual const double* env_objects(int ue) const = 0;
+  virtual long long env_footprint(int ue, int steps, bool grad) const = 0;
+  virtual int checkpoint_every() const = 0;
   // controller path: 0 auto, 1 per env (fused segment kernels), 2 batched
   virtual void set_controller_path(int path) = 0;
   virtual bool controller_batched() const = 0;
@@ -1879,6 +1888,53 @@ class SimImpl final : public SimBase {
     }
   }
 
+  // robot class of every robot entry: the first entry with the same
+  // geometry, spring table, output map and layer widths (computed once)
+  int env_class(int ue) const override {
+    if (robot_class_.empty()) {
+      const int nr = (int)hr_.size();
+      robot_class_.assign(nr, 0);
+      for (int r = 0; r < nr; ++r) {
+        robot_class_[r] = r;
+        for (int q = 0; q < r; ++q)
+          if (robot_class_[q] == q && same_robot(hr_[q], hr_[r])) { robot_class_[r] = q; break; }
+      }
+    }
+    return robot_class_[ed_host_[ienv(ue)].robot];
+  }
+  static bool same_robot(const HostRobot& a, const HostRobot& b) {
+    if (a.n_v != b.n_v || a.n_s != b.n_s || a.n_out != b.n_out || a.robot_id != b.robot_id ||
+        a.n_layers != b.n_layers)
+      return false;
+    for (int l = 0; l <= a.n_layers; ++l)
+      if (a.width[l] != b.width[l]) return false;
+    return a.objects == b.objects && a.sa == b.sa && a.sb == b.sb && a.out == b.out && a.len == b.len &&
+           a.stiff == b.stiff && a.coef == b.coef;
+  }
+  int env_vertices(int ue) const override { return hr_[ed_host_[ienv(ue)].robot].n_v; }
+  const double* env_objects(int ue) const override { return hr_[ed_host_[ienv(ue)].robot].objects.data(); }
+  // HBM bytes a request keeps resident while it is served (the terms of
+  // serving.footprint_bytes over this handle's own layer widths, the input
+  // layer in its compact form): state and checkpoints, trajectory and
+  // observables, targets, controller weights (x3 with gradient and
+  // optimiser-sized buffers) and, for gradient queries, the per-segment
+  // records of its reverse pass
+  long long env_footprint(int ue, int steps, bool grad) const override {
+    const HostRobot& h = hr_[ed_host_[ienv(ue)].robot];
+    const long long n = h.n_v, K = K_;
+    long long params = 0, widths_after = 0;
+    for (int l = 0; l < h.n_layers; ++l) {
+      params += (long long)h.width[l + 1] * h.width[l] + h.width[l + 1];
+      widths_after += h.width[l + 1];
+    }
+    const long long ckpt = 2 * 16 * n * (steps / K + 2);
+    const long long traj = 16 * n * steps + 32LL * steps + 24LL * steps;
+    const long long w = params * (long long)sizeof(R) * (grad ? 3 : 1);
+    const long long rec = grad ? K * (48 * n + 8 * widths_after + 4LL * h.width[0]) : 0;
+    return ckpt + traj + w + rec;
+  }
+  int checkpoint_every() const override { return K_; }
+
   void state_grads(double* gx, double* gv) override {
     CLS_REQUIRE(bwd_done_, "state gradients requested before cls_backward");
     if (gx) get_vstate(d_adjx_.p, gx);
@@ -1961,6 +2017,7 @@ class SimImpl final : public SimBase {
   int z_total_[kMaxLayers] = {0};
   long long z_base_[kMaxLayers] = {0};
   long long rec_z_total_ = 0;
+  mutable std::vector<int> robot_class_;  // env_class: first robot entry of each entry's class
   int smem_p0max_ = 0, smem_dmax_ = 0, smem_amax_ = 0, smem_omax_ = 0, threads_ = 256, n_sm_ = 148, n_ckpt_ = 0;
   int ctas_per_sm_ = 2, resident_ = 1;
   // controller span of the largest robot (elements) and whether the fused
@@ -2052,10 +2109,59 @@ class SimImpl final : public SimBase {
 
 }  // namespace cls
 
+namespace cls {
+
+// The slot scheduler's operations over a served handle (cls_admit /
+// cls_poll): the cls_serve_* primitives on the handle's stream.
+class SimSlotOps final : public SlotOps {
+ public:
+  explicit SimSlotOps(SimBase& s) : s_(s) { s_.sizes(&E_, &nv_, &T_); }
+  int n_slots() const override { return E_; }
+  int max_steps() const override { return T_; }
+  int checkpoint_every() const override { return s_.checkpoint_every(); }
+  int slot_class(int slot) const override { return s_.env_class(slot); }
+  int n_vertices(int slot) const override { return s_.env_vertices(slot); }
+  long long footprint(int slot, int steps, bool grad) const override {
+    return s_.env_footprint(slot, steps, grad);
+  }
+  void reset(int slot, const double* x0, const double* tv, const double* th, const double* tc) override {
+    s_.serve_reset_env(slot, x0 ? x0 : s_.env_objects(slot), nullptr, tv, th, tc);
+  }
+  void forward(const int* w, const int* st) override { s_.serve_forward(w, st); }
+  void backward(const int* w, const int* st) override { s_.serve_backward(w, st); }
+  void loss(const int* st, double* env) override { s_.serve_loss(st, env); }
+  void final_x(int slot, double* x) override { s_.serve_env_state(slot, x, nullptr); }
+  void wait() override {
+    const int rc = s_.synchronize();
+    if (rc != CLS_OK) throw Fail{rc, s_.err};
+  }
+
+ private:
+  SimBase& s_;
+  int E_ = 0, nv_ = 0, T_ = 0;
+};
+
+}  // namespace cls
+
 // ===================================================================== C ABI
 struct cls_sim {
   std::unique_ptr<cls::SimBase> impl;
+  // continuous-batching scheduler, created by the first cls_admit /
+  // cls_serve_tick (declared after impl: destroyed before it)
+  std::unique_ptr<cls::SimSlotOps> slot_ops;
+  std::unique_ptr<cls::SlotScheduler> sched;
+  int tick_segments = 1;
 };
+
+namespace cls {
+static SlotScheduler& scheduler(cls_sim* sim) {
+  if (!sim->sched) {
+    sim->slot_ops.reset(new SimSlotOps(*sim->impl));
+    sim->sched.reset(new SlotScheduler(*sim->slot_ops, sim->tick_segments));
+  }
+  return *sim->sched;
+}
+}  // namespace cls
 
 using cls::Fail;
 
@@ -2264,6 +2370,44 @@ int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* env) {
 }
 int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v) {
   return guarded(sim, [&](cls::SimBase& s) { s.serve_env_state(env, x, v); });
+}
+
+int cls_serve_tick(cls_sim* sim, int32_t tick_segments) {
+  return guarded(sim, [&](cls::SimBase&) {
+    CLS_REQUIRE(tick_segments >= 1, "tick_segments must be >= 1");
+    sim->tick_segments = tick_segments;
+    if (sim->sched) sim->sched->set_rounds(tick_segments);
+  });
+}
+
+int cls_admit(cls_sim* sim, const cls_request* req, int64_t bytes_budget, int32_t* slot) {
+  return guarded(sim, [&](cls::SimBase&) {
+    CLS_REQUIRE(req != nullptr && slot != nullptr, "request and slot are required");
+    *slot = cls::scheduler(sim).admit(req->id, req->robot, req->steps, req->grad != 0, req->x0, req->target_v,
+                                      req->target_h, req->target_c, bytes_budget);
+  });
+}
+
+int cls_poll(cls_sim* sim, uint64_t* done, int32_t capacity, int32_t* n_done, int32_t* n_active) {
+  return guarded(sim, [&](cls::SimBase&) {
+    CLS_REQUIRE(capacity >= 0 && (capacity == 0 || done != nullptr), "done needs capacity entries");
+    cls::SlotScheduler& q = cls::scheduler(sim);
+    q.poll();
+    const int k = q.report(done, capacity);
+    if (n_done) *n_done = k;
+    if (n_active) *n_active = q.active();
+  });
+}
+
+int cls_serve_result(cls_sim* sim, uint64_t id, int32_t* slot, double* loss_terms, double* final_x) {
+  return guarded(sim, [&](cls::SimBase&) {
+    const int s = cls::scheduler(sim).result(id, loss_terms, final_x);
+    if (slot) *slot = s;
+  });
+}
+
+int cls_serve_release(cls_sim* sim, uint64_t id) {
+  return guarded(sim, [&](cls::SimBase&) { cls::scheduler(sim).release(id); });
 }
 
 int cls_simulate(cls_sim* sim, int32_t steps, double* loss) {

@@ -360,6 +360,53 @@ int cls_serve_loss(cls_sim* sim, const int32_t* steps, double* loss_env);
 /* State at the end of the env's last forward window, [n_v][3] each. */
 int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v);
 
+/* ---------------------------------------------------------------------------
+ * Admission and polling (continuous batching in the library).  No reference
+ * counterpart: the reference trains one batch at a time
+ * (multitask/diffphy_trainer.py:219-256); serving.Server is the Python form
+ * of the same scheduler.  Every env of the handle is a slot with a robot
+ * entry (controller) of its own.  A request runs on a free slot of the robot
+ * class of slot `robot` (slots whose robot entries have the same geometry,
+ * spring table, output map and layer widths); cls_admit restarts that slot
+ * alone (cls_serve_reset_env) when the request's HBM footprint (state,
+ * checkpoints, trajectory, observables, targets, controller; reverse records
+ * for gradient queries) fits beside the admitted requests' in bytes_budget
+ * (< 0: no limit), else *slot = -1 and nothing changes.  cls_poll waits for
+ * the tick in flight, applies it (losses at the end of a first pass, the
+ * reverse pass of gradient queries, counted down one checkpoint segment per
+ * round) and issues the next tick: one forward window of tick_segments x
+ * checkpoint_every substeps for every slot in its first pass, then
+ * tick_segments reverse segments for every slot in its reverse pass; it
+ * reports the ids of finished requests (at most `capacity`; the rest at the
+ * next call) and the number of slots still running.  A finished request keeps
+ * its slot -- loss terms, final positions and, for gradient queries, the
+ * slot's weight gradients (cls_get_grads with robot = its slot) -- until
+ * cls_serve_release.  Requests admitted between polls join the next tick.
+ * Invalid ids, steps outside [2, max_steps] or a duplicate id fail with
+ * CLS_ERR_INVALID; a non-finite state or GEMM timeout seen at a tick's end
+ * is reported by cls_poll as by cls_synchronize.
+ * --------------------------------------------------------------------------- */
+typedef struct cls_request {
+  uint64_t id;              /* caller's request id (unique among admitted ones) */
+  int32_t robot;            /* a slot whose robot class the request runs on */
+  int32_t steps;            /* episode steps (cls_forward's `steps`) */
+  int32_t grad;             /* 1: forward + adjoint (weight gradients); 0: forward only */
+  const double* x0;         /* [n_v][3] initial positions; NULL: the robot's objects */
+  const double* target_v;   /* [max_steps][3]; NULL: zeros */
+  const double* target_h;   /* [max_steps]; NULL: zeros */
+  const double* target_c;   /* [max_steps]; NULL: zeros */
+} cls_request;
+/* Checkpoint segments a tick advances every request by (default 1); only
+ * with no tick in flight. */
+int cls_serve_tick(cls_sim* sim, int32_t tick_segments);
+int cls_admit(cls_sim* sim, const cls_request* req, int64_t bytes_budget, int32_t* slot);
+int cls_poll(cls_sim* sim, uint64_t* done, int32_t capacity, int32_t* n_done, int32_t* n_active);
+/* Slot, loss terms [8] (total, velocity, height, pose, rotation, weight,
+ * actuation, crawl; NULL: skipped) and final positions [n_v][3] (NULL:
+ * skipped) of a finished request. */
+int cls_serve_result(cls_sim* sim, uint64_t id, int32_t* slot, double* loss_terms, double* final_x);
+int cls_serve_release(cls_sim* sim, uint64_t id);
+
 /* Targets of one env for t in [t_from, max_steps) (rows tv [T - t_from][3],
  * th, tc [T - t_from]; NULL leaves that field), other times and envs
  * untouched: an interactive client changing its goal while its episode runs

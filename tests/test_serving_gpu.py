@@ -181,3 +181,64 @@ def test_mpm_requests_same_alone_in_mix_and_as_plain_batch():
                 assert rel_err(r.grads["act"], ref_g[0]) < 1e-5
             else:
                 assert r.grads is None
+
+
+@pytest.mark.parametrize("precision,rounds", [(32, 1), (64, 2)])
+def test_library_admission_and_poll_match_plain_batch(precision, rounds):
+    """The library's own scheduler (cls_admit / cls_poll over one handle whose
+    envs are the slots): requests admitted two per poll while earlier ones run
+    give the plain one-env batch's loss, final positions and gradients."""
+    from cls_b200.batch import MassSpringBatch
+    from cls_b200.serving import Request, request_targets
+    types = _types(precision)
+    del types["quad"]              # one handle: every robot of it has the same MLP depth
+    params = _params(400, precision)
+    kinds = ["lat120", "lat120", "lat300", "lat300", "lat120"]
+    b = MassSpringBatch([types[k].robot for k in kinds], list(range(len(kinds))), params)
+    try:
+        rng = np.random.default_rng(9)
+        for k in types:
+            s0 = kinds.index(k)
+            types[k].weights = []
+            for l in range(b.n_layers(s0)):
+                rows, cols = b.layer_shape(s0, l)
+                types[k].weights.append(((rng.random((rows, cols)) * 2 - 1) * np.sqrt(6.0 / cols),
+                                         rng.uniform(-0.1, 0.1, rows)))
+        for slot, k in enumerate(kinds):
+            for l, (W, bias) in enumerate(types[k].weights):
+                b.set_weights(slot, l, W, bias)
+        b.serve_tick(rounds)
+        reqs = [Request("lat120", 260, grad=False, seed=12), Request("lat300", 400, grad=True, seed=13),
+                Request("lat120", 333, grad=True, seed=15), Request("lat300", 75, grad=False, seed=16),
+                Request("lat120", 150, grad=True, seed=17), Request("lat300", 220, grad=True, seed=18),
+                Request("lat120", 2, grad=True, seed=19)]
+        pending = list(range(len(reqs)))
+        results = {}
+        for _ in range(400):
+            for rid in list(pending[:2]):
+                req = reqs[rid]
+                tv, th = request_targets(req.seed, b.T, req.steps, params.turn_period)
+                slot = b.admit(rid, kinds.index(req.kind), req.steps, req.grad, target_v=tv, target_h=th)
+                if slot >= 0:
+                    assert kinds[slot] == req.kind
+                    pending.remove(rid)
+            done, active = b.poll()
+            for rid in done:
+                slot, terms, x = b.serve_result(rid)
+                grads = [b.get_grads(slot, l) for l in range(b.n_layers(slot))] if reqs[rid].grad else None
+                results[rid] = (terms[0], grads, x)
+                b.serve_release(rid)
+            if not pending and active == 0:
+                break
+    finally:
+        b.close()
+    assert sorted(results) == list(range(len(reqs)))
+    tl, tg = (1e-6, 1e-5) if precision == 32 else (1e-10, 1e-10)
+    for rid, req in enumerate(reqs):
+        loss, grads, x = results[rid]
+        ref_loss, ref_grads, ref_x = _plain(types, params, req)
+        assert loss == pytest.approx(ref_loss, rel=tl, abs=1e-12)
+        assert rel_err(x, ref_x) < tl
+        if req.grad:
+            for (gW, gb), (rW, rb) in zip(grads, ref_grads):
+                assert rel_err(gW, rW) < tg and rel_err(gb, rb) < tg
