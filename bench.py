@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad-error", action="store_true",
                     help="skip the FP32-vs-FP64 gradient error block")
+    ap.add_argument("--grad-study", action="store_true",
+                    help="uneven: print the FP32-vs-FP64 gradient error of the workload's median robot "
+                         "against the episode length over seeded input draws (no timing)")
     ap.add_argument("--threads", type=int, default=0,
                     help="threads per CTA of the fused kernels (0: autotuned, see --no-autotune)")
     ap.add_argument("--no-autotune", action="store_true",
@@ -999,9 +1002,83 @@ def run_serve(a):
         torch.distributed.destroy_process_group()
 
 
+def grad_study(a):
+    """How the FP32 gradient's distance from an FP64 build of the same kernels
+    grows with the episode, on the uneven workload's median robot (<= 900
+    vertices), over seeded draws of its inputs:
+
+    * ``fp32_vs_fp64``: per horizon, 8 draws of the initial positions
+      (the rest pose x (1 + 1e-6 u), u ~ U(-1, 1)), every input
+      FP32-representable so that both builds see the same numbers: relative
+      2-norm errors of the weight gradients (worst layer), of d loss / d x0
+      and of the final positions;
+    * ``fp64_sensitivity``: the FP64 gradient's own change under 1e-7
+      relative perturbations of x0 (8 draws), i.e. how well the gradient of
+      the contact model is defined at the level of FP32 rounding."""
+    from cls_b200 import workloads
+    from cls_b200.batch import MassSpringBatch, default_params
+    robots = workloads.uneven_robots()
+    fit = [r for r in robots if r.n_vertices <= 900]
+    med = float(np.median([r.n_vertices for r in robots]))
+    one = min(fit, key=lambda r: abs(r.n_vertices - med))
+
+    def f32(x):
+        return np.asarray(x, np.float64).astype(np.float32).astype(np.float64)
+
+    def rel(x, y):
+        x, y = np.asarray(x, np.float64).ravel(), np.asarray(y, np.float64).ravel()
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+
+    robot = dataclasses.replace(one, objects=f32(one.objects), springs=f32(one.springs))
+
+    def run(prec, steps, x0):
+        b = MassSpringBatch([robot], [0], default_params(**workloads._params(steps, a.checkpoint,
+                                                                             precision=prec)))
+        rng = np.random.default_rng(5)
+        tv, th = workloads.targets(rng, steps, 1)
+        b.set_targets(f32(tv), f32(th))
+        for l in range(len(robot.hidden) + 1):
+            rows, cols = b.layer_shape(0, l)
+            W = (rng.uniform(-1, 1, (rows, cols)) * np.sqrt(6 / cols)).astype(np.float32)
+            b.set_weights(0, l, W.astype(np.float64), np.zeros(rows))
+        b.set_state(x0)
+        b.simulate(steps)
+        g = [b.get_grads(0, l)[0] for l in range(len(robot.hidden) + 1)]
+        gx0 = b.state_grads()[0]
+        xf = b.final_state()[0]
+        b.close()
+        return g, gx0, xf
+
+    pr = np.random.default_rng(77)
+    draws = [f32(robot.objects * (1 + 1e-6 * pr.uniform(-1, 1, robot.objects.shape))) for _ in range(8)]
+    out = {"study": "FP32 vs FP64 gradients against the episode length",
+           "robot": {"vertices": robot.n_vertices, "springs": robot.n_springs,
+                     "hidden": list(robot.hidden), "workload_median_vertices": med},
+           "checkpoint_every": a.checkpoint, "fp32_vs_fp64": [], "fp64_sensitivity": []}
+    for steps in (500, 1000, 1500, 2000):
+        row = {"substeps": steps, "grad_W_rel": [], "grad_x0_rel": [], "final_x_rel": []}
+        for xp in draws:
+            (g32, x32, f32x), (g64, x64, f64x) = run(32, steps, xp), run(64, steps, xp)
+            row["grad_W_rel"].append(max(rel(u, w) for u, w in zip(g32, g64)))
+            row["grad_x0_rel"].append(rel(x32, x64))
+            row["final_x_rel"].append(rel(f32x, f64x))
+        row["within_1e-4"] = sum(e <= 1e-4 for e in row["grad_W_rel"])
+        out["fp32_vs_fp64"].append(row)
+    for steps in (1000, 2000):
+        base = run(64, steps, draws[0])[0]
+        d = []
+        for k in range(8):
+            xp = draws[0] * (1 + 1e-7 * pr.uniform(-1, 1, draws[0].shape))
+            d.append(max(rel(u, w) for u, w in zip(run(64, steps, xp)[0], base)))
+        out["fp64_sensitivity"].append({"substeps": steps, "x0_perturbation": 1e-7, "grad_W_rel": d})
+    print(json.dumps(out))
+
+
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.grad_study:
+        grad_study(a)
+    elif a.impl == "reference":
         run_reference(a)
     elif a.config == "mpm":
         run_mpm(a)

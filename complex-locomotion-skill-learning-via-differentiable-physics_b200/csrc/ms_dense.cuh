@@ -128,7 +128,7 @@ ms_step_rev_kernel(MsArgs<R> a, int t_post, int t_pre, int t_begin, int t_end, i
   if (t_post >= 0) {
     const int kk = t_post - t_begin;
     const V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
-    for (int i = tid; i < N; i += nt) s.xs[i] = rx[i];
+    for (int i = tid; i < N; i += nt) s.xv.lo[i] = rx[i];  // x(t_post) only: rev_post reads p
     const R* dp = a.din + (size_t)3 * ed.v_off;
     for (int q = tid; q < 3 * N; q += nt) s.bufA[q] = dp[q];
     __syncthreads();

@@ -207,9 +207,9 @@ struct MsArgs {
 // ------------------------------------------------------------ shared memory
 // reduction scratch: 8 values x 32 warps, then 32 ints for arg-reductions;
 // the forward pass's fused observable reduction (11 sums and two extrema with
-// their indices per warp) takes kRedFwd.  The reverse pass keeps kRed: its
-// shared memory sits just under the 196 KB carveout step for the largest
-// benchmark robot, where 768 more bytes leave it 32 KB less L1.
+// their indices per warp) takes kRedFwd.  The reverse pass keeps kRed: with
+// its packed vertex rows its shared memory (155 KB for the largest
+// benchmark robot) sits under the 164 KB carveout step.
 constexpr int kRed = 320;
 constexpr int kRedFwd = 512;
 constexpr int kRedInt = 256;
@@ -257,14 +257,57 @@ __host__ __device__ inline size_t fwd_smem_bytes(int nmax, int dmax, int p0max, 
          rb(sizeof(R) * kRedFwd) + rb(nmax) + (imp_cap ? rb(sizeof(V4<R>) * imp_cap) : 0);
 }
 
-// Reverse-pass shared memory.  gvinc (v_inc, then its adjoint) is live only
-// from the v_inc recompute to the end of the spring adjoint; dz and part are
-// live only in the MLP adjoint that follows, so they share one region.
+// Two 3-vectors p, q of a vertex in 6 values of shared memory: lo[i] =
+// {p.x, p.y, p.z, q.x} (one 16-byte access in FP32), hi[i] = {q.y, q.z} (one
+// 8-byte access).  A row costs 24 bytes instead of two 16-byte rows, with the
+// same number of shared-memory accesses when both vectors are read.
+template <typename R>
+struct alignas(2 * sizeof(R)) V2 {
+  R x, y;
+};
+template <typename R>
+struct PairRows {
+  V4<R>* lo;
+  V2<R>* hi;
+  __device__ __forceinline__ V4<R> p(int i) const {
+    V4<R> u = lo[i];
+    u.w = 0;
+    return u;
+  }
+  __device__ __forceinline__ void get(int i, V4<R>& pv, V4<R>& qv) const {
+    const V4<R> u = lo[i];
+    const V2<R> h = hi[i];
+    pv.x = u.x; pv.y = u.y; pv.z = u.z; pv.w = 0;
+    qv.x = u.w; qv.y = h.x; qv.z = h.y; qv.w = 0;
+  }
+  __device__ __forceinline__ void set(int i, const V4<R>& pv, const V4<R>& qv) const {
+    V4<R> u;
+    u.x = pv.x; u.y = pv.y; u.z = pv.z; u.w = qv.x;
+    V2<R> h;
+    h.x = qv.y; h.y = qv.z;
+    lo[i] = u;
+    hi[i] = h;
+  }
+  // p of row i += d (q unchanged)
+  __device__ __forceinline__ void add_p(int i, R d0, R d1, R d2) const {
+    V4<R> u = lo[i];
+    u.x += d0; u.y += d1; u.z += d2;
+    lo[i] = u;
+  }
+};
+
+// Reverse-pass shared memory.  xv holds x(t), v(t) of the substep being
+// reversed, g the adjoint state (d x, d v).  io holds the controller outputs
+// [0, omax) and d loss / d output [obuf, obuf + omax) up to the output layer's
+// dz, then the transposed products (d loss / d layer input; 3 N position
+// columns for layer 0).  gvinc (v_inc, then its adjoint) is live only from
+// the v_inc recompute to the end of the spring adjoint; dz and part are live
+// only in the MLP adjoint that follows, so they share one region.
 template <typename R>
 struct RevSmem {
-  V4<R>* xs; V4<R>* vs; V4<R>* gx; V4<R>* gv;
+  PairRows<R> xv, g;
   R* bufA;         // controller outputs, then the transposed products
-  R* bufB;         // d loss / d output
+  R* bufB;         // d loss / d output (inside the same region as bufA)
   V4<R>* gvinc;    // union region, vertex phase
   R* dz;           // union region, MLP phase
   V4<R>* part;     // union region, MLP phase: blockDim partials
@@ -281,17 +324,25 @@ __host__ __device__ inline size_t rev_union_bytes(int nmax, int dmax, int thread
   return vert > mlp ? vert : mlp;
 }
 
+// offset of d loss / d output inside the outputs / products region, and the
+// region's size in values
+__host__ __device__ inline int rev_obuf(int omax) { return (omax + 63) & ~63; }
+__host__ __device__ inline int rev_io_values(int amax, int omax) {
+  const int o2 = rev_obuf(omax) + omax;
+  return amax > o2 ? amax : o2;
+}
+
 template <typename R>
 __device__ __forceinline__ RevSmem<R> carve_rev(char* base, const MsArgs<R>& a) {
   RevSmem<R> s;
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base + off; off += (bytes + 255) & ~size_t(255); return p; };
-  s.xs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
-  s.vs = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
-  s.gx = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
-  s.gv = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
-  s.bufA = (R*)take(sizeof(R) * a.smem_amax);
-  s.bufB = (R*)take(sizeof(R) * a.smem_omax);
+  s.xv.lo = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.xv.hi = (V2<R>*)take(sizeof(V2<R>) * a.smem_nmax);
+  s.g.lo = (V4<R>*)take(sizeof(V4<R>) * a.smem_nmax);
+  s.g.hi = (V2<R>*)take(sizeof(V2<R>) * a.smem_nmax);
+  s.bufA = (R*)take(sizeof(R) * rev_io_values(a.smem_amax, a.smem_omax));
+  s.bufB = s.bufA + rev_obuf(a.smem_omax);
   s.red = (R*)take(sizeof(R) * kRed);
   char* u = take(rev_union_bytes<R>(a.smem_nmax, a.smem_dmax, blockDim.x));
   s.gvinc = (V4<R>*)u;
@@ -307,7 +358,7 @@ template <typename R>
 __host__ __device__ inline size_t rev_smem_bytes(int nmax, int amax, int omax, int dmax, int threads,
                                                 size_t adj_cap) {
   auto rb = [](size_t b) { return (b + 255) & ~size_t(255); };
-  return 4 * rb(sizeof(V4<R>) * nmax) + rb(sizeof(R) * amax) + rb(sizeof(R) * omax) +
+  return 2 * (rb(sizeof(V4<R>) * nmax) + rb(sizeof(V2<R>) * nmax)) + rb(sizeof(R) * rev_io_values(amax, omax)) +
          rb(sizeof(R) * kRed) + rev_union_bytes<R>(nmax, dmax, threads) +
          (adj_cap ? rb(2 * sizeof(V4<R>) * adj_cap) : 0);
 }

@@ -609,15 +609,18 @@ __device__ __forceinline__ R spring_gact(R gact, R act, R act_seed_scale, R act_
 }
 
 template <typename R>
-__device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc<R>& in, int v, const V4<R>* xs,
-                                                   const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
-                                                   R act_seed_scale, R act_lim, bool act_seed, R (&gxs)[3],
-                                                   R (&gvs)[3]) {
+__device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc<R>& in, int v,
+                                                   const PairRows<R>& xv, const V4<R>* gvinc, const R* outv,
+                                                   R* gout, R act_seed_scale, R act_lim, bool act_seed,
+                                                   R (&gxs)[3], R (&gvs)[3]) {
   const int o = in.other;
   const int ia = in.side == 0 ? v : o, ib = in.side == 0 ? o : v;
   const R act = in.out >= 0 ? outv[in.out] : R(0);
-  const SpringAdj<R> t = spring_adjoint_terms<R>(a, xs[ia], xs[ib], vs[ia], vs[ib], gvinc[ia], gvinc[ib], act,
-                                                 in.l0, in.k, in.coef);
+  V4<R> xa, va, xb, vb;
+  xv.get(ia, xa, va);
+  xv.get(ib, xb, vb);
+  const SpringAdj<R> t = spring_adjoint_terms<R>(a, xa, xb, va, vb, gvinc[ia], gvinc[ib], act, in.l0, in.k,
+                                                 in.coef);
   if (in.side == 0) {
     gxs[0] += t.gd0; gxs[1] += t.gd1; gxs[2] += t.gd2;
     gvs[0] += t.h0; gvs[1] += t.h1; gvs[2] += t.h2;
@@ -634,17 +637,20 @@ __device__ __forceinline__ void spring_adjoint_one(const MsArgs<R>& a, const Inc
 // the table (same lanes, same order).  For robots whose table fits in shared
 // memory, in the fused reverse kernel (MsArgs::adj_cap).
 template <typename R>
-__device__ __forceinline__ void spring_adjoint_table(const MsArgs<R>& a, const RobotDesc& rb, const V4<R>* xs,
-                                                     const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
-                                                     V4<R>* adj, V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
-                                                     bool act_seed) {
+__device__ __forceinline__ void spring_adjoint_table(const MsArgs<R>& a, const RobotDesc& rb,
+                                                     const PairRows<R>& xv, const V4<R>* gvinc, const R* outv,
+                                                     R* gout, V4<R>* adj, const PairRows<R>& gs,
+                                                     R act_seed_scale, R act_lim, bool act_seed) {
   const unsigned long long pol = policy_evict_last();
   for (int sp = threadIdx.x; sp < rb.n_s; sp += blockDim.x) {
     const int4 ab = ldg_i4_hint(a.spr_ab + rb.spr_off + sp, pol);
     const V4<R> f = ldg4_hint<R>(a.spr_p + rb.spr_off + sp, pol);
     const R act = ab.z >= 0 ? outv[ab.z] : R(0);
-    const SpringAdj<R> t = spring_adjoint_terms<R>(a, xs[ab.x], xs[ab.y], vs[ab.x], vs[ab.y], gvinc[ab.x],
-                                                   gvinc[ab.y], act, f.x, f.y, f.z);
+    V4<R> xa, va, xb, vb;
+    xv.get(ab.x, xa, va);
+    xv.get(ab.y, xb, vb);
+    const SpringAdj<R> t = spring_adjoint_terms<R>(a, xa, xb, va, vb, gvinc[ab.x], gvinc[ab.y], act, f.x, f.y,
+                                                   f.z);
     V4<R> g; g.x = t.gd0; g.y = t.gd1; g.z = t.gd2; g.w = 0;
     V4<R> h; h.x = t.h0; h.y = t.h1; h.z = t.h2; h.w = 0;
     adj[2 * sp] = g;
@@ -682,11 +688,11 @@ __device__ __forceinline__ void spring_adjoint_table(const MsArgs<R>& a, const R
       }
     }
     if (l16 == 0 && v < N) {
-      V4<R> x = gx[v], w = gv[v];
+      V4<R> x, w;
+      gs.get(v, x, w);
       x.x += gxs[0]; x.y += gxs[1]; x.z += gxs[2];
       w.x += gvs[0]; w.y += gvs[1]; w.z += gvs[2];
-      gx[v] = x;
-      gv[v] = w;
+      gs.set(v, x, w);
     }
   }
 }
@@ -701,10 +707,10 @@ __device__ __forceinline__ void spring_adjoint_table(const MsArgs<R>& a, const R
 #define CLS_ADJ_U 2
 #endif
 template <typename R>
-__device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const RobotDesc& rb, const V4<R>* xs,
-                                                      const V4<R>* vs, const V4<R>* gvinc, const R* outv, R* gout,
-                                                      V4<R>* gx, V4<R>* gv, R act_seed_scale, R act_lim,
-                                                      bool act_seed) {
+__device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const RobotDesc& rb,
+                                                      const PairRows<R>& xv, const V4<R>* gvinc, const R* outv,
+                                                      R* gout, const PairRows<R>& gs, R act_seed_scale,
+                                                      R act_lim, bool act_seed) {
   constexpr int U = CLS_ADJ_U;
   const unsigned long long pol = policy_evict_last();
   const int lane = threadIdx.x & 31, wid = (threadIdx.x >> 5), nw = (blockDim.x >> 5);
@@ -732,10 +738,10 @@ __device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const 
       if (v < N) {
         int q = beg[k] + l16;
         if (q < end[k])
-          spring_adjoint_one<R>(a, first[k], v, xs, vs, gvinc, outv, gout, act_seed_scale, act_lim, act_seed,
-                                gxs, gvs);
+          spring_adjoint_one<R>(a, first[k], v, xv, gvinc, outv, gout, act_seed_scale, act_lim, act_seed, gxs,
+                                gvs);
         for (q += 16; q < end[k]; q += 16)
-          spring_adjoint_one<R>(a, load_inc<R>(a, rb, q, pol), v, xs, vs, gvinc, outv, gout, act_seed_scale,
+          spring_adjoint_one<R>(a, load_inc<R>(a, rb, q, pol), v, xv, gvinc, outv, gout, act_seed_scale,
                                 act_lim, act_seed, gxs, gvs);
       }
 #pragma unroll
@@ -747,11 +753,11 @@ __device__ __forceinline__ void spring_adjoint_gather(const MsArgs<R>& a, const 
         }
       }
       if (l16 == 0 && v < N) {
-        V4<R> x = gx[v], w = gv[v];
+        V4<R> x, w;
+        gs.get(v, x, w);
         x.x += gxs[0]; x.y += gxs[1]; x.z += gxs[2];
         w.x += gvs[0]; w.y += gvs[1]; w.z += gvs[2];
-        gx[v] = x;
-        gv[v] = w;
+        gs.set(v, x, w);
       }
     }
   }
@@ -778,7 +784,7 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     const V4<R>* rv = a.rec_v + (size_t)kslot * a.v_total + ed.v_off;
     // with v_inc[t] as recorded by the forward pass (into gvinc as scratch)
     const V4<R>* rvi = a.rec_vinc + (size_t)kslot * a.v_total + ed.v_off;
-    for (int i = tid; i < N; i += nt) { s.xs[i] = rx[i]; s.vs[i] = rv[i]; s.gvinc[i] = rvi[i]; }
+    for (int i = tid; i < N; i += nt) { s.xv.set(i, rx[i], rv[i]); s.gvinc[i] = rvi[i]; }
     for (int o = tid; o < nout; o += nt) {
       s.bufA[o] = act_f<R>(a.act_out, zl[o] + bout[o]);
       s.bufB[o] = 0;
@@ -787,8 +793,10 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
   __syncthreads();
   // adjoint of advance_toi(t + 1)
   for (int i = tid; i < N; i += nt) {
-    const V4<R> x = s.xs[i], v = s.vs[i], vi = s.gvinc[i];
-    const V4<R> gx1 = s.gx[i], gv1 = s.gv[i];
+    V4<R> x, v, gx1, gv1;
+    s.xv.get(i, x, v);
+    s.g.get(i, gx1, gv1);
+    const V4<R> vi = s.gvinc[i];
     R ov0 = a.drag_s * v.x + vi.x;
     R ov1 = a.drag_s * v.y + a.dt * a.gravity + vi.y;
     R ov2 = a.drag_s * v.z + vi.z;
@@ -822,8 +830,7 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     V4<R> gx0; gx0.x = gox0; gx0.y = gox1; gx0.z = gox2; gx0.w = 0;
     V4<R> gv0; gv0.x = a.drag_s * gov0; gv0.y = a.drag_s * gov1; gv0.z = a.drag_s * gov2; gv0.w = 0;
     V4<R> gvi; gvi.x = gov0; gvi.y = gov1; gvi.z = gov2; gvi.w = 0;
-    s.gx[i] = gx0;
-    s.gv[i] = gv0;
+    s.g.set(i, gx0, gv0);
     s.gvinc[i] = gvi;
   }
   __syncthreads();
@@ -835,11 +842,9 @@ __device__ __forceinline__ void rev_pre(const MsArgs<R>& a, const RobotDesc& rb,
     const R lim = act_seed ? dpow_half<R>(dabs<R>(a.tv[o].x) / R(0.08)) : R(0);
     const R act_scale = R(10) / R(st_e) / Br / R(rb.n_s);
     if (s.adj)
-      spring_adjoint_table<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.adj, s.gx, s.gv, act_scale, lim,
-                              act_seed);
+      spring_adjoint_table<R>(a, rb, s.xv, s.gvinc, s.bufA, s.bufB, s.adj, s.g, act_scale, lim, act_seed);
     else
-      spring_adjoint_gather<R>(a, rb, s.xs, s.vs, s.gvinc, s.bufA, s.bufB, s.gx, s.gv, act_scale, lim,
-                               act_seed);
+      spring_adjoint_gather<R>(a, rb, s.xv, s.gvinc, s.bufA, s.bufB, s.g, act_scale, lim, act_seed);
   }
   __syncthreads();
   // adjoint of the MLP's output activation
@@ -872,18 +877,12 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
       const R g0 = s.bufA[3 * i] / R(0.2), g1 = s.bufA[3 * i + 1] / R(0.2), g2 = s.bufA[3 * i + 2] / R(0.2);
       R gxi[3] = {g0, g1, g2};
       gc[0] -= g0; gc[1] -= g1; gc[2] -= g2;
-      if (a.x_full) seed_x_rotation_pose<R>(a, rb, ed, t, e, i, s.xs[i], Br, gxi, gc);
-      V4<R> g = s.gx[i];
-      g.x += gxi[0]; g.y += gxi[1]; g.z += gxi[2];
-      s.gx[i] = g;
+      if (a.x_full) seed_x_rotation_pose<R>(a, rb, ed, t, e, i, s.xv.p(i), Br, gxi, gc);
+      s.g.add_p(i, gxi[0], gxi[1], gxi[2]);
     }
     block_sum<R, 3>(gc, s.red);
     apply_center_velocity<R>(vseed, gc);
-    for (int i = tid; i < N; i += nt) {
-      V4<R> g = s.gx[i];
-      g.x += gc[0] * invN; g.y += gc[1] * invN; g.z += gc[2] * invN;
-      s.gx[i] = g;
-    }
+    for (int i = tid; i < N; i += nt) s.g.add_p(i, gc[0] * invN, gc[1] * invN, gc[2] * invN);
   }
   // adjoint of compute_height (running max of the lowest point) and upper height
   if (a.loss_mask & (LOSS_HEIGHT | LOSS_CRAWL)) {
@@ -893,7 +892,7 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
     if (gh != R(0)) {
       R lo = R(10); int li = -1;
       for (int i = tid; i < N; i += nt) {
-        const R y = s.xs[i].y;
+        const R y = s.xv.lo[i].y;
         if (!(lo < y)) { lo = y; li = i; }
       }
       block_argext<R>(lo, li, true, s.red, redi);
@@ -902,16 +901,16 @@ __device__ __forceinline__ void rev_post(const MsArgs<R>& a, const RobotDesc& rb
         const R prev = a.obs_height[(size_t)(t - 1) * a.n_envs + e];
         if (lo < prev) { hcarry = gh; gmin = 0; }
       }
-      if (tid == 0 && li >= 0 && gmin != R(0)) s.gx[li].y += gmin;
+      if (tid == 0 && li >= 0 && gmin != R(0)) s.g.lo[li].y += gmin;
     }
     if (gu != R(0)) {
       R hi = R(-10); int hix = -1;
       for (int i = tid; i < N; i += nt) {
-        const R y = s.xs[i].y;
+        const R y = s.xv.lo[i].y;
         if (!(y < hi)) { hi = y; hix = i; }
       }
       block_argext<R>(hi, hix, false, s.red, redi);
-      if (tid == 0 && hix >= 0) s.gx[hix].y += gu;
+      if (tid == 0 && hix >= 0) s.g.lo[hix].y += gu;
     }
   }
   __syncthreads();
@@ -936,11 +935,10 @@ __device__ __forceinline__ void rev_load_carry(const MsArgs<R>& a, const RobotDe
       }
       V4<R> g; g.x = gxi[0]; g.y = gxi[1]; g.z = gxi[2]; g.w = 0;
       V4<R> z; z.x = z.y = z.z = z.w = 0;
-      s.gx[i] = g;
-      s.gv[i] = z;
+      s.g.set(i, g, z);
     }
   } else {
-    for (int i = tid; i < N; i += nt) { s.gx[i] = a.adj_x[ed.v_off + i]; s.gv[i] = a.adj_v[ed.v_off + i]; }
+    for (int i = tid; i < N; i += nt) s.g.set(i, a.adj_x[ed.v_off + i], a.adj_v[ed.v_off + i]);
     hcarry = a.adj_h[e];
   }
   __syncthreads();
@@ -951,8 +949,10 @@ __device__ __forceinline__ void rev_store_carry(const MsArgs<R>& a, const RobotD
                                                 const RevSmem<R>& s, int e, R hcarry) {
   const int tid = threadIdx.x, nt = blockDim.x, N = rb.n_v;
   for (int i = tid; i < N; i += nt) {
-    a.adj_x[ed.v_off + i] = s.gx[i];
-    a.adj_v[ed.v_off + i] = s.gv[i];
+    V4<R> gx, gv;
+    s.g.get(i, gx, gv);
+    a.adj_x[ed.v_off + i] = gx;
+    a.adj_v[ed.v_off + i] = gv;
   }
   if (tid == 0) a.adj_h[e] = hcarry;
   __syncthreads();
