@@ -184,6 +184,7 @@ class SimBase {
   // vertex count, rest pose and the footprint of a request on it
   virtual int env_class(int ue) const = 0;
   virtual int env_vertices(int ue) const = 0;
+  virtual bool env_own_robot(int ue) const = 0;
   virtual const double* env_objects(int ue) const = 0;
   virtual long long env_footprint(int ue, int steps, bool grad) const = 0;
   virtual int checkpoint_every() const = 0;
@@ -1912,6 +1913,7 @@ class SimImpl final : public SimBase {
            a.stiff == b.stiff && a.coef == b.coef;
   }
   int env_vertices(int ue) const override { return hr_[ed_host_[ienv(ue)].robot].n_v; }
+  bool env_own_robot(int ue) const override { return rd_host_[ed_host_[ienv(ue)].robot].n_env == 1; }
   const double* env_objects(int ue) const override { return hr_[ed_host_[ienv(ue)].robot].objects.data(); }
   // HBM bytes a request keeps resident while it is served (the terms of
   // serving.footprint_bytes over this handle's own layer widths, the input
@@ -2121,6 +2123,7 @@ class SimSlotOps final : public SlotOps {
   int checkpoint_every() const override { return s_.checkpoint_every(); }
   int slot_class(int slot) const override { return s_.env_class(slot); }
   int n_vertices(int slot) const override { return s_.env_vertices(slot); }
+  bool own_controller(int slot) const override { return s_.env_own_robot(slot); }
   long long footprint(int slot, int steps, bool grad) const override {
     return s_.env_footprint(slot, steps, grad);
   }

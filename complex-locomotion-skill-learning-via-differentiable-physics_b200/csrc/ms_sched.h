@@ -35,6 +35,7 @@ struct SlotOps {
   virtual int checkpoint_every() const = 0;
   virtual int slot_class(int slot) const = 0;     // slots of one class run the same robot
   virtual int n_vertices(int slot) const = 0;
+  virtual bool own_controller(int slot) const = 0;  // no other env shares the slot's robot entry
   virtual long long footprint(int slot, int steps, bool grad) const = 0;
   virtual void reset(int slot, const double* x0, const double* tv, const double* th, const double* tc) = 0;
   virtual void forward(const int* windows, const int* steps) = 0;   // [n_slots][4], [n_slots]
@@ -81,6 +82,8 @@ class SlotScheduler {
     for (int i = 0; i < n && pick < 0; ++i)
       if (slots_[i].phase == FREE && ops_.slot_class(i) == cls) pick = i;
     if (pick < 0) return -1;
+    if (grad && !ops_.own_controller(pick))
+      throw SchedError("gradient queries need a slot whose robot entry (controller) no other env shares");
     const long long fp = ops_.footprint(pick, steps, grad);
     if (budget >= 0 && used_bytes_ + fp > budget) return -1;
     ops_.reset(pick, x0, tv, th, tc);

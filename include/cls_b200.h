@@ -382,7 +382,8 @@ int cls_serve_env_state(cls_sim* sim, int32_t env, double* x, double* v);
  * its slot -- loss terms, final positions and, for gradient queries, the
  * slot's weight gradients (cls_get_grads with robot = its slot) -- until
  * cls_serve_release.  Requests admitted between polls join the next tick.
- * Invalid ids, steps outside [2, max_steps] or a duplicate id fail with
+ * Invalid ids, steps outside [2, max_steps], a duplicate id or a gradient
+ * query on a slot whose robot entry other envs share fail with
  * CLS_ERR_INVALID; a non-finite state or GEMM timeout seen at a tick's end
  * is reported by cls_poll as by cls_synchronize.
  * --------------------------------------------------------------------------- */

@@ -7,7 +7,8 @@
 //   poll                                         -> launches, then {"done": [...], "active": a}
 //   result <id>                                  -> {"result": id, "slot": s, "terms": [...], "x": [...]}
 //   release <id> | rounds <n>                    -> {"ok": 1}
-// Failures print {"error": "..."}.  The fake's footprint is
+// Failures print {"error": "..."}.  A negative class marks slots whose
+// robot entry other slots share (no gradient queries).  The fake's footprint is
 // steps x (3 with gradients, else 1) + 1000 x slot class; its loss terms are
 // k + 10 x slot + 0.001 x steps; its final positions are (slot, steps, k).
 #include <cstdio>
@@ -30,6 +31,7 @@ struct FakeOps final : cls::SlotOps {
   int checkpoint_every() const override { return K; }
   int slot_class(int s) const override { return cls_[s]; }
   int n_vertices(int) const override { return 2; }
+  bool own_controller(int s) const override { return cls_[s] >= 0; }
   long long footprint(int s, int steps, bool grad) const override {
     return (long long)steps * (grad ? 3 : 1) + 1000LL * cls_[s];
   }

@@ -155,3 +155,15 @@ def test_errors_results_and_release(driver):
     fw = [o["forward"] for o in out if "forward" in o]
     assert fw == [[[0, 0, 50, 0, 0, 60]], [[0, 50, 59, 1, 0, 60]]]
     assert [o for o in out if "loss" in o] == [{"loss": [[0, 60]]}]
+
+
+def test_gradient_queries_need_a_controller_of_their_own(driver):
+    # slots 0 and 1 share one robot entry (class -1 in the fake), slot 2 does not
+    out = run(driver, [-1, -1, 0], 200, 50, 1, [
+        "admit 1 0 100 1 -1",     # gradient query on a shared controller: refused
+        "admit 2 0 100 0 -1",     # forward-only: fine
+        "admit 3 2 100 1 -1",     # own controller: fine
+    ])
+    assert [o for o in out if "error" in o] == [
+        {"error": "gradient queries need a slot whose robot entry (controller) no other env shares"}]
+    assert [o["slot"] for o in out if "admit" in o] == [0, 2]
