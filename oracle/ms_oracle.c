@@ -89,6 +89,41 @@ typedef struct {
 
 /* ---------------------------------------------------------------- helpers */
 #define IX3(p, t, k, i) (((((size_t)(t) * (p)->B + (k)) * (p)->N) + (i)) * 3)
+
+/* Precision-study hooks, compiled only into libms_oracle_study.so
+ * (-DORC_STUDY; tests/study_fp32_state.py drives them).  They model an
+ * implementation that computes in FP64 but stores chosen fields in FP32
+ * (ST_* bits of st_round: the value written is rounded to the nearest float),
+ * optionally keeps the positions exactly while every reader sees the rounded
+ * copy (ST_X_EXACT: a compensated position update), and records or forces
+ * the contact decisions of advance_toi.  Without ORC_STUDY every hook is the
+ * identity and the oracle is the plain FP64 restatement. */
+enum { ST_X = 1, ST_V = 2, ST_VINC = 4, ST_MLP = 8, ST_INPUT = 16, ST_ADJ = 32, ST_WSUM = 64,
+       ST_X_EXACT = 128 };
+#ifdef ORC_STUDY
+static int st_round = 0;
+static unsigned char* st_flags = NULL; /* [T][B][N] contact decisions */
+static int st_flag_mode = 0;           /* 1: record, 2: force */
+static double* st_xe = NULL;           /* [T][B][N][3] exact positions (ST_X_EXACT) */
+void orc_study_set(int round_bits, unsigned char* flags, int flag_mode, double* x_exact) {
+  st_round = round_bits;
+  st_flags = flags;
+  st_flag_mode = flags ? flag_mode : 0;
+  st_xe = x_exact;
+}
+#define ST_ROUND(bit, v) ((st_round & (bit)) ? (double)(float)(v) : (v))
+static int st_contact(const orc_ms* p, int t, int k, int i, int hit, int forward) {
+  size_t f = ((size_t)t * p->B + k) * p->N + i;
+  if (st_flag_mode == 2 || (st_flag_mode == 1 && !forward)) return st_flags[f];
+  if (st_flag_mode == 1) st_flags[f] = (unsigned char)hit;
+  return hit;
+}
+#define ST_XE(p, t, k, i) ((st_round & ST_X_EXACT) ? st_xe + IX3(p, t, k, i) : p->x + IX3(p, t, k, i))
+#else
+#define ST_ROUND(bit, v) (v)
+#define st_contact(p, t, k, i, hit, fw) (hit)
+#define ST_XE(p, t, k, i) (p->x + IX3(p, t, k, i))
+#endif
 #define IC3(p, t, k) ((((size_t)(t) * (p)->B) + (k)) * 3)
 #define IB(p, t, k) (((size_t)(t) * (p)->B) + (k))
 #define IS(p, t, k, s) ((((size_t)(t) * (p)->B + (k)) * (p)->S) + (s))
@@ -117,6 +152,7 @@ static void k_center(const orc_ms* p, int t, int k) {
   c[0] = c[1] = c[2] = 0.0;
   for (int i = 0; i < p->N; ++i)
     for (int d = 0; d < 3; ++d) c[d] += p->x[IX3(p, t, k, i) + d] / p->N;
+  for (int d = 0; d < 3; ++d) c[d] = ST_ROUND(ST_INPUT, c[d]);
 }
 
 /* compute_height: multitask/solver_mass_spring.py:158-173 */
@@ -165,7 +201,7 @@ static void k_nn_input(const orc_ms* p, int t, int k, int offset) {
   for (int j = 0; j < p->N; ++j) {
     const double* xj = p->x + IX3(p, t, k, j);
     for (int d = 0; d < 3; ++d) {
-      in[j * 6 + p->n_sin + d] = (xj[d] - c[d]) / 0.2;
+      in[j * 6 + p->n_sin + d] = ST_ROUND(ST_INPUT, (xj[d] - c[d]) / 0.2);
       in[j * 6 + p->n_sin + 3 + d] = 0.0;
     }
   }
@@ -193,8 +229,8 @@ static void k_mlp(const orc_ms* p, int t, int k, double* scratch_a, double* scra
       double s = 0.0;
       const double* w = p->W[l] + (size_t)i * nin;
       for (int j = 0; j < nin; ++j) s += w[j] * a_prev[j];
-      z[i] = s;
-      a_next[i] = actf(last ? p->act_out : p->act_hidden, s + p->b[l][i]);
+      z[i] = ST_ROUND(ST_MLP, s);
+      a_next[i] = ST_ROUND(ST_MLP, actf(last ? p->act_out : p->act_hidden, z[i] + p->b[l][i]));
     }
     a_prev = a_next;
   }
@@ -230,6 +266,10 @@ static void k_spring(const orc_ms* p, int t, int k) {
       ib[d] += imp;
     }
   }
+#ifdef ORC_STUDY
+  if (st_round & ST_VINC)
+    for (int i = 0; i < 3 * p->N; ++i) p->v_inc[IX3(p, t, k, 0) + i] = ST_ROUND(ST_VINC, p->v_inc[IX3(p, t, k, 0) + i]);
+#endif
 }
 
 /* advance_toi: multitask/solver_mass_spring.py:117-148; writes step t from t-1 */
@@ -237,14 +277,14 @@ static void k_advance(const orc_ms* p, int t, int k) {
   double s = exp(-p->dt * p->drag);
   for (int i = 0; i < p->N; ++i) {
     const double* v0 = p->v + IX3(p, t - 1, k, i);
-    const double* x0 = p->x + IX3(p, t - 1, k, i);
+    const double* x0 = ST_XE(p, t - 1, k, i);
     const double* vi = p->v_inc + IX3(p, t - 1, k, i);
     double ov[3], nv[3], nx[3];
     for (int d = 0; d < 3; ++d) ov[d] = s * v0[d] + (d == 1 ? p->dt * p->gravity : 0.0) + vi[d];
     double toi = 0.0;
     for (int d = 0; d < 3; ++d) nv[d] = ov[d];
     double nx1 = x0[1] + p->dt * ov[1];
-    if (nx1 < p->ground && ov[1] < -1e-4) {
+    if (st_contact(p, t, k, i, nx1 < p->ground && ov[1] < -1e-4, 1)) {
       toi = -(x0[1] - p->ground) / ov[1];
       double f = p->friction * (-ov[1]);
       nv[1] = 0.0;
@@ -254,7 +294,11 @@ static void k_advance(const orc_ms* p, int t, int k) {
     for (int d = 0; d < 3; ++d) nx[d] = x0[d] + toi * ov[d] + (p->dt - toi) * nv[d];
     double* v1 = p->v + IX3(p, t, k, i);
     double* x1 = p->x + IX3(p, t, k, i);
-    for (int d = 0; d < 3; ++d) { v1[d] = nv[d]; x1[d] = nx[d]; }
+    for (int d = 0; d < 3; ++d) { v1[d] = ST_ROUND(ST_V, nv[d]); x1[d] = ST_ROUND(ST_X, nx[d]); }
+#ifdef ORC_STUDY
+    if (st_round & ST_X_EXACT)
+      for (int d = 0; d < 3; ++d) { st_xe[IX3(p, t, k, i) + d] = nx[d]; x1[d] = (double)(float)nx[d]; }
+#endif
   }
 }
 
@@ -525,7 +569,7 @@ static void a_advance(const orc_ms* p, int t, int k) {
     double toi = 0.0;
     for (int d = 0; d < 3; ++d) nv[d] = ov[d];
     double nx1 = x0[1] + p->dt * ov[1];
-    int hit = (nx1 < p->ground && ov[1] < -1e-4);
+    int hit = st_contact(p, t, k, i, nx1 < p->ground && ov[1] < -1e-4, 0);
     double f = 0.0;
     if (hit) {
       toi = -(x0[1] - p->ground) / ov[1];
@@ -762,6 +806,21 @@ int orc_ms_backward(const orc_ms* p, int steps) {
         a_nn_input(p, t, k);
         a_height(p, t, k);
         a_center(p, t, k);
+#ifdef ORC_STUDY
+        if (st_round & ST_ADJ)
+          for (int i = 0; i < 3 * p->N; ++i) {
+            size_t o = IX3(p, t, k, 0) + i;
+            p->gx[o] = ST_ROUND(ST_ADJ, p->gx[o]);
+            p->gv[o] = ST_ROUND(ST_ADJ, p->gv[o]);
+            p->gv_inc[o] = ST_ROUND(ST_ADJ, p->gv_inc[o]);
+          }
+        if (st_round & ST_WSUM)
+          for (int l = 0; l < L; ++l) {
+            size_t n = (size_t)p->width[l + 1] * p->width[l];
+            for (size_t e = 0; e < n; ++e) gWt[l][e] = ST_ROUND(ST_WSUM, gWt[l][e]);
+            for (int e = 0; e < p->width[l + 1]; ++e) gbt[l][e] = ST_ROUND(ST_WSUM, gbt[l][e]);
+          }
+#endif
       }
     }
     free(ga_cur);

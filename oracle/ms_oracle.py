@@ -83,6 +83,33 @@ def library():
     return lib
 
 
+_study = None
+
+
+def study_library():
+    """The oracle built with its precision-study hooks (``make study``:
+    ``-DORC_STUDY``), for tests/study_fp32_state.py.  ``orc_study_set(bits,
+    flags, flag_mode, x_exact)`` selects the FP32-stored fields (the ST_* bits
+    of ms_oracle.c), the contact-decision array ([T][B][N] uint8; mode 1
+    records, 2 forces) and the exact-position array of ST_X_EXACT.  Assign it
+    to a MassSpringOracle's ``lib`` to run that oracle under the hooks."""
+    global _study
+    if _study is not None:
+        return _study
+    path = os.path.join(HERE, "libms_oracle_study.so")
+    src = os.path.join(HERE, "ms_oracle.c")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE, "study"])
+    lib = ctypes.CDLL(path)
+    for f in (lib.orc_ms_forward, lib.orc_ms_forward_eval, lib.orc_ms_loss, lib.orc_ms_backward):
+        f.argtypes = [ctypes.POINTER(_OrcMS), ctypes.c_int]
+        f.restype = ctypes.c_int
+    lib.orc_study_set.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.orc_study_set.restype = None
+    _study = lib
+    return lib
+
+
 def _p(a, ptr=_D):
     return a.ctypes.data_as(ptr)
 

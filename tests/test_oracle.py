@@ -142,3 +142,32 @@ def test_oracle_adam_matches_reference_formula():
         v_ref = 0.9 * v_ref + 0.1 * g * g
         w_ref -= 3e-4 * (m_ref / (1 - 0.9 ** (it + 1))) / (np.sqrt(v_ref / (1 - 0.9 ** (it + 1))) + 1e-8)
     np.testing.assert_allclose(w, w_ref, rtol=1e-14)
+
+
+def test_study_hooks_off_reproduce_the_oracle_and_round_when_on():
+    """The precision-study build of the oracle (tests/study_fp32_state.py) is
+    the plain oracle when its hooks are off, replays recorded contact
+    decisions exactly, and stores FP32-representable positions under ST_X."""
+    from oracle.ms_oracle import study_library
+    g = load_golden("quad_ref")
+    steps = int(g["steps"])
+    plain = oracle_from_golden(g)
+    plain.run(steps)
+    lib = study_library()
+    o = oracle_from_golden(g)
+    o.lib = lib
+    flags = np.zeros((o.T, o.B, o.N), np.uint8)
+    lib.orc_study_set(0, flags.ctypes.data, 1, None)
+    o.run(steps)
+    assert np.array_equal(o.x, plain.x) and np.array_equal(o.gW[0], plain.gW[0])
+    assert flags.any()
+    lib.orc_study_set(0, flags.ctypes.data, 2, None)  # force the recorded decisions
+    o.run(steps)
+    assert np.array_equal(o.x, plain.x) and np.array_equal(o.gW[0], plain.gW[0])
+    lib.orc_study_set(1, None, 0, None)  # ST_X
+    o.run(steps)
+    lib.orc_study_set(0, None, 0, None)
+    xs = o.x[1:steps]  # x[0] is the caller's input
+    assert np.array_equal(xs, xs.astype(np.float32).astype(np.float64))
+    assert not np.array_equal(xs, plain.x[1:steps])
+    assert max_rel(o.x[:steps], plain.x[:steps]) < 1e-6
