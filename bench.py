@@ -93,8 +93,10 @@ def parse():
     ap.add_argument("--controller", default="auto", choices=["auto", "per_env", "batched"],
                     help="controller path: batched = one tensor-core GEMM per layer over all envs "
                          "of a robot type (automatic for types with >= 256 envs)")
-    ap.add_argument("--tick-segments", type=int, default=4,
-                    help="serve: checkpoint segments a tick advances every request by")
+    ap.add_argument("--tick-segments", type=int, default=2,
+                    help="serve: checkpoint segments a tick advances every request by (measured on "
+                         "B200, 6 s of arrivals: 1 / 2 / 4 segments gave p50 135 / 133 / 183 ms, "
+                         "p99 1.22 / 1.18 / 1.19 s at the same throughput)")
     a = ap.parse_args()
     if a.robots is None:
         a.robots = DEFAULT_ENVS[a.config]
