@@ -60,7 +60,7 @@ SERVE_SECONDS_PER_STEP = 2.0  # seconds of arrivals per bench step
 # capture of this workload at 128 robots x 100 substeps (the 512-robot workload
 # is too large to capture); the traffic reported below scales the full launch's
 # algorithmic bytes by it.
-TRAFFIC_RATIO = {"reverse": 8.620194e9 / 10.330433e9, "recompute": 8.787660e9 / 10.441533e9}
+TRAFFIC_RATIO = {"reverse": 8.622361e9 / 10.330433e9, "recompute": 8.787660e9 / 10.441533e9}
 UNIT = "env-substeps/s"
 SERVE_MPM_SLOTS = 4     # whole-rollout MPM slots of the serving workload (one-env handles)
 
@@ -93,6 +93,9 @@ def parse():
     ap.add_argument("--controller", default="auto", choices=["auto", "per_env", "batched"],
                     help="controller path: batched = one tensor-core GEMM per layer over all envs "
                          "of a robot type (automatic for types with >= 256 envs)")
+    ap.add_argument("--particle-order", default="base_runs", choices=["cells", "base_runs"],
+                    help="mpm: internal particle order (base_runs: sorted by base cell, each warp's "
+                         "runs of equal base cells summed by shuffles before the grid reductions)")
     ap.add_argument("--tick-segments", type=int, default=2,
                     help="serve: checkpoint segments a tick advances every request by (measured on "
                          "B200, 6 s of arrivals: 1 / 2 / 4 segments gave p50 135 / 133 / 183 ms, "
@@ -179,7 +182,7 @@ def config_dict(a, n_gpus):
                         "muscle groups), 64^3 grid, neo-Hookean E=1e4 nu=0.3, dt 1e-4, %d envs x %d "
                         "substeps, checkpoint every %d, centre loss" % (a.robots, a.substeps, a.checkpoint),
             "envs_per_gpu": a.robots, "substeps": a.substeps, "checkpoint_every": a.checkpoint,
-            "parallelism": par,
+            "particle_order": a.particle_order, "parallelism": par,
             "l2": "state trajectory checkpoints and per-step records exceed L2"}
 
 
@@ -702,7 +705,8 @@ def run_mpm(a):
     import cls_b200
     from cls_b200 import workloads
     T = a.substeps
-    b, pos = workloads.mpm_batch(n_envs=a.robots, steps=T, K=a.checkpoint, seed=1000 * rank)
+    b, pos = workloads.mpm_batch(n_envs=a.robots, steps=T, K=a.checkpoint, seed=1000 * rank,
+                                 particle_order=a.particle_order)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     env_substeps = b.E * T
@@ -757,8 +761,11 @@ def run_mpm(a):
                                     for k in kinds}}
     # the particle kernels' working set (~33 MB of grid, ~24 MB of particles
     # for 8 envs) is L2-resident: their scatter roofline is the measured rate
-    # of the 16-byte vector reductions they issue (27 per particle and step:
-    # P2G in the forward kernels, G2P^T's velocity adjoint in the reverse)
+    # of 16-byte vector reductions, against which each kernel's 27 node
+    # updates per particle and step are counted (P2G in the forward kernels,
+    # G2P^T's velocity adjoint in the reverse; with the base-cell order the
+    # forward kernels issue one reduction per run of lanes on one base cell,
+    # fewer than 27 per particle)
     from cls_b200 import mpm as mpm_mod
     n_nodes = b.E * (64 // 4) ** 3 * 64
     red_peak = mpm_mod.reduction_peak(n_nodes)
@@ -768,7 +775,8 @@ def run_mpm(a):
         if prof_n.get(k, 0) > 0:
             rate = reds * prof_n[k] / (prof_ms[k] / 1e3)
             scatter[k] = {"achieved": rate, "frac": rate / red_peak}
-    roofline["scatter"] = {"bound": "l2 vector reductions", "unit": "reductions/s", "peak": red_peak,
+    roofline["scatter"] = {"bound": "l2 vector reductions", "unit": "node updates/s", "peak": red_peak,
+                           "particle_order": a.particle_order,
                            "peak_source": "measured in this run (cls_mpm_reduction_peak, %d nodes)" % n_nodes,
                            "per_kernel": scatter}
 

@@ -81,6 +81,7 @@ struct Phys {
   const R* pw;                                // [P] particle weights of the centre
   const int* chunk_start;                     // [n_chunks] first internal particle
   const int* chunk_len;                       // [n_chunks] particles (<= kChunk)
+  int runs;                                   // 1: base-cell order, run-summed scatters
 };
 
 // Forward particle kernel: G2P of step f (mode bit 1) and/or P2G of step g
@@ -383,6 +384,53 @@ __device__ __forceinline__ void red4<double>(V4<double>* p, double x, double y, 
   if (w != 0.0) atomicAdd(&p->w, w);
 }
 
+// Runs of consecutive lanes whose particles share a base cell (the
+// CLS_MPM_ORDER_BASE_RUNS order puts them next to each other; runs are found
+// from the current base cells, so the result is exact for any order).  head:
+// first lane of its run; last: the run's last lane; steps: ceil(log2) of the
+// warp's longest run.  Invalid lanes are runs of their own.  All lanes call it.
+struct WarpRuns {
+  int last, steps;
+  bool head;
+};
+template <int D>
+__device__ __forceinline__ WarpRuns warp_runs(bool valid, const int base[D]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  bool same = __shfl_up_sync(full, valid ? 1 : 0, 1) != 0 && valid && lane > 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) same = (__shfl_up_sync(full, base[d], 1) == base[d]) && same;
+  WarpRuns r;
+  r.head = !same;
+  const unsigned heads = __ballot_sync(full, r.head);
+  const unsigned after = lane == 31 ? 0u : (heads >> (lane + 1)) << (lane + 1);
+  r.last = after ? __ffs(after) - 2 : 31;
+  const int longest = (int)__reduce_max_sync(full, r.head ? (unsigned)(r.last - lane + 1) : 1u);
+  r.steps = longest > 1 ? 32 - __clz(longest - 1) : 0;
+  return r;
+}
+
+// Sum (x, y, z, w) over the lanes of each run (segmented suffix sums by
+// shuffles: after the steps, a run's first lane holds the run's total) and
+// add the total to *p from that lane, when `issue` is set there.  All lanes
+// call it with the same runs.
+template <typename R>
+__device__ __forceinline__ void run_red4(const WarpRuns& r, V4<R>* p, R x, R y, R z, R w, bool issue) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  for (int s = 0, off = 1; s < r.steps; ++s, off <<= 1) {
+    const R ox = __shfl_down_sync(full, x, off), oy = __shfl_down_sync(full, y, off);
+    const R oz = __shfl_down_sync(full, z, off), ow = __shfl_down_sync(full, w, off);
+    if (lane + off <= r.last) {
+      x += ox;
+      y += oy;
+      z += oz;
+      w += ow;
+    }
+  }
+  if (issue && r.head) red4<R>(p, x, y, z, w);
+}
+
 // The CTA's box of base cells, extended by the stencil (+2 per dim): the
 // nodes a CTA stages in shared memory.  n = 0 when the box exceeds the tile
 // capacity (global-atomic fallback).
@@ -631,6 +679,11 @@ __global__ void __launch_bounds__(kChunk, CLS_MPM_FWD_MIN_BLOCKS) mpm_fwd_kernel
     }
   }
   warp_bbox<D>(a.bbox + (size_t)e * 2 * D, valid, base);
+  WarpRuns runs;
+  runs.head = true;
+  runs.last = lane;
+  runs.steps = 0;
+  if (c.runs) runs = warp_runs<D>(valid, base);
   Box<D> bx;
   bx.n = 0;
   if (SM & kScatterTile) bx = warp_box<R, D>(c, valid, base);
@@ -644,6 +697,40 @@ __global__ void __launch_bounds__(kChunk, CLS_MPM_FWD_MIN_BLOCKS) mpm_fwd_kernel
       wt_tile[3 * cap + li] = 0;
     }
     __syncwarp();
+  }
+  if (c.runs) {
+    // base-cell order: each run of lanes on one base cell adds its 27 node
+    // contributions with one reduction per node (run_red4).  The stencil loop
+    // stays rolled: unrolled, the shuffles made the kernel instruction-fetch
+    // bound (measured slower)
+    R mv[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) mv[i] = c.mass * v[i];
+#pragma unroll 1
+    for (int nq = 0; nq < K::NN; ++nq) {
+      int o[D];
+      K::offs(nq, o);
+      R wt = 1;
+#pragma unroll
+      for (int d = 0; d < D; ++d) wt *= o[d] == 0 ? w[0][d] : (o[d] == 1 ? w[1][d] : w[2][d]);
+      R mom[3] = {0, 0, 0};
+      long long nidx = 0;
+      if (valid) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          R s = mv[i];
+#pragma unroll
+          for (int j = 0; j < D; ++j) s += aff[i * D + j] * ((R)o[j] - fx[j]);
+          mom[i] = wt * s;
+        }
+        int I[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) I[d] = base[d] + o[d];
+        nidx = node_index<R, D>(c, e, I);
+      }
+      run_red4<R>(runs, a.acc + nidx, mom[0], mom[1], mom[2], valid ? wt * c.mass : R(0), valid);
+    }
+    return;
   }
   {
     // every lane runs the offsets so that the warp can sync between them

@@ -99,6 +99,11 @@ class MpmImpl final : public MpmBase {
     MPM_REQUIRE(p.tile_nodes <= 1024, "tile_nodes must be at most 1024");
     sm_mode_ = p.tile_nodes > 0 ? (kStageGather | kScatterTile) : 0;
     tile_cap_ = p.tile_nodes > 0 ? p.tile_nodes : 0;
+    MPM_REQUIRE(p.particle_order == CLS_MPM_ORDER_CELLS || p.particle_order == CLS_MPM_ORDER_BASE_RUNS,
+                "particle_order must be CLS_MPM_ORDER_CELLS or CLS_MPM_ORDER_BASE_RUNS");
+    MPM_REQUIRE(p.particle_order == CLS_MPM_ORDER_CELLS || tile_cap_ == 0,
+                "CLS_MPM_ORDER_BASE_RUNS needs tile_nodes <= 0");
+    runs_ = p.particle_order == CLS_MPM_ORDER_BASE_RUNS;
     nb_ = (n_grid_ + Blk<D>::SIDE - 1) / Blk<D>::SIDE;
     nblk_ = 1;
     for (int d = 0; d < D; ++d) nblk_ *= nb_;
@@ -176,14 +181,18 @@ class MpmImpl final : public MpmBase {
   // position), cut into chunks of at most kChunk (below); inside a chunk the
   // i-th particle of every cell comes first, so that a warp's lanes sit in
   // different cells.
+  // CLS_MPM_ORDER_BASE_RUNS: the same Morton order over the stencils' base
+  // cells (floor(x / dx - 0.5)), cut into plain runs of kChunk, without the
+  // interleave, so that particles sharing a base cell sit in consecutive lanes.
   void build_order(const cls_mpm_body& b) {
     std::vector<unsigned long long> key(P_);
     std::map<unsigned long long, int> cells;
+    const double shift = runs_ ? 0.5 : 0.0;
     for (int u = 0; u < P_; ++u) {
       unsigned long long k = 0;
       int cc[D];
       for (int d = 0; d < D; ++d) {
-        const double c = std::floor(b.positions[(size_t)u * D + d] * n_grid_);
+        const double c = std::floor(b.positions[(size_t)u * D + d] * n_grid_ - shift);
         cc[d] = (int)std::min<double>(std::max<double>(c, 0.0), n_grid_ - 1);
       }
       for (int bit = 20; bit >= 0; --bit)
@@ -228,7 +237,8 @@ class MpmImpl final : public MpmBase {
       const int c0 = chunk_start_h_[ch], len = chunk_len_h_[ch];
       std::vector<int> pos(len);
       std::iota(pos.begin(), pos.end(), 0);
-      std::stable_sort(pos.begin(), pos.end(), [&](int a, int c) { return a % per_cell < c % per_cell; });
+      if (!runs_)
+        std::stable_sort(pos.begin(), pos.end(), [&](int a, int c) { return a % per_cell < c % per_cell; });
       for (int t = 0; t < len; ++t) perm_[c0 + t] = order[c0 + pos[t]];
     }
   }
@@ -237,6 +247,7 @@ class MpmImpl final : public MpmBase {
     Phys<R> c;
     std::memset(&c, 0, sizeof(c));
     c.E = E_; c.P = P_; c.M = M_; c.material = p_.material; c.n_chunks = n_chunks_; c.tile_cap = tile_cap_;
+    c.runs = runs_ ? 1 : 0;
     c.n_grid = n_grid_; c.nb = nb_; c.bound = p_.bound; c.nblk = nblk_; c.EP = (long long)E_ * P_;
     c.dx = (R)(1.0 / n_grid_); c.inv_dx = (R)n_grid_; c.dt = (R)p_.dt;
     c.ks = (R)(p_.dt * p_.p_vol * 4.0 * n_grid_ * n_grid_);
@@ -611,6 +622,7 @@ class MpmImpl final : public MpmBase {
   std::vector<double> loss_w_;
   std::vector<int> perm_;  // internal particle -> user particle
   std::vector<int> chunk_start_h_, chunk_len_h_;
+  bool runs_ = false;  // CLS_MPM_ORDER_BASE_RUNS
   bool fwd_done_ = false, bwd_done_ = false;
   Buf<R> ck_x_, ck_v_, ck_C_, ck_F_;
   Buf<R> X_[2], Fw_[2], RX_[2], RV_[2], RC_[2], RF_[2], AX_[2], AF_[2];
@@ -663,6 +675,7 @@ void cls_mpm_default_params(cls_mpm_params* p) {
   p->la = 40.0;
   p->act_strength = 4.0;
   p->mass = 1.0;
+  p->particle_order = CLS_MPM_ORDER_BASE_RUNS;
 }
 
 int cls_mpm_create(const cls_mpm_body* body, const cls_mpm_params* params, int32_t n_envs,

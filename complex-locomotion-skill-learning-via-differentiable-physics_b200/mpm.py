@@ -24,7 +24,8 @@ class MPMParams(ctypes.Structure):
     _fields_ = [("max_steps", _i32), ("n_grid", _i32), ("bound", _i32), ("material", _i32),
                 ("precision", _i32), ("checkpoint_every", _i32), ("dt", _d), ("gravity", _d),
                 ("p_vol", _d), ("mu", _d), ("la", _d), ("act_strength", _d), ("mass", _d),
-                ("tile_nodes", _i32)]
+                ("tile_nodes", _i32), ("particle_order", _i32)]
+PARTICLE_ORDER = {"cells": 0, "base_runs": 1}
 
 
 _SIGS = {
@@ -81,6 +82,8 @@ def default_params(**over):
     for k, v in over.items():
         if k == "material" and isinstance(v, str):
             v = MATERIAL[v]
+        if k == "particle_order" and isinstance(v, str):
+            v = PARTICLE_ORDER[v]
         setattr(p, k, v)
     return p
 

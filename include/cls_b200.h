@@ -467,10 +467,26 @@ typedef struct {
                                    nodes (at most 1024) for the gathers and scatters; 0
                                    (default) or < 0: gathers through L1 and 16-byte vector
                                    reductions straight to the grid */
+  int32_t particle_order;       /* internal particle order (results are the same up to the
+                                   order of FP additions): CLS_MPM_ORDER_CELLS (0) or
+                                   CLS_MPM_ORDER_BASE_RUNS (1, cls_mpm_default_params) */
 } cls_mpm_params;
 
+/* CLS_MPM_ORDER_CELLS: Morton order of the initial cells with the 32 lanes of
+ * a warp in 32 different cells (every lane's reductions on distinct nodes).
+ * CLS_MPM_ORDER_BASE_RUNS: particles sorted by the base cell of their stencil
+ * (floor(x / dx - 0.5)) at creation, so that lanes of a warp form runs that
+ * scatter to the same 27 nodes; in the forward P2G each run's contributions
+ * are summed by warp shuffles and its first lane issues one 16-byte reduction
+ * per node (runs are found every substep from the current positions, so any
+ * motion stays exact); the adjoint's scatter reduces per lane.  tile_nodes
+ * must be <= 0. */
+#define CLS_MPM_ORDER_CELLS 0
+#define CLS_MPM_ORDER_BASE_RUNS 1
+
 /* Fills *p with the reference's 2D MPM constants (dt 1e-3, gravity -10,
- * n_grid 32, bound 3, p_vol 1, mu = la = 40, act_strength 4, mass 1). */
+ * n_grid 32, bound 3, p_vol 1, mu = la = 40, act_strength 4, mass 1), no
+ * tiles and the base-cell particle order. */
 void cls_mpm_default_params(cls_mpm_params* p);
 /* Replaces SolverMPM.__init__ + initialize_robot (solver_mpm.py:7-58). */
 int cls_mpm_create(const cls_mpm_body* body, const cls_mpm_params* params, int32_t n_envs,
