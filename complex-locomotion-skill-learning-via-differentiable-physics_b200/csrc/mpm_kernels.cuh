@@ -701,18 +701,22 @@ __global__ void __launch_bounds__(kChunk, CLS_MPM_FWD_MIN_BLOCKS) mpm_fwd_kernel
   if (c.runs) {
     // base-cell order: each run of lanes on one base cell adds its 27 node
     // contributions with one reduction per node (run_red4).  The stencil loop
-    // stays rolled: unrolled, the shuffles made the kernel instruction-fetch
-    // bound (measured slower)
+    // is partly rolled: fully unrolled, the shuffles made the kernel
+    // instruction-fetch bound (measured slower)
     R mv[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) mv[i] = c.mass * v[i];
+    // the last axis rolled, the first two unrolled (9 nodes per iteration)
 #pragma unroll 1
-    for (int nq = 0; nq < K::NN; ++nq) {
-      int o[D];
-      K::offs(nq, o);
-      R wt = 1;
+    for (int ol = 0; ol < (D == 3 ? 3 : 1); ++ol) {
+      const R wl = D == 3 ? (ol == 0 ? w[0][D - 1] : (ol == 1 ? w[1][D - 1] : w[2][D - 1])) : R(1);
 #pragma unroll
-      for (int d = 0; d < D; ++d) wt *= o[d] == 0 ? w[0][d] : (o[d] == 1 ? w[1][d] : w[2][d]);
+    for (int nq = 0; nq < 9; ++nq) {
+      int o[D];
+      o[0] = nq % 3;
+      o[1] = nq / 3;
+      if (D == 3) o[D - 1] = ol;
+      const R wt = w[o[0]][0] * w[o[1]][1] * wl;
       R mom[3] = {0, 0, 0};
       long long nidx = 0;
       if (valid) {
@@ -729,6 +733,7 @@ __global__ void __launch_bounds__(kChunk, CLS_MPM_FWD_MIN_BLOCKS) mpm_fwd_kernel
         nidx = node_index<R, D>(c, e, I);
       }
       run_red4<R>(runs, a.acc + nidx, mom[0], mom[1], mom[2], valid ? wt * c.mass : R(0), valid);
+    }
     }
     return;
   }

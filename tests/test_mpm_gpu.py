@@ -167,3 +167,55 @@ def test_mpm3d_legged_body_64_grid_50_substeps_matches_oracle(precision, order):
     for name, ref in (("act", o.gact), ("x0", o.gx0), ("v0", o.gv0), ("F0", o.gF0)):
         assert rel_err(gr[name], ref) < tg, name
     b.close()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_mpm3d_base_runs_long_runs_match_oracle(precision):
+    """Dense clusters (60 particles per base cell: runs as long as a warp,
+    runs broken by motion) through the base-cell order's run sums, against
+    the oracle and against the cells order."""
+    from cls_b200.mpm import MPMBatch
+    rng = np.random.default_rng(7)
+    n_grid, dx = 24, 1.0 / 24
+    # each cluster inside one base cell (centred on a node; a particle's base
+    # cell is floor(x / dx - 0.5)): runs of 60 lanes, cut into a full warp
+    # and the rest; the edge particles leave the base cell within the steps
+    centres = np.array([[10.0, 7.0, 11.0], [12.0, 7.0, 11.0], [11.0, 9.0, 12.0]]) * dx
+    pts = np.concatenate([c + rng.uniform(-0.499, 0.499, size=(60, 3)) * dx for c in centres])
+    musc = (np.arange(len(pts)) % 3) - 1
+    fib = rng.normal(size=pts.shape)
+    fib /= np.linalg.norm(fib, axis=1, keepdims=True)
+    steps, B = 10, 2
+    kw = dict(dim=3, n_grid=n_grid, dt=2e-4, p_vol=1.0, mu=3846.0, la=5769.0, act_strength=500.0,
+              gravity=-10.0, bound=3)
+    o = MPMOracle(pts, musc, B, steps, material="neo_hookean", fibre=fib, n_muscles=2, **kw)
+    o.act[...] = rng.uniform(-1, 1, o.act.shape)
+    o.v[0] = rng.normal(scale=0.2, size=o.v[0].shape)
+    # weighted centre: the plain centre of mass does not move under internal
+    # (actuation) stress, which would leave d loss / d act at round-off level
+    pw = 1.0 + 0.3 * (np.arange(len(pts)) % 5)
+    o.loss_pw[...] = pw
+    o.loss_w[steps] = 1.0
+    o.loss_w[4] = 0.3
+    o.target[...] = 0.45
+    L = o.run(steps)
+    tf, tg = TOL[precision]
+    out = {}
+    for order in ("base_runs", "cells"):
+        b = MPMBatch(pts, musc, B, fibre=fib, n_muscles=2, max_steps=steps, material="neo_hookean",
+                     precision=precision, checkpoint_every=4, mass=1.0, particle_order=order, **kw)
+        b.set_state(np.broadcast_to(pts, (B,) + pts.shape), o.v[0])
+        b.set_actuation(o.act)
+        b.set_loss(o.loss_w, o.target, pw)
+        Lg = b.run(steps)
+        assert abs(Lg - L) <= tg * abs(L)
+        x = b.final_state()[0]
+        assert max_rel(x, o.x[steps]) < tf
+        gr = b.grads()
+        for name, ref in (("act", o.gact), ("x0", o.gx0), ("v0", o.gv0), ("F0", o.gF0)):
+            assert rel_err(gr[name], ref) < tg, (order, name)
+        out[order] = (Lg, x)
+        b.close()
+    if precision == 64:
+        assert out["base_runs"][0] == pytest.approx(out["cells"][0], rel=1e-12)
+        assert max_rel(out["base_runs"][1], out["cells"][1]) < 1e-12
