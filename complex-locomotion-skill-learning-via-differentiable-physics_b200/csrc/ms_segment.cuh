@@ -1064,30 +1064,38 @@ __global__ void ms_loss_kernel(MsArgs<R> a, double* out, const int* envs) {
         acc[LS_ACT] += fmax(fabs(act) - lim, 0.0) / rb.n_s / Br / st * 10;
       }
     }
-    if ((a.loss_mask & LOSS_ROTATION) && a.x_full && t >= 1 && t % tp > rp) {
-      const V4<R> c1 = a.obs_center[o], c0 = a.obs_center[o - (size_t)rp * a.n_envs];
-      const double ang = (double)a.th[o - (size_t)rp * a.n_envs] * 72. / 180. * 3.1415926535;
-      const double ca = cos(ang), sn = sin(ang);
-      for (int i = 0; i < N; ++i) {
-        const V4<R> x1 = a.x_full[(size_t)t * a.v_total + ed.v_off + i];
-        const V4<R> x0 = a.x_full[(size_t)(t - rp) * a.v_total + ed.v_off + i];
-        const double t0x = (double)x1.x - c1.x, t0y = (double)x1.y - c1.y, t0z = (double)x1.z - c1.z;
-        const double t1x = (double)x0.x - c0.x, t1y = (double)x0.y - c0.y, t1z = (double)x0.z - c0.z;
-        const double ex = t0x - (ca * t1x - sn * t1z), ey = t0y - t1y, ez = t0z - (sn * t1x + ca * t1z);
-        acc[LS_ROT] += (ex * ex + ey * ey + ez * ez) / st / 40;
+  }
+  // per-vertex terms over the trajectory: one warp per substep, its lanes
+  // over the vertices (coalesced rows of x_full)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((a.loss_mask & (LOSS_ROTATION | LOSS_POSE)) && a.x_full) {
+    for (int t = 1 + wid; t <= tmax; t += nw) {
+      const size_t o = (size_t)t * a.n_envs + e;
+      const V4<R>* xt = a.x_full + (size_t)t * a.v_total + ed.v_off;
+      if ((a.loss_mask & LOSS_ROTATION) && t % tp > rp) {
+        const V4<R> c1 = a.obs_center[o], c0 = a.obs_center[o - (size_t)rp * a.n_envs];
+        const double ang = (double)a.th[o - (size_t)rp * a.n_envs] * 72. / 180. * 3.1415926535;
+        const double ca = cos(ang), sn = sin(ang);
+        const V4<R>* xr = a.x_full + (size_t)(t - rp) * a.v_total + ed.v_off;
+        for (int i = lane; i < N; i += 32) {
+          const V4<R> x1 = xt[i], x0 = xr[i];
+          const double t0x = (double)x1.x - c1.x, t0y = (double)x1.y - c1.y, t0z = (double)x1.z - c1.z;
+          const double t1x = (double)x0.x - c0.x, t1y = (double)x0.y - c0.y, t1z = (double)x0.z - c0.z;
+          const double ex = t0x - (ca * t1x - sn * t1z), ey = t0y - t1y, ez = t0z - (sn * t1x + ca * t1z);
+          acc[LS_ROT] += (ex * ex + ey * ey + ez * ez) / st / 40;
+        }
       }
-    }
-    if ((a.loss_mask & LOSS_POSE) && a.x_full && t >= 1 && t % jp == 0) {
-      for (int i = 0; i < N; ++i) {
-        const V4<R> x1 = a.x_full[(size_t)t * a.v_total + ed.v_off + i];
-        const V4<R> p = a.init_obj[ed.v_off + i];
-        const double dx = (double)x1.x - p.x, dy = (double)x1.y - p.y, dz = (double)x1.z - p.z;
-        acc[LS_POSE] += (dx * dx + dy * dy + dz * dz) / Br / (st / jp);
+      if ((a.loss_mask & LOSS_POSE) && t % jp == 0) {
+        for (int i = lane; i < N; i += 32) {
+          const V4<R> x1 = xt[i];
+          const V4<R> p = a.init_obj[ed.v_off + i];
+          const double dx = (double)x1.x - p.x, dy = (double)x1.y - p.y, dz = (double)x1.z - p.z;
+          acc[LS_POSE] += (dx * dx + dy * dy + dz * dz) / Br / (st / jp);
+        }
       }
     }
   }
   // deterministic block reduction (max for slot 7)
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int m = 0; m < 8; ++m) {
     double v = acc[m];
     for (int off = 16; off > 0; off >>= 1) {
