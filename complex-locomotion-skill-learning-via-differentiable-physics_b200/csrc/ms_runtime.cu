@@ -413,10 +413,30 @@ class SimImpl final : public SimBase {
     V_ = voff;
     in_total_ = inoff;
     for (int l = 0; l < L_; ++l) z_total_[l] = zoff[l];
+    // controller records: K slots (one segment) or, for episodes of several
+    // segments, one slot per substep of the longest episode (slot = t), so
+    // that backward() runs the weight-gradient products once over all
+    // substeps instead of once per segment.  Whole-episode slots only when no
+    // robot type takes the batched controller by default and they need at
+    // most a quarter of the free device memory.
+    rec_slots_ = K_;
+    {
+      bool auto_dense = true;
+      for (int r = 0; r < nr; ++r)
+        if (count[r] > 0 && count[r] < kAutoDenseEnvs) auto_dense = false;
+      long long per_slot = in_total_;
+      for (int l = 0; l < L_; ++l) per_slot += 2LL * z_total_[l];
+      const long long slots_all = std::max(K_, T_ - 1);
+      size_t free_b = 0, total_b = 0;
+      CLS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      if (T_ - 1 > K_ && !auto_dense &&
+          (double)(slots_all - K_) * per_slot * sizeof(R) <= 0.25 * (double)free_b)
+        rec_slots_ = (int)slots_all;
+    }
     long long zb = 0;
     for (int l = 0; l < L_; ++l) {
       z_base_[l] = zb;
-      zb += (long long)K_ * z_total_[l];
+      zb += (long long)rec_slots_ * z_total_[l];
     }
     rec_z_total_ = zb;
     // processing order: heaviest envs first (longest-processing-time first)
@@ -446,14 +466,18 @@ class SimImpl final : public SimBase {
     use_shape(p_.threads_per_block > 0 ? p_.threads_per_block : auto_threads(), -1);
     // GEMM tiles (per robot, per layer); a robot shared by many envs splits
     // its K = envs x substeps rows over several CTAs (about 2048 rows each)
-    for (int r = 0; r < nr; ++r) {
-      if (count[r] == 0) continue;
-      const long long rows = (long long)K_ * count[r];
-      const int nsplit = (int)std::max<long long>(1, std::min<long long>(64, rows / 2048));
-      for (int l = 0; l < L_; ++l)
-        for (int i0 = 0; i0 < hr_[r].width[l + 1]; i0 += 64)
-          for (int j0 = 0; j0 < hr_[r].width[l]; j0 += 64)
-            for (int sp = 0; sp < nsplit; ++sp) tiles_host_.push_back({r, l, i0, j0, sp, nsplit});
+    for (int pass = 0; pass < (rec_slots_ > K_ ? 2 : 1); ++pass) {
+      // pass 0: tiles over one segment's rows; pass 1: over the whole episode
+      std::vector<GemmTile>& tl = pass ? tiles_ep_ : tiles_host_;
+      for (int r = 0; r < nr; ++r) {
+        if (count[r] == 0) continue;
+        const long long rows = (long long)(pass ? rec_slots_ : K_) * count[r];
+        const int nsplit = (int)std::max<long long>(1, std::min<long long>(64, rows / 2048));
+        for (int l = 0; l < L_; ++l)
+          for (int i0 = 0; i0 < hr_[r].width[l + 1]; i0 += 64)
+            for (int j0 = 0; j0 < hr_[r].width[l]; j0 += 64)
+              for (int sp = 0; sp < nsplit; ++sp) tl.push_back({r, l, i0, j0, sp, nsplit});
+      }
     }
     // device allocations
     const int n_seg_max = (T_ - 1 + K_ - 1) / K_ + 1;
@@ -486,7 +510,7 @@ class SimImpl final : public SimBase {
     d_recx_.alloc((size_t)K_ * V_);
     d_recv_.alloc((size_t)K_ * V_);
     d_recvinc_.alloc((size_t)K_ * V_);
-    d_recin_.alloc((size_t)K_ * in_total_);
+    d_recin_.alloc((size_t)rec_slots_ * in_total_);
     d_recz_.alloc(rec_z_total_);
     d_recdz_.alloc(rec_z_total_);
     d_head_.alloc(V_);
@@ -512,6 +536,7 @@ class SimImpl final : public SimBase {
     d_iter_.alloc(1);
     d_lossenv_.alloc((size_t)E * 8);
     d_tiles_.alloc(std::max<size_t>(1, tiles_host_.size()));
+    d_tiles_ep_.alloc(std::max<size_t>(1, tiles_ep_.size()));
     d_opt_segs_.alloc(opt_segs_.size());
     d_pack_segs_.alloc(pack_segs_.size());
     CLS_CUDA(cudaMemcpy(d_opt_segs_.p, opt_segs_.data(), sizeof(OptSeg) * opt_segs_.size(),
@@ -548,6 +573,9 @@ class SimImpl final : public SimBase {
       CLS_CUDA(cudaMemcpy(d_spring_out_.p, spring_out.data(), sizeof(int) * spring_out.size(),
                           cudaMemcpyHostToDevice));
     }
+    if (!tiles_ep_.empty())
+      CLS_CUDA(cudaMemcpy(d_tiles_ep_.p, tiles_ep_.data(), sizeof(GemmTile) * tiles_ep_.size(),
+                          cudaMemcpyHostToDevice));
     if (!tiles_host_.empty())
       CLS_CUDA(cudaMemcpy(d_tiles_.p, tiles_host_.data(), sizeof(GemmTile) * tiles_host_.size(),
                           cudaMemcpyHostToDevice));
@@ -1245,11 +1273,20 @@ class SimImpl final : public SimBase {
     const int n_seg = (t_last + K_ - 1) / K_;
     CLS_CUDA(cudaMemsetAsync(d_gw_.p, 0, sizeof(R) * d_gw_.n, stream));
     CLS_CUDA(cudaMemsetAsync(d_gb_.p, 0, sizeof(R) * d_gb_.n, stream));
-    MsArgs<R> a = args(steps);
+    const MsArgs<R> a0 = args(steps);
     int qslot = qslot_;
+    // whole-episode records: segment s's records sit at slots t (the
+    // segment's slot kk = t - t0 shifted by t0), and the weight-gradient
+    // products run once after the loop over slots [0, t_last)
+    const bool episode = rec_slots_ > K_ && !dense_ && !per_env && n_seg > 1 && !tiles_ep_.empty();
     for (int s = n_seg - 1; s >= 0; --s) {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
       const bool recompute = !(recorded_ && n_seg == 1);
+      MsArgs<R> a = a0;
+      if (episode) {
+        for (int l = 0; l < L_; ++l) a.z_base[l] += (long long)t0 * z_total_[l];
+        a.rec_in += (size_t)t0 * in_total_;
+      }
       if (dense_ && !per_env) {
         if (recompute) dense_pass(a, t0, t1, FWD_RECORD, s, false, PK_RECOMP);
         dense_reverse(a, t0, t1, s == n_seg - 1);
@@ -1266,6 +1303,7 @@ class SimImpl final : public SimBase {
           });
         });
       }
+      if (episode) continue;
       if (dense_ && !per_env && !wg_jobs_.empty()) {
         // FP32 batched path: record transposes + tensor-core tiles, in chunks
         // of at most wg_chunk_ record slots (the operand buffers' size)
@@ -1283,6 +1321,11 @@ class SimImpl final : public SimBase {
         });
       }
     }
+    if (episode)
+      timed(PK_WGRAD, [&] {
+        ms_wgrad_kernel<R><<<(int)tiles_ep_.size(), 256, 0, stream>>>(a0, d_tiles_ep_.p, t_last, d_gw_.p,
+                                                                        d_gb_.p);
+      });
     CLS_CUDA(cudaGetLastError());
     bwd_done_ = true;
   }
@@ -2033,6 +2076,8 @@ class SimImpl final : public SimBase {
   std::vector<EnvDesc> ed_host_;
   std::vector<RobotDesc> rd_host_;
   std::vector<GemmTile> tiles_host_;
+  std::vector<GemmTile> tiles_ep_;  // weight-gradient tiles over whole-episode records
+  int rec_slots_ = 1;               // controller-record slots (K, or one per substep)
   std::vector<int> inv_perm_, serve_order_h_, serve_st_tmp_;
   std::vector<int4> serve_win_h_, serve_w_tmp_;
   DevBuf<int> d_env_steps_, d_sorder_, d_squeue_;
@@ -2105,7 +2150,7 @@ class SimImpl final : public SimBase {
 
  private:
   DevBuf<double> d_lossenv_, d_stage_, d_tns_;
-  DevBuf<GemmTile> d_tiles_;
+  DevBuf<GemmTile> d_tiles_, d_tiles_ep_;
   DevBuf<OptSeg> d_opt_segs_, d_pack_segs_;
 };
 
