@@ -1127,8 +1127,9 @@ template <typename R>
 __global__ void __launch_bounds__(256)
 ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
   constexpr int TM = 64, TN = 64, TK = 16;
-  __shared__ R sA[TK][TM];
-  __shared__ R sB[TK][TN];
+  static_assert(TK * TM / 4 == 256 && TK * TN / 4 == 256, "one 4-value group per thread and operand");
+  __shared__ __align__(32) R sA[TK][TM];
+  __shared__ __align__(32) R sB[TK][TN];
   const GemmTile tl = tiles[blockIdx.x];
   const RobotDesc& rb = a.robots[tl.robot];
   const int l = tl.layer;
@@ -1152,28 +1153,40 @@ ms_wgrad_kernel(MsArgs<R> a, const GemmTile* tiles, int kseg, R* gw, R* gb) {
     for (int q = 0; q < 4; ++q) acc[p][q] = 0;
   R bacc[4] = {0, 0, 0, 0};
   const R* biasp = (l > 0) ? a.bias + rb.b_off[l - 1] : nullptr;
+  // staging: thread (rr, c4) loads 4 consecutive values of row rr of each
+  // operand in one 16-byte access (record rows are padded to 4 values and
+  // start on 4-value boundaries); padding columns of a row are read but
+  // only reach outputs that are not stored
+  const int rr = threadIdx.x >> 4, c4 = (threadIdx.x & 15) * 4;
+  const int rin = l == 0 ? rb.pitch[0] : ap;  // B-operand row length in the records
   for (int r0 = row_lo; r0 < row_hi; r0 += TK) {
-    for (int q = threadIdx.x; q < TK * TM; q += 256) {
-      const int rr = q / TM, ii = q % TM;
-      const int rho = r0 + rr, i = tl.i0 + ii;
-      R va = 0, vb = 0;
+    {
+      const int rho = r0 + rr;
+      V4<R> va, vb;
+      va.x = va.y = va.z = va.w = 0;
+      vb = va;
       if (rho < row_hi) {
         const int k = rho / nb, b = rho - k * nb;
-        if (i < M)
-          va = a.rec_dz[a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * zp + i];
-        const int j = tl.j0 + ii;
-        if (j < Ncol) {
+        const int i = tl.i0 + c4, j = tl.j0 + c4;
+        if (i < zp)
+          va = ldg4<R>(reinterpret_cast<const V4<R>*>(
+              a.rec_dz + a.z_base[l] + (size_t)k * a.z_total[l] + e0.z_off[l] + (size_t)b * zp + i));
+        if (j < rin) {
           if (l == 0) {
-            vb = a.rec_in[(size_t)k * a.in_total + e0.in_off + (size_t)b * rb.pitch[0] + j];
+            vb = ldg4<R>(reinterpret_cast<const V4<R>*>(a.rec_in + (size_t)k * a.in_total + e0.in_off +
+                                                        (size_t)b * rin + j));
           } else {
-            const R z = a.rec_z[a.z_base[l - 1] + (size_t)k * a.z_total[l - 1] + e0.z_off[l - 1] +
-                                (size_t)b * ap + j];
-            vb = act_f<R>(a.act_hidden, z + biasp[j]);
+            const V4<R> z = ldg4<R>(reinterpret_cast<const V4<R>*>(
+                a.rec_z + a.z_base[l - 1] + (size_t)k * a.z_total[l - 1] + e0.z_off[l - 1] + (size_t)b * ap + j));
+            vb.x = j < Ncol ? act_f<R>(a.act_hidden, z.x + biasp[j]) : R(0);
+            vb.y = j + 1 < Ncol ? act_f<R>(a.act_hidden, z.y + biasp[j + 1]) : R(0);
+            vb.z = j + 2 < Ncol ? act_f<R>(a.act_hidden, z.z + biasp[j + 2]) : R(0);
+            vb.w = j + 3 < Ncol ? act_f<R>(a.act_hidden, z.w + biasp[j + 3]) : R(0);
           }
         }
       }
-      sA[rr][ii] = va;
-      sB[rr][ii] = vb;
+      *reinterpret_cast<V4<R>*>(&sA[rr][c4]) = va;
+      *reinterpret_cast<V4<R>*>(&sB[rr][c4]) = vb;
     }
     __syncthreads();
 #pragma unroll
