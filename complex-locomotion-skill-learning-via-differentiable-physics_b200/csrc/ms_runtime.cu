@@ -1229,7 +1229,7 @@ class SimImpl final : public SimBase {
 
   void loss_device() {
     MsArgs<R> a = args(steps_);
-    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 256, 0, stream>>>(a, d_lossenv_.p, nullptr); });
+    timed(PK_LOSS, [&] { ms_loss_kernel<R><<<E_, 512, 0, stream>>>(a, d_lossenv_.p, nullptr); });
     CLS_CUDA(cudaGetLastError());
   }
 
