@@ -110,6 +110,7 @@ template <typename R>
 struct MsArgs {
   // sizes and constants
   int n_envs, T, steps, K;           // trajectory length, episode steps, checkpoint interval
+  int rec_from;                      // FWD_RECTAIL: first substep the first pass records
   int n_items;                       // work items (entries of `order`) in this launch
   int n_sin, dup_v, dup_h, dup_c;
   int act_hidden, act_out;

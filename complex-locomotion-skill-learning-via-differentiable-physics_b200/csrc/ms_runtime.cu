@@ -1009,7 +1009,24 @@ class SimImpl final : public SimBase {
     // pass records what the segment's recompute would (same kernels, same
     // values), and the reverse pass starts without a recompute
     recorded_ = !eval && t_end <= K_;
-    const int mode = FWD_CKPT | FWD_OBS | (recorded_ ? FWD_RECORD : 0);
+    int mode = FWD_CKPT | FWD_OBS | (recorded_ ? FWD_RECORD : 0);
+    // an episode of several segments run as one batched launch: the first
+    // pass also records the last segment (FWD_RECTAIL), whose recompute the
+    // reverse pass then skips; the records land where that segment's
+    // recompute would put them (whole-episode controller records: slot t)
+    tail_recorded_ = false;
+    tail_episode_ = false;
+    if (!eval && t_end > K_ && !dense_ && !per_env) {
+      const int n_seg = (t_end + K_ - 1) / K_;
+      a.rec_from = (n_seg - 1) * K_;
+      tail_episode_ = episode_records();
+      if (tail_episode_) {
+        for (int l = 0; l < L_; ++l) a.z_base[l] += (long long)a.rec_from * z_total_[l];
+        a.rec_in += (size_t)a.rec_from * in_total_;
+      }
+      mode |= FWD_RECTAIL;
+      tail_recorded_ = true;
+    }
     if (dense_ && !per_env) {
       dense_pass(a, 0, t_end, mode, 0, true, PK_FWD);
     } else {
@@ -1278,10 +1295,12 @@ class SimImpl final : public SimBase {
     // whole-episode records: segment s's records sit at slots t (the
     // segment's slot kk = t - t0 shifted by t0), and the weight-gradient
     // products run once after the loop over slots [0, t_last)
-    const bool episode = rec_slots_ > K_ && !dense_ && !per_env && n_seg > 1 && !tiles_ep_.empty();
+    const bool episode = episode_records() && !dense_ && !per_env && n_seg > 1;
+    // the first pass recorded the last segment in the layout this pass reads
+    const bool tail = tail_recorded_ && !dense_ && !per_env && n_seg > 1 && tail_episode_ == episode;
     for (int s = n_seg - 1; s >= 0; --s) {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
-      const bool recompute = !(recorded_ && n_seg == 1);
+      const bool recompute = !(recorded_ && n_seg == 1) && !(tail && s == n_seg - 1);
       MsArgs<R> a = a0;
       if (episode) {
         for (int l = 0; l < L_; ++l) a.z_base[l] += (long long)t0 * z_total_[l];
@@ -2078,6 +2097,10 @@ class SimImpl final : public SimBase {
   std::vector<GemmTile> tiles_host_;
   std::vector<GemmTile> tiles_ep_;  // weight-gradient tiles over whole-episode records
   int rec_slots_ = 1;               // controller-record slots (K, or one per substep)
+  bool episode_records() const { return rec_slots_ > K_ && !tiles_ep_.empty(); }
+  // the first pass recorded the last segment (FWD_RECTAIL), in the
+  // whole-episode layout when tail_episode_
+  bool tail_recorded_ = false, tail_episode_ = false;
   std::vector<int> inv_perm_, serve_order_h_, serve_st_tmp_;
   std::vector<int4> serve_win_h_, serve_w_tmp_;
   DevBuf<int> d_env_steps_, d_sorder_, d_squeue_;

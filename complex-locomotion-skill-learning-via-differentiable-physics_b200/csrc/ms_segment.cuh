@@ -5,7 +5,11 @@
 
 namespace cls {
 
-enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4, FWD_CKEND = 8 };
+// FWD_RECTAIL (first pass of an episode of several segments): substeps from
+// MsArgs::rec_from on are recorded at slot t - rec_from, as the last
+// segment's recompute would record them, so the reverse pass starts without
+// that recompute.
+enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4, FWD_CKEND = 8, FWD_RECTAIL = 16 };
 
 // episode steps of env e (per-env in served batches)
 template <typename R>
@@ -400,8 +404,12 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
     __syncthreads();
     CLS_PHASE_START();
     for (int t = t_begin; t < t_end; ++t) {
-      const int kk = t - t_begin;
-      fwd_pre<R>(a, rb, ed, s, e, t, t_begin, mode, kk, (mode & FWD_RECORD) != 0, false, hprev);
+      int kk = t - t_begin, mode_t = mode;
+      if ((mode & FWD_RECTAIL) && t >= a.rec_from) {
+        mode_t |= FWD_RECORD;
+        kk = t - a.rec_from;
+      }
+      fwd_pre<R>(a, rb, ed, s, e, t, t_begin, mode_t, kk, (mode_t & FWD_RECORD) != 0, false, hprev);
       CLS_PHASE(a, 10);
       // -- MLP (nn.py:130-146): z = W a, a' = act(z + b)
       R* out = nullptr;
@@ -409,7 +417,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
         const R* in = (l == 0) ? s.ain : ((l & 1) ? s.buf0 : s.buf1);
         R* y = (l & 1) ? s.buf1 : s.buf0;
         const int nout = rb.width[l + 1];
-        R* zrec = (mode & FWD_RECORD) ? a.rec_z + a.z_base[l] + (size_t)kk * a.z_total[l] + ed.z_off[l]
+        R* zrec = (mode_t & FWD_RECORD) ? a.rec_z + a.z_base[l] + (size_t)kk * a.z_total[l] + ed.z_off[l]
                                       : nullptr;
         const int act = l == L - 1 ? a.act_out : a.act_hidden;
         if (s.w)
@@ -425,7 +433,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
         out = y;
       }
       CLS_PHASE(a, 13);
-      fwd_post<R>(a, rb, ed, s, t, mode, kk, out);
+      fwd_post<R>(a, rb, ed, s, t, mode_t, kk, out);
       CLS_PHASE(a, 16);
     }
     fwd_finish<R>(a, rb, ed, s, t_begin, t_end, mode);
