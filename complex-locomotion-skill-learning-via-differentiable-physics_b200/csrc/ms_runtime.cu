@@ -1014,17 +1014,17 @@ class SimImpl final : public SimBase {
     // pass also records the last segment (FWD_RECTAIL), whose recompute the
     // reverse pass then skips; the records land where that segment's
     // recompute would put them (whole-episode controller records: slot t)
+    // With whole-episode controller records it also records the controller
+    // of every substep at slot t (FWD_RECCTRL), and the reverse pass's
+    // recomputes replay the controller outputs from those records
+    // (FWD_REPLAY) instead of evaluating the controller again.
     tail_recorded_ = false;
     tail_episode_ = false;
     if (!eval && t_end > K_ && !dense_ && !per_env) {
       const int n_seg = (t_end + K_ - 1) / K_;
       a.rec_from = (n_seg - 1) * K_;
       tail_episode_ = episode_records();
-      if (tail_episode_) {
-        for (int l = 0; l < L_; ++l) a.z_base[l] += (long long)a.rec_from * z_total_[l];
-        a.rec_in += (size_t)a.rec_from * in_total_;
-      }
-      mode |= FWD_RECTAIL;
+      mode |= FWD_RECTAIL | (tail_episode_ ? FWD_RECCTRL : 0);
       tail_recorded_ = true;
     }
     if (dense_ && !per_env) {
@@ -1310,10 +1310,13 @@ class SimImpl final : public SimBase {
         if (recompute) dense_pass(a, t0, t1, FWD_RECORD, s, false, PK_RECOMP);
         dense_reverse(a, t0, t1, s == n_seg - 1);
       } else {
+        // the first pass recorded every substep's controller in this layout:
+        // replay its outputs
+        const int rmode = FWD_RECORD | (tail && episode ? FWD_REPLAY : 0);
         if (recompute)
           each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {
             timed(PK_RECOMP, [&] {
-              fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, FWD_RECORD, s);
+              fwd_fn()<<<grid, threads_, fwd_smem_, stream>>>(b, t0, t1, rmode, s);
             });
           });
         each_launch(per_env, a, qslot, [&](const MsArgs<R>& b, int grid) {

@@ -9,7 +9,14 @@ namespace cls {
 // MsArgs::rec_from on are recorded at slot t - rec_from, as the last
 // segment's recompute would record them, so the reverse pass starts without
 // that recompute.
-enum FwdMode : int { FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4, FWD_CKEND = 8, FWD_RECTAIL = 16 };
+// FWD_RECCTRL (first pass, whole-episode controller records): the controller
+// records (input, pre-activations) of every substep at slot t.
+// FWD_REPLAY (recompute over those records): the controller outputs of each
+// substep come from its recorded output-layer pre-activations (the same
+// values, so the same state bit for bit) instead of the inputs and products.
+enum FwdMode : int {
+  FWD_CKPT = 1, FWD_OBS = 2, FWD_RECORD = 4, FWD_CKEND = 8, FWD_RECTAIL = 16, FWD_RECCTRL = 32, FWD_REPLAY = 64
+};
 
 // episode steps of env e (per-env in served batches)
 template <typename R>
@@ -181,7 +188,7 @@ __device__ __forceinline__ int next_item(const MsArgs<R>& a, int* s_item) {
 template <typename R>
 __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb, const EnvDesc& ed,
                                         const FwdSmem<R>& s, int e, int t, int t_begin, int mode,
-                                        int kslot, bool rec_in, bool rec_pad, R& hprev) {
+                                        int kslot, bool rec_in, bool rec_pad, R& hprev, int kc = -1) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int N = rb.n_v;
   const R invN = R(1) / R(N);
@@ -303,7 +310,7 @@ __device__ __forceinline__ void fwd_pre(const MsArgs<R>& a, const RobotDesc& rb,
   {
     const int pitch0 = rb.pitch[0];
     const int nrec = rec_pad ? pitch0 : nc;
-    R* rin = rec_in ? a.rec_in + (size_t)kslot * a.in_total + ed.in_off : nullptr;
+    R* rin = rec_in ? a.rec_in + (size_t)(kc >= 0 ? kc : kslot) * a.in_total + ed.in_off : nullptr;
     for (int q = tid; q < pitch0; q += nt) {
       if (q >= p0 && q < nc && q - p0 < nt) continue;  // loaded ahead (pre)
       R val = 0;
@@ -409,7 +416,28 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
         mode_t |= FWD_RECORD;
         kk = t - a.rec_from;
       }
-      fwd_pre<R>(a, rb, ed, s, e, t, t_begin, mode_t, kk, (mode_t & FWD_RECORD) != 0, false, hprev);
+      if (mode & FWD_REPLAY) {
+        // state records of t, then the controller outputs from the recorded
+        // output-layer pre-activations (act(z + b), as dense_forward forms them)
+        if (mode_t & FWD_RECORD) {
+          V4<R>* rx = a.rec_x + (size_t)kk * a.v_total + ed.v_off;
+          V4<R>* rv = a.rec_v + (size_t)kk * a.v_total + ed.v_off;
+          for (int i = tid; i < N; i += nt) { rx[i] = s.xs[i]; rv[i] = s.vs[i]; }
+        }
+        const int lo = L - 1, nout = rb.width[L];
+        const R* zr = a.rec_z + a.z_base[lo] + (size_t)kk * a.z_total[lo] + ed.z_off[lo];
+        const R* bo = s.w ? s.b + (rb.b_off[lo] - rb.b_off[0]) : a.bias + rb.b_off[lo];
+        R* y = (lo & 1) ? s.buf1 : s.buf0;
+        for (int o = tid; o < ((nout + 3) & ~3); o += nt) y[o] = o < nout ? act_f<R>(a.act_out, zr[o] + bo[o]) : R(0);
+        __syncthreads();
+        fwd_post<R>(a, rb, ed, s, t, mode_t, kk, y);
+        continue;
+      }
+      // controller records: at slot t over the whole episode (FWD_RECCTRL),
+      // else with the state records at kk
+      const bool rec_ctrl = (mode_t & FWD_RECORD) || (mode & FWD_RECCTRL);
+      const int kc = (mode & FWD_RECCTRL) ? t : kk;
+      fwd_pre<R>(a, rb, ed, s, e, t, t_begin, mode_t, kk, rec_ctrl, false, hprev, kc);
       CLS_PHASE(a, 10);
       // -- MLP (nn.py:130-146): z = W a, a' = act(z + b)
       R* out = nullptr;
@@ -417,8 +445,7 @@ ms_forward_kernel(MsArgs<R> a, int t_begin0, int t_end0, int mode, int src_slot0
         const R* in = (l == 0) ? s.ain : ((l & 1) ? s.buf0 : s.buf1);
         R* y = (l & 1) ? s.buf1 : s.buf0;
         const int nout = rb.width[l + 1];
-        R* zrec = (mode_t & FWD_RECORD) ? a.rec_z + a.z_base[l] + (size_t)kk * a.z_total[l] + ed.z_off[l]
-                                      : nullptr;
+        R* zrec = rec_ctrl ? a.rec_z + a.z_base[l] + (size_t)kc * a.z_total[l] + ed.z_off[l] : nullptr;
         const int act = l == L - 1 ? a.act_out : a.act_hidden;
         if (s.w)
           dense_forward<R, true>(s.w + (rb.w_off[l] - rb.w_off[0]), rb.pitch[l], nout,
