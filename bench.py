@@ -508,7 +508,12 @@ def run_ours(a):
           file=sys.stderr)
 
     # roofline of the dominant kernel (CUDA events around each launch above)
-    alg = workloads.algorithmic_bytes(robots, env_robot, batched=batched)
+    # per-env path over several checkpoint segments: the library keeps the
+    # whole episode's controller records when they fit a quarter of the free
+    # memory (they do for these workloads) and its recomputes replay the
+    # controller from them
+    replay = not batched and a.substeps - 1 > a.checkpoint
+    alg = workloads.algorithmic_bytes(robots, env_robot, batched=batched, replay=replay)
     subs_total = a.substeps - 1
     cands = ["forward", "recompute", "reverse"] + (["ctrl_gemm", "ctrl_gemm_adj"] if batched else [])
     top = max(cands, key=lambda k: prof_ms[k])

@@ -102,7 +102,7 @@ def _widths(rb):
     return [(-(-3 * N // 4) * 4) + 8 + 2 + 1] + list(rb.hidden) + [rb.n_outputs if rb.n_outputs > 0 else S]
 
 
-def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4, batched=False):
+def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4, batched=False, replay=False):
     """Compulsory DRAM bytes per substep of the whole batch, per kernel.
 
     Fused per-env path, per env-substep of robot r (N vertices, S springs, MLP
@@ -114,7 +114,13 @@ def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4, ba
       reverse:   weights + record reads 32 N + 4 sum rows (z) + writes 4 sum rows
                  (dz) + trajectory reads 32 N (rotation loss at t - rp, t + rp)
     The spring table (32 B per incidence, 2 S per robot) is read from L2 each
-    substep and counted once per pass.
+    substep and counted once per pass.  With ``replay`` (whole-episode
+    controller records, episodes of several segments), the first pass also
+    writes every substep's controller records (4 n_c + 4 sum rows) and the
+    recompute reads only the output layer's pre-activations (4 n_out) instead
+    of the weights:
+      forward:   weights + trajectory 16 N + 4 n_c + 4 sum rows
+      recompute: record writes 32 N (x, v) + 4 n_out
 
     Batched-controller path, step kernels only (the controller's GEMMs are
     counted in FLOPs by controller_flops), per env-substep:
@@ -142,8 +148,12 @@ def algorithmic_bytes(robots, env_robot, keep_trajectory=True, dtype_bytes=4, ba
         wbytes = sum(widths[l + 1] * pitch[l] for l in range(len(widths) - 1)) * dtype_bytes
         rows = sum(widths[1:]) * dtype_bytes
         springs = 2 * S * 32
-        out["forward"] += wbytes + springs + traj
-        out["recompute"] += wbytes + springs + 32 * N + widths[0] * dtype_bytes + rows
+        if replay:
+            out["forward"] += wbytes + springs + traj + widths[0] * dtype_bytes + rows
+            out["recompute"] += springs + 32 * N + widths[-1] * dtype_bytes
+        else:
+            out["forward"] += wbytes + springs + traj
+            out["recompute"] += wbytes + springs + 32 * N + widths[0] * dtype_bytes + rows
         out["reverse"] += wbytes + springs + 32 * N + 2 * rows + 2 * traj
     return out
 
