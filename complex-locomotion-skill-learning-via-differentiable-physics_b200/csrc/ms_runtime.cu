@@ -1010,7 +1010,7 @@ class SimImpl final : public SimBase {
     // values), and the reverse pass starts without a recompute
     recorded_ = !eval && t_end <= K_;
     int mode = FWD_CKPT | FWD_OBS | (recorded_ ? FWD_RECORD : 0);
-    // an episode of several segments run as one batched launch: the first
+    // an episode of several segments run by the fused kernels: the first
     // pass also records the last segment (FWD_RECTAIL), whose recompute the
     // reverse pass then skips; the records land where that segment's
     // recompute would put them (whole-episode controller records: slot t)
@@ -1020,7 +1020,7 @@ class SimImpl final : public SimBase {
     // (FWD_REPLAY) instead of evaluating the controller again.
     tail_recorded_ = false;
     tail_episode_ = false;
-    if (!eval && t_end > K_ && !dense_ && !per_env) {
+    if (!eval && t_end > K_ && (!dense_ || per_env)) {
       const int n_seg = (t_end + K_ - 1) / K_;
       a.rec_from = (n_seg - 1) * K_;
       tail_episode_ = episode_records();
@@ -1295,9 +1295,9 @@ class SimImpl final : public SimBase {
     // whole-episode records: segment s's records sit at slots t (the
     // segment's slot kk = t - t0 shifted by t0), and the weight-gradient
     // products run once after the loop over slots [0, t_last)
-    const bool episode = episode_records() && !dense_ && !per_env && n_seg > 1;
+    const bool episode = episode_records() && (!dense_ || per_env) && n_seg > 1;
     // the first pass recorded the last segment in the layout this pass reads
-    const bool tail = tail_recorded_ && !dense_ && !per_env && n_seg > 1 && tail_episode_ == episode;
+    const bool tail = tail_recorded_ && (!dense_ || per_env) && n_seg > 1 && tail_episode_ == episode;
     for (int s = n_seg - 1; s >= 0; --s) {
       const int t0 = s * K_, t1 = std::min(t0 + K_, t_last);
       const bool recompute = !(recorded_ && n_seg == 1) && !(tail && s == n_seg - 1);
