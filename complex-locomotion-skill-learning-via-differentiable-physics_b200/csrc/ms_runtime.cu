@@ -1010,14 +1010,13 @@ class SimImpl final : public SimBase {
     // values), and the reverse pass starts without a recompute
     recorded_ = !eval && t_end <= K_;
     int mode = FWD_CKPT | FWD_OBS | (recorded_ ? FWD_RECORD : 0);
-    // an episode of several segments run by the fused kernels: the first
-    // pass also records the last segment (FWD_RECTAIL), whose recompute the
-    // reverse pass then skips; the records land where that segment's
-    // recompute would put them (whole-episode controller records: slot t)
-    // With whole-episode controller records it also records the controller
-    // of every substep at slot t (FWD_RECCTRL), and the reverse pass's
-    // recomputes replay the controller outputs from those records
-    // (FWD_REPLAY) instead of evaluating the controller again.
+    // An episode of several segments run by the fused kernels: the first
+    // pass also records the last segment (FWD_RECTAIL) where that segment's
+    // recompute would, and the reverse pass skips that recompute.  With
+    // whole-episode controller records it also records every substep's
+    // controller at slot t (FWD_RECCTRL), and the reverse pass's recomputes
+    // replay the controller outputs from those records (FWD_REPLAY) instead
+    // of evaluating the controller again.
     tail_recorded_ = false;
     tail_episode_ = false;
     if (!eval && t_end > K_ && (!dense_ || per_env)) {
