@@ -42,3 +42,31 @@ def test_checkpoint_defaults():
     assert a.checkpoint == 50
     _, a = _args(["--config", "mpm"])
     assert a.checkpoint == 50
+
+
+def test_algorithmic_bytes_of_the_replaying_recompute():
+    """With the controller replayed from the first pass's records, the
+    recompute moves no controller weights and the first pass writes every
+    substep's controller records on top of its weight stream."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from cls_b200 import robot_design
+    from cls_b200.batch import Robot
+    from cls_b200 import workloads
+    rng = np.random.default_rng(0)
+    robots = []
+    for n in (60, 300):
+        obj, spr = robot_design.random_lattice(rng, n)
+        robots.append(Robot.actuated_outputs(obj, spr, hidden=[128, 128]))
+    env_robot = [0, 1]
+    base = workloads.algorithmic_bytes(robots, env_robot)
+    rep = workloads.algorithmic_bytes(robots, env_robot, replay=True)
+    widths = [workloads._widths(r) for r in robots]
+    wbytes = sum(sum(w[l + 1] * (-(-w[l] // 4) * 4) for l in range(len(w) - 1)) * 4 for w in widths)
+    rows = sum(sum(w[1:]) * 4 for w in widths)
+    inputs = sum(w[0] * 4 for w in widths)
+    outputs = sum(w[-1] * 4 for w in widths)
+    assert rep["reverse"] == base["reverse"]
+    assert rep["forward"] == pytest.approx(base["forward"] + inputs + rows)
+    assert rep["recompute"] == pytest.approx(base["recompute"] - wbytes - inputs - rows + outputs)
+    assert rep["recompute"] < 0.2 * base["recompute"]
